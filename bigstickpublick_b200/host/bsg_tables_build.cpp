@@ -1,0 +1,1081 @@
+// Host-side table builder: fills the BIGSTICK module arrays that bsg_create()
+// consumes, for full (untruncated) M-scheme spaces.  CPU only; it plays the
+// role of the Fortran host's setup (src/bigstick_main.f90:305-676), so that
+// this project can produce the same kind of tables without a Fortran
+// compiler.  See include/bsg_host.h for the list of reference stages.
+//
+// Conventions follow the reference:
+//  * s.p. states are sorted by W, parity, |m| with the reference's selection
+//    sort (src/bspstates.f90:110-225) and split into "left" (m<0, label -i)
+//    and "right" (m>=0, label +i) halves (make_hspsqn, :235-332);
+//  * an SD is a (left haiku, right haiku) pair; sectors are ordered by parity
+//    then jz (ascending for protons, descending for neutrons,
+//    src/bbasislib.f90:227-324); inside a sector SDs come in (right block,
+//    left block) pairs with the left haiku as the slow index
+//    (src/bjumplib_weld.f90:377-382);
+//  * basis index = pstart(ip) + nstart(in) (combinebasis,
+//    src/bbasislib.f90:540-677);
+//  * jump isd/fsd hold pstart/nstart values (bjumplib_weld.f90:791-792);
+//    two-body jumps inside one sector keep only isd >= fsd (:414-420) and the
+//    diagonal pair matrix element carries a factor 1/2 (btbme.f90:1402-1407);
+//  * uncoupled pp/nn matrix elements are packed lower triangles per (M,par)
+//    section of pairs (bjumplib_weld.f90:635-642); pn ones are full squares
+//    per (M,par) section, addressed by cpnpair(b,a)+dpnpair(d,c)
+//    (btbmepn.f90:417-487);
+//  * when there are at least two valence particles the single-particle
+//    energies are folded into the two-body part with the factor 1/(A-1)
+//    (src/bsppot.f90:20-238).
+//
+// Where the reference's internal orderings could not be reproduced without
+// running it (haiku order inside a block, jump order inside a sector jump,
+// pair order inside an (M,par) section) a fixed deterministic order is used;
+// the GPU path never depends on those orders.
+
+#include "bsg_host.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <unordered_map>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_err;
+
+struct SPS {
+    int nr, l, j2, m2, w, par, orb;
+};
+
+// ---------------------------------------------------------------- CG -------
+double g_lfact[256];
+bool g_lfact_ready = false;
+void init_lfact() {
+    if (g_lfact_ready) return;
+    g_lfact[0] = 0.0;
+    for (int i = 1; i < 256; ++i) g_lfact[i] = g_lfact[i - 1] + std::log((double)i);
+    g_lfact_ready = true;
+}
+// <j1/2 m1/2 j2/2 m2/2 | J/2 M/2>, all arguments doubled (Racah's formula).
+double cg2(int j1, int m1, int j2, int m2, int J, int M) {
+    if (m1 + m2 != M) return 0.0;
+    if (std::abs(m1) > j1 || std::abs(m2) > j2 || std::abs(M) > J) return 0.0;
+    if (J > j1 + j2 || J < std::abs(j1 - j2)) return 0.0;
+    if (((j1 + m1) & 1) || ((j2 + m2) & 1) || ((J + M) & 1) || ((j1 + j2 + J) & 1)) return 0.0;
+    const int a = (j1 + j2 - J) / 2, b = (j1 - j2 + J) / 2, c = (-j1 + j2 + J) / 2;
+    const int d = (j1 + j2 + J) / 2 + 1;
+    double pre = 0.5 * (std::log((double)(J + 1)) + g_lfact[a] + g_lfact[b] + g_lfact[c] - g_lfact[d]);
+    pre += 0.5 * (g_lfact[(j1 + m1) / 2] + g_lfact[(j1 - m1) / 2] + g_lfact[(j2 + m2) / 2] +
+                  g_lfact[(j2 - m2) / 2] + g_lfact[(J + M) / 2] + g_lfact[(J - M) / 2]);
+    double sum = 0.0;
+    for (int k = 0; k <= 200; ++k) {
+        const int t1 = a - k, t2 = (j1 - m1) / 2 - k, t3 = (j2 + m2) / 2 - k;
+        const int t4 = (J - j2 + m1) / 2 + k, t5 = (J - j1 - m2) / 2 + k;
+        if (t1 < 0 || t2 < 0 || t3 < 0) break;
+        if (t4 < 0 || t5 < 0) continue;
+        const double den = g_lfact[k] + g_lfact[t1] + g_lfact[t2] + g_lfact[t3] + g_lfact[t4] + g_lfact[t5];
+        const double term = std::exp(pre - den);
+        sum += (k & 1) ? -term : term;
+    }
+    return sum;
+}
+
+inline int popc(uint64_t x) { return __builtin_popcountll(x); }
+// number of occupied states strictly below q
+inline int nbelow(uint64_t bits, int q) { return popc(bits & ((q == 0) ? 0ull : ((1ull << q) - 1ull))); }
+
+// ------------------------------------------------------- species basis -----
+struct Haiku {
+    uint64_t bits;  // over the half space (left: bit i = left state i)
+    int jz2, par;
+};
+struct HBlock {
+    int nh, pidx, jz2;
+    std::vector<uint64_t> haikus;
+};
+struct Sector {
+    int pidx, jz2;
+    int64_t xsdstart = 0, xsdend = -1;  // 1-based
+    std::vector<std::pair<int, int>> blocks;  // (right block, left block)
+};
+struct SpeciesBasis {
+    int N = 0;
+    int nl = 0, nr = 0;
+    std::vector<SPS> left, right;       // hspsqn(-it,:), hspsqn(it,:)
+    std::vector<int> q_orb, q_m2, q_par;  // per combined label q
+    std::vector<HBlock> rblocks, lblocks;
+    std::vector<Sector> sectors;
+    std::vector<uint64_t> sd_bits;     // per SD (0-based index = isd-1)
+    std::vector<int> sd_sector;        // 0-based sector of each SD
+    std::unordered_map<uint64_t, int64_t> sd_index;  // bits -> 0-based SD index
+};
+
+inline int pidx_of(int par) { return par > 0 ? 1 : 2; }
+inline int par_of_idx(int p) { return p == 1 ? 1 : -1; }
+inline int parmult(int p1, int p2) { return (p1 == p2) ? 1 : 2; }
+
+// s.p. states: extract_sps + sort_spsqn + make_hspsqn
+void make_sps(const bsg_model_spec *s, bool allsamepar, bool allsameW, SpeciesBasis &sb) {
+    std::vector<SPS> sp;
+    for (int i = 0; i < s->norb; ++i) {
+        const bsg_orbit &o = s->orbits[i];
+        for (int m = -o.j2; m <= o.j2; m += 2) {
+            SPS x;
+            x.nr = o.nr; x.l = o.l; x.j2 = o.j2; x.m2 = m; x.w = o.w;
+            x.par = allsamepar ? 1 : ((o.l & 1) ? -1 : 1);
+            x.orb = i;
+            sp.push_back(x);
+        }
+    }
+    const int n = (int)sp.size();
+    // selection sort with swap on W (src/bspstates.f90:125-145)
+    if (!allsameW) {
+        for (int is = 0; is < n; ++is) {
+            int k = is, w = sp[is].w;
+            SPS tmp = sp[is];
+            for (int j = is + 1; j < n; ++j)
+                if (sp[j].w < w) { k = j; w = sp[j].w; tmp = sp[j]; }
+            if (k != is) { sp[k] = sp[is]; sp[is] = tmp; }
+        }
+    }
+    // on parity within each W (:149-181)
+    if (!allsamepar) {
+        int istart = 0;
+        while (istart < n) {
+            int iend = istart;
+            for (int is = istart; is < n; ++is)
+                if (sp[is].w == sp[istart].w) iend = is;
+            for (int is = istart; is <= iend; ++is) {
+                int k = is, par = sp[is].par;
+                SPS tmp = sp[is];
+                for (int j = is + 1; j <= iend; ++j)
+                    if (sp[j].par < par) { k = j; par = sp[j].par; tmp = sp[j]; }
+                if (k != is) { sp[k] = sp[is]; sp[is] = tmp; }
+            }
+            istart = iend + 1;
+        }
+    }
+    // on |m| within each (W, par) (:185-213)
+    {
+        int istart = 0;
+        while (istart < n) {
+            int iend = istart;
+            for (int is = istart; is < n; ++is)
+                if (sp[is].w == sp[istart].w && sp[is].par == sp[istart].par) iend = is;
+            for (int is = istart; is <= iend; ++is) {
+                int k = is, m = sp[is].m2;
+                SPS tmp = sp[is];
+                for (int j = is + 1; j <= iend; ++j)
+                    if (std::abs(sp[j].m2) < std::abs(m)) { k = j; m = sp[j].m2; tmp = sp[j]; }
+                if (k != is) { sp[k] = sp[is]; sp[is] = tmp; }
+            }
+            istart = iend + 1;
+        }
+    }
+    // split (make_hspsqn :254-271)
+    sb.left.clear(); sb.right.clear();
+    for (auto &x : sp) (x.m2 >= 0 ? sb.right : sb.left).push_back(x);
+    sb.nl = (int)sb.left.size();
+    sb.nr = (int)sb.right.size();
+    sb.q_orb.resize(sb.nl + sb.nr);
+    sb.q_m2.resize(sb.nl + sb.nr);
+    sb.q_par.resize(sb.nl + sb.nr);
+    for (int i = 0; i < sb.nl; ++i) { sb.q_orb[i] = sb.left[i].orb; sb.q_m2[i] = sb.left[i].m2; sb.q_par[i] = sb.left[i].par; }
+    for (int i = 0; i < sb.nr; ++i) {
+        sb.q_orb[sb.nl + i] = sb.right[i].orb; sb.q_m2[sb.nl + i] = sb.right[i].m2; sb.q_par[sb.nl + i] = sb.right[i].par;
+    }
+}
+
+// all haikus of size k over `states`, grouped into blocks keyed (k, pidx, jz2)
+void make_blocks(const std::vector<SPS> &states, int kmin, int kmax, std::vector<HBlock> &blocks) {
+    const int ns = (int)states.size();
+    std::map<std::tuple<int, int, int>, std::vector<uint64_t>> groups;
+    if (ns > 62) return;
+    for (int k = kmin; k <= kmax; ++k) {
+        if (k < 0 || k > ns) continue;
+        // enumerate k-subsets in increasing bitmask order (Gosper's hack)
+        if (k == 0) {
+            groups[std::make_tuple(0, 1, 0)].push_back(0ull);
+            continue;
+        }
+        uint64_t x = (1ull << k) - 1ull;
+        const uint64_t lim = 1ull << ns;
+        while (x < lim) {
+            int jz = 0, par = 1;
+            for (int i = 0; i < ns; ++i)
+                if (x >> i & 1ull) { jz += states[i].m2; par *= states[i].par; }
+            groups[std::make_tuple(k, pidx_of(par), jz)].push_back(x);
+            const uint64_t c = x & (~x + 1ull), r = x + c;
+            x = (((r ^ x) >> 2) / c) | r;
+        }
+    }
+    blocks.clear();
+    for (auto &g : groups) {  // std::map order: nh, parity index, jz ascending
+        HBlock b;
+        b.nh = std::get<0>(g.first);
+        b.pidx = std::get<1>(g.first);
+        b.jz2 = std::get<2>(g.first);
+        b.haikus = std::move(g.second);
+        blocks.push_back(std::move(b));
+    }
+}
+
+int find_block(const std::vector<HBlock> &bl, int nh, int pidx, int jz2) {
+    for (size_t i = 0; i < bl.size(); ++i)
+        if (bl[i].nh == nh && bl[i].pidx == pidx && bl[i].jz2 == jz2) return (int)i;
+    return -1;
+}
+
+// sector candidates (pidx, jz2) that some (right block, left block) pair reaches
+std::map<std::pair<int, int>, int> sector_candidates(const SpeciesBasis &sb) {
+    std::map<std::pair<int, int>, int> cand;
+    for (auto &rb : sb.rblocks)
+        for (auto &lb : sb.lblocks)
+            if (rb.nh + lb.nh == sb.N) cand[{parmult(rb.pidx, lb.pidx), rb.jz2 + lb.jz2}] = 1;
+    return cand;
+}
+
+// fill one sector's blocks and SD list (count_fill_sectors_w_blocks)
+void fill_sector(SpeciesBasis &sb, Sector &sec, int64_t &next_sd) {
+    sec.xsdstart = next_sd + 1;
+    int nhmin = 1 << 30, nhmax = -1;
+    for (auto &rb : sb.rblocks) { nhmin = std::min(nhmin, rb.nh); nhmax = std::max(nhmax, rb.nh); }
+    for (int nh = nhmin; nh <= nhmax; ++nh) {
+        const int nhc = sb.N - nh;
+        for (int parh = 1; parh <= 2; ++parh) {
+            const int parhc = parmult(sec.pidx, parh);
+            std::vector<int> rbs;
+            for (size_t i = 0; i < sb.rblocks.size(); ++i)
+                if (sb.rblocks[i].nh == nh && sb.rblocks[i].pidx == parh) rbs.push_back((int)i);
+            std::sort(rbs.begin(), rbs.end(), [&](int a, int b) { return sb.rblocks[a].jz2 < sb.rblocks[b].jz2; });
+            for (int ir : rbs) {
+                const int jzhc = sec.jz2 - sb.rblocks[ir].jz2;
+                const int il = find_block(sb.lblocks, nhc, parhc, jzhc);
+                if (il < 0) continue;
+                sec.blocks.push_back({ir, il});
+                const HBlock &R = sb.rblocks[ir], &L = sb.lblocks[il];
+                for (uint64_t lh : L.haikus)       // left haiku: slow index
+                    for (uint64_t rh : R.haikus) { // right haiku: fast index
+                        const uint64_t bits = lh | (rh << sb.nl);
+                        sb.sd_index[bits] = next_sd;
+                        sb.sd_bits.push_back(bits);
+                        sb.sd_sector.push_back(-1);
+                        ++next_sd;
+                    }
+            }
+        }
+    }
+    sec.xsdend = next_sd;
+}
+
+// ------------------------------------------------------------ jumps --------
+struct SectJump {
+    int is, fs;        // 0-based sectors
+    int64_t nstart;    // 0-based offset into the jump arrays
+    int64_t njumps;
+    bool diag;
+};
+struct Jumps1 {
+    std::vector<int64_t> isd, fsd;
+    std::vector<int16_t> cop, dop;
+    std::vector<int8_t> phase;
+};
+struct Jumps2 {
+    std::vector<int64_t> isd, fsd;
+    std::vector<int32_t> op;
+    std::vector<int8_t> phase;
+};
+
+inline int signed_label(const SpeciesBasis &sb, int q) { return q < sb.nl ? -(q + 1) : (q - sb.nl + 1); }
+
+// a^+_i a_k |s>, phase relative to the canonical ascending-label product
+inline int phase1(uint64_t bits, int i, int k) {
+    if (i == k) return 1;
+    int p = nbelow(bits, k);
+    const uint64_t b1 = bits & ~(1ull << k);
+    p += nbelow(b1, i);
+    return (p & 1) ? -1 : 1;
+}
+// a^+_i a^+_j a_l a_k |s> with i<j, k<l
+inline int phase2(uint64_t bits, int i, int j, int k, int l) {
+    int p = nbelow(bits, k);
+    uint64_t b = bits & ~(1ull << k);
+    p += nbelow(b, l);
+    b &= ~(1ull << l);
+    p += nbelow(b, j);
+    b |= (1ull << j);
+    p += nbelow(b, i);
+    return (p & 1) ? -1 : 1;
+}
+
+// ----------------------------------------------------- interaction ---------
+struct Coupled {
+    int norb = 0;
+    std::vector<int> j2;
+    std::map<std::tuple<int, int, int, int, int, int>, double> v;  // canonical key
+    // canonical form and sign of V_JT(a,b,c,d)
+    std::tuple<int, int, int, int, int, int> canon(int a, int b, int c, int d, int J, int T, int &sign) const {
+        sign = 1;
+        if (a < b) { std::swap(a, b); if ((((j2[a] + j2[b]) / 2 + J + T) & 1)) sign = -sign; }
+        if (c < d) { std::swap(c, d); if ((((j2[c] + j2[d]) / 2 + J + T) & 1)) sign = -sign; }
+        if (std::make_pair(a, b) < std::make_pair(c, d)) { std::swap(a, c); std::swap(b, d); }
+        return std::make_tuple(a, b, c, d, J, T);
+    }
+    bool pair_ok(int a, int b, int J, int T) const {
+        if (J > (j2[a] + j2[b]) / 2 || J < std::abs(j2[a] - j2[b]) / 2) return false;
+        if (a == b && ((J + T) % 2 == 0)) return false;
+        return true;
+    }
+    double get(int a, int b, int c, int d, int J, int T) const {
+        if (!pair_ok(a, b, J, T) || !pair_ok(c, d, J, T)) return 0.0;
+        int sg;
+        auto key = canon(a, b, c, d, J, T, sg);
+        auto it = v.find(key);
+        if (it == v.end()) return 0.0;
+        return sg * it->second;
+    }
+};
+
+struct Pairs {
+    // XX: pairs (q1<q2) ; PN: (qp, qn)
+    std::vector<std::pair<int, int>> list;     // sorted order
+    std::vector<int> M, pidx;                  // per sorted pair
+    std::vector<int64_t> sec_first, sec_n, sec_mestart;  // per section
+    std::vector<int> pair_sec;                 // section of each sorted pair
+    std::map<std::pair<int, int>, int64_t> index;  // (q1,q2) -> 1-based sorted index
+    std::vector<int64_t> dense;                    // same, dense [q1*ns2 + q2]
+    int ns2 = 0;
+    int64_t nmat = 0;
+    void make_dense(int n1, int n2) {
+        ns2 = n2;
+        dense.assign((size_t)n1 * n2, 0);
+        for (auto &kv : index) dense[(size_t)kv.first.first * n2 + kv.first.second] = kv.second;
+    }
+    int64_t at(int q1, int q2) const { return dense[(size_t)q1 * ns2 + q2]; }
+};
+
+void make_xx_pairs(const SpeciesBasis &sb, Pairs &P) {
+    const int ns = sb.nl + sb.nr;
+    struct Tmp { int q1, q2, M, pidx; int64_t tri; };
+    std::vector<Tmp> v;
+    for (int q2 = 0; q2 < ns; ++q2)
+        for (int q1 = 0; q1 < q2; ++q1) {
+            Tmp t;
+            t.q1 = q1; t.q2 = q2;
+            t.M = (sb.q_m2[q1] + sb.q_m2[q2]) / 2;
+            t.pidx = pidx_of(sb.q_par[q1] * sb.q_par[q2]);
+            const int64_t a = q1 + 1, b = q2 + 1;  // pair = isps + (jsps-1)(jsps-2)/2
+            t.tri = a + (b - 1) * (b - 2) / 2;
+            v.push_back(t);
+        }
+    std::stable_sort(v.begin(), v.end(), [](const Tmp &x, const Tmp &y) {
+        if (x.M != y.M) return x.M < y.M;
+        if (x.pidx != y.pidx) return x.pidx < y.pidx;
+        return x.tri < y.tri;
+    });
+    P.list.clear(); P.M.clear(); P.pidx.clear(); P.pair_sec.clear();
+    P.sec_first.clear(); P.sec_n.clear(); P.sec_mestart.clear(); P.index.clear();
+    int64_t nme = 0;
+    for (size_t i = 0; i < v.size(); ++i) {
+        if (i == 0 || v[i].M != v[i - 1].M || v[i].pidx != v[i - 1].pidx) {
+            if (!P.sec_n.empty()) nme += P.sec_n.back() * (P.sec_n.back() + 1) / 2;
+            P.sec_first.push_back((int64_t)i + 1);  // 1-based first index
+            P.sec_n.push_back(0);
+            P.sec_mestart.push_back(nme);
+        }
+        P.sec_n.back() += 1;
+        P.list.push_back({v[i].q1, v[i].q2});
+        P.M.push_back(v[i].M);
+        P.pidx.push_back(v[i].pidx);
+        P.pair_sec.push_back((int)P.sec_n.size() - 1);
+        P.index[{v[i].q1, v[i].q2}] = (int64_t)i + 1;
+    }
+    if (!P.sec_n.empty()) nme += P.sec_n.back() * (P.sec_n.back() + 1) / 2;
+    P.nmat = nme;
+    P.make_dense(ns, ns);
+}
+
+// itbme for sorted pair indices c, d (1-based, same section): triangle packing
+inline int64_t xx_label(const Pairs &P, int64_t c, int64_t d) {
+    const int s = P.pair_sec[c - 1];
+    const int64_t iref = P.sec_first[s] - 1, istart = P.sec_mestart[s];
+    const int64_t hi = std::max(c, d), lo = std::min(c, d);
+    return istart + (hi - iref) * (hi - iref - 1) / 2 + lo - iref;
+}
+
+void make_pn_pairs(const SpeciesBasis &pb, const SpeciesBasis &nb, Pairs &P) {
+    struct Tmp { int qp, qn, M, pidx; };
+    std::vector<Tmp> v;
+    const int nsp = pb.nl + pb.nr, nsn = nb.nl + nb.nr;
+    for (int qp = 0; qp < nsp; ++qp)
+        for (int qn = 0; qn < nsn; ++qn) {
+            Tmp t;
+            t.qp = qp; t.qn = qn;
+            t.M = (pb.q_m2[qp] + nb.q_m2[qn]) / 2;
+            t.pidx = pidx_of(pb.q_par[qp] * nb.q_par[qn]);
+            v.push_back(t);
+        }
+    std::stable_sort(v.begin(), v.end(), [](const Tmp &x, const Tmp &y) {
+        if (x.M != y.M) return x.M < y.M;
+        return x.pidx < y.pidx;
+    });
+    P.list.clear(); P.M.clear(); P.pidx.clear(); P.pair_sec.clear();
+    P.sec_first.clear(); P.sec_n.clear(); P.sec_mestart.clear(); P.index.clear();
+    int64_t nme = 0;
+    for (size_t i = 0; i < v.size(); ++i) {
+        if (i == 0 || v[i].M != v[i - 1].M || v[i].pidx != v[i - 1].pidx) {
+            if (!P.sec_n.empty()) nme += P.sec_n.back() * P.sec_n.back();
+            P.sec_first.push_back((int64_t)i + 1);
+            P.sec_n.push_back(0);
+            P.sec_mestart.push_back(nme);
+        }
+        P.sec_n.back() += 1;
+        P.list.push_back({v[i].qp, v[i].qn});
+        P.M.push_back(v[i].M);
+        P.pidx.push_back(v[i].pidx);
+        P.pair_sec.push_back((int)P.sec_n.size() - 1);
+        P.index[{v[i].qp, v[i].qn}] = (int64_t)i + 1;
+    }
+    if (!P.sec_n.empty()) nme += P.sec_n.back() * P.sec_n.back();
+    P.nmat = nme;
+    P.make_dense(nsp, nsn);
+}
+
+// ------------------------------------------------------------ sort ---------
+// sort1bjumps / sort1bjumps_ins (src/bsortjumpslib.f90:190-290): shell sort
+// with a fixed stride table, key = `key`, carried = the rest.
+void shell_sort_1b(int64_t ndim, int64_t *other, int64_t *key, int16_t *cop, int16_t *dop, int8_t *ph) {
+    static const int64_t strides[28] = {23422578909LL, 10410035071LL, 4626682254LL, 2056303224LL,
+                                        913912544LL,  406183353LL,   180525935LL,  80233749LL,
+                                        35659463LL,   15848650LL,    7043844LL,    3130597LL,
+                                        1391376LL,    463792LL,      198768LL,     86961LL,
+                                        33936LL,      13776LL,       4592LL,       1968LL,
+                                        861LL,        336LL,         112LL,        48LL,
+                                        21LL,         7LL,           3LL,          1LL};
+    for (int ks = 0; ks < 28; ++ks) {
+        const int64_t stride = strides[ks];
+        if (stride > ndim) continue;
+        for (int64_t off = 0; off < stride; ++off) {
+            // Fortran: do j = off+stride+1, ndim, stride  (1-based)
+            for (int64_t j = off + stride + 1; j <= ndim; j += stride) {
+                const int64_t s_o = other[j - 1], s_k = key[j - 1];
+                const int16_t s_c = cop[j - 1], s_d = dop[j - 1];
+                const int8_t s_p = ph[j - 1];
+                int64_t k = j, i = k - stride;
+                while (i > 0) {
+                    if (key[i - 1] <= s_k) break;
+                    other[k - 1] = other[i - 1]; key[k - 1] = key[i - 1];
+                    cop[k - 1] = cop[i - 1]; dop[k - 1] = dop[i - 1]; ph[k - 1] = ph[i - 1];
+                    k = i;
+                    i -= stride;
+                }
+                other[k - 1] = s_o; key[k - 1] = s_k; cop[k - 1] = s_c; dop[k - 1] = s_d; ph[k - 1] = s_p;
+            }
+        }
+    }
+}
+
+// --------------------------------------------------------- container -------
+struct Built {
+    SpeciesBasis pb, nb;
+    std::vector<int64_t> pstart, nstart;
+    Jumps1 p1, n1;
+    Jumps2 p2, n2;
+    std::vector<SectJump> p1sj, n1sj, p2sj, n2sj;
+    std::vector<float> hmatpp, hmatnn, hmatpn;
+    std::vector<int64_t> cpn, dpn;
+    std::vector<float> pspe_h, nspe_h;
+    std::vector<int32_t> optype, hchar;
+    std::vector<int64_t> pxstart, pxend, nxstart, nxend, cstride;
+    std::vector<int64_t> ps_start, ps_end, ns_start, ns_end;
+    std::vector<int32_t> ps_jz, ps_par, ns_jz, ns_par, ps_conj;
+    std::vector<int32_t> spo_p, spm_p, spo_n, spm_n;
+    Pairs ppairs, npairs, pnpairs;
+    // chain-rule bookkeeping: per matrix element, list of (tbme line, coef)
+    std::vector<std::vector<std::pair<int, double>>> jac_pp, jac_nn, jac_pn;
+    std::vector<std::vector<std::pair<int, double>>> jspe_pp, jspe_nn, jspe_pn;
+    int ntbme = 0, norb = 0;
+};
+
+// coupled matrix element table with per-line provenance for the jacobian
+struct Interaction {
+    Coupled C;
+    // canonical key -> list of (tbme line, sign) contributing to it
+    std::map<std::tuple<int, int, int, int, int, int>, std::vector<std::pair<int, int>>> prov;
+};
+
+// V_JT(a,b,c,d) as a linear combination of file lines: returns value, and
+// appends (line, coef) scaled by `w`
+double coupled_with_prov(const Interaction &I, int a, int b, int c, int d, int J, int T, double w,
+                         std::vector<std::pair<int, double>> *acc) {
+    const Coupled &C = I.C;
+    if (!C.pair_ok(a, b, J, T) || !C.pair_ok(c, d, J, T)) return 0.0;
+    int sg;
+    auto key = C.canon(a, b, c, d, J, T, sg);
+    auto it = C.v.find(key);
+    if (it == C.v.end()) return 0.0;
+    if (acc) {
+        auto pit = I.prov.find(key);
+        if (pit != I.prov.end())
+            for (auto &pr : pit->second) acc->push_back({pr.first, w * sg * pr.second});
+    }
+    return sg * it->second;
+}
+
+void compress(std::vector<std::pair<int, double>> &v) {
+    std::map<int, double> m;
+    for (auto &p : v) m[p.first] += p.second;
+    v.clear();
+    for (auto &p : m)
+        if (p.second != 0.0) v.push_back(p);
+}
+
+int build(const bsg_model_spec *s, Built &B) {
+    init_lfact();
+    if (!s || s->norb <= 0 || !s->orbits) { g_err = "bad model spec"; return BSG_ERR_ARG; }
+    if (s->np < 0 || s->nn < 0) { g_err = "negative particle number"; return BSG_ERR_ARG; }
+    B.norb = s->norb;
+    B.ntbme = s->ntbme;
+    bool allsamepar = true, allsameW = true;
+    for (int i = 0; i < s->norb; ++i) {
+        if ((s->orbits[i].l & 1) != (s->orbits[0].l & 1)) allsamepar = false;
+        if (s->orbits[i].w != s->orbits[0].w) allsameW = false;
+        if (s->orbits[i].j2 <= 0 || (s->orbits[i].j2 & 1) == 0) { g_err = "orbit j must be half-integer"; return BSG_ERR_ARG; }
+    }
+    const int iparity_idx = allsamepar ? 1 : pidx_of(s->parity >= 0 ? 1 : -1);
+
+    // ---- s.p. states and haiku blocks per species
+    SpeciesBasis *sbs[2] = {&B.pb, &B.nb};
+    const int Ns[2] = {s->np, s->nn};
+    for (int it = 0; it < 2; ++it) {
+        SpeciesBasis &sb = *sbs[it];
+        sb.N = Ns[it];
+        make_sps(s, allsamepar, allsameW, sb);
+        if (sb.nl + sb.nr > 62) { g_err = "more than 62 s.p. states per species"; return BSG_ERR_UNSUPPORTED; }
+        if (sb.N > sb.nl + sb.nr) { g_err = "too many particles for the space"; return BSG_ERR_ARG; }
+        make_blocks(sb.right, std::max(0, sb.N - sb.nl), std::min(sb.N, sb.nr), sb.rblocks);
+        make_blocks(sb.left, std::max(0, sb.N - sb.nr), std::min(sb.N, sb.nl), sb.lblocks);
+    }
+    // ---- sectors: protons parity 1..2 / jz ascending; neutrons jz descending
+    auto pc = sector_candidates(B.pb), nc = sector_candidates(B.nb);
+    std::vector<std::pair<int, int>> psec, nsec;
+    for (int p = 1; p <= 2; ++p) {
+        std::vector<int> jzs;
+        for (auto &c : pc)
+            if (c.first.first == p) {
+                const int jzn = s->jz2 - c.first.second;
+                const int pn = parmult(iparity_idx, p);
+                if (nc.count({pn, jzn})) jzs.push_back(c.first.second);
+            }
+        std::sort(jzs.begin(), jzs.end());
+        for (int jz : jzs) psec.push_back({p, jz});
+    }
+    {
+        std::vector<int> porder = (iparity_idx == 1) ? std::vector<int>{1, 2} : std::vector<int>{2, 1};
+        for (int p : porder) {
+            std::vector<int> jzs;
+            for (auto &c : nc)
+                if (c.first.first == p) {
+                    const int jzp = s->jz2 - c.first.second;
+                    const int pp = parmult(iparity_idx, p);
+                    if (pc.count({pp, jzp})) jzs.push_back(c.first.second);
+                }
+            std::sort(jzs.begin(), jzs.end(), std::greater<int>());
+            for (int jz : jzs) nsec.push_back({p, jz});
+        }
+    }
+    if (psec.empty() || nsec.empty()) { g_err = "no basis states for this Jz/parity"; return BSG_ERR_ARG; }
+    for (int it = 0; it < 2; ++it) {
+        SpeciesBasis &sb = *sbs[it];
+        auto &lst = it == 0 ? psec : nsec;
+        int64_t next = 0;
+        for (auto &ps : lst) {
+            Sector sec;
+            sec.pidx = ps.first;
+            sec.jz2 = ps.second;
+            fill_sector(sb, sec, next);
+            for (int64_t k = sec.xsdstart - 1; k < sec.xsdend; ++k) sb.sd_sector[k] = (int)sb.sectors.size();
+            sb.sectors.push_back(std::move(sec));
+        }
+    }
+    const int nps = (int)B.pb.sectors.size(), nns = (int)B.nb.sectors.size();
+    std::vector<int> pconj(nps, -1), nconj(nns, -1);
+    for (int a = 0; a < nps; ++a)
+        for (int b = 0; b < nns; ++b)
+            if (B.pb.sectors[a].jz2 + B.nb.sectors[b].jz2 == s->jz2 &&
+                parmult(B.pb.sectors[a].pidx, B.nb.sectors[b].pidx) == iparity_idx) {
+                pconj[a] = b;
+                nconj[b] = a;
+            }
+    for (int a = 0; a < nps; ++a)
+        if (pconj[a] < 0) { g_err = "proton sector without conjugate"; return BSG_ERR_BAD_TABLE; }
+
+    // ---- combinebasis (src/bbasislib.f90:540-677)
+    const int64_t nsdp = (int64_t)B.pb.sd_bits.size(), nsdn = (int64_t)B.nb.sd_bits.size();
+    B.pstart.assign(nsdp, -1);
+    B.nstart.assign(nsdn, -1);
+    int64_t dimbasis = 1, pcount = 0, ncount = 0;
+    for (int is = 0; is < nps; ++is) {
+        const Sector &ps = B.pb.sectors[is];
+        const Sector &ns = B.nb.sectors[pconj[is]];
+        const int64_t ndim = ns.xsdend - ns.xsdstart + 1;
+        if (nconj[pconj[is]] == is) {
+            for (int64_t in = 1; in <= ndim; ++in) B.nstart[ncount++] = in;
+        }
+        const int64_t pdim = ps.xsdend - ps.xsdstart + 1;
+        for (int64_t ip = 0; ip < pdim; ++ip) {
+            B.pstart[pcount++] = dimbasis - 1;
+            dimbasis += ndim;
+        }
+    }
+    dimbasis -= 1;
+    if (pcount != nsdp || ncount != nsdn) { g_err = "combinebasis count mismatch"; return BSG_ERR_BAD_TABLE; }
+
+    // ---- interaction: coupled V_JT canonicalized with provenance
+    Interaction I;
+    I.C.norb = s->norb;
+    for (int i = 0; i < s->norb; ++i) I.C.j2.push_back(s->orbits[i].j2);
+    for (int i = 0; i < s->ntbme; ++i) {
+        const bsg_tbme &t = s->tbme[i];
+        const int a = t.a - 1, b = t.b - 1, c = t.c - 1, d = t.d - 1;
+        if (a < 0 || b < 0 || c < 0 || d < 0 || a >= s->norb || b >= s->norb || c >= s->norb || d >= s->norb) {
+            g_err = "TBME orbit label out of range";
+            return BSG_ERR_ARG;
+        }
+        if (!I.C.pair_ok(a, b, t.J, t.T) || !I.C.pair_ok(c, d, t.J, t.T)) continue;
+        int sg;
+        auto key = I.C.canon(a, b, c, d, t.J, t.T, sg);
+        I.C.v[key] += sg * t.v;
+        I.prov[key].push_back({i, sg});
+    }
+    const double vscale = s->tbme_scale;
+    const int A = s->np + s->nn;
+    const bool call_spe = (A <= 1);
+    const double afac = (A > 1) ? 1.0 / (double)(A - 1) : 0.0;
+    std::vector<double> spe(s->norb, 0.0);
+    for (int i = 0; i < s->norb; ++i) spe[i] = s->spe ? s->spe_scale * s->spe[i] : 0.0;
+
+    // ---- pp / nn uncoupled (uncoupleXXtbme, src/btbme.f90:1209-1551)
+    const int nspsp = B.pb.nl + B.pb.nr;
+    for (int it = 0; it < 2; ++it) {
+        SpeciesBasis &sb = *sbs[it];
+        Pairs &P = it == 0 ? B.ppairs : B.npairs;
+        make_xx_pairs(sb, P);
+        std::vector<float> &H = it == 0 ? B.hmatpp : B.hmatnn;
+        auto &jac = it == 0 ? B.jac_pp : B.jac_nn;
+        auto &jspe = it == 0 ? B.jspe_pp : B.jspe_nn;
+        H.assign(P.nmat, 0.0f);
+        jac.assign(P.nmat, {});
+        jspe.assign(P.nmat, {});
+        if (sb.N < 2) continue;
+        for (size_t s_ = 0; s_ < P.sec_n.size(); ++s_) {
+            const int64_t first = P.sec_first[s_], n = P.sec_n[s_];
+            for (int64_t c = first; c < first + n; ++c)
+                for (int64_t d = first; d <= c; ++d) {
+                    const int64_t lab = xx_label(P, c, d);
+                    const int i = P.list[c - 1].first, j = P.list[c - 1].second;
+                    const int k = P.list[d - 1].first, l = P.list[d - 1].second;
+                    const int a = sb.q_orb[i], b = sb.q_orb[j], cc = sb.q_orb[k], dd = sb.q_orb[l];
+                    const int ja = I.C.j2[a], jb = I.C.j2[b], jc = I.C.j2[cc], jd = I.C.j2[dd];
+                    const int M2 = sb.q_m2[i] + sb.q_m2[j];
+                    const double zab = (a == b) ? std::sqrt(2.0) : 1.0, zcd = (cc == dd) ? std::sqrt(2.0) : 1.0;
+                    double v = 0.0;
+                    std::vector<std::pair<int, double>> pv;
+                    for (int J = 0; J <= 20; ++J) {
+                        const double cgab = cg2(ja, sb.q_m2[i], jb, sb.q_m2[j], 2 * J, M2);
+                        if (cgab == 0.0) continue;
+                        const double cgcd = cg2(jc, sb.q_m2[k], jd, sb.q_m2[l], 2 * J, M2);
+                        if (cgcd == 0.0) continue;
+                        const double w = zab * zcd * cgab * cgcd * vscale;
+                        v += w * coupled_with_prov(I, a, b, cc, dd, J, 1, w, &pv);
+                    }
+                    std::vector<std::pair<int, double>> ps;
+                    if (c == d) {  // SPE folded into the diagonal pair (bsppot.f90:83-106)
+                        v += afac * (spe[a] + spe[b]);
+                        ps.push_back({a, afac * s->spe_scale});
+                        ps.push_back({b, afac * s->spe_scale});
+                        v *= 0.5;  // hermitian doubling of diagonal jumps
+                        for (auto &x : pv) x.second *= 0.5;
+                        for (auto &x : ps) x.second *= 0.5;
+                    }
+                    H[lab - 1] = (float)v;
+                    compress(pv);
+                    compress(ps);
+                    jac[lab - 1] = std::move(pv);
+                    jspe[lab - 1] = std::move(ps);
+                }
+        }
+    }
+    // ---- pn uncoupled (count_uncouplepn, src/btbmepn.f90:177-587)
+    make_pn_pairs(B.pb, B.nb, B.pnpairs);
+    {
+        Pairs &P = B.pnpairs;
+        const int pl = B.pb.nl, pr = B.pb.nr, nl = B.nb.nl, nr = B.nb.nr;
+        const int64_t ld = (int64_t)(nl + nr + 1);
+        B.cpn.assign(ld * (pl + pr + 1), 0);
+        B.dpn.assign(ld * (pl + pr + 1), 0);
+        B.hmatpn.assign(P.nmat, 0.0f);
+        B.jac_pn.assign(P.nmat, {});
+        B.jspe_pn.assign(P.nmat, {});
+        const bool have_pn = (s->np >= 1 && s->nn >= 1);
+        for (size_t s_ = 0; s_ < P.sec_n.size(); ++s_) {
+            const int64_t first = P.sec_first[s_], n = P.sec_n[s_], nme = P.sec_mestart[s_];
+            for (int64_t pos = 1; pos <= n; ++pos) {
+                const int qp = P.list[first + pos - 2].first, qn = P.list[first + pos - 2].second;
+                const int sp = signed_label(B.pb, qp), sn = signed_label(B.nb, qn);
+                const int64_t idx = (int64_t)(sn + nl) + (int64_t)(sp + pl) * ld;
+                B.cpn[idx] = (pos - 1) * n;
+                B.dpn[idx] = pos + nme;
+            }
+            if (!have_pn) continue;
+            for (int64_t cpos = 1; cpos <= n; ++cpos)
+                for (int64_t dpos = 1; dpos <= n; ++dpos) {
+                    const int64_t lab = nme + (cpos - 1) * n + dpos;
+                    const int qa = P.list[first + cpos - 2].first, qb = P.list[first + cpos - 2].second;
+                    const int qc = P.list[first + dpos - 2].first, qd = P.list[first + dpos - 2].second;
+                    const int a = B.pb.q_orb[qa], b = B.nb.q_orb[qb], c = B.pb.q_orb[qc], d = B.nb.q_orb[qd];
+                    const int ja = I.C.j2[a], jb = I.C.j2[b], jc = I.C.j2[c], jd = I.C.j2[d];
+                    const int M2 = B.pb.q_m2[qa] + B.nb.q_m2[qb];
+                    const double zab = (a == b) ? std::sqrt(2.0) : 1.0, zcd = (c == d) ? std::sqrt(2.0) : 1.0;
+                    double v = 0.0;
+                    std::vector<std::pair<int, double>> pv;
+                    for (int J = 0; J <= 20; ++J) {
+                        const double cgab = cg2(ja, B.pb.q_m2[qa], jb, B.nb.q_m2[qb], 2 * J, M2);
+                        if (cgab == 0.0) continue;
+                        const double cgcd = cg2(jc, B.pb.q_m2[qc], jd, B.nb.q_m2[qd], 2 * J, M2);
+                        if (cgcd == 0.0) continue;
+                        const double w = 0.5 * zab * zcd * cgab * cgcd * vscale;
+                        for (int T = 0; T <= 1; ++T) v += w * coupled_with_prov(I, a, b, c, d, J, T, w, &pv);
+                    }
+                    std::vector<std::pair<int, double>> ps;
+                    if (cpos == dpos) {  // SPE folded into pn (bsppot.f90:185-226)
+                        v += afac * (spe[a] + spe[b]);
+                        ps.push_back({a, afac * s->spe_scale});
+                        ps.push_back({b, afac * s->spe_scale});
+                    }
+                    B.hmatpn[lab - 1] = (float)v;
+                    compress(pv);
+                    compress(ps);
+                    B.jac_pn[lab - 1] = std::move(pv);
+                    B.jspe_pn[lab - 1] = std::move(ps);
+                }
+        }
+    }
+    (void)nspsp;
+
+    // ---- jumps
+    // one-body: proton sector jumps (is >= fs), each with its conjugate
+    // neutron sector jump (conj(is) -> conj(fs))
+    auto gen1 = [&](SpeciesBasis &sb, const std::vector<int64_t> &xstart, int is, int fs, Jumps1 &J) {
+        int64_t cnt = 0;
+        const Sector &S = sb.sectors[is];
+        const int ns = sb.nl + sb.nr;
+        for (int64_t sd = S.xsdstart - 1; sd < S.xsdend; ++sd) {
+            const uint64_t bits = sb.sd_bits[sd];
+            for (int k = 0; k < ns; ++k) {
+                if (!(bits >> k & 1ull)) continue;
+                for (int i = 0; i < ns; ++i) {
+                    if (i != k && (bits >> i & 1ull)) continue;
+                    const uint64_t nb2 = (bits & ~(1ull << k)) | (1ull << i);
+                    auto f = sb.sd_index.find(nb2);
+                    if (f == sb.sd_index.end()) continue;
+                    if (sb.sd_sector[f->second] != fs) continue;
+                    J.isd.push_back(xstart[sd]);
+                    J.fsd.push_back(xstart[f->second]);
+                    J.cop.push_back((int16_t)signed_label(sb, i));
+                    J.dop.push_back((int16_t)signed_label(sb, k));
+                    J.phase.push_back((int8_t)phase1(bits, i, k));
+                    ++cnt;
+                }
+            }
+        }
+        return cnt;
+    };
+    auto gen2 = [&](SpeciesBasis &sb, const std::vector<int64_t> &xstart, const Pairs &P, int is, int fs, Jumps2 &J) {
+        int64_t cnt = 0;
+        const Sector &S = sb.sectors[is];
+        const int ns = sb.nl + sb.nr;
+        const bool halve = (is == fs);
+        std::vector<int> occ, tgt;
+        for (int64_t sd = S.xsdstart - 1; sd < S.xsdend; ++sd) {
+            const uint64_t bits = sb.sd_bits[sd];
+            occ.clear();
+            for (int q = 0; q < ns; ++q)
+                if (bits >> q & 1ull) occ.push_back(q);
+            for (size_t x = 0; x < occ.size(); ++x)
+                for (size_t y = x + 1; y < occ.size(); ++y) {
+                    const int k = occ[x], l = occ[y];
+                    const uint64_t rest = bits & ~(1ull << k) & ~(1ull << l);
+                    tgt.clear();
+                    for (int q = 0; q < ns; ++q)
+                        if (!(rest >> q & 1ull)) tgt.push_back(q);
+                    const int64_t dpair = P.at(k, l);
+                    for (size_t u = 0; u < tgt.size(); ++u)
+                        for (size_t v = u + 1; v < tgt.size(); ++v) {
+                            const int i = tgt[u], j = tgt[v];
+                            const int64_t cpair = P.at(i, j);
+                            if (P.pair_sec[cpair - 1] != P.pair_sec[dpair - 1]) continue;  // M, parity
+                            const uint64_t nb2 = rest | (1ull << i) | (1ull << j);
+                            auto f = sb.sd_index.find(nb2);
+                            if (f == sb.sd_index.end()) continue;
+                            if (sb.sd_sector[f->second] != fs) continue;
+                            if (halve && sd < f->second) continue;  // keep isd >= fsd
+                            J.isd.push_back(xstart[sd]);
+                            J.fsd.push_back(xstart[f->second]);
+                            J.op.push_back((int32_t)xx_label(P, cpair, dpair));
+                            J.phase.push_back((int8_t)phase2(bits, i, j, k, l));
+                            ++cnt;
+                        }
+                }
+        }
+        return cnt;
+    };
+    std::map<std::pair<int, int>, int> n1sj_of;
+    for (int is = 0; is < nps; ++is)
+        for (int fs = 0; fs <= is; ++fs) {
+            if (s->np < 1 || s->nn < 1) continue;
+            SectJump sj;
+            sj.is = is; sj.fs = fs; sj.diag = (is == fs);
+            sj.nstart = (int64_t)B.p1.isd.size();
+            sj.njumps = gen1(B.pb, B.pstart, is, fs, B.p1);
+            if (sj.njumps == 0) continue;
+            const int in = pconj[is], fn = pconj[fs];
+            if (!n1sj_of.count({in, fn})) {
+                SectJump nj;
+                nj.is = in; nj.fs = fn; nj.diag = (in == fn);
+                nj.nstart = (int64_t)B.n1.isd.size();
+                nj.njumps = gen1(B.nb, B.nstart, in, fn, B.n1);
+                n1sj_of[{in, fn}] = (int)B.n1sj.size();
+                B.n1sj.push_back(nj);
+            }
+            B.p1sj.push_back(sj);
+        }
+    if (s->np >= 2)
+        for (int is = 0; is < nps; ++is) {
+            SectJump sj;
+            sj.is = is; sj.fs = is; sj.diag = true;
+            sj.nstart = (int64_t)B.p2.isd.size();
+            sj.njumps = gen2(B.pb, B.pstart, B.ppairs, is, is, B.p2);
+            if (sj.njumps > 0) B.p2sj.push_back(sj);
+        }
+    if (s->nn >= 2)
+        for (int is = 0; is < nns; ++is) {
+            SectJump sj;
+            sj.is = is; sj.fs = is; sj.diag = true;
+            sj.nstart = (int64_t)B.n2.isd.size();
+            sj.njumps = gen2(B.nb, B.nstart, B.npairs, is, is, B.n2);
+            if (sj.njumps > 0) B.n2sj.push_back(sj);
+        }
+
+    // ---- single-particle energies per SD when call_spe (makespeme)
+    if (call_spe) {
+        B.pspe_h.assign(nsdp, 0.0f);
+        B.nspe_h.assign(nsdn, 0.0f);
+        for (int it = 0; it < 2; ++it) {
+            SpeciesBasis &sb = *sbs[it];
+            auto &out = it == 0 ? B.pspe_h : B.nspe_h;
+            for (size_t sd = 0; sd < sb.sd_bits.size(); ++sd) {
+                double e = 0.0;
+                for (int q = 0; q < sb.nl + sb.nr; ++q)
+                    if (sb.sd_bits[sd] >> q & 1ull) e += spe[sb.q_orb[q]];
+                out[sd] = (float)e;
+            }
+        }
+    }
+
+    // ---- opbundles in draft_opbundles order (src/bparallel_opbundles.f90:72-95)
+    auto add = [&](int op, int hc, int64_t px0, int64_t px1, int64_t nx0, int64_t nx1) {
+        B.optype.push_back(op); B.hchar.push_back(hc);
+        B.pxstart.push_back(px0); B.pxend.push_back(px1);
+        B.nxstart.push_back(nx0); B.nxend.push_back(nx1);
+        B.cstride.push_back(1);
+    };
+    auto find_sj = [](const std::vector<SectJump> &v, int is, int fs) -> int {
+        for (size_t i = 0; i < v.size(); ++i)
+            if (v[i].is == is && v[i].fs == fs) return (int)i;
+        return -1;
+    };
+    auto emit = [&](const char *kind, int hc) {
+        for (int fs = 0; fs < nps; ++fs)
+            for (int is = fs; is < nps; ++is) {
+                if (!std::strcmp(kind, "PP")) {
+                    const int x = find_sj(B.p2sj, is, fs);
+                    if (x < 0) continue;
+                    const Sector &ns = B.nb.sectors[pconj[is]];
+                    add(BSG_OP_PP, hc, B.p2sj[x].nstart + 1, B.p2sj[x].nstart + B.p2sj[x].njumps, ns.xsdstart, ns.xsdend);
+                } else if (!std::strcmp(kind, "NN")) {
+                    if (is != fs) continue;
+                    const int x = find_sj(B.n2sj, pconj[is], pconj[is]);
+                    if (x < 0) continue;
+                    const Sector &ps = B.pb.sectors[is];
+                    add(BSG_OP_NN, hc, ps.xsdstart, ps.xsdend, B.n2sj[x].nstart + 1, B.n2sj[x].nstart + B.n2sj[x].njumps);
+                } else {  // PN
+                    const int x = find_sj(B.p1sj, is, fs);
+                    if (x < 0) continue;
+                    const int y = n1sj_of.count({pconj[is], pconj[fs]}) ? n1sj_of[{pconj[is], pconj[fs]}] : -1;
+                    if (y < 0 || B.n1sj[y].njumps == 0) continue;
+                    const bool herm = (is == fs && B.p1sj[x].diag && B.n1sj[y].diag);
+                    if ((hc == BSG_H_HERM) != herm) continue;
+                    add(BSG_OP_PN, hc, B.p1sj[x].nstart + 1, B.p1sj[x].nstart + B.p1sj[x].njumps,
+                        B.n1sj[y].nstart + 1, B.n1sj[y].nstart + B.n1sj[y].njumps);
+                }
+            }
+    };
+    if (call_spe)
+        for (int is = 0; is < nps; ++is) {
+            const Sector &ps = B.pb.sectors[is];
+            const Sector &ns = B.nb.sectors[pconj[is]];
+            add(BSG_OP_SPE, BSG_H_HERM, ps.xsdstart, ps.xsdend, ns.xsdstart, ns.xsdend);
+        }
+    emit("PP", BSG_H_FWD);
+    emit("NN", BSG_H_FWD);
+    emit("PN", BSG_H_FWD);
+    emit("PN", BSG_H_HERM);
+    emit("PP", BSG_H_BWD);
+    emit("NN", BSG_H_BWD);
+    emit("PN", BSG_H_BWD);
+
+    // ---- sort_bundled_jumps (src/bsortjumpslib.f90:21-175): per PN bundle,
+    // protons on fsd, neutrons on isd
+    for (size_t ib = 0; ib < B.optype.size(); ++ib) {
+        if (B.optype[ib] != BSG_OP_PN) continue;
+        const int64_t sp0 = B.pxstart[ib] - 1, np_ = B.pxend[ib] - sp0;
+        const int64_t sn0 = B.nxstart[ib] - 1, nn_ = B.nxend[ib] - sn0;
+        shell_sort_1b(np_, B.p1.isd.data() + sp0, B.p1.fsd.data() + sp0, B.p1.cop.data() + sp0,
+                      B.p1.dop.data() + sp0, B.p1.phase.data() + sp0);
+        shell_sort_1b(nn_, B.n1.fsd.data() + sn0, B.n1.isd.data() + sn0, B.n1.cop.data() + sn0,
+                      B.n1.dop.data() + sn0, B.n1.phase.data() + sn0);
+    }
+
+    // ---- sector / s.p. bookkeeping for the caller
+    for (auto &sec : B.pb.sectors) {
+        B.ps_start.push_back(sec.xsdstart); B.ps_end.push_back(sec.xsdend);
+        B.ps_jz.push_back(sec.jz2); B.ps_par.push_back(par_of_idx(sec.pidx));
+    }
+    for (int a = 0; a < nps; ++a) B.ps_conj.push_back(pconj[a] + 1);
+    for (auto &sec : B.nb.sectors) {
+        B.ns_start.push_back(sec.xsdstart); B.ns_end.push_back(sec.xsdend);
+        B.ns_jz.push_back(sec.jz2); B.ns_par.push_back(par_of_idx(sec.pidx));
+    }
+    for (int q = 0; q < B.pb.nl + B.pb.nr; ++q) { B.spo_p.push_back(B.pb.q_orb[q]); B.spm_p.push_back(B.pb.q_m2[q]); }
+    for (int q = 0; q < B.nb.nl + B.nb.nr; ++q) { B.spo_n.push_back(B.nb.q_orb[q]); B.spm_n.push_back(B.nb.q_m2[q]); }
+    (void)dimbasis;
+    return BSG_OK;
+}
+
+template <typename T>
+const T *ptr_or_null(const std::vector<T> &v) { return v.empty() ? nullptr : v.data(); }
+
+}  // namespace
+
+extern "C" {
+
+const char *bsg_host_last_error(void) { return g_err.c_str(); }
+
+int bsg_host_build(const bsg_model_spec *spec, bsg_host_tables **out) {
+    if (!out) { g_err = "null output"; return BSG_ERR_ARG; }
+    *out = nullptr;
+    Built *B = new (std::nothrow) Built();
+    if (!B) { g_err = "host allocation failed"; return BSG_ERR_NOMEM; }
+    int st;
+    try {
+        st = build(spec, *B);
+    } catch (const std::bad_alloc &) {
+        g_err = "host allocation failed";
+        st = BSG_ERR_NOMEM;
+    } catch (const std::exception &e) {
+        g_err = std::string("builder exception: ") + e.what();
+        st = BSG_ERR_BAD_TABLE;
+    }
+    if (st != BSG_OK) { delete B; return st; }
+    bsg_host_tables *h = (bsg_host_tables *)std::calloc(1, sizeof(bsg_host_tables));
+    if (!h) { delete B; g_err = "host allocation failed"; return BSG_ERR_NOMEM; }
+    bsg_tables &t = h->t;
+    t.nsd_p = (int64_t)B->pstart.size();
+    t.nsd_n = (int64_t)B->nstart.size();
+    {
+        int64_t dim = 0;
+        for (size_t is = 0; is < B->ps_start.size(); ++is) {
+            const int64_t pd = B->ps_end[is] - B->ps_start[is] + 1;
+            const int c = B->ps_conj[is] - 1;
+            dim += pd * (B->ns_end[c] - B->ns_start[c] + 1);
+        }
+        t.dimbasis = dim;
+    }
+    t.pstart = ptr_or_null(B->pstart);
+    t.nstart = ptr_or_null(B->nstart);
+    t.np1b = (int64_t)B->p1.isd.size();
+    t.p1b_isd = ptr_or_null(B->p1.isd); t.p1b_fsd = ptr_or_null(B->p1.fsd);
+    t.p1b_cop = ptr_or_null(B->p1.cop); t.p1b_dop = ptr_or_null(B->p1.dop); t.p1b_phase = ptr_or_null(B->p1.phase);
+    t.nn1b = (int64_t)B->n1.isd.size();
+    t.n1b_isd = ptr_or_null(B->n1.isd); t.n1b_fsd = ptr_or_null(B->n1.fsd);
+    t.n1b_cop = ptr_or_null(B->n1.cop); t.n1b_dop = ptr_or_null(B->n1.dop); t.n1b_phase = ptr_or_null(B->n1.phase);
+    t.np2b = (int64_t)B->p2.isd.size();
+    t.p2b_isd = ptr_or_null(B->p2.isd); t.p2b_fsd = ptr_or_null(B->p2.fsd);
+    t.p2b_op = ptr_or_null(B->p2.op); t.p2b_phase = ptr_or_null(B->p2.phase);
+    t.nn2b = (int64_t)B->n2.isd.size();
+    t.n2b_isd = ptr_or_null(B->n2.isd); t.n2b_fsd = ptr_or_null(B->n2.fsd);
+    t.n2b_op = ptr_or_null(B->n2.op); t.n2b_phase = ptr_or_null(B->n2.phase);
+    t.nmatpp = (int64_t)B->hmatpp.size(); t.hmatpp = ptr_or_null(B->hmatpp);
+    t.nmatnn = (int64_t)B->hmatnn.size(); t.hmatnn = ptr_or_null(B->hmatnn);
+    t.nmatpn = (int64_t)B->hmatpn.size(); t.hmatpn = ptr_or_null(B->hmatpn);
+    t.nhsps_pl = B->pb.nl; t.nhsps_pr = B->pb.nr;
+    t.nhsps_nl = B->nb.nl; t.nhsps_nr = B->nb.nr;
+    t.cpnpair = ptr_or_null(B->cpn); t.dpnpair = ptr_or_null(B->dpn);
+    t.call_spe = B->pspe_h.empty() ? 0 : 1;
+    t.pspe_h = ptr_or_null(B->pspe_h); t.nspe_h = ptr_or_null(B->nspe_h);
+    t.nbundles = (int64_t)B->optype.size();
+    t.optype = ptr_or_null(B->optype); t.hchar = ptr_or_null(B->hchar);
+    t.pxstart = ptr_or_null(B->pxstart); t.pxend = ptr_or_null(B->pxend);
+    t.nxstart = ptr_or_null(B->nxstart); t.nxend = ptr_or_null(B->nxend);
+    t.cstride = ptr_or_null(B->cstride);
+    h->nsectors_p = (int32_t)B->ps_start.size();
+    h->nsectors_n = (int32_t)B->ns_start.size();
+    h->psector_start = B->ps_start.data(); h->psector_end = B->ps_end.data();
+    h->psector_jz2 = B->ps_jz.data(); h->psector_par = B->ps_par.data();
+    h->nsector_start = B->ns_start.data(); h->nsector_end = B->ns_end.data();
+    h->nsector_jz2 = B->ns_jz.data(); h->nsector_par = B->ns_par.data();
+    h->psector_conj = B->ps_conj.data();
+    h->nhsps_p = B->pb.nl + B->pb.nr;
+    h->nhsps_n = B->nb.nl + B->nb.nr;
+    h->sp_orb_p = B->spo_p.data(); h->sp_m2_p = B->spm_p.data();
+    h->sp_orb_n = B->spo_n.data(); h->sp_m2_n = B->spm_n.data();
+    h->sd_bits_p = B->pb.sd_bits.data(); h->sd_bits_n = B->nb.sd_bits.data();
+    h->npairs_pp = (int64_t)B->ppairs.list.size();
+    h->npairs_nn = (int64_t)B->npairs.list.size();
+    h->npairs_pn = (int64_t)B->pnpairs.list.size();
+    h->priv = B;
+    *out = h;
+    return BSG_OK;
+}
+
+void bsg_host_free(bsg_host_tables *h) {
+    if (!h) return;
+    delete (Built *)h->priv;
+    std::free(h);
+}
+
+int bsg_host_me_jacobian(const bsg_host_tables *h, int kind, double *d_tbme, double *d_spe) {
+    if (!h || !h->priv || kind < 0 || kind > 2) { g_err = "bad jacobian request"; return BSG_ERR_ARG; }
+    const Built *B = (const Built *)h->priv;
+    const auto &jac = kind == 0 ? B->jac_pp : kind == 1 ? B->jac_nn : B->jac_pn;
+    const auto &jsp = kind == 0 ? B->jspe_pp : kind == 1 ? B->jspe_nn : B->jspe_pn;
+    const size_t nmat = jac.size();
+    if (d_tbme) {
+        std::memset(d_tbme, 0, sizeof(double) * nmat * (size_t)std::max(1, B->ntbme));
+        for (size_t k = 0; k < nmat; ++k)
+            for (auto &p : jac[k]) d_tbme[k * (size_t)B->ntbme + p.first] += p.second;
+    }
+    if (d_spe) {
+        std::memset(d_spe, 0, sizeof(double) * nmat * (size_t)B->norb);
+        for (size_t k = 0; k < nmat; ++k)
+            for (auto &p : jsp[k]) d_spe[k * (size_t)B->norb + p.first] += p.second;
+    }
+    return BSG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,201 @@
+/*
+ * bsg.h -- C ABI of the B200 M-scheme Hamiltonian engine (libbsgpu.so).
+ *
+ * The engine replaces BIGSTICK's on-the-fly factorized matvec and the Lanczos
+ * loop around it.  The Fortran host keeps building the basis, sectors, jumps,
+ * opbundles and uncoupled matrix elements; it passes plain pointers to those
+ * module arrays through this ABI (ISO_C_BINDING).  The
+ * arrays are uploaded to the device unchanged; every derived index the GPU
+ * kernels need lives in separate device buffers.
+ *
+ * Index conventions are the reference's (Fortran, 1-based):
+ *   basis state = pstart(ip) + nstart(in)  (pstart 0-based offset, nstart
+ *   1-based), jump isd/fsd already hold pstart/nstart values, op labels and
+ *   hmat indices are 1-based, cpnpair/dpnpair are 2-D Fortran arrays with
+ *   bounds (-nhsps(-2):nhsps(2), -nhsps(-1):nhsps(1)), first index fastest.
+ *
+ * Every entry point returns an int status (BSG_OK == 0).  Nothing aborts,
+ * traps or exits; the last error message is latched in the context.
+ */
+#ifndef BSG_H
+#define BSG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (replace the reference's `stop N`, e.g.
+ *      src/bapplyhlibOMP.f90:943, :1446 and :1971) ---- */
+#define BSG_OK               0
+#define BSG_ERR_BAD_TABLE    1   /* table failed validation before upload      */
+#define BSG_ERR_OOB_INDEX    2   /* an index points outside its array          */
+#define BSG_ERR_CUDA         3   /* CUDA runtime error                         */
+#define BSG_ERR_NOMEM        4   /* device or host allocation failed           */
+#define BSG_ERR_TIMEOUT      5   /* a bounded device wait gave up              */
+#define BSG_ERR_NAN          6   /* non-finite value found in a vector         */
+#define BSG_ERR_ARG          7   /* bad argument                               */
+#define BSG_ERR_UNSUPPORTED  8   /* valid input outside what this build covers */
+#define BSG_ERR_NOT_CONVERGED 9  /* Lanczos hit its iteration cap              */
+
+/* ---- opbundle optype / hchar (src/bmodules_parallel.f90:275-311) ---- */
+#define BSG_OP_SPE 1
+#define BSG_OP_PP  2
+#define BSG_OP_NN  3
+#define BSG_OP_PN  4
+#define BSG_H_FWD  'f'
+#define BSG_H_BWD  'b'
+#define BSG_H_HERM 'h'
+
+/* ---- vector precision (lanc_prec, src/bmodules_main.f90:171) ---- */
+#define BSG_PREC_FP32 4
+#define BSG_PREC_FP64 8
+
+/* ---- bsg_applyh flags ---- */
+#define BSG_ACCUMULATE   1   /* vout += H vin (the reference's semantics after
+                                initialize_final zeroes vec2); else vout = H vin */
+#define BSG_DEVICE_PTRS  2   /* vin/vout are device pointers; else host memory  */
+
+/*
+ * Plain pointers to the reference's module arrays after setup
+ * (src/bigstick_main.f90:650-676: jumps sorted by sort_bundled_jumps,
+ * hmat* filled by uncoupleXXtbme / count_uncouplepn).
+ */
+typedef struct bsg_tables {
+    /* basis: src/bbasislib.f90:16-19, combinebasis :540-677 */
+    int64_t dimbasis;
+    int64_t nsd_p, nsd_n;              /* nXsd(1), nXsd(2)                   */
+    const int64_t *pstart;             /* [nsd_p]                            */
+    const int64_t *nstart;             /* [nsd_n]                            */
+
+    /* one-body jumps: src/bmodules_main.f90:643-666 */
+    int64_t np1b;
+    const int64_t *p1b_isd, *p1b_fsd;
+    const int16_t *p1b_cop, *p1b_dop;
+    const int8_t  *p1b_phase;
+    int64_t nn1b;
+    const int64_t *n1b_isd, *n1b_fsd;
+    const int16_t *n1b_cop, *n1b_dop;
+    const int8_t  *n1b_phase;
+
+    /* two-body jumps: src/bmodules_main.f90:668-680 */
+    int64_t np2b;
+    const int64_t *p2b_isd, *p2b_fsd;
+    const int32_t *p2b_op;
+    const int8_t  *p2b_phase;
+    int64_t nn2b;
+    const int64_t *n2b_isd, *n2b_fsd;
+    const int32_t *n2b_op;
+    const int8_t  *n2b_phase;
+
+    /* uncoupled matrix elements, float32: src/bmodules_main.f90:873-875 */
+    int64_t nmatpp, nmatnn, nmatpn;
+    const float *hmatpp, *hmatnn, *hmatpn;   /* 1-based labels index these */
+
+    /* cpnpair/dpnpair: src/btbmepn.f90:126-131 */
+    int32_t nhsps_pl, nhsps_pr;        /* nhsps(-1), nhsps(1)                */
+    int32_t nhsps_nl, nhsps_nr;        /* nhsps(-2), nhsps(2)                */
+    const int64_t *cpnpair, *dpnpair;  /* [(nl+nr+1)*(pl+pr+1)], column-major */
+
+    /* SPE case (only when call_spe, src/bsppot.f90:20-34): src/bdiagh.f90:5-13 */
+    int32_t call_spe;
+    const float *pspe_h;               /* [nsd_p] or NULL                    */
+    const float *nspe_h;               /* [nsd_n] or NULL                    */
+
+    /* opbundles as struct-of-arrays: src/bmodules_parallel.f90:275-311 */
+    int64_t nbundles;
+    const int32_t *optype;             /* BSG_OP_*                           */
+    const int32_t *hchar;              /* 'f', 'b', 'h'                      */
+    const int64_t *pxstart, *pxend, *nxstart, *nxend, *cstride;
+} bsg_tables;
+
+typedef struct bsg_config {
+    int32_t device;        /* CUDA device ordinal                              */
+    int32_t max_nb;        /* largest block size bsg_applyh will be given      */
+    int32_t validate;      /* 1: run the host-side table validator at create   */
+    int32_t reserved;
+} bsg_config;
+
+typedef struct bsg_ctx bsg_ctx;
+
+/* Lanczos parameters (src/blanczosmain.f90:1413-2153, src/bmodules_flags.f90) */
+typedef struct bsg_lanczos_params {
+    int32_t nkeep;         /* states wanted                                    */
+    int32_t niter;         /* iterations per restart cycle (max if no restart) */
+    int32_t nthick_add;    /* extra Ritz vectors kept on thick restart (0: off)*/
+    int32_t max_restarts;  /* max_num_thick_restart                            */
+    int32_t nb;            /* block size: 1 = lanczos_p, >1 = lanczos_block     */
+    int32_t matvec_prec;   /* BSG_PREC_FP32 or BSG_PREC_FP64 for applyH         */
+    int32_t fixed_iter;    /* 1: run exactly niter iterations (no conv. test)  */
+    int32_t ncheck;        /* states in the convergence test (nkeep+ncheck_ex) */
+    double  converge_tol;  /* converge_tol0_def = 1e-3 (blanczoslib.f90:2642)  */
+    int32_t want_vectors;  /* 1: return nkeep eigenvectors (fp64, dim x nkeep) */
+    int32_t pivot;         /* 0: uniform 1/sqrt(dim) (blanczoslib.f90:825-831) */
+    uint64_t seed;         /* random restart / block pivot seed                */
+} bsg_lanczos_params;
+
+typedef struct bsg_report {
+    int32_t iterations;        /* iterations in the last cycle              */
+    int32_t total_iterations;  /* including thick-restart cycles            */
+    int32_t restarts;          /* thick restarts done                       */
+    int32_t random_restarts;   /* beta collapses handled                    */
+    int32_t matvecs;           /* applyH calls (block calls count once)     */
+    int32_t converged;
+    double  t_matvec_ms;       /* device time in applyH                     */
+    double  t_reorth_ms;       /* device time in reorthogonalization        */
+    double  t_eig_ms;          /* device time in projected eigen-solves     */
+    double  t_total_ms;
+} bsg_report;
+
+/* ---- lifecycle ---- */
+int  bsg_create(const bsg_tables *t, const bsg_config *cfg, bsg_ctx **out);
+int  bsg_destroy(bsg_ctx *ctx);
+const char *bsg_strerror(int status);
+/* copies the latched message of the last failing call on ctx */
+int  bsg_last_error(const bsg_ctx *ctx, char *buf, size_t len);
+
+/* ---- applyH: replaces applyHbundled_omp('n') (src/bapplyhlibOMP.f90:882)
+ *      for nb == 1 and applyHbundled_block_omp (src/bapplyhlibOMP_block.f90:43)
+ *      for nb > 1.  Vectors of nb interleaved vectors: element (state s,
+ *      vector v) at (s-1)*nb + v (src/bmodules_block.f90:19-22).
+ *      prec: BSG_PREC_FP32 (float vectors, fp32 accumulation) or
+ *      BSG_PREC_FP64 (double vectors, fp32 matrix elements promoted). ---- */
+int  bsg_applyh(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec, int flags);
+/* same on a caller-provided cudaStream_t (device pointers only) */
+int  bsg_applyh_stream(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec,
+                       int flags, void *cuda_stream);
+
+/* ---- Lanczos: replaces lanczos_p (src/blanczosmain.f90:1413) and
+ *      lanczos_block (:1804) with thick restart; everything stays on the
+ *      device.  evals[nkeep]; evecs (host, fp64, dim x nkeep column-major) or
+ *      NULL.  pivot_vec: optional host fp64 start vector (dim*nb) or NULL. ---- */
+int  bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const double *pivot_vec,
+                 double *evals, double *evecs, bsg_report *rep);
+
+/* ---- adjoint: Hellmann-Feynman gradient dE_k/dhmat for the uncoupled
+ *      matrix elements (the transposed-jump contraction of
+ *      src/bdenslib4.f90:129-729).  evecs: host fp64 dim x nstates column-major
+ *      (normalized).  Outputs (host, fp64): dpp[nstates*nmatpp],
+ *      dnn[nstates*nmatnn], dpn[nstates*nmatpn], dspe_p[nstates*nsd_p] and
+ *      dspe_n[nstates*nsd_n] (the last two only when call_spe; may be NULL). ---- */
+int  bsg_grad(bsg_ctx *ctx, const double *evecs, int nstates,
+              double *dpp, double *dnn, double *dpn, double *dspe_p, double *dspe_n);
+
+/* ---- introspection used by tests and the benchmark ---- */
+typedef struct bsg_stats {
+    int64_t n_ops_pp, n_ops_nn, n_ops_pn, n_ops_spe;  /* inner-loop updates / matvec */
+    int64_t jump_bytes;        /* bytes of jump + label tables uploaded        */
+    int64_t derived_bytes;     /* bytes of derived device indices              */
+    int64_t n_rows;            /* proton SDs (output rows)                     */
+    int64_t n_contrib;         /* row contributions                            */
+    int32_t kernel_launches_per_matvec;
+    int32_t reserved;
+} bsg_stats;
+int  bsg_get_stats(const bsg_ctx *ctx, bsg_stats *st);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BSG_H */

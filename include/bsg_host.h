@@ -1,0 +1,91 @@
+/*
+ * bsg_host.h -- C ABI of the host-side table builder (libbsghost.so).
+ *
+ * In a BIGSTICK build the Fortran host produces the tables that bsg_create()
+ * consumes (basis, sectors, jumps, opbundles, uncoupled matrix elements).  No
+ * Fortran compiler is available to this project, so this CPU library restates
+ * that setup for full (untruncated) M-scheme spaces and fills the same arrays,
+ * in the same element types and with the same index conventions.  It is not
+ * part of the GPU path: it only produces the inputs of bsg.h.
+ *
+ * Reference stages restated here:
+ *   s.p. states      src/bspstates.f90:53-332 (extract_sps, sort_spsqn,
+ *                    make_hspsqn)
+ *   sectors, basis   src/bbasislib.f90:227-677 (count_create_sectors,
+ *                    count_fill_sectors_w_blocks, combinebasis)
+ *   jumps            src/bjumplib_weld.f90:296-809 (isd = blockstart-1 +
+ *                    (iladd-1)*niradd + iradd; hermitian half isd >= fsd on
+ *                    diagonal two-body blocks)
+ *   opbundles        src/bparallel_opbundles.f90:36-708
+ *   jump sort        src/bsortjumpslib.f90:21-290 (shell sort, fixed strides)
+ *   matrix elements  src/btbme.f90:1209-1551, src/btbmepn.f90:177-587,
+ *                    src/binput_tbme.f90:898-2027, src/bsppot.f90:20-238
+ */
+#ifndef BSG_HOST_H
+#define BSG_HOST_H
+
+#include <stdint.h>
+#include "bsg.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* one orbit line of an isospin .sps file: n l j w (src/binput.f90) */
+typedef struct bsg_orbit {
+    int32_t nr, l, j2, w;      /* j2 = 2j */
+} bsg_orbit;
+
+/* coupled J-T two-body matrix element line "a b c d J T V" of an isospin
+ * .int file (src/binput_tbme.f90:898-1240), orbit labels 1-based */
+typedef struct bsg_tbme {
+    int32_t a, b, c, d, J, T;
+    double v;
+} bsg_tbme;
+
+typedef struct bsg_model_spec {
+    int32_t norb;
+    const bsg_orbit *orbits;   /* same orbits for protons and neutrons      */
+    int32_t np, nn;            /* valence protons, neutrons                 */
+    int32_t jz2;               /* 2 x Jz of the system                      */
+    int32_t parity;            /* +1 / -1 (ignored when all orbits share it) */
+    int32_t ntbme;
+    const bsg_tbme *tbme;
+    const double *spe;         /* [norb] single-particle energies           */
+    double spe_scale;          /* xspe                                      */
+    double tbme_scale;         /* (A0/A)^x                                   */
+} bsg_model_spec;
+
+/* owning container: every pointer in .t points into memory owned here */
+typedef struct bsg_host_tables {
+    bsg_tables t;
+    int32_t nsectors_p, nsectors_n;
+    int64_t *psector_start, *psector_end;  /* 1-based SD ranges per sector */
+    int32_t *psector_jz2, *psector_par;
+    int64_t *nsector_start, *nsector_end;
+    int32_t *nsector_jz2, *nsector_par;
+    int32_t *psector_conj;                 /* conjugate neutron sector (1-based) */
+    int32_t nhsps_p, nhsps_n;              /* total s.p. states per species */
+    /* s.p. states in builder order: combined label q (0-based); signed label
+     * is -(q+1) for q < nl (left, m<0) else q-nl+1 (right, m>=0) */
+    int32_t *sp_orb_p, *sp_m2_p, *sp_orb_n, *sp_m2_n;
+    uint64_t *sd_bits_p, *sd_bits_n;       /* occupation bitmasks per SD   */
+    /* pair bookkeeping for the adjoint chain rule (coupled <- uncoupled) */
+    int64_t npairs_pp, npairs_nn, npairs_pn;
+    void *priv;                            /* builder internals            */
+} bsg_host_tables;
+
+int  bsg_host_build(const bsg_model_spec *spec, bsg_host_tables **out);
+void bsg_host_free(bsg_host_tables *h);
+const char *bsg_host_last_error(void);
+
+/* d hmat / d V_JT(ab,cd) chain-rule coefficients: for uncoupled label index
+ * k (0-based) of species kind (0 = pp, 1 = nn, 2 = pn) the coefficient of
+ * each file TBME line i: dhmat[k]/dV_i.  Dense [nmat x ntbme] double.
+ * Also dhmat/dspe_a for each orbit ([nmat x norb]) through SPE subsumption. */
+int  bsg_host_me_jacobian(const bsg_host_tables *h, int kind, double *d_tbme, double *d_spe);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BSG_HOST_H */

@@ -1,0 +1,99 @@
+"""ORACLE -- test infrastructure only.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this package, as the checker.  The product (bigstickpublick_b200) never
+imports, links or calls it.
+
+* liboracle.so (oracle_applyh.c): plain-C restatement of BIGSTICK's
+  applyHbundled_omp / applyHbundled_block_omp loops, plus the OpenMP
+  serial-path split routines used as the timed CPU baseline.
+* dense_h.py: independent dense Hamiltonian from second quantization.
+* lanczos.py: numpy restatement of lanczos_p / lanczos_block with full
+  reorthogonalization, convergence test and thick restart.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+def build(force=False):
+    """Compile oracle_applyh.c into oracle/liboracle.so with gcc."""
+    out = os.path.join(_HERE, "liboracle.so")
+    src = os.path.join(_HERE, "oracle_applyh.c")
+    if force or not os.path.exists(out) or os.path.getmtime(out) < os.path.getmtime(src):
+        subprocess.check_call(["gcc", "-std=c11", "-O3", "-march=x86-64-v2", "-fopenmp", "-fPIC",
+                               "-shared", src, "-o", out])
+    return out
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = build()
+        L = C.CDLL(path)
+        L.oracle_applyh.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]
+        L.oracle_applyh.restype = C.c_int
+        L.oracle_applyh_omp.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]
+        L.oracle_applyh_omp.restype = C.c_int
+        L.oracle_count_ops.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+        L.oracle_count_ops.restype = None
+        _LIB = L
+    return _LIB
+
+
+def _tp(tables):
+    t = tables.as_ctypes()
+    return C.cast(C.pointer(t), C.c_void_p), t
+
+
+def applyh(tables, vin, nb=1, accumulate_into=None):
+    """H vin (one thread, reference loop order).  vin: float32 or float64 array
+    of dim*nb (interleaved block layout); returns a new array (or accumulates
+    into `accumulate_into`)."""
+    vin = np.ascontiguousarray(vin)
+    prec = 4 if vin.dtype == np.float32 else 8
+    out = np.zeros_like(vin) if accumulate_into is None else accumulate_into
+    p, keep = _tp(tables)
+    st = lib().oracle_applyh(p, vin.ctypes.data, out.ctypes.data, nb, prec)
+    if st != 0:
+        raise RuntimeError(f"oracle_applyh status {st}")
+    return out
+
+
+def applyh_omp(tables, vin, nb=1, nthreads=None, out=None):
+    vin = np.ascontiguousarray(vin)
+    prec = 4 if vin.dtype == np.float32 else 8
+    if out is None:
+        out = np.zeros_like(vin)
+    p, keep = _tp(tables)
+    st = lib().oracle_applyh_omp(p, vin.ctypes.data, out.ctypes.data, nb, prec,
+                                 nthreads or os.cpu_count())
+    if st != 0:
+        raise RuntimeError(f"oracle_applyh_omp status {st}")
+    return out
+
+
+def count_ops(tables):
+    """(spe, pp, nn, pn) inner-loop updates per matvec."""
+    ops = (C.c_int64 * 4)()
+    p, keep = _tp(tables)
+    lib().oracle_count_ops(p, ops)
+    return tuple(int(x) for x in ops)
+
+
+def dense_from_applyh(tables, prec=8):
+    """Dense H by applying the oracle matvec to unit vectors (small dims)."""
+    n = tables.dim
+    dt = np.float64 if prec == 8 else np.float32
+    H = np.zeros((n, n), dtype=np.float64)
+    e = np.zeros(n, dtype=dt)
+    for i in range(n):
+        e[:] = 0
+        e[i] = 1
+        H[:, i] = applyh(tables, e)
+    return H

@@ -1,0 +1,286 @@
+/*
+ * ORACLE -- test infrastructure only.  Nothing in the product links, imports
+ * or calls this file; only tests/, __graft_entry__.smoke() and bench.py's CPU
+ * baseline use it, as the checker.
+ *
+ * Plain-C restatement of BIGSTICK's factorized matvec on the host:
+ *
+ *   oracle_applyh()      applyHbundled_omp with one thread
+ *                        (src/bapplyhlibOMP.f90:882-1657: SPE :988-1011,
+ *                        NN :1012-1066, PP :1068-1241, PN :1242-1442) and its
+ *                        block form applyHbundled_block_omp
+ *                        (src/bapplyhlibOMP_block.f90:43-886) for nb > 1.
+ *   oracle_applyh_omp()  the OpenMP serial-path split routines
+ *                        applyhPPbundled_g / applyhNNbundled_g /
+ *                        applyhPNbundled_g (src/bapplyhlib1.f90:325-818):
+ *                        PP threads over neutron SD chunks, NN over proton SD
+ *                        chunks, PN forward over proton-jump chunks cut at
+ *                        p1b_fsd changes, PN backward over neutron-jump chunks
+ *                        cut at n1b_isd changes (jumps are sorted that way,
+ *                        src/bsortjumpslib.f90:57-95).  Used as the timed CPU
+ *                        baseline.
+ *
+ * Arithmetic follows the reference: xme is real(4) (hmat * phase), the update
+ * is vout = vout + xme*vin in the vector precision (float for lanc_prec=4,
+ * double for lanc_prec=8), accumulating into vout.
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../include/bsg.h"
+
+#define CPN(t, b, a) ((t)->cpnpair[(int64_t)((b) + (t)->nhsps_nl) + \
+                      (int64_t)((a) + (t)->nhsps_pl) * (int64_t)((t)->nhsps_nl + (t)->nhsps_nr + 1)])
+#define DPN(t, d, c) ((t)->dpnpair[(int64_t)((d) + (t)->nhsps_nl) + \
+                      (int64_t)((c) + (t)->nhsps_pl) * (int64_t)((t)->nhsps_nl + (t)->nhsps_nr + 1)])
+
+/* one bundle, serial, vector element type T, block size nb */
+#define DEFINE_BUNDLE(T, NAME)                                                           \
+static void NAME(const bsg_tables *t, int64_t ib, const T *vin, T *vout, int nb) {        \
+    const int op = t->optype[ib];                                                        \
+    const int hc = t->hchar[ib];                                                         \
+    const int64_t px0 = t->pxstart[ib], px1 = t->pxend[ib];                              \
+    const int64_t nx0 = t->nxstart[ib], nx1 = t->nxend[ib];                              \
+    const int64_t cs = t->cstride[ib] > 0 ? t->cstride[ib] : 1;                          \
+    if (op == BSG_OP_SPE) {                                                              \
+        for (int64_t ip = px0; ip <= px1; ++ip) {                                        \
+            const float pspe = t->pspe_h[ip - 1];                                        \
+            int64_t statef = t->pstart[ip - 1] + t->nstart[nx0 - 1];                     \
+            for (int64_t in = nx0; in <= nx1; ++in) {                                    \
+                const float nspe = t->nspe_h[in - 1];                                    \
+                const float e = pspe + nspe;                                             \
+                for (int v = 0; v < nb; ++v)                                             \
+                    vout[(statef - 1) * nb + v] += vin[(statef - 1) * nb + v] * (T)e;    \
+                ++statef;                                                                \
+            }                                                                            \
+        }                                                                                \
+    } else if (op == BSG_OP_NN) {                                                        \
+        const int64_t *s1 = hc == 'b' ? t->n2b_fsd : t->n2b_isd;                         \
+        const int64_t *s2 = hc == 'b' ? t->n2b_isd : t->n2b_fsd;                         \
+        for (int64_t csd = px0; csd <= px1; csd += cs) {                                 \
+            const int64_t psd = t->pstart[csd - 1];                                      \
+            for (int64_t x = nx0; x <= nx1; ++x) {                                       \
+                float xme = t->hmatnn[t->n2b_op[x - 1] - 1];                             \
+                xme = xme * (float)t->n2b_phase[x - 1];                                  \
+                const int64_t si = s1[x - 1] + psd, sf = s2[x - 1] + psd;                \
+                for (int v = 0; v < nb; ++v)                                             \
+                    vout[(sf - 1) * nb + v] += (T)xme * vin[(si - 1) * nb + v];          \
+            }                                                                            \
+        }                                                                                \
+    } else if (op == BSG_OP_PP) {                                                        \
+        const int64_t *s1 = hc == 'b' ? t->p2b_fsd : t->p2b_isd;                         \
+        const int64_t *s2 = hc == 'b' ? t->p2b_isd : t->p2b_fsd;                         \
+        for (int64_t x = px0; x <= px1; ++x) {                                           \
+            float xme = t->hmatpp[t->p2b_op[x - 1] - 1];                                 \
+            xme = xme * (float)t->p2b_phase[x - 1];                                      \
+            const int64_t psdi = s1[x - 1], psdf = s2[x - 1];                            \
+            for (int64_t csd = nx0; csd <= nx1; csd += cs) {                             \
+                const int64_t nsd = t->nstart[csd - 1];                                  \
+                const int64_t sf = psdf + nsd, si = psdi + nsd;                          \
+                for (int v = 0; v < nb; ++v)                                             \
+                    vout[(sf - 1) * nb + v] += (T)xme * vin[(si - 1) * nb + v];          \
+            }                                                                            \
+        }                                                                                \
+    } else if (op == BSG_OP_PN) {                                                        \
+        for (int64_t pj = px0; pj <= px1; ++pj) {                                        \
+            const int64_t psdi = t->p1b_isd[pj - 1], psdf = t->p1b_fsd[pj - 1];          \
+            const int phasep = t->p1b_phase[pj - 1];                                     \
+            const int a = t->p1b_cop[pj - 1], c = t->p1b_dop[pj - 1];                    \
+            for (int64_t nj = nx0; nj <= nx1; ++nj) {                                    \
+                const int b = t->n1b_cop[nj - 1], d = t->n1b_dop[nj - 1];                \
+                const int phasen = t->n1b_phase[nj - 1];                                 \
+                float xme = t->hmatpn[CPN(t, b, a) + DPN(t, d, c) - 1];                  \
+                xme = xme * (float)phasep * (float)phasen;                               \
+                const int64_t sf = t->n1b_fsd[nj - 1] + psdf;                            \
+                const int64_t si = t->n1b_isd[nj - 1] + psdi;                            \
+                if (hc != 'b') {                                                         \
+                    for (int v = 0; v < nb; ++v)                                         \
+                        vout[(sf - 1) * nb + v] += (T)xme * vin[(si - 1) * nb + v];      \
+                } else {                                                                 \
+                    for (int v = 0; v < nb; ++v)                                         \
+                        vout[(si - 1) * nb + v] += (T)xme * vin[(sf - 1) * nb + v];      \
+                }                                                                        \
+            }                                                                            \
+        }                                                                                \
+    }                                                                                    \
+}
+
+DEFINE_BUNDLE(float, bundle_f32)
+DEFINE_BUNDLE(double, bundle_f64)
+
+/* vout += H vin over all opbundles, in table order (one thread) */
+int oracle_applyh(const bsg_tables *t, const void *vin, void *vout, int nb, int prec) {
+    if (!t || !vin || !vout || nb < 1) return BSG_ERR_ARG;
+    for (int64_t ib = 0; ib < t->nbundles; ++ib) {
+        if (prec == BSG_PREC_FP32)
+            bundle_f32(t, ib, (const float *)vin, (float *)vout, nb);
+        else
+            bundle_f64(t, ib, (const double *)vin, (double *)vout, nb);
+    }
+    return BSG_OK;
+}
+
+/* ----------------------------------------------------------- OpenMP ---- */
+/* chunk boundaries of [lo, hi] (1-based, inclusive) into at most nthr pieces,
+ * each cut moved forward until key[] changes (src/bsortjumpslib.f90:491-713
+ * makes the same kind of cut for startp_thread / startn_thread) */
+static int cut_ranges(int64_t lo, int64_t hi, const int64_t *key, int nthr, int64_t *starts) {
+    const int64_t n = hi - lo + 1;
+    int k = 0;
+    starts[k++] = lo;
+    for (int th = 1; th < nthr; ++th) {
+        int64_t c = lo + (n * th) / nthr;
+        if (c <= starts[k - 1]) continue;
+        while (c <= hi && key[c - 1] == key[c - 2]) ++c;
+        if (c > hi) break;
+        if (c > starts[k - 1]) starts[k++] = c;
+    }
+    starts[k] = hi + 1;
+    return k;
+}
+
+#define DEFINE_OMP(T, NAME)                                                              \
+static void NAME(const bsg_tables *t, const T *vin, T *vout, int nb, int nthr,           \
+                 int64_t *cuts) {                                                        \
+    for (int64_t ib = 0; ib < t->nbundles; ++ib) {                                       \
+        const int op = t->optype[ib];                                                    \
+        const int hc = t->hchar[ib];                                                     \
+        const int64_t px0 = t->pxstart[ib], px1 = t->pxend[ib];                          \
+        const int64_t nx0 = t->nxstart[ib], nx1 = t->nxend[ib];                          \
+        const int64_t cs = t->cstride[ib] > 0 ? t->cstride[ib] : 1;                      \
+        if (op == BSG_OP_PP) {                                                           \
+            const int64_t *s1 = hc == 'b' ? t->p2b_fsd : t->p2b_isd;                     \
+            const int64_t *s2 = hc == 'b' ? t->p2b_isd : t->p2b_fsd;                     \
+            const int64_t nc = (nx1 + cs - nx0) / cs;                                    \
+            _Pragma("omp parallel num_threads(nthr)")                                    \
+            {                                                                            \
+                int me = 0, nt = 1;                                                      \
+                OMP_IDS(me, nt);                                                         \
+                const int64_t chunk = (nc + nt - 1) / nt;                                \
+                const int64_t i0 = (int64_t)me * chunk, i1 = i0 + chunk < nc ? i0 + chunk : nc; \
+                for (int64_t x = px0; x <= px1; ++x) {                                   \
+                    float xme = t->hmatpp[t->p2b_op[x - 1] - 1];                         \
+                    xme = xme * (float)t->p2b_phase[x - 1];                              \
+                    const int64_t psdi = s1[x - 1], psdf = s2[x - 1];                    \
+                    for (int64_t ic = i0; ic < i1; ++ic) {                               \
+                        const int64_t nsd = t->nstart[nx0 + ic * cs - 1];                \
+                        const int64_t sf = psdf + nsd, si = psdi + nsd;                  \
+                        for (int v = 0; v < nb; ++v)                                     \
+                            vout[(sf - 1) * nb + v] += (T)xme * vin[(si - 1) * nb + v];  \
+                    }                                                                    \
+                }                                                                        \
+            }                                                                            \
+        } else if (op == BSG_OP_NN) {                                                    \
+            const int64_t *s1 = hc == 'b' ? t->n2b_fsd : t->n2b_isd;                     \
+            const int64_t *s2 = hc == 'b' ? t->n2b_isd : t->n2b_fsd;                     \
+            const int64_t nc = (px1 + cs - px0) / cs;                                    \
+            _Pragma("omp parallel for schedule(static) num_threads(nthr)")               \
+            for (int64_t ic = 0; ic < nc; ++ic) {                                        \
+                const int64_t psd = t->pstart[px0 + ic * cs - 1];                        \
+                for (int64_t x = nx0; x <= nx1; ++x) {                                   \
+                    float xme = t->hmatnn[t->n2b_op[x - 1] - 1];                         \
+                    xme = xme * (float)t->n2b_phase[x - 1];                              \
+                    const int64_t si = s1[x - 1] + psd, sf = s2[x - 1] + psd;            \
+                    for (int v = 0; v < nb; ++v)                                         \
+                        vout[(sf - 1) * nb + v] += (T)xme * vin[(si - 1) * nb + v];      \
+                }                                                                        \
+            }                                                                            \
+        } else if (op == BSG_OP_PN && hc != 'b') {                                       \
+            const int k = cut_ranges(px0, px1, t->p1b_fsd, nthr, cuts);                  \
+            _Pragma("omp parallel for schedule(dynamic,1) num_threads(nthr)")            \
+            for (int th = 0; th < k; ++th) {                                             \
+                for (int64_t pj = cuts[th]; pj < cuts[th + 1]; ++pj) {                   \
+                    const int64_t psdi = t->p1b_isd[pj - 1], psdf = t->p1b_fsd[pj - 1];  \
+                    const int phasep = t->p1b_phase[pj - 1];                             \
+                    const int a = t->p1b_cop[pj - 1], c = t->p1b_dop[pj - 1];            \
+                    for (int64_t nj = nx0; nj <= nx1; ++nj) {                            \
+                        const int b = t->n1b_cop[nj - 1], d = t->n1b_dop[nj - 1];        \
+                        float xme = t->hmatpn[CPN(t, b, a) + DPN(t, d, c) - 1];          \
+                        xme = xme * (float)phasep * (float)t->n1b_phase[nj - 1];         \
+                        const int64_t sf = t->n1b_fsd[nj - 1] + psdf;                    \
+                        const int64_t si = t->n1b_isd[nj - 1] + psdi;                    \
+                        for (int v = 0; v < nb; ++v)                                     \
+                            vout[(sf - 1) * nb + v] += (T)xme * vin[(si - 1) * nb + v];  \
+                    }                                                                    \
+                }                                                                        \
+            }                                                                            \
+        } else if (op == BSG_OP_PN) {                                                    \
+            const int k = cut_ranges(nx0, nx1, t->n1b_isd, nthr, cuts);                  \
+            _Pragma("omp parallel for schedule(dynamic,1) num_threads(nthr)")            \
+            for (int th = 0; th < k; ++th) {                                             \
+                for (int64_t nj = cuts[th]; nj < cuts[th + 1]; ++nj) {                   \
+                    const int64_t nsdi = t->n1b_isd[nj - 1], nsdf = t->n1b_fsd[nj - 1];  \
+                    const int b = t->n1b_cop[nj - 1], d = t->n1b_dop[nj - 1];            \
+                    const int phasen = t->n1b_phase[nj - 1];                             \
+                    for (int64_t pj = px0; pj <= px1; ++pj) {                            \
+                        const int a = t->p1b_cop[pj - 1], c = t->p1b_dop[pj - 1];        \
+                        float xme = t->hmatpn[CPN(t, b, a) + DPN(t, d, c) - 1];          \
+                        xme = xme * (float)t->p1b_phase[pj - 1] * (float)phasen;         \
+                        const int64_t si = nsdi + t->p1b_isd[pj - 1];                    \
+                        const int64_t sf = nsdf + t->p1b_fsd[pj - 1];                    \
+                        for (int v = 0; v < nb; ++v)                                     \
+                            vout[(si - 1) * nb + v] += (T)xme * vin[(sf - 1) * nb + v];  \
+                    }                                                                    \
+                }                                                                        \
+            }                                                                            \
+        } else if (op == BSG_OP_SPE) {                                                   \
+            const int64_t np_ = px1 - px0 + 1;                                           \
+            _Pragma("omp parallel for schedule(static) num_threads(nthr)")               \
+            for (int64_t k2 = 0; k2 < np_; ++k2) {                                       \
+                const int64_t ip = px0 + k2;                                             \
+                const float pspe = t->pspe_h[ip - 1];                                    \
+                int64_t statef = t->pstart[ip - 1] + t->nstart[nx0 - 1];                 \
+                for (int64_t in = nx0; in <= nx1; ++in) {                                \
+                    const float e = pspe + t->nspe_h[in - 1];                            \
+                    for (int v = 0; v < nb; ++v)                                         \
+                        vout[(statef - 1) * nb + v] += vin[(statef - 1) * nb + v] * (T)e; \
+                    ++statef;                                                            \
+                }                                                                        \
+            }                                                                            \
+        }                                                                                \
+    }                                                                                    \
+}
+
+#ifdef _OPENMP
+#define OMP_IDS(me, nt) do { me = omp_get_thread_num(); nt = omp_get_num_threads(); } while (0)
+#else
+#define OMP_IDS(me, nt) do { me = 0; nt = 1; } while (0)
+#endif
+
+DEFINE_OMP(float, omp_f32)
+DEFINE_OMP(double, omp_f64)
+
+/* vout += H vin with nthreads OpenMP threads (the CPU baseline) */
+int oracle_applyh_omp(const bsg_tables *t, const void *vin, void *vout, int nb, int prec, int nthreads) {
+    if (!t || !vin || !vout || nb < 1) return BSG_ERR_ARG;
+    if (nthreads < 1) nthreads = 1;
+    int64_t *cuts = (int64_t *)malloc(sizeof(int64_t) * (size_t)(nthreads + 2));
+    if (!cuts) return BSG_ERR_NOMEM;
+    if (prec == BSG_PREC_FP32)
+        omp_f32(t, (const float *)vin, (float *)vout, nb, nthreads, cuts);
+    else
+        omp_f64(t, (const double *)vin, (double *)vout, nb, nthreads, cuts);
+    free(cuts);
+    return BSG_OK;
+}
+
+/* number of inner-loop updates one applyH executes (the N_ops of the
+ * algorithmic-bytes model) split by optype */
+void oracle_count_ops(const bsg_tables *t, int64_t *ops /* [4]: spe, pp, nn, pn */) {
+    ops[0] = ops[1] = ops[2] = ops[3] = 0;
+    for (int64_t ib = 0; ib < t->nbundles; ++ib) {
+        const int64_t cs = t->cstride[ib] > 0 ? t->cstride[ib] : 1;
+        const int64_t np_ = t->pxend[ib] - t->pxstart[ib] + 1;
+        const int64_t nn_ = t->nxend[ib] - t->nxstart[ib] + 1;
+        switch (t->optype[ib]) {
+        case BSG_OP_SPE: ops[0] += np_ * nn_; break;
+        case BSG_OP_PP: ops[1] += np_ * ((nn_ + cs - 1) / cs); break;
+        case BSG_OP_NN: ops[2] += ((np_ + cs - 1) / cs) * nn_; break;
+        case BSG_OP_PN: ops[3] += np_ * nn_; break;
+        }
+    }
+}
