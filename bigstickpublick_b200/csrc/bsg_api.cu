@@ -1,0 +1,658 @@
+// C ABI entry points: create / destroy / applyH / stats / errors, the
+// host-side table validator and the derivation of the row layouts.
+//
+// bsg_create receives the reference's module arrays (bsg.h), validates every
+// index before anything touches the GPU (the reference's own checks are
+// check_opbundle_bounds, src/bparallel_opbundles.f90:1232-1286, and the
+// sortedness check of src/bsortjumpslib.f90:228-241), uploads the arrays
+// unchanged, and derives the output-stationary row layout in separate
+// buffers.  It replaces getLoadDist / set_bundledXY_threadstart
+// (src/bapplyhlibOMP.f90:34-868, src/bsortjumpslib.f90:491-713): instead of
+// per-thread output ranges, each output row gets the list of contributions
+// that land in it.
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <numeric>
+#include <unordered_map>
+
+#include "bsg_internal.h"
+
+namespace bsg {
+
+int set_err(bsg_ctx *ctx, int code, const std::string &msg) {
+    if (ctx) ctx->last_error = msg;
+    return code;
+}
+
+int cuda_check(bsg_ctx *ctx, cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return BSG_OK;
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        return set_err(ctx, BSG_ERR_NOMEM, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+    return set_err(ctx, BSG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int dev_alloc(bsg_ctx *ctx, DevBuf &b, size_t bytes) {
+    dev_free(b);
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) {
+        b.p = nullptr;
+        return cuda_check(ctx, e, "cudaMalloc");
+    }
+    b.bytes = bytes;
+    return BSG_OK;
+}
+
+void dev_free(DevBuf &b) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+int upload(bsg_ctx *ctx, DevBuf &b, const void *src, size_t bytes) {
+    int st = dev_alloc(ctx, b, bytes);
+    if (st) return st;
+    if (bytes && src) return cuda_check(ctx, cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice), "upload");
+    return BSG_OK;
+}
+
+const TileSet *get_tiles(bsg_ctx *ctx, int tp) {
+    auto it = ctx->tiles.find(tp);
+    if (it != ctx->tiles.end()) return &it->second;
+    // tiles of tp positions, heaviest rows first (longest-processing-time order)
+    std::vector<int32_t> order(ctx->nrows);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int32_t x, int32_t y) { return ctx->h_work[x] > ctx->h_work[y]; });
+    std::vector<Tile> tiles;
+    for (int32_t r : order)
+        for (int32_t p0 = 0; p0 < ctx->h_rowlen[r]; p0 += tp) {
+            Tile t;
+            t.row = r;
+            t.pos0 = p0;
+            t.npos = std::min(tp, ctx->h_rowlen[r] - p0);
+            t.pad = 0;
+            tiles.push_back(t);
+        }
+    TileSet ts;
+    if (upload(ctx, ts.buf, tiles.data(), tiles.size() * sizeof(Tile))) return nullptr;
+    ts.ntiles = (int32_t)tiles.size();
+    auto res = ctx->tiles.emplace(tp, ts);
+    return &res.first->second;
+}
+
+}  // namespace bsg
+
+using namespace bsg;
+
+namespace {
+
+struct Validator {
+    bsg_ctx *ctx;
+    std::string msg;
+    int fail(const std::string &m) {
+        msg = m;
+        return BSG_ERR_BAD_TABLE;
+    }
+};
+
+template <typename T>
+bool nonnull(const T *p, int64_t n) { return n == 0 || p != nullptr; }
+
+// CSR by output position, stable (table order inside a position)
+template <typename Rec>
+void csr_by_out(const std::vector<int32_t> &out, const std::vector<Rec> &recs, int32_t nout,
+                std::vector<int32_t> &ptr, std::vector<Rec> &sorted) {
+    ptr.assign(nout + 1, 0);
+    for (int32_t o : out) ptr[o + 1]++;
+    for (int32_t i = 0; i < nout; ++i) ptr[i + 1] += ptr[i];
+    std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
+    sorted.resize(recs.size());
+    for (size_t k = 0; k < recs.size(); ++k) sorted[fill[out[k]]++] = recs[k];
+}
+
+int derive(bsg_ctx *ctx, const bsg_tables *t) {
+    Validator V{ctx, ""};
+    // ---- basic presence and sizes
+    if (t->dimbasis <= 0 || t->nsd_p <= 0 || t->nsd_n <= 0)
+        return set_err(ctx, BSG_ERR_BAD_TABLE, "empty basis");
+    if (!t->pstart || !t->nstart) return set_err(ctx, BSG_ERR_BAD_TABLE, "pstart/nstart missing");
+    if (!nonnull(t->p1b_isd, t->np1b) || !nonnull(t->p1b_fsd, t->np1b) || !nonnull(t->p1b_cop, t->np1b) ||
+        !nonnull(t->p1b_dop, t->np1b) || !nonnull(t->p1b_phase, t->np1b) || !nonnull(t->n1b_isd, t->nn1b) ||
+        !nonnull(t->n1b_fsd, t->nn1b) || !nonnull(t->n1b_cop, t->nn1b) || !nonnull(t->n1b_dop, t->nn1b) ||
+        !nonnull(t->n1b_phase, t->nn1b) || !nonnull(t->p2b_isd, t->np2b) || !nonnull(t->p2b_fsd, t->np2b) ||
+        !nonnull(t->p2b_op, t->np2b) || !nonnull(t->p2b_phase, t->np2b) || !nonnull(t->n2b_isd, t->nn2b) ||
+        !nonnull(t->n2b_fsd, t->nn2b) || !nonnull(t->n2b_op, t->nn2b) || !nonnull(t->n2b_phase, t->nn2b) ||
+        !nonnull(t->hmatpp, t->nmatpp) || !nonnull(t->hmatnn, t->nmatnn) || !nonnull(t->hmatpn, t->nmatpn))
+        return set_err(ctx, BSG_ERR_BAD_TABLE, "a table with nonzero length has a null pointer");
+    if (t->nbundles < 0 || (t->nbundles > 0 && (!t->optype || !t->hchar || !t->pxstart || !t->pxend ||
+                                                 !t->nxstart || !t->nxend || !t->cstride)))
+        return set_err(ctx, BSG_ERR_BAD_TABLE, "opbundle arrays missing");
+    if (t->dimbasis > (int64_t)INT32_MAX * 8 || t->nsd_p > INT32_MAX || t->nmatpn >= INT32_MAX)
+        return set_err(ctx, BSG_ERR_UNSUPPORTED, "table sizes beyond this build's index widths");
+
+    // ---- rows (proton SDs): pstart strictly increasing, row lengths
+    const int64_t nrows = t->nsd_p;
+    ctx->nrows = nrows;
+    ctx->h_rowlen.assign(nrows, 0);
+    if (t->pstart[0] != 0) return set_err(ctx, BSG_ERR_BAD_TABLE, "pstart(1) must be 0");
+    for (int64_t p = 0; p < nrows; ++p) {
+        const int64_t end = (p + 1 < nrows) ? t->pstart[p + 1] : t->dimbasis;
+        const int64_t len = end - t->pstart[p];
+        if (len <= 0 || len > INT32_MAX / 2)
+            return set_err(ctx, BSG_ERR_BAD_TABLE, "pstart not strictly increasing at proton SD " + std::to_string(p + 1));
+        ctx->h_rowlen[p] = (int32_t)len;
+    }
+    ctx->max_rowlen = *std::max_element(ctx->h_rowlen.begin(), ctx->h_rowlen.end());
+    for (int64_t n = 0; n < t->nsd_n; ++n)
+        if (t->nstart[n] < 1 || t->nstart[n] > ctx->max_rowlen)
+            return set_err(ctx, BSG_ERR_OOB_INDEX, "nstart out of range at neutron SD " + std::to_string(n + 1));
+    std::unordered_map<int64_t, int32_t> row_of;
+    row_of.reserve(nrows * 2);
+    for (int64_t p = 0; p < nrows; ++p) row_of[t->pstart[p]] = (int32_t)p;
+    auto rowof = [&](int64_t pst, int32_t &r) -> bool {
+        auto it = row_of.find(pst);
+        if (it == row_of.end()) return false;
+        r = it->second;
+        return true;
+    };
+
+    const int nl_n = t->nhsps_nl, nr_n = t->nhsps_nr, nl_p = t->nhsps_pl, nr_p = t->nhsps_pr;
+    if (nl_n < 0 || nr_n < 0 || nl_p < 0 || nr_p < 0 || nl_n + nr_n > 250)
+        return set_err(ctx, BSG_ERR_BAD_TABLE, "bad nhsps bounds");
+    const int32_t ld = nl_n + nr_n + 1;
+    const int64_t ncpn = (int64_t)ld * (nl_p + nr_p + 1);
+    if (t->nmatpn > 0 && (!t->cpnpair || !t->dpnpair)) return set_err(ctx, BSG_ERR_BAD_TABLE, "cpnpair/dpnpair missing");
+    std::vector<int32_t> cpn32(ncpn, 0), dpn32(ncpn, 0);
+    if (t->cpnpair)
+        for (int64_t i = 0; i < ncpn; ++i) {
+            if (t->cpnpair[i] < 0 || t->cpnpair[i] > t->nmatpn || t->dpnpair[i] < 0 || t->dpnpair[i] > t->nmatpn)
+                return set_err(ctx, BSG_ERR_OOB_INDEX, "cpnpair/dpnpair entry outside hmatpn");
+            cpn32[i] = (int32_t)t->cpnpair[i];
+            dpn32[i] = (int32_t)t->dpnpair[i];
+        }
+
+    // ---- neutron operators
+    struct NKey {
+        int kind, dir;
+        int64_t x0, x1;
+        bool operator<(const NKey &o) const {
+            return std::tie(kind, dir, x0, x1) < std::tie(o.kind, o.dir, o.x0, o.x1);
+        }
+    };
+    std::map<NKey, int32_t> nop_id;
+    std::vector<NOp> nops;
+    std::vector<int32_t> nop_maxin;
+    std::vector<int32_t> nptr_all;
+    std::vector<PNRec> pnrec_all;
+    std::vector<NNRec> nnrec_all;
+    std::vector<int32_t> nnrec_op_all;
+    auto get_nop = [&](int kind, int dir, int64_t x0, int64_t x1, int32_t &id) -> int {
+        NKey k{kind, dir, x0, x1};
+        auto it = nop_id.find(k);
+        if (it != nop_id.end()) { id = it->second; return BSG_OK; }
+        const int64_t n = x1 - x0 + 1;
+        std::vector<int32_t> out(n);
+        int32_t maxin = -1, maxout = -1;
+        NOp op{};
+        op.kind = kind;
+        if (kind == 1) {
+            std::vector<PNRec> recs(n);
+            for (int64_t x = x0; x <= x1; ++x) {
+                const int64_t isd = t->n1b_isd[x - 1], fsd = t->n1b_fsd[x - 1];
+                const int b = t->n1b_cop[x - 1], d = t->n1b_dop[x - 1];
+                if (isd < 1 || fsd < 1 || isd > ctx->max_rowlen || fsd > ctx->max_rowlen)
+                    return V.fail("n1b isd/fsd out of range at jump " + std::to_string(x));
+                if (b < -nl_n || b > nr_n || d < -nl_n || d > nr_n || b == 0 || d == 0)
+                    return V.fail("n1b_cop/dop outside the neutron half spaces at jump " + std::to_string(x));
+                const int ph = t->n1b_phase[x - 1];
+                if (ph != 1 && ph != -1) return V.fail("n1b_phase not +-1");
+                PNRec r;
+                r.in = (int32_t)((dir == 0 ? isd : fsd) - 1);
+                out[x - x0] = (int32_t)((dir == 0 ? fsd : isd) - 1);
+                r.b = (uint8_t)(b + nl_n);
+                r.d = (uint8_t)(d + nl_n);
+                r.ph = (int8_t)ph;
+                r.pad = 0;
+                recs[x - x0] = r;
+                maxin = std::max(maxin, r.in);
+                maxout = std::max(maxout, out[x - x0]);
+            }
+            std::vector<int32_t> ptr;
+            std::vector<PNRec> sorted;
+            csr_by_out(out, recs, maxout + 1, ptr, sorted);
+            op.rec_base = (int64_t)pnrec_all.size();
+            op.ptr_base = (int64_t)nptr_all.size();
+            op.nout = maxout + 1;
+            pnrec_all.insert(pnrec_all.end(), sorted.begin(), sorted.end());
+            nptr_all.insert(nptr_all.end(), ptr.begin(), ptr.end());
+        } else {
+            std::vector<NNRec> recs(n);
+            std::vector<int32_t> ops(n);
+            for (int64_t x = x0; x <= x1; ++x) {
+                const int64_t isd = t->n2b_isd[x - 1], fsd = t->n2b_fsd[x - 1];
+                if (isd < 1 || fsd < 1 || isd > ctx->max_rowlen || fsd > ctx->max_rowlen)
+                    return V.fail("n2b isd/fsd out of range at jump " + std::to_string(x));
+                const int32_t opl = t->n2b_op[x - 1];
+                if (opl < 1 || opl > t->nmatnn) return V.fail("n2b_op outside hmatnn at jump " + std::to_string(x));
+                const int ph = t->n2b_phase[x - 1];
+                if (ph != 1 && ph != -1) return V.fail("n2b_phase not +-1");
+                NNRec r;
+                r.in = (int32_t)((dir == 0 ? isd : fsd) - 1);
+                out[x - x0] = (int32_t)((dir == 0 ? fsd : isd) - 1);
+                float xme = t->hmatnn[opl - 1];
+                xme = xme * (float)ph;
+                r.me = xme;
+                recs[x - x0] = r;
+                ops[x - x0] = opl;
+                maxin = std::max(maxin, r.in);
+                maxout = std::max(maxout, out[x - x0]);
+            }
+            std::vector<int32_t> ptr;
+            std::vector<NNRec> sorted;
+            csr_by_out(out, recs, maxout + 1, ptr, sorted);
+            std::vector<int32_t> sorted_ops;
+            csr_by_out(out, ops, maxout + 1, ptr, sorted_ops);
+            op.rec_base = (int64_t)nnrec_all.size();
+            op.ptr_base = (int64_t)nptr_all.size();
+            op.nout = maxout + 1;
+            nnrec_all.insert(nnrec_all.end(), sorted.begin(), sorted.end());
+            nnrec_op_all.insert(nnrec_op_all.end(), sorted_ops.begin(), sorted_ops.end());
+            nptr_all.insert(nptr_all.end(), ptr.begin(), ptr.end());
+        }
+        id = (int32_t)nops.size();
+        nops.push_back(op);
+        nop_maxin.push_back(maxin);
+        nop_id[k] = id;
+        return BSG_OK;
+    };
+
+    // ---- contributions per row
+    std::vector<std::pair<int32_t, PPContrib>> pp;
+    std::vector<int32_t> pp_op_tmp;
+    std::vector<std::pair<int32_t, NNContrib>> nn;
+    std::vector<std::pair<int32_t, PNContrib>> pn;
+    std::vector<std::pair<int32_t, SPEContrib>> spe;
+    int64_t ops[4] = {0, 0, 0, 0};
+    for (int64_t ib = 0; ib < t->nbundles; ++ib) {
+        const int op = t->optype[ib], hc = t->hchar[ib];
+        const int64_t px0 = t->pxstart[ib], px1 = t->pxend[ib], nx0 = t->nxstart[ib], nx1 = t->nxend[ib];
+        const int64_t cs = t->cstride[ib];
+        const std::string where = " (opbundle " + std::to_string(ib + 1) + ")";
+        if (hc != 'f' && hc != 'b' && hc != 'h') return set_err(ctx, BSG_ERR_BAD_TABLE, "bad hchar" + where);
+        if (cs < 1) return set_err(ctx, BSG_ERR_BAD_TABLE, "cstride < 1" + where);
+        if (px1 < px0 || nx1 < nx0) continue;  // empty bundle: no work
+        const bool bwd = (hc == 'b');
+        if (op == BSG_OP_PP) {
+            if (px0 < 1 || px1 > t->np2b || nx0 < 1 || nx1 > t->nsd_n)
+                return set_err(ctx, BSG_ERR_OOB_INDEX, "PP range" + where);
+            if (cs != 1) return set_err(ctx, BSG_ERR_UNSUPPORTED, "PP cstride != 1" + where);
+            for (int64_t c = nx0 + 1; c <= nx1; ++c)
+                if (t->nstart[c - 1] != t->nstart[c - 2] + 1)
+                    return set_err(ctx, BSG_ERR_UNSUPPORTED, "PP neutron run not contiguous" + where);
+            const int32_t lo = (int32_t)(t->nstart[nx0 - 1] - 1), hi = (int32_t)(t->nstart[nx1 - 1] - 1);
+            for (int64_t x = px0; x <= px1; ++x) {
+                int32_t ri, rf;
+                const int64_t s1 = bwd ? t->p2b_fsd[x - 1] : t->p2b_isd[x - 1];
+                const int64_t s2 = bwd ? t->p2b_isd[x - 1] : t->p2b_fsd[x - 1];
+                if (!rowof(s1, ri) || !rowof(s2, rf))
+                    return set_err(ctx, BSG_ERR_OOB_INDEX, "p2b isd/fsd is not a pstart value" + where);
+                if (hi >= ctx->h_rowlen[ri] || hi >= ctx->h_rowlen[rf])
+                    return set_err(ctx, BSG_ERR_OOB_INDEX, "PP neutron run longer than the row" + where);
+                const int32_t opl = t->p2b_op[x - 1];
+                if (opl < 1 || opl > t->nmatpp) return set_err(ctx, BSG_ERR_OOB_INDEX, "p2b_op outside hmatpp" + where);
+                const int ph = t->p2b_phase[x - 1];
+                if (ph != 1 && ph != -1) return set_err(ctx, BSG_ERR_BAD_TABLE, "p2b_phase not +-1" + where);
+                PPContrib c{};
+                c.q_off = s1;
+                float xme = t->hmatpp[opl - 1];
+                xme = xme * (float)ph;
+                c.me = xme;
+                c.lo = lo;
+                c.hi = hi;
+                pp.push_back({rf, c});
+                pp_op_tmp.push_back(opl);
+            }
+            ops[1] += (px1 - px0 + 1) * (nx1 - nx0 + 1);
+        } else if (op == BSG_OP_NN) {
+            if (px0 < 1 || px1 > t->nsd_p || nx0 < 1 || nx1 > t->nn2b)
+                return set_err(ctx, BSG_ERR_OOB_INDEX, "NN range" + where);
+            int32_t id;
+            int st = get_nop(0, bwd ? 1 : 0, nx0, nx1, id);
+            if (st) return set_err(ctx, st, V.msg + where);
+            int64_t nrow_b = 0;
+            for (int64_t csd = px0; csd <= px1; csd += cs) {
+                const int32_t r = (int32_t)(csd - 1);
+                if (nops[id].nout > ctx->h_rowlen[r] || nop_maxin[id] >= ctx->h_rowlen[r])
+                    return set_err(ctx, BSG_ERR_OOB_INDEX, "NN jump outside the row" + where);
+                NNContrib c{id};
+                nn.push_back({r, c});
+                ++nrow_b;
+            }
+            ops[2] += nrow_b * (nx1 - nx0 + 1);
+        } else if (op == BSG_OP_PN) {
+            if (px0 < 1 || px1 > t->np1b || nx0 < 1 || nx1 > t->nn1b)
+                return set_err(ctx, BSG_ERR_OOB_INDEX, "PN range" + where);
+            int32_t id;
+            int st = get_nop(1, bwd ? 1 : 0, nx0, nx1, id);
+            if (st) return set_err(ctx, st, V.msg + where);
+            // every (a,c) x (b,d) combination of the bundle must address hmatpn
+            std::vector<std::pair<int, int>> ac, bd;
+            {
+                std::vector<char> seen((size_t)(nl_p + nr_p + 1) * (nl_p + nr_p + 1), 0);
+                for (int64_t x = px0; x <= px1; ++x) {
+                    const int a = t->p1b_cop[x - 1], c = t->p1b_dop[x - 1];
+                    if (a < -nl_p || a > nr_p || c < -nl_p || c > nr_p || a == 0 || c == 0)
+                        return set_err(ctx, BSG_ERR_OOB_INDEX, "p1b_cop/dop outside the proton half spaces" + where);
+                    char &s = seen[(size_t)(a + nl_p) * (nl_p + nr_p + 1) + (c + nl_p)];
+                    if (!s) { s = 1; ac.push_back({a, c}); }
+                }
+                std::vector<char> seen2((size_t)ld * ld, 0);
+                for (int64_t x = nx0; x <= nx1; ++x) {
+                    const int b = t->n1b_cop[x - 1], d = t->n1b_dop[x - 1];
+                    char &s = seen2[(size_t)(b + nl_n) * ld + (d + nl_n)];
+                    if (!s) { s = 1; bd.push_back({b, d}); }
+                }
+                for (auto &p1 : ac)
+                    for (auto &p2 : bd) {
+                        const int64_t i1 = (int64_t)(p2.first + nl_n) + (int64_t)(p1.first + nl_p) * ld;
+                        const int64_t i2 = (int64_t)(p2.second + nl_n) + (int64_t)(p1.second + nl_p) * ld;
+                        const int64_t idx = t->cpnpair[i1] + t->dpnpair[i2];
+                        if (idx < 1 || idx > t->nmatpn)
+                            return set_err(ctx, BSG_ERR_OOB_INDEX, "cpnpair+dpnpair outside hmatpn" + where);
+                    }
+            }
+            for (int64_t x = px0; x <= px1; ++x) {
+                int32_t ri, rf;
+                const int64_t s1 = bwd ? t->p1b_fsd[x - 1] : t->p1b_isd[x - 1];
+                const int64_t s2 = bwd ? t->p1b_isd[x - 1] : t->p1b_fsd[x - 1];
+                if (!rowof(s1, ri) || !rowof(s2, rf))
+                    return set_err(ctx, BSG_ERR_OOB_INDEX, "p1b isd/fsd is not a pstart value" + where);
+                if (nops[id].nout > ctx->h_rowlen[rf] || nop_maxin[id] >= ctx->h_rowlen[ri])
+                    return set_err(ctx, BSG_ERR_OOB_INDEX, "PN neutron jump outside the row" + where);
+                const int ph = t->p1b_phase[x - 1];
+                if (ph != 1 && ph != -1) return set_err(ctx, BSG_ERR_BAD_TABLE, "p1b_phase not +-1" + where);
+                PNContrib c{};
+                c.q_off = s1;
+                c.nop = id;
+                c.acol = (int16_t)(t->p1b_cop[x - 1] + nl_p);
+                c.ccol = (int16_t)(t->p1b_dop[x - 1] + nl_p);
+                c.php = (float)ph;
+                pn.push_back({rf, c});
+            }
+            ops[3] += (px1 - px0 + 1) * (nx1 - nx0 + 1);
+        } else if (op == BSG_OP_SPE) {
+            if (!t->call_spe || !t->pspe_h || !t->nspe_h)
+                return set_err(ctx, BSG_ERR_BAD_TABLE, "SPE bundle without pspe_h/nspe_h" + where);
+            if (px0 < 1 || px1 > t->nsd_p || nx0 < 1 || nx1 > t->nsd_n)
+                return set_err(ctx, BSG_ERR_OOB_INDEX, "SPE range" + where);
+            for (int64_t ip = px0; ip <= px1; ++ip) {
+                SPEContrib c{};
+                c.pspe = t->pspe_h[ip - 1];
+                c.lo = (int32_t)(t->nstart[nx0 - 1] - 1);
+                c.hi = c.lo + (int32_t)(nx1 - nx0);
+                c.n0 = (int32_t)(nx0 - 1);
+                if (c.hi >= ctx->h_rowlen[ip - 1])
+                    return set_err(ctx, BSG_ERR_OOB_INDEX, "SPE run longer than the row" + where);
+                spe.push_back({(int32_t)(ip - 1), c});
+            }
+            ops[0] += (px1 - px0 + 1) * (nx1 - nx0 + 1);
+        } else {
+            return set_err(ctx, BSG_ERR_BAD_TABLE, "unknown optype" + where);
+        }
+    }
+    ctx->stats.n_ops_spe = ops[0];
+    ctx->stats.n_ops_pp = ops[1];
+    ctx->stats.n_ops_nn = ops[2];
+    ctx->stats.n_ops_pn = ops[3];
+
+    // ---- flatten into per-row CSR (stable: keeps bundle order inside a row;
+    // PN contributions grouped by neutron operator for cache reuse)
+    auto by_row = [&](auto &v, std::vector<int32_t> &ptr, auto &flat, std::vector<int32_t> *perm) {
+        std::vector<size_t> idx(v.size());
+        std::iota(idx.begin(), idx.end(), 0);
+        std::stable_sort(idx.begin(), idx.end(), [&](size_t x, size_t y) { return v[x].first < v[y].first; });
+        ptr.assign(nrows + 1, 0);
+        for (auto &e : v) ptr[e.first + 1]++;
+        for (int64_t r = 0; r < nrows; ++r) ptr[r + 1] += ptr[r];
+        flat.resize(v.size());
+        if (perm) perm->resize(v.size());
+        for (size_t k = 0; k < idx.size(); ++k) {
+            flat[k] = v[idx[k]].second;
+            if (perm) (*perm)[k] = (int32_t)idx[k];
+        }
+    };
+    std::stable_sort(pn.begin(), pn.end(), [](const std::pair<int32_t, PNContrib> &x, const std::pair<int32_t, PNContrib> &y) {
+        if (x.first != y.first) return x.first < y.first;
+        return x.second.nop < y.second.nop;
+    });
+    std::vector<int32_t> spe_ptr, pp_perm;
+    std::vector<SPEContrib> h_spe;
+    by_row(pp, ctx->h_pp_ptr, ctx->h_pp, &pp_perm);
+    ctx->h_pp_op.resize(pp_perm.size());
+    for (size_t k = 0; k < pp_perm.size(); ++k) ctx->h_pp_op[k] = pp_op_tmp[pp_perm[k]];
+    by_row(nn, ctx->h_nn_ptr, ctx->h_nn, nullptr);
+    by_row(pn, ctx->h_pn_ptr, ctx->h_pn, nullptr);
+    by_row(spe, spe_ptr, h_spe, nullptr);
+    ctx->h_nops = nops;
+    ctx->h_nnrec_op = nnrec_op_all;
+
+    // per-row work estimate (operations) for tile ordering
+    ctx->h_work.assign(nrows, 0);
+    for (int64_t r = 0; r < nrows; ++r) {
+        int64_t w = 0;
+        for (int32_t c = ctx->h_pp_ptr[r]; c < ctx->h_pp_ptr[r + 1]; ++c) w += ctx->h_pp[c].hi - ctx->h_pp[c].lo + 1;
+        for (int32_t c = ctx->h_nn_ptr[r]; c < ctx->h_nn_ptr[r + 1]; ++c) {
+            const NOp &o = nops[ctx->h_nn[c].nop];
+            w += nptr_all[o.ptr_base + o.nout];
+        }
+        for (int32_t c = ctx->h_pn_ptr[r]; c < ctx->h_pn_ptr[r + 1]; ++c) {
+            const NOp &o = nops[ctx->h_pn[c].nop];
+            w += nptr_all[o.ptr_base + o.nout];
+        }
+        ctx->h_work[r] = (int32_t)std::min<int64_t>(w, INT32_MAX);
+    }
+
+    // ---- upload: raw tables (unchanged) and derived layouts
+    auto up = [&](DevBuf &b, const void *src, size_t bytes) { return upload(ctx, b, src, bytes); };
+    int st = 0;
+    std::vector<int64_t> row_off(t->pstart, t->pstart + nrows);
+    const void *raw_ptrs[] = {t->pstart, t->nstart, t->p1b_isd, t->p1b_fsd, t->p1b_cop, t->p1b_dop, t->p1b_phase,
+                              t->n1b_isd, t->n1b_fsd, t->n1b_cop, t->n1b_dop, t->n1b_phase,
+                              t->p2b_isd, t->p2b_fsd, t->p2b_op, t->p2b_phase,
+                              t->n2b_isd, t->n2b_fsd, t->n2b_op, t->n2b_phase,
+                              t->hmatpp, t->hmatnn, t->cpnpair, t->dpnpair};
+    const size_t raw_bytes[] = {8 * (size_t)t->nsd_p, 8 * (size_t)t->nsd_n, 8 * (size_t)t->np1b, 8 * (size_t)t->np1b,
+                                2 * (size_t)t->np1b, 2 * (size_t)t->np1b, (size_t)t->np1b,
+                                8 * (size_t)t->nn1b, 8 * (size_t)t->nn1b, 2 * (size_t)t->nn1b, 2 * (size_t)t->nn1b, (size_t)t->nn1b,
+                                8 * (size_t)t->np2b, 8 * (size_t)t->np2b, 4 * (size_t)t->np2b, (size_t)t->np2b,
+                                8 * (size_t)t->nn2b, 8 * (size_t)t->nn2b, 4 * (size_t)t->nn2b, (size_t)t->nn2b,
+                                4 * (size_t)t->nmatpp, 4 * (size_t)t->nmatnn,
+                                t->cpnpair ? 8 * (size_t)ncpn : 0, t->dpnpair ? 8 * (size_t)ncpn : 0};
+    const int nraw = (int)(sizeof(raw_bytes) / sizeof(raw_bytes[0]));
+    ctx->raw.resize(nraw);
+    int64_t jb = 0;
+    for (int i = 0; i < nraw && !st; ++i) {
+        st = up(ctx->raw[i], raw_ptrs[i], raw_bytes[i]);
+        jb += (int64_t)raw_bytes[i];
+    }
+    if (st) return st;
+    ctx->stats.jump_bytes = jb;
+    // hmatpn doubles as raw table and kernel operand
+    if ((st = up(ctx->hmatpn, t->hmatpn, 4 * (size_t)t->nmatpn))) return st;
+    ctx->stats.jump_bytes += 4 * t->nmatpn;
+    std::vector<float> nspe(t->nsd_n, 0.0f);
+    if (t->call_spe && t->nspe_h) std::copy(t->nspe_h, t->nspe_h + t->nsd_n, nspe.begin());
+    if ((st = up(ctx->row_off, row_off.data(), 8 * row_off.size())) ||
+        (st = up(ctx->pp_ptr, ctx->h_pp_ptr.data(), 4 * ctx->h_pp_ptr.size())) ||
+        (st = up(ctx->nn_ptr, ctx->h_nn_ptr.data(), 4 * ctx->h_nn_ptr.size())) ||
+        (st = up(ctx->pn_ptr, ctx->h_pn_ptr.data(), 4 * ctx->h_pn_ptr.size())) ||
+        (st = up(ctx->spe_ptr, spe_ptr.data(), 4 * spe_ptr.size())) ||
+        (st = up(ctx->pp, ctx->h_pp.data(), sizeof(PPContrib) * ctx->h_pp.size())) ||
+        (st = up(ctx->nn, ctx->h_nn.data(), sizeof(NNContrib) * ctx->h_nn.size())) ||
+        (st = up(ctx->pn, ctx->h_pn.data(), sizeof(PNContrib) * ctx->h_pn.size())) ||
+        (st = up(ctx->spe, h_spe.data(), sizeof(SPEContrib) * h_spe.size())) ||
+        (st = up(ctx->nops, nops.data(), sizeof(NOp) * nops.size())) ||
+        (st = up(ctx->nptr, nptr_all.data(), 4 * nptr_all.size())) ||
+        (st = up(ctx->pnrec, pnrec_all.data(), sizeof(PNRec) * pnrec_all.size())) ||
+        (st = up(ctx->nnrec, nnrec_all.data(), sizeof(NNRec) * nnrec_all.size())) ||
+        (st = up(ctx->cpn, cpn32.data(), 4 * cpn32.size())) || (st = up(ctx->dpn, dpn32.data(), 4 * dpn32.size())) ||
+        (st = up(ctx->nspe, nspe.data(), 4 * nspe.size())) ||
+        (st = up(ctx->pp_op, ctx->h_pp_op.data(), 4 * ctx->h_pp_op.size())) ||
+        (st = up(ctx->nnrec_op, nnrec_op_all.data(), 4 * nnrec_op_all.size())) ||
+        (st = up(ctx->hmatpp_d, t->hmatpp, 4 * (size_t)t->nmatpp)) ||
+        (st = up(ctx->hmatnn_d, t->hmatnn, 4 * (size_t)t->nmatnn)))
+        return st;
+    ctx->stats.derived_bytes = (int64_t)(8 * row_off.size() + 4 * (ctx->h_pp_ptr.size() * 3 + spe_ptr.size()) +
+                                         sizeof(PPContrib) * ctx->h_pp.size() + sizeof(NNContrib) * ctx->h_nn.size() +
+                                         sizeof(PNContrib) * ctx->h_pn.size() + sizeof(SPEContrib) * h_spe.size() +
+                                         sizeof(NOp) * nops.size() + 4 * nptr_all.size() +
+                                         sizeof(PNRec) * pnrec_all.size() + sizeof(NNRec) * nnrec_all.size());
+    ctx->stats.n_rows = nrows;
+    ctx->stats.n_contrib = (int64_t)(ctx->h_pp.size() + ctx->h_nn.size() + ctx->h_pn.size() + h_spe.size());
+
+    RowArgs &a = ctx->args;
+    a.row_off = (const int64_t *)ctx->row_off.p;
+    a.pp_ptr = (const int32_t *)ctx->pp_ptr.p;
+    a.nn_ptr = (const int32_t *)ctx->nn_ptr.p;
+    a.pn_ptr = (const int32_t *)ctx->pn_ptr.p;
+    a.spe_ptr = (const int32_t *)ctx->spe_ptr.p;
+    a.pp = (const PPContrib *)ctx->pp.p;
+    a.nn = (const NNContrib *)ctx->nn.p;
+    a.pn = (const PNContrib *)ctx->pn.p;
+    a.spe = (const SPEContrib *)ctx->spe.p;
+    a.nops = (const NOp *)ctx->nops.p;
+    a.nptr = (const int32_t *)ctx->nptr.p;
+    a.pnrec = (const PNRec *)ctx->pnrec.p;
+    a.nnrec = (const NNRec *)ctx->nnrec.p;
+    a.hmatpn = (const float *)ctx->hmatpn.p;
+    a.cpn = (const int32_t *)ctx->cpn.p;
+    a.dpn = (const int32_t *)ctx->dpn.p;
+    a.nspe = (const float *)ctx->nspe.p;
+    a.ld_cpn = ld;
+    a.ncpn = (int32_t)ncpn;
+    return BSG_OK;
+}
+
+void free_ctx(bsg_ctx *ctx) {
+    for (auto &b : ctx->raw) dev_free(b);
+    DevBuf *bufs[] = {&ctx->row_off, &ctx->pp_ptr, &ctx->nn_ptr, &ctx->pn_ptr, &ctx->spe_ptr, &ctx->pp, &ctx->nn,
+                      &ctx->pn, &ctx->spe, &ctx->nops, &ctx->nptr, &ctx->pnrec, &ctx->nnrec, &ctx->hmatpn,
+                      &ctx->cpn, &ctx->dpn, &ctx->nspe, &ctx->pp_op, &ctx->nnrec_op, &ctx->hmatpp_d,
+                      &ctx->hmatnn_d, &ctx->scratch_in, &ctx->scratch_out};
+    for (DevBuf *b : bufs) dev_free(*b);
+    for (auto &kv : ctx->tiles) dev_free(kv.second.buf);
+    ctx->tiles.clear();
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    ctx->ev0 = ctx->ev1 = nullptr;
+    ctx->stream = nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *bsg_strerror(int status) {
+    switch (status) {
+    case BSG_OK: return "ok";
+    case BSG_ERR_BAD_TABLE: return "table failed validation";
+    case BSG_ERR_OOB_INDEX: return "index outside its array";
+    case BSG_ERR_CUDA: return "CUDA error";
+    case BSG_ERR_NOMEM: return "out of memory";
+    case BSG_ERR_TIMEOUT: return "bounded device wait timed out";
+    case BSG_ERR_NAN: return "non-finite value";
+    case BSG_ERR_ARG: return "bad argument";
+    case BSG_ERR_UNSUPPORTED: return "unsupported input";
+    case BSG_ERR_NOT_CONVERGED: return "not converged";
+    default: return "unknown status";
+    }
+}
+
+int bsg_last_error(const bsg_ctx *ctx, char *buf, size_t len) {
+    if (!ctx || !buf || len == 0) return BSG_ERR_ARG;
+    std::snprintf(buf, len, "%s", ctx->last_error.c_str());
+    return BSG_OK;
+}
+
+int bsg_create(const bsg_tables *t, const bsg_config *cfg, bsg_ctx **out) {
+    if (!out) return BSG_ERR_ARG;
+    *out = nullptr;
+    if (!t) return BSG_ERR_ARG;
+    bsg_ctx *ctx = new (std::nothrow) bsg_ctx();
+    if (!ctx) return BSG_ERR_NOMEM;
+    ctx->device = cfg ? cfg->device : 0;
+    ctx->max_nb = (cfg && cfg->max_nb > 0) ? cfg->max_nb : 16;
+    int st = cuda_check(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+    if (!st) st = cuda_check(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "stream");
+    if (!st) st = cuda_check(ctx, cudaEventCreate(&ctx->ev0), "event");
+    if (!st) st = cuda_check(ctx, cudaEventCreate(&ctx->ev1), "event");
+    if (!st) {
+        ctx->t = *t;
+        ctx->dim = t->dimbasis;
+        try {
+            st = derive(ctx, t);
+        } catch (const std::bad_alloc &) {
+            st = set_err(ctx, BSG_ERR_NOMEM, "host allocation failed while deriving row layouts");
+        }
+    }
+    if (st) {
+        std::fprintf(stderr, "bsg_create: %s: %s\n", bsg_strerror(st), ctx->last_error.c_str());
+        free_ctx(ctx);
+        delete ctx;
+        return st;
+    }
+    ctx->stats.kernel_launches_per_matvec = 1;
+    *out = ctx;
+    return BSG_OK;
+}
+
+int bsg_destroy(bsg_ctx *ctx) {
+    if (!ctx) return BSG_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    free_ctx(ctx);
+    delete ctx;
+    return BSG_OK;
+}
+
+int bsg_applyh_stream(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec, int flags, void *stream) {
+    if (!ctx) return BSG_ERR_ARG;
+    if (!vin || !vout || nb < 1 || nb > 64 || (prec != BSG_PREC_FP32 && prec != BSG_PREC_FP64))
+        return set_err(ctx, BSG_ERR_ARG, "bsg_applyh: bad arguments");
+    if (vin == vout) return set_err(ctx, BSG_ERR_ARG, "bsg_applyh: vin and vout must not alias");
+    int st = cuda_check(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+    if (st) return st;
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    const int acc = (flags & BSG_ACCUMULATE) ? 1 : 0;
+    if (flags & BSG_DEVICE_PTRS) return launch_applyh(ctx, vin, vout, nb, prec, acc, s);
+    // host pointers: copy in, apply, copy out (the drop-in path for vec1/vec2)
+    const size_t bytes = (size_t)ctx->dim * nb * (prec == BSG_PREC_FP32 ? 4 : 8);
+    if (ctx->scratch_in.bytes < bytes) {
+        if ((st = dev_alloc(ctx, ctx->scratch_in, bytes)) || (st = dev_alloc(ctx, ctx->scratch_out, bytes))) return st;
+    }
+    st = cuda_check(ctx, cudaMemcpyAsync(ctx->scratch_in.p, vin, bytes, cudaMemcpyHostToDevice, s), "H2D vin");
+    if (!st && acc) st = cuda_check(ctx, cudaMemcpyAsync(ctx->scratch_out.p, vout, bytes, cudaMemcpyHostToDevice, s), "H2D vout");
+    if (!st) st = launch_applyh(ctx, ctx->scratch_in.p, ctx->scratch_out.p, nb, prec, acc, s);
+    if (!st) st = cuda_check(ctx, cudaMemcpyAsync(vout, ctx->scratch_out.p, bytes, cudaMemcpyDeviceToHost, s), "D2H vout");
+    if (!st) st = cuda_check(ctx, cudaStreamSynchronize(s), "applyh sync");
+    return st;
+}
+
+int bsg_applyh(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec, int flags) {
+    return bsg_applyh_stream(ctx, vin, vout, nb, prec, flags, nullptr);
+}
+
+int bsg_get_stats(const bsg_ctx *ctx, bsg_stats *st) {
+    if (!ctx || !st) return BSG_ERR_ARG;
+    *st = ctx->stats;
+    return BSG_OK;
+}
+
+}  // extern "C"

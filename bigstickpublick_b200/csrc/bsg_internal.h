@@ -1,0 +1,146 @@
+// Internal declarations shared by the engine's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/bsg.h"
+
+namespace bsg {
+
+// ---- derived (device) layouts, built once at bsg_create from the unchanged
+// tables.  Positions are 0-based neutron positions inside a proton-SD row
+// (position = nstart - 1); a row's first basis state (0-based) is pstart(ip).
+
+// PP row contribution: out[row][pos] += me * in[q_off + pos], pos in [lo, hi]
+struct PPContrib {
+    int64_t q_off;
+    float me;        // hmatpp(op) * phase, rounded to float as the reference
+    int32_t lo, hi;
+    int32_t pad;
+};
+// PN row contribution: out[row][pos] += sum over neutron-op records r at pos of
+//   hmatpn(cpn(r.b,a)+dpn(r.d,c)) * php * r.ph * in[q_off + r.in]
+struct PNContrib {
+    int64_t q_off;
+    int32_t nop;       // neutron operator id
+    int16_t acol;      // (a + nhsps(-1)) column of cpnpair
+    int16_t ccol;      // (c + nhsps(-1)) column of dpnpair
+    float php;         // proton jump phase
+    int32_t pad;
+};
+// NN row contribution: out[row][pos] += sum over records r at pos of r.me * in[row + r.in]
+struct NNContrib {
+    int32_t nop;
+};
+// SPE row contribution: out[row][pos] += (pspe + nspe[n0 + pos - lo]) * in[row + pos]
+struct SPEContrib {
+    float pspe;
+    int32_t lo, hi;
+    int32_t n0;       // 0-based neutron SD index at pos == lo
+};
+// neutron operator: records sorted by output position
+struct NOp {
+    int64_t rec_base;   // first record
+    int64_t ptr_base;   // first entry of its [nout+1] pointer array
+    int32_t nout;
+    int32_t kind;       // 0 = NN (me records), 1 = PN (label records)
+};
+// PN record: input position and the neutron creation/destruction columns
+struct PNRec {
+    int32_t in;
+    uint8_t b, d;       // b + nhsps(-2), d + nhsps(-2): row of cpnpair/dpnpair
+    int8_t ph;
+    int8_t pad;
+};
+// NN record: input position and hmatnn(op)*phase
+struct NNRec {
+    int32_t in;
+    float me;
+};
+struct Tile {
+    int32_t row;
+    int32_t pos0;
+    int32_t npos;
+    int32_t pad;
+};
+
+struct RowArgs {
+    const int64_t *row_off;       // [nrows] pstart
+    const int32_t *pp_ptr, *nn_ptr, *pn_ptr, *spe_ptr;  // [nrows+1]
+    const PPContrib *pp;
+    const NNContrib *nn;
+    const PNContrib *pn;
+    const SPEContrib *spe;
+    const NOp *nops;
+    const int32_t *nptr;          // pointer arrays of all neutron ops
+    const PNRec *pnrec;
+    const NNRec *nnrec;
+    const float *hmatpn;
+    const int32_t *cpn, *dpn;     // cpnpair/dpnpair as int32 (validated)
+    const float *nspe;
+    int32_t ld_cpn;               // nhsps(-2)+nhsps(2)+1
+    int32_t ncpn;                 // entries of cpn
+    const Tile *tiles;
+    int32_t ntiles;
+    int32_t accumulate;
+};
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+struct TileSet {
+    DevBuf buf;
+    int32_t ntiles = 0;
+};
+
+}  // namespace bsg
+
+struct bsg_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    bsg_tables t{};           // sizes only (pointers are host-owned by caller)
+    int64_t dim = 0, nrows = 0;
+    int32_t max_rowlen = 0;
+    int32_t max_nb = 16;
+    // raw tables on the device (byte-identical copies)
+    std::vector<bsg::DevBuf> raw;
+    // derived
+    bsg::DevBuf row_off, pp_ptr, nn_ptr, pn_ptr, spe_ptr, pp, nn, pn, spe, nops, nptr, pnrec, nnrec;
+    bsg::DevBuf hmatpn, cpn, dpn, nspe, hmatpp_d, hmatnn_d;
+    bsg::RowArgs args{};
+    std::map<int, bsg::TileSet> tiles;   // tile size -> tiles
+    std::vector<int32_t> h_rowlen;
+    std::vector<int32_t> h_work;         // per-row work estimate
+    // host copies kept for the adjoint
+    std::vector<int32_t> h_pp_ptr, h_nn_ptr, h_pn_ptr;
+    std::vector<bsg::PPContrib> h_pp;
+    std::vector<int32_t> h_pp_op;        // hmatpp label of each PP contribution
+    std::vector<bsg::NNContrib> h_nn;
+    std::vector<bsg::PNContrib> h_pn;
+    std::vector<bsg::NOp> h_nops;
+    std::vector<int32_t> h_nnrec_op;     // hmatnn label of each NN record
+    bsg::DevBuf pp_op, nnrec_op;
+    bsg_stats stats{};
+    // scratch vectors for host-pointer applyh
+    bsg::DevBuf scratch_in, scratch_out;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace bsg {
+int set_err(bsg_ctx *ctx, int code, const std::string &msg);
+int cuda_check(bsg_ctx *ctx, cudaError_t e, const char *what);
+int dev_alloc(bsg_ctx *ctx, DevBuf &b, size_t bytes);
+void dev_free(DevBuf &b);
+int upload(bsg_ctx *ctx, DevBuf &b, const void *src, size_t bytes);
+const TileSet *get_tiles(bsg_ctx *ctx, int tp);
+int launch_applyh(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec, int accumulate,
+                  cudaStream_t s);
+}  // namespace bsg

@@ -1,0 +1,153 @@
+"""Python face of libbsgpu.so (the sm_100a engine).
+
+Mirrors the reference's operator interface for this path:
+
+* ``Hamiltonian(tables)``        -- bsg_create: validate + upload the tables
+* ``H.applyh(vin, vout=None, accumulate=False)``
+                                 -- applyHbundled_omp('n') / applyHbundled_block_omp:
+                                    vout (+)= H vin, nb inferred from the shape
+                                    (dim,) or (dim, nb) (interleaved layout)
+* ``H.lanczos(...)``             -- lanczos_p / lanczos_block with thick restart
+* ``H.grad(evecs)``              -- adjoint: dE/dhmat for every uncoupled label
+
+Errors raise ``BsgError`` with the status name and the latched message; there
+is no CPU fallback anywhere on this path.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+
+
+class BsgError(RuntimeError):
+    def __init__(self, status, msg):
+        self.status = status
+        super().__init__(f"{_abi.STATUS_NAMES.get(status, status)}: {msg}")
+
+
+def _is_torch(x):
+    return type(x).__module__.startswith("torch")
+
+
+class Hamiltonian:
+    def __init__(self, tables, device=0, max_nb=16, validate=True):
+        self.lib = _abi.gpu_lib()
+        self.tables = tables
+        self._ct = tables.as_ctypes()
+        cfg = _abi.BsgConfig(device, max_nb, 1 if validate else 0, 0)
+        h = C.c_void_p()
+        st = self.lib.bsg_create(C.byref(self._ct), C.byref(cfg), C.byref(h))
+        if st != 0:
+            raise BsgError(st, "bsg_create failed (see stderr for the validator message)")
+        self.h = h
+        self.dim = tables.dim
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.bsg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st, what):
+        if st != 0:
+            buf = C.create_string_buffer(512)
+            self.lib.bsg_last_error(self.h, buf, 512)
+            raise BsgError(st, f"{what}: {buf.value.decode()}")
+
+    def stats(self):
+        s = _abi.BsgStats()
+        self._check(self.lib.bsg_get_stats(self.h, C.byref(s)), "bsg_get_stats")
+        return {k: getattr(s, k) for k, _ in s._fields_}
+
+    # ------------------------------------------------------------ applyH
+    def applyh(self, vin, vout=None, accumulate=False, stream=None):
+        """vout (+)= H vin.  numpy arrays use host pointers (copies inside the
+        call); torch CUDA tensors use device pointers on the current stream."""
+        nb = 1 if vin.ndim == 1 else int(vin.shape[1])
+        if vin.shape[0] != self.dim:
+            raise ValueError(f"vector length {vin.shape[0]} != dim {self.dim}")
+        if _is_torch(vin):
+            import torch
+            prec = 4 if vin.dtype == torch.float32 else 8
+            if vin.dtype not in (torch.float32, torch.float64) or not vin.is_cuda or not vin.is_contiguous():
+                raise ValueError("torch input must be a contiguous CUDA float32/float64 tensor")
+            if vout is None:
+                vout = torch.empty_like(vin)
+            flags = _abi.BSG_DEVICE_PTRS | (_abi.BSG_ACCUMULATE if accumulate else 0)
+            s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+            st = self.lib.bsg_applyh_stream(self.h, C.c_void_p(vin.data_ptr()), C.c_void_p(vout.data_ptr()),
+                                            nb, prec, flags, C.c_void_p(s))
+            self._check(st, "bsg_applyh")
+            return vout
+        vin = np.ascontiguousarray(vin)
+        if vin.dtype not in (np.float32, np.float64):
+            raise ValueError("vector dtype must be float32 or float64")
+        prec = 4 if vin.dtype == np.float32 else 8
+        if vout is None:
+            vout = np.zeros_like(vin)
+        flags = _abi.BSG_ACCUMULATE if accumulate else 0
+        st = self.lib.bsg_applyh(self.h, vin.ctypes.data, vout.ctypes.data, nb, prec, flags)
+        self._check(st, "bsg_applyh")
+        return vout
+
+    # ----------------------------------------------------------- Lanczos
+    def lanczos(self, nkeep=10, niter=300, nthick_add=0, max_restarts=0, nb=1, matvec_prec=8,
+                fixed_iter=False, ncheck=None, converge_tol=1e-3, want_vectors=False, pivot=None,
+                seed=12345):
+        p = _abi.BsgLanczosParams()
+        p.nkeep = nkeep
+        p.niter = niter
+        p.nthick_add = nthick_add
+        p.max_restarts = max_restarts
+        p.nb = nb
+        p.matvec_prec = matvec_prec
+        p.fixed_iter = 1 if fixed_iter else 0
+        p.ncheck = ncheck if ncheck is not None else nkeep + 5
+        p.converge_tol = converge_tol
+        p.want_vectors = 1 if want_vectors else 0
+        p.pivot = 0
+        p.seed = seed
+        ev = np.zeros(nkeep, dtype=np.float64)
+        vecs = np.zeros((nkeep, self.dim), dtype=np.float64) if want_vectors else None
+        pv = None
+        if pivot is not None:
+            pv = np.ascontiguousarray(pivot, dtype=np.float64)
+            if pv.size != self.dim * nb:
+                raise ValueError("pivot must have dim*nb entries")
+        rep = _abi.BsgReport()
+        st = self.lib.bsg_lanczos(self.h, C.byref(p),
+                                  pv.ctypes.data_as(_abi.f64p) if pv is not None else None,
+                                  ev.ctypes.data_as(_abi.f64p),
+                                  vecs.ctypes.data_as(_abi.f64p) if vecs is not None else None,
+                                  C.byref(rep))
+        self._check(st, "bsg_lanczos")
+        report = {k: getattr(rep, k) for k, _ in rep._fields_}
+        return ev, (vecs.T.copy() if vecs is not None else None), report
+
+    # ----------------------------------------------------------- adjoint
+    def grad(self, evecs):
+        """dE_k/dhmat for each state k: dict of (nstates, nmat) arrays for
+        'pp', 'nn', 'pn' (and 'spe_p', 'spe_n' when call_spe)."""
+        ev = np.ascontiguousarray(np.asarray(evecs, dtype=np.float64).T)  # (nstates, dim)
+        ns = ev.shape[0]
+        s = self.tables.s
+        out = {"pp": np.zeros((ns, s["nmatpp"])), "nn": np.zeros((ns, s["nmatnn"])),
+               "pn": np.zeros((ns, s["nmatpn"]))}
+        sp = sn = None
+        if s["call_spe"]:
+            out["spe_p"] = np.zeros((ns, s["nsd_p"]))
+            out["spe_n"] = np.zeros((ns, s["nsd_n"]))
+            sp, sn = out["spe_p"], out["spe_n"]
+        st = self.lib.bsg_grad(self.h, ev.ctypes.data_as(_abi.f64p), ns,
+                               out["pp"].ctypes.data_as(_abi.f64p), out["nn"].ctypes.data_as(_abi.f64p),
+                               out["pn"].ctypes.data_as(_abi.f64p),
+                               sp.ctypes.data_as(_abi.f64p) if sp is not None else None,
+                               sn.ctypes.data_as(_abi.f64p) if sn is not None else None)
+        self._check(st, "bsg_grad")
+        return out
