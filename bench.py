@@ -1,0 +1,322 @@
+#!/usr/bin/env python
+"""Benchmark: BIGSTICK M-scheme applyH on B200.
+
+Default workload: sd shell, 6 protons + 6 neutrons, 2Jz = 0 (M-scheme dim
+93,710), seeded synthetic isospin interaction (63 TBMEs ~ N(0,1) MeV, seed 2,
+SPEs -3.9/-3.2/+2.1 MeV), FP32 applyH (fp32 matrix elements, fp32 vectors,
+fp32 accumulation).  One step = one applyH over one vector.
+
+Timing: W warm-up matvecs, then exactly K timed matvecs; before every timed
+matvec the L2 is flushed by writing a 256 MiB buffer, and the matvec kernel
+itself is timed with CUDA events on its stream; barrier + synchronize on both
+sides; max over ranks.  `e2e` calls the C ABI with pinned host buffers, so
+the host->device copy of the input and the device->host copy of the output
+are inside each timed step.
+
+`--impl reference` times the reference's CPU algorithm for this path on the
+host cores: the reference is Fortran and no Fortran compiler exists in this
+image, so it runs the oracle's C restatement of applyHbundled_g with its
+OpenMP partition (kind "port").
+
+Multi-GPU: the matvec does not shard across GPUs in this build; --gpus N runs
+N independent replicas (one per rank) and reports the aggregate rate.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "applyH matvec/s & HBM-roofline %, mixed vs FP64 GPU at ≤1e-6 rel eigval err"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+WORKLOADS = {
+    # name: (shell, np, nn, jz2, seed)
+    "sd6p6n": ("sd", 6, 6, 0, 2),
+    "sd2p2n": ("sd", 2, 2, 0, 1),
+    "pf4p4n": ("pf", 4, 4, 0, 3),
+}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+def make_tables(name):
+    from bigstickpublick_b200 import model
+    shell, np_, nn, jz2, seed = WORKLOADS[name]
+    m = model.sd_model(np_, nn, seed=seed, jz2=jz2) if shell == "sd" else model.pf_model(np_, nn, seed=seed, jz2=jz2)
+    return model.build_tables(m)
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sms, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sms.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sms)) if sms else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sms)}
+
+
+def alg_bytes(stats, tables, nb, s):
+    """B_alg = N_ops*nb*(s_in + 2 s_out) + J_bytes + dim*nb*(s_in + s_out).
+    J_bytes = 21 B per stored jump + pstart/nstart (8 B each) + hmat (4 B each)."""
+    nops = stats["n_ops_pp"] + stats["n_ops_nn"] + stats["n_ops_pn"] + stats["n_ops_spe"]
+    S = tables.s
+    jumps = S["np1b"] + S["nn1b"] + S["np2b"] + S["nn2b"]
+    jb = 21 * jumps + 8 * (S["nsd_p"] + S["nsd_n"]) + 4 * (S["nmatpp"] + S["nmatnn"] + S["nmatpn"])
+    return nops * nb * 3 * s + jb + tables.dim * nb * 2 * s, nops
+
+
+def cpu_baseline(tables, nb, prec, budget_s=10.0, nthreads=None):
+    import oracle
+    dt = np.float32 if prec == 4 else np.float64
+    rng = np.random.default_rng(0)
+    vin = rng.standard_normal(tables.dim * nb).astype(dt)
+    out = np.zeros_like(vin)
+    nthreads = nthreads or os.cpu_count()
+    oracle.applyh_omp(tables, vin, nb=nb, nthreads=nthreads, out=out)  # warm-up
+    n, t0 = 0, time.perf_counter()
+    while True:
+        out[:] = 0
+        oracle.applyh_omp(tables, vin, nb=nb, nthreads=nthreads, out=out)
+        n += 1
+        el = time.perf_counter() - t0
+        if el > budget_s or n >= 2000:
+            break
+    return n / el, nthreads, n, el
+
+
+def traffic_from_profile(workload, nb, prec):
+    p = os.path.join(ROOT, "profiles", "applyh_traffic.json")
+    if not os.path.exists(p):
+        return None
+    try:
+        d = json.load(open(p))
+        return d.get(f"{workload}:nb{nb}:p{prec}")
+    except Exception:
+        return None
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    tables = make_tables(args.workload)
+    per_step = []
+    n_total = 0
+    t_total = 0.0
+    nthreads = os.cpu_count()
+    for _ in range(args.warmup):
+        cpu_baseline(tables, args.nb, args.prec, budget_s=0.0, nthreads=nthreads)
+    for _ in range(args.steps):
+        rate, cores, n, el = cpu_baseline(tables, args.nb, args.prec, budget_s=args.ref_budget, nthreads=nthreads)
+        per_step.append(rate)
+        n_total += n
+        t_total += el
+    value = n_total / t_total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "matvec/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_total / max(1, n_total),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if args.prec == 4 else "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "nb": args.nb, "dim": tables.dim},
+        "cpu_baseline": {"value": value, "unit": "matvec/s", "cores": nthreads, "kind": "port",
+                         "sample": f"{n_total} matvecs over {t_total:.1f} s (reference is Fortran; "
+                                   "no Fortran compiler in the image)"},
+        "e2e": {"value": value, "unit": "matvec/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="sd6p6n", choices=sorted(WORKLOADS))
+    ap.add_argument("--nb", type=int, default=1)
+    ap.add_argument("--prec", type=int, default=4, choices=[4, 8])
+    ap.add_argument("--ref-budget", type=float, default=3.0)
+    ap.add_argument("--cpu-budget", type=float, default=10.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    from bigstickpublick_b200.engine import Hamiltonian
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    tables = make_tables(args.workload)
+    H = Hamiltonian(tables, device=local)
+    st = H.stats()
+    nb, prec = args.nb, args.prec
+    dt = torch.float32 if prec == 4 else torch.float64
+    s_bytes = 4 if prec == 4 else 8
+    g = torch.Generator(device="cuda").manual_seed(1234)
+    shape = (tables.dim,) if nb == 1 else (tables.dim, nb)
+    vin = torch.randn(shape, dtype=dt, device="cuda", generator=g)
+    vout = torch.empty_like(vin)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
+    stream = torch.cuda.current_stream()
+
+    for _ in range(args.warmup):
+        H.applyh(vin, vout)
+    barrier()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier()
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        evs[k][0].record(stream)
+        H.applyh(vin, vout)
+        evs[k][1].record(stream)
+    barrier()
+    kern_ms = [a.elapsed_time(b) for a, b in evs]
+    # warm-L2 rate (vectors resident in L2, the steady state inside Lanczos)
+    w0, w1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0.record(stream)
+    for _ in range(args.steps):
+        H.applyh(vin, vout)
+    w1.record(stream)
+    barrier()
+    warm_ms = w0.elapsed_time(w1) / args.steps
+    clocks = sampler.stop()
+
+    total_ms = float(sum(kern_ms))
+    if dist is not None:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * args.steps / (total_ms / 1e3)
+
+    # ---- end to end through the C ABI with pinned host buffers
+    hin = torch.empty(shape, dtype=dt, pin_memory=True)
+    hin.copy_(vin.cpu())
+    hout = torch.empty(shape, dtype=dt, pin_memory=True)
+    hin_np, hout_np = hin.numpy(), hout.numpy()
+    for _ in range(2):
+        H.applyh(hin_np, hout_np)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        H.applyh(hin_np, hout_np)  # H2D copy, kernel, D2H copy, synchronize
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = world * args.steps / e2e_s
+    vbytes = tables.dim * nb * s_bytes
+
+    peaks, peak_kind = load_peaks()
+    balg, nops = alg_bytes(st, tables, nb, s_bytes)
+    mean_s = total_ms / 1e3 / args.steps
+    achieved = balg / mean_s / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "matvec/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if prec == 4 else "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "dim": tables.dim, "nb": nb,
+                   "interaction": "seeded synthetic isospin TBMEs N(0,1) MeV",
+                   "l2": "flushed (256 MiB write) before every timed matvec; kernel timed alone",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e, "unit": "matvec/s", "h2d_bytes_per_step": vbytes, "d2h_bytes_per_step": vbytes},
+        "gpu_launches": args.steps * st["kernel_launches_per_matvec"],
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": traffic_from_profile(args.workload, nb, prec),
+                     "peak_kind": peak_kind, "alg_bytes_per_launch": balg, "ops_per_matvec": nops},
+        "clocks": clocks,
+        "warm_l2_matvec_per_s": world / (warm_ms / 1e3),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, cores, n, el = cpu_baseline(tables, nb, prec, budget_s=args.cpu_budget)
+        line["cpu_baseline"] = {"value": rate, "unit": "matvec/s", "cores": cores, "kind": "port",
+                                "sample": f"{n} full matvecs of the same workload in {el:.1f} s, "
+                                          "oracle C restatement of applyHbundled_g with OpenMP"}
+    if rank == 0:
+        print(json.dumps(line))
+    del H
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -76,19 +76,26 @@ template <> struct Vec<double, 4, true> : VecD2<4> {};
 template <> struct Vec<double, 8, true> : VecD2<8> {};
 template <> struct Vec<double, 16, true> : VecD2<16> {};
 
+constexpr int kWarps = kRowWarps;
+
+__host__ __device__ constexpr size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+// One CTA = one tile of one output row: positions pos0 + lane + 32*i.  Warp w
+// handles the contributions assigned to slot (row, w) at setup (balanced by
+// estimated work) and accumulates in registers; the eight partial sums are
+// added in fixed warp order at the end, so the result does not depend on
+// scheduling.
 // ld: elements between consecutive states (the block size nb); v0: first
-// vector column handled by this launch; FULL: ld == NB (aligned vector loads)
-template <typename T, int NB, int ITEMS, int BLOCK, bool FULL>
-__global__ void __launch_bounds__(BLOCK) k_rows(const RowArgs a, const T *__restrict__ vin,
-                                                T *__restrict__ vout, const int ld, const int v0) {
-    extern __shared__ int32_t s_tab[];
-    for (int i = threadIdx.x; i < a.ncpn; i += BLOCK) {
-        s_tab[i] = a.cpn[i];
-        s_tab[a.ncpn + i] = a.dpn[i];
-    }
-    __syncthreads();
-    const int32_t *__restrict__ s_cpn = s_tab;
-    const int32_t *__restrict__ s_dpn = s_tab + a.ncpn;
+// vector column handled by this launch; FULL: ld == NB and aligned base.
+// mstride: floats of per-warp shared memory for the PN matrix-element table.
+template <typename T, int NB, int ITEMS, bool FULL>
+__global__ void __launch_bounds__(kWarps * 32) k_rows(const RowArgs a, const T *__restrict__ vin,
+                                                      T *__restrict__ vout, const int ld, const int v0,
+                                                      const int mstride) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float *__restrict__ Mw = reinterpret_cast<float *>(smem) + (size_t)warp * mstride;
+    T *__restrict__ part = reinterpret_cast<T *>(smem + align16(sizeof(float) * (size_t)kWarps * mstride));
 
     const Tile tile = a.tiles[blockIdx.x];
     const int row = tile.row;
@@ -99,7 +106,7 @@ __global__ void __launch_bounds__(BLOCK) k_rows(const RowArgs a, const T *__rest
     bool valid[ITEMS];
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) {
-        const int local = threadIdx.x + i * BLOCK;
+        const int local = lane + 32 * i;
         pos[i] = tile.pos0 + local;
         valid[i] = local < tile.npos;
 #pragma unroll
@@ -108,8 +115,9 @@ __global__ void __launch_bounds__(BLOCK) k_rows(const RowArgs a, const T *__rest
 
     // ---- PP: out[pos] += me * in[q_off + pos]   (src/bapplyhlibOMP.f90:1068-1241)
     {
-        const int c0 = a.pp_ptr[row], c1 = a.pp_ptr[row + 1];
-        for (int c = c0; c < c1; ++c) {
+        const int slot = row * kWarps + warp;
+        const int c1 = a.pp_ptr[slot + 1];
+        for (int c = a.pp_ptr[slot]; c < c1; ++c) {
             const PPContrib pc = a.pp[c];
             const T me = (T)pc.me;
 #pragma unroll
@@ -125,59 +133,94 @@ __global__ void __launch_bounds__(BLOCK) k_rows(const RowArgs a, const T *__rest
     }
     // ---- NN: out[pos] += sum r.me * in[row + r.in]   (:1012-1066)
     {
-        const int c0 = a.nn_ptr[row], c1 = a.nn_ptr[row + 1];
-        for (int c = c0; c < c1; ++c) {
+        const int slot = row * kWarps + warp;
+        const int c1 = a.nn_ptr[slot + 1];
+        const T *__restrict__ src = vin + (size_t)roff * ld + v0;
+        for (int c = a.nn_ptr[slot]; c < c1; ++c) {
             const NOp op = a.nops[a.nn[c].nop];
             const int32_t *__restrict__ ptr = a.nptr + op.ptr_base;
-            const NNRec *__restrict__ rec = a.nnrec + op.rec_base;
+            const int2 *__restrict__ rec = reinterpret_cast<const int2 *>(a.nnrec + op.rec_base);
 #pragma unroll
             for (int i = 0; i < ITEMS; ++i) {
                 if (!valid[i] || pos[i] >= op.nout) continue;
                 const int k0 = __ldg(ptr + pos[i]), k1 = __ldg(ptr + pos[i] + 1);
-                for (int k = k0; k < k1; ++k) {
-                    const int2 r = __ldg(reinterpret_cast<const int2 *>(rec + k));
-                    const T me = (T)__int_as_float(r.y);
-                    T x[NB];
-                    Vec<T, NB, FULL>::load(vin + (size_t)(roff + r.x) * ld + v0, x);
+                int k = k0;
+                for (; k + 1 < k1; k += 2) {
+                    const int2 r0 = __ldg(rec + k), r1 = __ldg(rec + k + 1);
+                    T x0[NB], x1[NB];
+                    Vec<T, NB, FULL>::load(src + (size_t)r0.x * ld, x0);
+                    Vec<T, NB, FULL>::load(src + (size_t)r1.x * ld, x1);
+                    const T m0 = (T)__int_as_float(r0.y), m1 = (T)__int_as_float(r1.y);
 #pragma unroll
-                    for (int v = 0; v < NB; ++v) acc[i][v] += me * x[v];
+                    for (int v = 0; v < NB; ++v) { acc[i][v] += m0 * x0[v]; acc[i][v] += m1 * x1[v]; }
+                }
+                if (k < k1) {
+                    const int2 r0 = __ldg(rec + k);
+                    T x0[NB];
+                    Vec<T, NB, FULL>::load(src + (size_t)r0.x * ld, x0);
+                    const T m0 = (T)__int_as_float(r0.y);
+#pragma unroll
+                    for (int v = 0; v < NB; ++v) acc[i][v] += m0 * x0[v];
                 }
             }
         }
     }
     // ---- PN: out[pos] += sum hmatpn(cpn(b,a)+dpn(d,c))*php*phn * in[q_off + r.in]  (:1242-1442)
+    // The warp first tabulates hmatpn(cpn(b,a)+dpn(d,c))*php for the proton
+    // jump's (a,c) and every distinct neutron (b,d) of the operator; a record
+    // then costs one shared load, the neutron phase is its sign bit.
     {
-        const int c0 = a.pn_ptr[row], c1 = a.pn_ptr[row + 1];
-        for (int c = c0; c < c1; ++c) {
+        const int slot = row * kWarps + warp;
+        const int c1 = a.pn_ptr[slot + 1];
+        for (int c = a.pn_ptr[slot]; c < c1; ++c) {
             const PNContrib pc = a.pn[c];
             const NOp op = a.nops[pc.nop];
-            const int32_t *__restrict__ ptr = a.nptr + op.ptr_base;
-            const PNRec *__restrict__ rec = a.pnrec + op.rec_base;
             const int acol = pc.acol * a.ld_cpn, ccol = pc.ccol * a.ld_cpn;
+            for (int k = lane; k < op.nbd; k += 32) {
+                const BDPair bd = a.bd[op.bd_base + k];
+                const int idx = __ldg(a.cpn + bd.b + acol) + __ldg(a.dpn + bd.d + ccol);
+                float xme = __ldg(a.hmatpn + idx - 1);
+                Mw[k] = xme * pc.php;
+            }
+            __syncwarp();
+            const int32_t *__restrict__ ptr = a.nptr + op.ptr_base;
+            const int2 *__restrict__ rec = reinterpret_cast<const int2 *>(a.pnrec + op.rec_base);
+            const T *__restrict__ src = vin + (size_t)pc.q_off * ld + v0;
 #pragma unroll
             for (int i = 0; i < ITEMS; ++i) {
                 if (!valid[i] || pos[i] >= op.nout) continue;
                 const int k0 = __ldg(ptr + pos[i]), k1 = __ldg(ptr + pos[i] + 1);
-                for (int k = k0; k < k1; ++k) {
-                    const int2 r = __ldg(reinterpret_cast<const int2 *>(rec + k));
-                    const int b = r.y & 0xff, d = (r.y >> 8) & 0xff;
-                    const float ph = (float)(int8_t)((r.y >> 16) & 0xff);
-                    const int idx = s_cpn[b + acol] + s_dpn[d + ccol];
-                    float xme = __ldg(a.hmatpn + idx - 1);
-                    xme = xme * pc.php * ph;
-                    const T me = (T)xme;
-                    T x[NB];
-                    Vec<T, NB, FULL>::load(vin + (size_t)(pc.q_off + r.x) * ld + v0, x);
+                int k = k0;
+                for (; k + 1 < k1; k += 2) {
+                    const int2 r0 = __ldg(rec + k), r1 = __ldg(rec + k + 1);
+                    T x0[NB], x1[NB];
+                    Vec<T, NB, FULL>::load(src + (size_t)r0.x * ld, x0);
+                    Vec<T, NB, FULL>::load(src + (size_t)r1.x * ld, x1);
+                    // neutron phase: int8 at bits 16..23, its sign moved to bit 31
+                    const float f0 = __int_as_float(__float_as_int(Mw[r0.y & 0xffff]) ^ ((r0.y << 8) & 0x80000000));
+                    const float f1 = __int_as_float(__float_as_int(Mw[r1.y & 0xffff]) ^ ((r1.y << 8) & 0x80000000));
+                    const T m0 = (T)f0, m1 = (T)f1;
 #pragma unroll
-                    for (int v = 0; v < NB; ++v) acc[i][v] += me * x[v];
+                    for (int v = 0; v < NB; ++v) { acc[i][v] += m0 * x0[v]; acc[i][v] += m1 * x1[v]; }
+                }
+                if (k < k1) {
+                    const int2 r0 = __ldg(rec + k);
+                    T x0[NB];
+                    Vec<T, NB, FULL>::load(src + (size_t)r0.x * ld, x0);
+                    const float f0 = __int_as_float(__float_as_int(Mw[r0.y & 0xffff]) ^ ((r0.y << 8) & 0x80000000));
+                    const T m0 = (T)f0;
+#pragma unroll
+                    for (int v = 0; v < NB; ++v) acc[i][v] += m0 * x0[v];
                 }
             }
+            __syncwarp();
         }
     }
     // ---- SPE: out[pos] += (pspe + nspe) * in[pos]   (:988-1011)
     {
-        const int c0 = a.spe_ptr[row], c1 = a.spe_ptr[row + 1];
-        for (int c = c0; c < c1; ++c) {
+        const int slot = row * kWarps + warp;
+        const int c1 = a.spe_ptr[slot + 1];
+        for (int c = a.spe_ptr[slot]; c < c1; ++c) {
             const SPEContrib sc = a.spe[c];
 #pragma unroll
             for (int i = 0; i < ITEMS; ++i) {
@@ -191,56 +234,88 @@ __global__ void __launch_bounds__(BLOCK) k_rows(const RowArgs a, const T *__rest
             }
         }
     }
-    // ---- single write of every owned output element
+    // ---- fixed-order reduction over the warps, single write per element
+    constexpr int TP = 32 * ITEMS;
 #pragma unroll
-    for (int i = 0; i < ITEMS; ++i) {
-        if (!valid[i]) continue;
-        T *o = vout + (size_t)(roff + pos[i]) * ld + v0;
+    for (int i = 0; i < ITEMS; ++i)
 #pragma unroll
-        for (int v = 0; v < NB; ++v) o[v] = a.accumulate ? o[v] + acc[i][v] : acc[i][v];
+        for (int v = 0; v < NB; ++v) part[((size_t)warp * TP + lane + 32 * i) * NB + v] = acc[i][v];
+    __syncthreads();
+    const int nel = tile.npos * NB;
+    for (int e = threadIdx.x; e < nel; e += kWarps * 32) {
+        T s = part[e];
+#pragma unroll
+        for (int w = 1; w < kWarps; ++w) s += part[(size_t)w * TP * NB + e];
+        const int lp = e / NB, v = e - lp * NB;
+        T *o = vout + (size_t)(roff + tile.pos0 + lp) * ld + v0 + v;
+        *o = a.accumulate ? *o + s : s;
     }
 }
-
-constexpr int kBlock = 128;
 
 template <typename T, int NB, int ITEMS>
 static int launch_one(bsg_ctx *ctx, const T *vin, T *vout, int ld, int v0, int accumulate,
                       cudaStream_t s) {
-    const TileSet *ts = get_tiles(ctx, kBlock * ITEMS);
+    const TileSet *ts = get_tiles(ctx, 32 * ITEMS);
     if (!ts) return ctx->last_error.empty() ? BSG_ERR_NOMEM : BSG_ERR_CUDA;
     if (ts->ntiles == 0) return BSG_OK;
     RowArgs a = ctx->args;
     a.tiles = (const Tile *)ts->buf.p;
     a.ntiles = ts->ntiles;
     a.accumulate = accumulate;
-    const size_t smem = sizeof(int32_t) * 2 * (size_t)a.ncpn;
+    const int mstride = (a.max_nbd + 3) & ~3;
+    const size_t smem = align16(sizeof(float) * (size_t)kWarps * mstride) +
+                        sizeof(T) * (size_t)kWarps * 32 * ITEMS * NB;
     // aligned vector loads only when each state's NB values are contiguous and
     // the base pointer is 16-byte aligned
     const bool full = (ld == NB) && ((reinterpret_cast<uintptr_t>(vin) & 15u) == 0);
-    if (full)
-        k_rows<T, NB, ITEMS, kBlock, true><<<ts->ntiles, kBlock, smem, s>>>(a, vin, vout, ld, v0);
-    else
-        k_rows<T, NB, ITEMS, kBlock, false><<<ts->ntiles, kBlock, smem, s>>>(a, vin, vout, ld, v0);
+    cudaError_t e;
+    if (full) {
+        auto k = k_rows<T, NB, ITEMS, true>;
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess) k<<<ts->ntiles, kWarps * 32, smem, s>>>(a, vin, vout, ld, v0, mstride);
+    } else {
+        auto k = k_rows<T, NB, ITEMS, false>;
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess) k<<<ts->ntiles, kWarps * 32, smem, s>>>(a, vin, vout, ld, v0, mstride);
+    }
+    if (e != cudaSuccess) return cuda_check(ctx, e, "applyh smem attribute");
     return cuda_check(ctx, cudaGetLastError(), "applyh kernel launch");
+}
+
+// tile width: 32*ITEMS positions, ITEMS the smallest power of two covering the
+// median row, capped so that ITEMS*NB accumulators stay in registers
+template <typename T, int NB>
+static int launch_nb(bsg_ctx *ctx, const T *vin, T *vout, int ld, int v0, int accumulate, cudaStream_t s) {
+    constexpr int cap = NB >= 8 ? 1 : (NB == 4 ? 2 : (NB == 2 ? 4 : 8));
+    int items = 1;
+    while (items < cap && 32 * items < ctx->median_rowlen) items *= 2;
+    if (items >= 8 && cap >= 8) return launch_one<T, NB, (cap >= 8 ? 8 : 1)>(ctx, vin, vout, ld, v0, accumulate, s);
+    if (items >= 4 && cap >= 4) return launch_one<T, NB, (cap >= 4 ? 4 : 1)>(ctx, vin, vout, ld, v0, accumulate, s);
+    if (items >= 2 && cap >= 2) return launch_one<T, NB, (cap >= 2 ? 2 : 1)>(ctx, vin, vout, ld, v0, accumulate, s);
+    return launch_one<T, NB, 1>(ctx, vin, vout, ld, v0, accumulate, s);
 }
 
 template <typename T>
 static int launch_typed(bsg_ctx *ctx, const T *vin, T *vout, int nb, int accumulate, cudaStream_t s) {
-    // nb is covered by column chunks of 16/8/4/2/1 vectors
-    int v0 = 0, st = BSG_OK;
-    while (v0 < nb && st == BSG_OK) {
-        const int rem = nb - v0;
-        if (rem >= 16) { st = launch_one<T, 16, 1>(ctx, vin, vout, nb, v0, accumulate, s); v0 += 16; }
-        else if (rem >= 8) { st = launch_one<T, 8, 1>(ctx, vin, vout, nb, v0, accumulate, s); v0 += 8; }
-        else if (rem >= 4) { st = launch_one<T, 4, 1>(ctx, vin, vout, nb, v0, accumulate, s); v0 += 4; }
-        else if (rem >= 2) { st = launch_one<T, 2, 2>(ctx, vin, vout, nb, v0, accumulate, s); v0 += 2; }
-        else { st = launch_one<T, 1, 4>(ctx, vin, vout, nb, v0, accumulate, s); v0 += 1; }
+    switch (nb) {
+    case 1: return launch_nb<T, 1>(ctx, vin, vout, nb, 0, accumulate, s);
+    case 2: return launch_nb<T, 2>(ctx, vin, vout, nb, 0, accumulate, s);
+    case 4: return launch_nb<T, 4>(ctx, vin, vout, nb, 0, accumulate, s);
+    case 8: return launch_nb<T, 8>(ctx, vin, vout, nb, 0, accumulate, s);
+    case 16: return launch_nb<T, 16>(ctx, vin, vout, nb, 0, accumulate, s);
+    default: {
+        // other block sizes: one column pass per vector (strided layout)
+        int st = BSG_OK;
+        for (int v0 = 0; v0 < nb && st == BSG_OK; ++v0) st = launch_nb<T, 1>(ctx, vin, vout, nb, v0, accumulate, s);
+        return st;
     }
-    return st;
+    }
 }
 
 int launch_applyh(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec, int accumulate,
                   cudaStream_t s) {
+    if (ctx->args.max_nbd > 8192)
+        return set_err(ctx, BSG_ERR_UNSUPPORTED, "a neutron sector jump has more than 8192 distinct (b,d) pairs");
     if (prec == BSG_PREC_FP32)
         return launch_typed<float>(ctx, (const float *)vin, (float *)vout, nb, accumulate, s);
     return launch_typed<double>(ctx, (const double *)vin, (double *)vout, nb, accumulate, s);

@@ -149,6 +149,11 @@ int derive(bsg_ctx *ctx, const bsg_tables *t) {
         ctx->h_rowlen[p] = (int32_t)len;
     }
     ctx->max_rowlen = *std::max_element(ctx->h_rowlen.begin(), ctx->h_rowlen.end());
+    {
+        std::vector<int32_t> tmp(ctx->h_rowlen);
+        std::nth_element(tmp.begin(), tmp.begin() + tmp.size() / 2, tmp.end());
+        ctx->median_rowlen = tmp[tmp.size() / 2];
+    }
     for (int64_t n = 0; n < t->nsd_n; ++n)
         if (t->nstart[n] < 1 || t->nstart[n] > ctx->max_rowlen)
             return set_err(ctx, BSG_ERR_OOB_INDEX, "nstart out of range at neutron SD " + std::to_string(n + 1));
@@ -192,6 +197,7 @@ int derive(bsg_ctx *ctx, const bsg_tables *t) {
     std::vector<PNRec> pnrec_all;
     std::vector<NNRec> nnrec_all;
     std::vector<int32_t> nnrec_op_all;
+    std::vector<BDPair> bd_all;
     auto get_nop = [&](int kind, int dir, int64_t x0, int64_t x1, int32_t &id) -> int {
         NKey k{kind, dir, x0, x1};
         auto it = nop_id.find(k);
@@ -203,6 +209,8 @@ int derive(bsg_ctx *ctx, const bsg_tables *t) {
         op.kind = kind;
         if (kind == 1) {
             std::vector<PNRec> recs(n);
+            std::vector<int32_t> bdk((size_t)ld * ld, -1);
+            std::vector<BDPair> bdl;
             for (int64_t x = x0; x <= x1; ++x) {
                 const int64_t isd = t->n1b_isd[x - 1], fsd = t->n1b_fsd[x - 1];
                 const int b = t->n1b_cop[x - 1], d = t->n1b_dop[x - 1];
@@ -212,23 +220,31 @@ int derive(bsg_ctx *ctx, const bsg_tables *t) {
                     return V.fail("n1b_cop/dop outside the neutron half spaces at jump " + std::to_string(x));
                 const int ph = t->n1b_phase[x - 1];
                 if (ph != 1 && ph != -1) return V.fail("n1b_phase not +-1");
+                int32_t &kk = bdk[(size_t)(b + nl_n) * ld + (d + nl_n)];
+                if (kk < 0) {
+                    kk = (int32_t)bdl.size();
+                    bdl.push_back(BDPair{(uint8_t)(b + nl_n), (uint8_t)(d + nl_n)});
+                }
                 PNRec r;
                 r.in = (int32_t)((dir == 0 ? isd : fsd) - 1);
                 out[x - x0] = (int32_t)((dir == 0 ? fsd : isd) - 1);
-                r.b = (uint8_t)(b + nl_n);
-                r.d = (uint8_t)(d + nl_n);
+                r.k = (uint16_t)kk;
                 r.ph = (int8_t)ph;
                 r.pad = 0;
                 recs[x - x0] = r;
                 maxin = std::max(maxin, r.in);
                 maxout = std::max(maxout, out[x - x0]);
             }
+            if (bdl.size() > 65535) return V.fail("too many distinct (b,d) pairs in a neutron sector jump");
             std::vector<int32_t> ptr;
             std::vector<PNRec> sorted;
             csr_by_out(out, recs, maxout + 1, ptr, sorted);
             op.rec_base = (int64_t)pnrec_all.size();
             op.ptr_base = (int64_t)nptr_all.size();
             op.nout = maxout + 1;
+            op.bd_base = (int32_t)bd_all.size();
+            op.nbd = (int32_t)bdl.size();
+            bd_all.insert(bd_all.end(), bdl.begin(), bdl.end());
             pnrec_all.insert(pnrec_all.end(), sorted.begin(), sorted.end());
             nptr_all.insert(nptr_all.end(), ptr.begin(), ptr.end());
         } else {
@@ -411,15 +427,70 @@ int derive(bsg_ctx *ctx, const bsg_tables *t) {
     ctx->stats.n_ops_nn = ops[2];
     ctx->stats.n_ops_pn = ops[3];
 
-    // ---- flatten into per-row CSR (stable: keeps bundle order inside a row;
-    // PN contributions grouped by neutron operator for cache reuse)
-    auto by_row = [&](auto &v, std::vector<int32_t> &ptr, auto &flat, std::vector<int32_t> *perm) {
+    // ---- assign each row's contributions to the kWarps warps of its CTA by
+    // longest-processing-time (heaviest first to the least loaded warp), then
+    // flatten into CSR over (row, warp) slots.  Inside a slot the bundle order
+    // is kept (PN grouped by neutron operator for cache reuse).
+    std::stable_sort(pn.begin(), pn.end(), [](const std::pair<int32_t, PNContrib> &x, const std::pair<int32_t, PNContrib> &y) {
+        if (x.first != y.first) return x.first < y.first;
+        return x.second.nop < y.second.nop;
+    });
+    auto nrec_of = [&](int32_t id) -> int64_t { return nptr_all[nops[id].ptr_base + nops[id].nout]; };
+    const int W = kRowWarps;
+    std::vector<uint8_t> w_pp(pp.size()), w_nn(nn.size()), w_pn(pn.size()), w_spe(spe.size());
+    {
+        struct Ref { int64_t wgt; int8_t type; int32_t idx; };
+        std::vector<std::vector<int32_t>> by[4];
+        for (int k = 0; k < 4; ++k) by[k].assign(0, {});
+        std::vector<int32_t> cnt[4], start[4];
+        auto bucket = [&](auto &v, int k) {
+            cnt[k].assign(nrows + 1, 0);
+            for (auto &e : v) cnt[k][e.first + 1]++;
+            for (int64_t r = 0; r < nrows; ++r) cnt[k][r + 1] += cnt[k][r];
+            start[k].assign(v.size(), 0);
+            std::vector<int32_t> fill(cnt[k].begin(), cnt[k].end() - 1);
+            for (size_t i = 0; i < v.size(); ++i) start[k][fill[v[i].first]++] = (int32_t)i;
+        };
+        bucket(pp, 0); bucket(nn, 1); bucket(pn, 2); bucket(spe, 3);
+        std::vector<Ref> refs;
+        for (int64_t r = 0; r < nrows; ++r) {
+            refs.clear();
+            for (int32_t q = cnt[0][r]; q < cnt[0][r + 1]; ++q) {
+                const auto &c = pp[start[0][q]].second;
+                refs.push_back({(int64_t)(c.hi - c.lo + 1), 0, start[0][q]});
+            }
+            for (int32_t q = cnt[1][r]; q < cnt[1][r + 1]; ++q)
+                refs.push_back({nrec_of(nn[start[1][q]].second.nop) + 32, 1, start[1][q]});
+            for (int32_t q = cnt[2][r]; q < cnt[2][r + 1]; ++q) {
+                const int32_t id = pn[start[2][q]].second.nop;
+                refs.push_back({nrec_of(id) + nops[id].nbd + 32, 2, start[2][q]});
+            }
+            for (int32_t q = cnt[3][r]; q < cnt[3][r + 1]; ++q) {
+                const auto &c = spe[start[3][q]].second;
+                refs.push_back({(int64_t)(c.hi - c.lo + 1), 3, start[3][q]});
+            }
+            std::stable_sort(refs.begin(), refs.end(), [](const Ref &x, const Ref &y) { return x.wgt > y.wgt; });
+            int64_t load[kRowWarps] = {0};
+            for (const Ref &f : refs) {
+                int best = 0;
+                for (int w = 1; w < W; ++w)
+                    if (load[w] < load[best]) best = w;
+                load[best] += f.wgt;
+                (f.type == 0 ? w_pp : f.type == 1 ? w_nn : f.type == 2 ? w_pn : w_spe)[f.idx] = (uint8_t)best;
+            }
+        }
+    }
+    auto by_slot = [&](auto &v, const std::vector<uint8_t> &wv, std::vector<int32_t> &ptr, auto &flat,
+                       std::vector<int32_t> *perm) {
+        const int64_t nslot = nrows * W;
+        std::vector<int64_t> key(v.size());
+        for (size_t i = 0; i < v.size(); ++i) key[i] = (int64_t)v[i].first * W + wv[i];
         std::vector<size_t> idx(v.size());
         std::iota(idx.begin(), idx.end(), 0);
-        std::stable_sort(idx.begin(), idx.end(), [&](size_t x, size_t y) { return v[x].first < v[y].first; });
-        ptr.assign(nrows + 1, 0);
-        for (auto &e : v) ptr[e.first + 1]++;
-        for (int64_t r = 0; r < nrows; ++r) ptr[r + 1] += ptr[r];
+        std::stable_sort(idx.begin(), idx.end(), [&](size_t x, size_t y) { return key[x] < key[y]; });
+        ptr.assign(nslot + 1, 0);
+        for (int64_t k : key) ptr[k + 1]++;
+        for (int64_t r = 0; r < nslot; ++r) ptr[r + 1] += ptr[r];
         flat.resize(v.size());
         if (perm) perm->resize(v.size());
         for (size_t k = 0; k < idx.size(); ++k) {
@@ -427,18 +498,16 @@ int derive(bsg_ctx *ctx, const bsg_tables *t) {
             if (perm) (*perm)[k] = (int32_t)idx[k];
         }
     };
-    std::stable_sort(pn.begin(), pn.end(), [](const std::pair<int32_t, PNContrib> &x, const std::pair<int32_t, PNContrib> &y) {
-        if (x.first != y.first) return x.first < y.first;
-        return x.second.nop < y.second.nop;
-    });
+    if (pp.size() > (size_t)INT32_MAX || pn.size() > (size_t)INT32_MAX)
+        return set_err(ctx, BSG_ERR_UNSUPPORTED, "more than 2^31 row contributions");
     std::vector<int32_t> spe_ptr, pp_perm;
     std::vector<SPEContrib> h_spe;
-    by_row(pp, ctx->h_pp_ptr, ctx->h_pp, &pp_perm);
+    by_slot(pp, w_pp, ctx->h_pp_ptr, ctx->h_pp, &pp_perm);
     ctx->h_pp_op.resize(pp_perm.size());
     for (size_t k = 0; k < pp_perm.size(); ++k) ctx->h_pp_op[k] = pp_op_tmp[pp_perm[k]];
-    by_row(nn, ctx->h_nn_ptr, ctx->h_nn, nullptr);
-    by_row(pn, ctx->h_pn_ptr, ctx->h_pn, nullptr);
-    by_row(spe, spe_ptr, h_spe, nullptr);
+    by_slot(nn, w_nn, ctx->h_nn_ptr, ctx->h_nn, nullptr);
+    by_slot(pn, w_pn, ctx->h_pn_ptr, ctx->h_pn, nullptr);
+    by_slot(spe, w_spe, spe_ptr, h_spe, nullptr);
     ctx->h_nops = nops;
     ctx->h_nnrec_op = nnrec_op_all;
 
@@ -446,15 +515,9 @@ int derive(bsg_ctx *ctx, const bsg_tables *t) {
     ctx->h_work.assign(nrows, 0);
     for (int64_t r = 0; r < nrows; ++r) {
         int64_t w = 0;
-        for (int32_t c = ctx->h_pp_ptr[r]; c < ctx->h_pp_ptr[r + 1]; ++c) w += ctx->h_pp[c].hi - ctx->h_pp[c].lo + 1;
-        for (int32_t c = ctx->h_nn_ptr[r]; c < ctx->h_nn_ptr[r + 1]; ++c) {
-            const NOp &o = nops[ctx->h_nn[c].nop];
-            w += nptr_all[o.ptr_base + o.nout];
-        }
-        for (int32_t c = ctx->h_pn_ptr[r]; c < ctx->h_pn_ptr[r + 1]; ++c) {
-            const NOp &o = nops[ctx->h_pn[c].nop];
-            w += nptr_all[o.ptr_base + o.nout];
-        }
+        for (int32_t c = ctx->h_pp_ptr[r * W]; c < ctx->h_pp_ptr[(r + 1) * W]; ++c) w += ctx->h_pp[c].hi - ctx->h_pp[c].lo + 1;
+        for (int32_t c = ctx->h_nn_ptr[r * W]; c < ctx->h_nn_ptr[(r + 1) * W]; ++c) w += nrec_of(ctx->h_nn[c].nop);
+        for (int32_t c = ctx->h_pn_ptr[r * W]; c < ctx->h_pn_ptr[(r + 1) * W]; ++c) w += nrec_of(ctx->h_pn[c].nop);
         ctx->h_work[r] = (int32_t)std::min<int64_t>(w, INT32_MAX);
     }
 
@@ -501,6 +564,7 @@ int derive(bsg_ctx *ctx, const bsg_tables *t) {
         (st = up(ctx->nptr, nptr_all.data(), 4 * nptr_all.size())) ||
         (st = up(ctx->pnrec, pnrec_all.data(), sizeof(PNRec) * pnrec_all.size())) ||
         (st = up(ctx->nnrec, nnrec_all.data(), sizeof(NNRec) * nnrec_all.size())) ||
+        (st = up(ctx->bd, bd_all.data(), sizeof(BDPair) * bd_all.size())) ||
         (st = up(ctx->cpn, cpn32.data(), 4 * cpn32.size())) || (st = up(ctx->dpn, dpn32.data(), 4 * dpn32.size())) ||
         (st = up(ctx->nspe, nspe.data(), 4 * nspe.size())) ||
         (st = up(ctx->pp_op, ctx->h_pp_op.data(), 4 * ctx->h_pp_op.size())) ||
@@ -530,6 +594,13 @@ int derive(bsg_ctx *ctx, const bsg_tables *t) {
     a.nptr = (const int32_t *)ctx->nptr.p;
     a.pnrec = (const PNRec *)ctx->pnrec.p;
     a.nnrec = (const NNRec *)ctx->nnrec.p;
+    a.bd = (const BDPair *)ctx->bd.p;
+    int32_t max_nbd = 0;
+    for (auto &o : nops) max_nbd = std::max(max_nbd, o.nbd);
+    a.max_nbd = max_nbd;
+    ctx->h_bd = bd_all;
+    ctx->h_pnrec = pnrec_all;
+    ctx->h_nptr = nptr_all;
     a.hmatpn = (const float *)ctx->hmatpn.p;
     a.cpn = (const int32_t *)ctx->cpn.p;
     a.dpn = (const int32_t *)ctx->dpn.p;
@@ -542,7 +613,7 @@ int derive(bsg_ctx *ctx, const bsg_tables *t) {
 void free_ctx(bsg_ctx *ctx) {
     for (auto &b : ctx->raw) dev_free(b);
     DevBuf *bufs[] = {&ctx->row_off, &ctx->pp_ptr, &ctx->nn_ptr, &ctx->pn_ptr, &ctx->spe_ptr, &ctx->pp, &ctx->nn,
-                      &ctx->pn, &ctx->spe, &ctx->nops, &ctx->nptr, &ctx->pnrec, &ctx->nnrec, &ctx->hmatpn,
+                      &ctx->pn, &ctx->spe, &ctx->nops, &ctx->nptr, &ctx->pnrec, &ctx->nnrec, &ctx->bd, &ctx->hmatpn,
                       &ctx->cpn, &ctx->dpn, &ctx->nspe, &ctx->pp_op, &ctx->nnrec_op, &ctx->hmatpp_d,
                       &ctx->hmatnn_d, &ctx->scratch_in, &ctx->scratch_out};
     for (DevBuf *b : bufs) dev_free(*b);
@@ -622,14 +693,13 @@ int bsg_destroy(bsg_ctx *ctx) {
     return BSG_OK;
 }
 
-int bsg_applyh_stream(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec, int flags, void *stream) {
-    if (!ctx) return BSG_ERR_ARG;
+namespace {
+int applyh_on(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec, int flags, cudaStream_t s) {
     if (!vin || !vout || nb < 1 || nb > 64 || (prec != BSG_PREC_FP32 && prec != BSG_PREC_FP64))
         return set_err(ctx, BSG_ERR_ARG, "bsg_applyh: bad arguments");
     if (vin == vout) return set_err(ctx, BSG_ERR_ARG, "bsg_applyh: vin and vout must not alias");
     int st = cuda_check(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
     if (st) return st;
-    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
     const int acc = (flags & BSG_ACCUMULATE) ? 1 : 0;
     if (flags & BSG_DEVICE_PTRS) return launch_applyh(ctx, vin, vout, nb, prec, acc, s);
     // host pointers: copy in, apply, copy out (the drop-in path for vec1/vec2)
@@ -645,8 +715,19 @@ int bsg_applyh_stream(bsg_ctx *ctx, const void *vin, void *vout, int nb, int pre
     return st;
 }
 
+}  // namespace
+
+// stream: the caller's cudaStream_t; NULL means the legacy default stream
+int bsg_applyh_stream(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec, int flags, void *stream) {
+    if (!ctx) return BSG_ERR_ARG;
+    return applyh_on(ctx, vin, vout, nb, prec, flags, (cudaStream_t)stream);
+}
+
+// runs on the context's own stream and returns when the result is in vout
+// (host pointers) or when the kernel has been queued (device pointers)
 int bsg_applyh(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec, int flags) {
-    return bsg_applyh_stream(ctx, vin, vout, nb, prec, flags, nullptr);
+    if (!ctx) return BSG_ERR_ARG;
+    return applyh_on(ctx, vin, vout, nb, prec, flags, ctx->stream);
 }
 
 int bsg_get_stats(const bsg_ctx *ctx, bsg_stats *st) {

@@ -12,6 +12,9 @@
 
 namespace bsg {
 
+// warps per applyH CTA; each row's contributions are split over them
+constexpr int kRowWarps = 8;
+
 // ---- derived (device) layouts, built once at bsg_create from the unchanged
 // tables.  Positions are 0-based neutron positions inside a proton-SD row
 // (position = nstart - 1); a row's first basis state (0-based) is pstart(ip).
@@ -49,13 +52,20 @@ struct NOp {
     int64_t ptr_base;   // first entry of its [nout+1] pointer array
     int32_t nout;
     int32_t kind;       // 0 = NN (me records), 1 = PN (label records)
+    int32_t bd_base;    // PN: first entry of its distinct (b,d) list
+    int32_t nbd;        // PN: number of distinct (b,d) neutron label pairs
 };
-// PN record: input position and the neutron creation/destruction columns
+// PN record: input position, index of its (b,d) pair in the operator's
+// distinct-pair list, neutron jump phase
 struct PNRec {
     int32_t in;
-    uint8_t b, d;       // b + nhsps(-2), d + nhsps(-2): row of cpnpair/dpnpair
+    uint16_t k;         // (b,d) pair = bd_list[bd_base + k]
     int8_t ph;
     int8_t pad;
+};
+// distinct (b,d) pair of a PN neutron operator: rows of cpnpair/dpnpair
+struct BDPair {
+    uint8_t b, d;       // b + nhsps(-2), d + nhsps(-2)
 };
 // NN record: input position and hmatnn(op)*phase
 struct NNRec {
@@ -71,7 +81,7 @@ struct Tile {
 
 struct RowArgs {
     const int64_t *row_off;       // [nrows] pstart
-    const int32_t *pp_ptr, *nn_ptr, *pn_ptr, *spe_ptr;  // [nrows+1]
+    const int32_t *pp_ptr, *nn_ptr, *pn_ptr, *spe_ptr;  // [nrows*kRowWarps+1] (row, warp) slots
     const PPContrib *pp;
     const NNContrib *nn;
     const PNContrib *pn;
@@ -80,11 +90,13 @@ struct RowArgs {
     const int32_t *nptr;          // pointer arrays of all neutron ops
     const PNRec *pnrec;
     const NNRec *nnrec;
+    const BDPair *bd;
     const float *hmatpn;
     const int32_t *cpn, *dpn;     // cpnpair/dpnpair as int32 (validated)
     const float *nspe;
     int32_t ld_cpn;               // nhsps(-2)+nhsps(2)+1
     int32_t ncpn;                 // entries of cpn
+    int32_t max_nbd;              // largest nbd of any PN operator
     const Tile *tiles;
     int32_t ntiles;
     int32_t accumulate;
@@ -109,15 +121,19 @@ struct bsg_ctx {
     bsg_tables t{};           // sizes only (pointers are host-owned by caller)
     int64_t dim = 0, nrows = 0;
     int32_t max_rowlen = 0;
+    int32_t median_rowlen = 0;
     int32_t max_nb = 16;
     // raw tables on the device (byte-identical copies)
     std::vector<bsg::DevBuf> raw;
     // derived
-    bsg::DevBuf row_off, pp_ptr, nn_ptr, pn_ptr, spe_ptr, pp, nn, pn, spe, nops, nptr, pnrec, nnrec;
+    bsg::DevBuf row_off, pp_ptr, nn_ptr, pn_ptr, spe_ptr, pp, nn, pn, spe, nops, nptr, pnrec, nnrec, bd;
     bsg::DevBuf hmatpn, cpn, dpn, nspe, hmatpp_d, hmatnn_d;
     bsg::RowArgs args{};
     std::map<int, bsg::TileSet> tiles;   // tile size -> tiles
     std::vector<int32_t> h_rowlen;
+    std::vector<bsg::BDPair> h_bd;
+    std::vector<bsg::PNRec> h_pnrec;
+    std::vector<int32_t> h_nptr;
     std::vector<int32_t> h_work;         // per-row work estimate
     // host copies kept for the adjoint
     std::vector<int32_t> h_pp_ptr, h_nn_ptr, h_pn_ptr;

@@ -1,0 +1,499 @@
+// bsg_lanczos: scalar and block Lanczos with full reorthogonalization and
+// thick restart, everything on the device in FP64 except the applyH call
+// (FP32 or FP64 as requested).
+//
+// Restates lanczos_p (src/blanczosmain.f90:1413-1793) and lanczos_block
+// (:1804-2153):
+//   * pivot: uniform 1/sqrt(dim) (initialize_lanczos_vector option 0,
+//     src/blanczoslib.f90:825-831); block pivots are seeded pseudo-random
+//     columns (the reference uses the compiler's random_number,
+//     src/bblock_algebra.f90:107-113, which is not reproducible);
+//   * each step: W = H V_i; alpha = V_i^T W; W -= V_i alpha
+//     (br_remove_prev_overlap / grab_alpha_blockv2); one classical
+//     Gram-Schmidt pass against every earlier history vector
+//     (br_orthogonalize(1) / compute_W); scalar: beta = |W|, V_{i+1} = W/beta
+//     (br_normalize); block: S = W^T W = U L U^T, beta = L^1/2 U^T,
+//     V_{i+1} = W U L^-1/2 (spectral_decomp, src/bblock_algebra.f90:684-856);
+//   * beta collapse (beta < 1e-4 beta_prev) -> random restart against the
+//     history (random_restart_with_history, src/breorthog.f90:1471-1482);
+//     beta < 0.1 beta_prev -> second full Gram-Schmidt pass
+//     (src/blanczosmain.f90:1634-1660);
+//   * projected matrix: tridiagonal / band plus the arrow left by thick
+//     restart (src/blanczoslib.f90:195-221); its lowest eigenvalues for the
+//     convergence test come from Sturm bisection (scalar) or Jacobi (block)
+//     on the device;
+//   * convergence_test option 0 (src/blanczoslib.f90:2660-2800): mean energy
+//     change over ncheck states, scaled by (1+restarts)/sqrt(ncheck+1),
+//     below converge_tol;
+//   * thick restart when the next step would be the niter-th
+//     (thick_restart_sub_p, src/blanczoslib.f90:1656-1894): Ritz pairs of the
+//     projected matrix without its last block, alpha_i = theta_i,
+//     coupling beta_prev * y_last,i, basis V <- V Y (br_transform_basis), the
+//     last Lanczos block continues the recursion.
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "bsg_internal.h"
+#include "lanczos_kernels.h"
+
+using namespace bsg;
+
+namespace bsg {
+cudaError_t random_cols(double *W, int nB, int64_t n, int64_t ld, uint64_t seed, cudaStream_t s);
+}
+
+namespace {
+
+struct Lz {
+    bsg_ctx *ctx;
+    cudaStream_t s;
+    int64_t n;
+    int nb, prec;
+    int maxcol;      // history columns
+    DevBuf hist, W, X, Y, tmp, partial, coef, sqp, sq, Adev, Vtmp, Zdev, wdev, stat, al, bt, ev, M;
+    std::vector<double> T;  // host projected matrix (maxcol x maxcol), row-major
+    float t_mv = 0, t_ort = 0, t_eig = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+
+    double *col(int j) { return (double *)hist.p + (int64_t)j * n; }
+    double &Tm(int i, int j) { return T[(size_t)i * maxcol + j]; }
+};
+
+#define CK(expr)                                              \
+    do {                                                      \
+        cudaError_t _e = (expr);                              \
+        if (_e != cudaSuccess) return cuda_check(L.ctx, _e, #expr); \
+    } while (0)
+#define ST(expr)                 \
+    do {                         \
+        int _s = (expr);         \
+        if (_s != BSG_OK) return _s; \
+    } while (0)
+
+float elapsed(Lz &L) {
+    float ms = 0.f;
+    cudaEventSynchronize(L.e1);
+    cudaEventElapsedTime(&ms, L.e0, L.e1);
+    return ms;
+}
+
+// dense symmetric eigenproblem of T[0:m,0:m] on the device; evals (host) and
+// optionally eigenvectors (host, row-major m x m, column j = vector j)
+int eig_dense(Lz &L, int m, std::vector<double> &w, std::vector<double> *Z) {
+    std::vector<double> A((size_t)m * m);
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j) A[(size_t)i * m + j] = 0.5 * (L.Tm(i, j) + L.Tm(j, i));
+    cudaEventRecord(L.e0, L.s);
+    CK(cudaMemcpyAsync(L.Adev.p, A.data(), sizeof(double) * m * m, cudaMemcpyHostToDevice, L.s));
+    CK(jacobi(m, (double *)L.Adev.p, (double *)L.Vtmp.p, (double *)L.wdev.p, (double *)L.Zdev.p, (int *)L.stat.p, L.s));
+    w.resize(m);
+    CK(cudaMemcpyAsync(w.data(), L.wdev.p, sizeof(double) * m, cudaMemcpyDeviceToHost, L.s));
+    int st = 0;
+    CK(cudaMemcpyAsync(&st, L.stat.p, sizeof(int), cudaMemcpyDeviceToHost, L.s));
+    if (Z) {
+        Z->resize((size_t)m * m);
+        CK(cudaMemcpyAsync(Z->data(), L.Zdev.p, sizeof(double) * m * m, cudaMemcpyDeviceToHost, L.s));
+    }
+    cudaEventRecord(L.e1, L.s);
+    CK(cudaStreamSynchronize(L.s));
+    L.t_eig += elapsed(L);
+    if (st) return set_err(L.ctx, BSG_ERR_NOT_CONVERGED, "Jacobi eigensolver did not converge");
+    return BSG_OK;
+}
+
+// lowest nwant eigenvalues of the scalar projected matrix (arrow k, size m)
+int eig_arrow(Lz &L, int m, int k, int nwant, std::vector<double> &e) {
+    std::vector<double> al(m), bt(std::max(m, 1), 0.0);
+    for (int i = 0; i < m; ++i) al[i] = L.Tm(i, i);
+    for (int i = 0; i < k; ++i) bt[i] = L.Tm(k, i);
+    for (int i = k; i + 1 < m; ++i) bt[i] = L.Tm(i + 1, i);
+    // Gershgorin bounds
+    double glo = 1e300, ghi = -1e300;
+    for (int i = 0; i < m; ++i) {
+        double r = 0.0;
+        if (i < k) r = std::fabs(bt[i]);
+        if (i == k) for (int j = 0; j < k; ++j) r += std::fabs(bt[j]);
+        if (i >= k && i + 1 < m) r += std::fabs(bt[i]);
+        if (i > k) r += std::fabs(bt[i - 1]);
+        glo = std::min(glo, al[i] - r);
+        ghi = std::max(ghi, al[i] + r);
+    }
+    const double pad = 1e-12 * std::max(std::fabs(glo), std::fabs(ghi)) + 1e-300;
+    glo -= pad;
+    ghi += pad;
+    nwant = std::min(nwant, m);
+    cudaEventRecord(L.e0, L.s);
+    CK(cudaMemcpyAsync(L.al.p, al.data(), sizeof(double) * m, cudaMemcpyHostToDevice, L.s));
+    CK(cudaMemcpyAsync(L.bt.p, bt.data(), sizeof(double) * m, cudaMemcpyHostToDevice, L.s));
+    CK(bisect_arrow(m, k, (const double *)L.al.p, (const double *)L.bt.p, nwant, glo, ghi, (double *)L.ev.p, L.s));
+    e.resize(nwant);
+    CK(cudaMemcpyAsync(e.data(), L.ev.p, sizeof(double) * nwant, cudaMemcpyDeviceToHost, L.s));
+    cudaEventRecord(L.e1, L.s);
+    CK(cudaStreamSynchronize(L.s));
+    L.t_eig += elapsed(L);
+    return BSG_OK;
+}
+
+// classical Gram-Schmidt of W (nb columns) against history columns [0, k);
+// optional column sums of squares into host sq
+int cgs(Lz &L, int k, std::vector<double> *sq) {
+    double *C = (double *)L.coef.p;
+    if (k > 0) CK(multidot(L.col(0), k, (const double *)L.W.p, L.nb, L.n, L.n, (double *)L.partial.p, C, L.s));
+    CK(sub_gemv(L.col(0), k, C, (double *)L.W.p, L.nb, L.n, L.n, sq ? (double *)L.sqp.p : nullptr,
+                sq ? (double *)L.sq.p : nullptr, L.s));
+    if (sq) {
+        sq->resize(L.nb);
+        CK(cudaMemcpyAsync(sq->data(), L.sq.p, sizeof(double) * L.nb, cudaMemcpyDeviceToHost, L.s));
+        CK(cudaStreamSynchronize(L.s));
+    }
+    return BSG_OK;
+}
+
+// V_{next} (nb columns at history column `dst`) from W: scalar normalization
+// or the block spectral decomposition; returns the beta block (nb x nb,
+// row-major beta[a][c]) and the smallest overlap eigenvalue
+int next_block(Lz &L, int dst, const std::vector<double> &sq, std::vector<double> &beta, double &lmin, double &lmax) {
+    const int nb = L.nb;
+    beta.assign((size_t)nb * nb, 0.0);
+    if (nb == 1) {
+        const double b = std::sqrt(std::max(sq[0], 0.0));
+        beta[0] = b;
+        lmin = lmax = sq[0];
+        if (b == 0.0) return BSG_OK;
+        const double inv = 1.0 / b;
+        CK(cudaMemcpyAsync(L.M.p, &inv, sizeof(double), cudaMemcpyHostToDevice, L.s));
+        CK(scale_cols((const double *)L.W.p, L.col(dst), (const double *)L.M.p, 1, L.n, L.n, L.s));
+        return BSG_OK;
+    }
+    // S = W^T W -> U L U^T
+    CK(multidot((const double *)L.W.p, nb, (const double *)L.W.p, nb, L.n, L.n, (double *)L.partial.p,
+                (double *)L.coef.p, L.s));
+    std::vector<double> S((size_t)nb * nb);
+    CK(cudaMemcpyAsync(S.data(), L.coef.p, sizeof(double) * nb * nb, cudaMemcpyDeviceToHost, L.s));
+    CK(cudaStreamSynchronize(L.s));
+    std::vector<double> A((size_t)nb * nb), w, Z;
+    for (int i = 0; i < nb; ++i)
+        for (int j = 0; j < nb; ++j) A[(size_t)i * nb + j] = 0.5 * (S[(size_t)i * nb + j] + S[(size_t)j * nb + i]);
+    CK(cudaMemcpyAsync(L.Adev.p, A.data(), sizeof(double) * nb * nb, cudaMemcpyHostToDevice, L.s));
+    CK(jacobi(nb, (double *)L.Adev.p, (double *)L.Vtmp.p, (double *)L.wdev.p, (double *)L.Zdev.p, (int *)L.stat.p, L.s));
+    w.resize(nb);
+    Z.resize((size_t)nb * nb);
+    CK(cudaMemcpyAsync(w.data(), L.wdev.p, sizeof(double) * nb, cudaMemcpyDeviceToHost, L.s));
+    CK(cudaMemcpyAsync(Z.data(), L.Zdev.p, sizeof(double) * nb * nb, cudaMemcpyDeviceToHost, L.s));
+    CK(cudaStreamSynchronize(L.s));
+    lmin = w[0];
+    lmax = w[nb - 1];
+    // beta = L^1/2 U^T ; M = U L^-1/2
+    std::vector<double> Mh((size_t)nb * nb);
+    for (int a = 0; a < nb; ++a) {
+        const double l = std::max(w[a], 0.0);
+        const double sl = std::sqrt(l), il = (l > 0.0) ? 1.0 / sl : 0.0;
+        for (int c = 0; c < nb; ++c) {
+            beta[(size_t)a * nb + c] = sl * Z[(size_t)c * nb + a];  // (L^1/2 U^T)[a][c] = sqrt(l_a) U[c][a]
+            Mh[(size_t)c * nb + a] = Z[(size_t)c * nb + a] * il;     // (U L^-1/2)[c][a]
+        }
+    }
+    CK(cudaMemcpyAsync(L.M.p, Mh.data(), sizeof(double) * nb * nb, cudaMemcpyHostToDevice, L.s));
+    CK(transform((const double *)L.W.p, nb, (const double *)L.M.p, nb, nb, L.col(dst), L.n, L.n, L.n, L.s));
+    return BSG_OK;
+}
+
+int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, double *evecs, bsg_report *rep) {
+    bsg_ctx *ctx = L.ctx;
+    const int nb = L.nb;
+    const int64_t n = L.n;
+    const int nkeep = p->nkeep, niter = p->niter;
+    const bool thick = (p->nthick_add > 0 || p->max_restarts > 0);
+    const int nthick = std::min(nkeep + std::max(p->nthick_add, 0), niter * nb - 2 * nb);
+    const int ncheck = std::max(1, p->ncheck > 0 ? p->ncheck : nkeep + 5);
+    const double tol = p->converge_tol > 0 ? p->converge_tol : 1e-3;
+    L.maxcol = niter * nb + nb;
+    L.T.assign((size_t)L.maxcol * L.maxcol, 0.0);
+
+    // ---- pivot block into history columns [0, nb)
+    if (pivot) {
+        std::vector<double> hp((size_t)n * nb);
+        for (int64_t s_ = 0; s_ < n; ++s_)
+            for (int b = 0; b < nb; ++b) hp[(size_t)b * n + s_] = pivot[(size_t)s_ * nb + b];
+        CK(cudaMemcpyAsync(L.W.p, hp.data(), sizeof(double) * n * nb, cudaMemcpyHostToDevice, L.s));
+        CK(cudaStreamSynchronize(L.s));
+    } else if (nb == 1) {
+        std::vector<double> hp(n, 1.0 / std::sqrt((double)n));
+        CK(cudaMemcpyAsync(L.W.p, hp.data(), sizeof(double) * n, cudaMemcpyHostToDevice, L.s));
+        CK(cudaStreamSynchronize(L.s));
+    } else {
+        CK(random_cols((double *)L.W.p, nb, n, n, p->seed, L.s));
+    }
+    std::vector<double> sq, beta;
+    double lmin, lmax;
+    ST(cgs(L, 0, &sq));
+    ST(next_block(L, 0, sq, beta, lmin, lmax));
+    if (lmax <= 0.0 || lmin <= 1e-14 * lmax) return set_err(ctx, BSG_ERR_ARG, "pivot block is rank deficient");
+
+    int cur = 0;          // first history column of the current block
+    int mT = 0;           // size of the valid projected matrix
+    int restarts = 0, rnd = 0, total = 0, matvecs = 0;
+    int karrow = 0;       // arrow size of the projected matrix after a thick restart
+    double beta_prev = -1.0;
+    bool finished = false, converged = false;
+    std::vector<double> eold, e;
+    int iter = 0;         // block iterations in this cycle (the reference's iter)
+    while (!finished) {
+        ++iter;
+        ++total;
+        // ---- W = H V
+        CK(pack(L.col(cur), nb, n, n, L.X.p, L.prec, L.s));
+        cudaEventRecord(L.e0, L.s);
+        ST(launch_applyh(ctx, L.X.p, L.Y.p, nb, L.prec, 0, L.s));
+        cudaEventRecord(L.e1, L.s);
+        CK(unpack(L.Y.p, nb, n, n, (double *)L.W.p, L.prec, L.s));
+        ++matvecs;
+        L.t_mv += elapsed(L);
+        // ---- alpha = V^T W ; W -= V alpha ; CGS against [0, cur)
+        cudaEventRecord(L.e0, L.s);
+        CK(multidot(L.col(cur), nb, (const double *)L.W.p, nb, n, n, (double *)L.partial.p, (double *)L.coef.p, L.s));
+        std::vector<double> alpha((size_t)nb * nb);
+        CK(cudaMemcpyAsync(alpha.data(), L.coef.p, sizeof(double) * nb * nb, cudaMemcpyDeviceToHost, L.s));
+        CK(sub_gemv(L.col(cur), nb, (const double *)L.coef.p, (double *)L.W.p, nb, n, n, nullptr, nullptr, L.s));
+        ST(cgs(L, cur, &sq));
+        // ---- scalar beta checks (src/blanczosmain.f90:1634-1660)
+        if (nb == 1 && iter > 1 && beta_prev > 0.0) {
+            const double b = std::sqrt(std::max(sq[0], 0.0));
+            if (b < 1e-4 * beta_prev) {
+                // random restart: keep the tiny beta, continue from a random
+                // direction orthogonal to the whole history
+                CK(random_cols((double *)L.W.p, 1, n, n, p->seed + 7919ull * (uint64_t)(rnd + 1), L.s));
+                ST(cgs(L, cur + 1, &sq));
+                ST(cgs(L, cur + 1, &sq));
+                ++rnd;
+                std::vector<double> b2;
+                ST(next_block(L, cur + 1, sq, b2, lmin, lmax));
+                beta.assign(1, b);
+                goto stored;
+            } else if (b < 0.1 * beta_prev) {
+                ST(cgs(L, cur + 1, &sq));  // second full pass, v_i included
+            }
+        }
+        if (nb > 1) {
+            // block: guard against a rank-deficient residual block
+            ST(next_block(L, cur + nb, sq, beta, lmin, lmax));
+            if (lmin <= 1e-20 * std::max(lmax, 1.0)) {
+                CK(random_cols((double *)L.tmp.p, nb, n, n, p->seed + 104729ull * (uint64_t)(rnd + 1), L.s));
+                const double eps = 1e-7 * std::sqrt(std::max(lmax, 1e-30));
+                std::vector<double> e2(nb, eps);
+                CK(cudaMemcpyAsync(L.M.p, e2.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, L.s));
+                CK(scale_cols((const double *)L.tmp.p, (double *)L.tmp.p, (const double *)L.M.p, nb, n, n, L.s));
+                // W += eps R, then orthogonalize again
+                std::vector<double> one((size_t)nb * nb, 0.0);
+                for (int b = 0; b < nb; ++b) one[(size_t)b * nb + b] = -1.0;
+                CK(cudaMemcpyAsync(L.coef.p, one.data(), sizeof(double) * nb * nb, cudaMemcpyHostToDevice, L.s));
+                CK(sub_gemv((const double *)L.tmp.p, nb, (const double *)L.coef.p, (double *)L.W.p, nb, n, n,
+                            nullptr, nullptr, L.s));
+                ST(cgs(L, cur + nb, &sq));
+                ST(next_block(L, cur + nb, sq, beta, lmin, lmax));
+                ++rnd;
+            }
+        } else {
+            ST(next_block(L, cur + 1, sq, beta, lmin, lmax));
+        }
+    stored:
+        cudaEventRecord(L.e1, L.s);
+        CK(cudaStreamSynchronize(L.s));
+        L.t_ort += elapsed(L);
+        // ---- projected matrix
+        for (int a = 0; a < nb; ++a)
+            for (int c = 0; c < nb; ++c) {
+                const double v = 0.5 * (alpha[(size_t)a * nb + c] + alpha[(size_t)c * nb + a]);
+                L.Tm(cur + a, cur + c) = v;
+            }
+        for (int a = 0; a < nb; ++a)
+            for (int c = 0; c < nb; ++c) {
+                L.Tm(cur + nb + a, cur + c) = beta[(size_t)a * nb + c];
+                L.Tm(cur + c, cur + nb + a) = beta[(size_t)a * nb + c];
+            }
+        beta_prev = (nb == 1) ? beta[0] : 1.0;
+        mT = cur + nb;
+        cur += nb;
+        // ---- eigenvalues and convergence (convergence_test option 0)
+        if (cur >= niter * nb) finished = true;
+        if (!p->fixed_iter && mT > ncheck && mT < (int64_t)n) {
+            if (nb == 1)
+                ST(eig_arrow(L, mT, karrow, ncheck, e));
+            else {
+                std::vector<double> w;
+                ST(eig_dense(L, mT, w, nullptr));
+                e.assign(w.begin(), w.begin() + std::min<int>(ncheck, mT));
+            }
+            if ((int)eold.size() == (int)e.size()) {
+                double ed = 0.0;
+                for (size_t j = 0; j < e.size(); ++j) ed += std::fabs(eold[j] - e[j]);
+                ed = ed / std::sqrt((double)e.size() + 1.0) * (1.0 + restarts);
+                if (ed < tol) {
+                    finished = true;
+                    converged = true;
+                }
+            }
+            eold = e;
+        }
+        if (mT >= (int64_t)n) { finished = true; converged = true; }  // Krylov space exhausted
+        if (p->fixed_iter && finished) converged = true;
+        // ---- thick restart
+        if (thick && !finished && cur + nb > (niter - 1) * nb) {
+            if (restarts >= p->max_restarts) {
+                finished = true;
+                break;
+            }
+            const int m = mT - nb;           // projected matrix without its last block
+            const int k = std::min(nthick, m - 1);
+            std::vector<double> w, Z;
+            ST(eig_dense(L, m, w, &Z));
+            // coupling rows: beta_prev block between block [m-nb, m) and [m, m+nb)
+            std::vector<double> bp((size_t)nb * nb);
+            for (int a = 0; a < nb; ++a)
+                for (int c = 0; c < nb; ++c) bp[(size_t)a * nb + c] = L.Tm(m + a, m - nb + c);
+            // V[0:k] = V[0:m] Y[:, 0:k] (through tmp), continuation block -> [k, k+nb)
+            cudaEventRecord(L.e0, L.s);
+            std::vector<double> Yk((size_t)m * k);
+            for (int j = 0; j < m; ++j)
+                for (int l = 0; l < k; ++l) Yk[(size_t)j * k + l] = Z[(size_t)j * m + l];
+            DevBuf Yd;
+            ST(upload(ctx, Yd, Yk.data(), sizeof(double) * Yk.size()));
+            cudaError_t te = transform(L.col(0), m, (const double *)Yd.p, k, k, (double *)L.tmp.p, n, n, n, L.s);
+            if (te == cudaSuccess)
+                te = cudaMemcpyAsync(L.col(0), L.tmp.p, sizeof(double) * n * k, cudaMemcpyDeviceToDevice, L.s);
+            if (te == cudaSuccess)
+                te = cudaMemcpyAsync(L.col(k), L.col(m), sizeof(double) * n * nb, cudaMemcpyDeviceToDevice, L.s);
+            cudaStreamSynchronize(L.s);
+            dev_free(Yd);
+            CK(te);
+            cudaEventRecord(L.e1, L.s);
+            L.t_ort += elapsed(L);
+            std::fill(L.T.begin(), L.T.end(), 0.0);
+            for (int i = 0; i < k; ++i) L.Tm(i, i) = w[i];
+            for (int a = 0; a < nb; ++a)
+                for (int i = 0; i < k; ++i) {
+                    double c_ = 0.0;
+                    for (int c = 0; c < nb; ++c) c_ += bp[(size_t)a * nb + c] * Z[(size_t)(m - nb + c) * m + i];
+                    L.Tm(k + a, i) = c_;
+                    L.Tm(i, k + a) = c_;
+                }
+            cur = k;
+            mT = k;
+            karrow = k;
+            ++restarts;
+            iter = k / nb;
+            beta_prev = -1.0;
+        }
+    }
+
+    // ---- final Ritz pairs of T[0:mT] (lanczos_output, src/blanczoslib.f90:1268)
+    std::vector<double> w, Z;
+    ST(eig_dense(L, mT, w, evecs ? &Z : nullptr));
+    const int nk = std::min(nkeep, mT);
+    for (int j = 0; j < nkeep; ++j) evals[j] = (j < nk) ? w[j] : NAN;
+    if (evecs) {
+        std::vector<double> Yk((size_t)mT * nk);
+        for (int j = 0; j < mT; ++j)
+            for (int l = 0; l < nk; ++l) Yk[(size_t)j * nk + l] = Z[(size_t)j * mT + l];
+        DevBuf Yd, out;
+        ST(upload(ctx, Yd, Yk.data(), sizeof(double) * Yk.size()));
+        int st2 = dev_alloc(ctx, out, sizeof(double) * (size_t)n * nk);
+        if (st2) { dev_free(Yd); return st2; }
+        cudaError_t te = transform(L.col(0), mT, (const double *)Yd.p, nk, nk, (double *)out.p, n, n, n, L.s);
+        if (te == cudaSuccess)
+            te = cudaMemcpyAsync(evecs, out.p, sizeof(double) * (size_t)n * nk, cudaMemcpyDeviceToHost, L.s);
+        if (te == cudaSuccess) te = cudaStreamSynchronize(L.s);
+        dev_free(Yd);
+        dev_free(out);
+        CK(te);
+        for (size_t i = (size_t)n * nk; i < (size_t)n * nkeep; ++i) evecs[i] = NAN;
+    }
+    if (rep) {
+        rep->iterations = iter;
+        rep->total_iterations = total;
+        rep->restarts = restarts;
+        rep->random_restarts = rnd;
+        rep->matvecs = matvecs;
+        rep->converged = converged ? 1 : 0;
+        rep->t_matvec_ms = L.t_mv;
+        rep->t_reorth_ms = L.t_ort;
+        rep->t_eig_ms = L.t_eig;
+    }
+    return BSG_OK;
+}
+
+}  // namespace
+
+extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const double *pivot, double *evals,
+                           double *evecs, bsg_report *rep) {
+    if (!ctx) return BSG_ERR_ARG;
+    if (!p || !evals) return set_err(ctx, BSG_ERR_ARG, "bsg_lanczos: null argument");
+    if (p->nb < 1 || p->nb > 16 || p->nkeep < 1 || p->niter < 2 ||
+        (p->matvec_prec != BSG_PREC_FP32 && p->matvec_prec != BSG_PREC_FP64))
+        return set_err(ctx, BSG_ERR_ARG, "bsg_lanczos: bad parameters");
+    if ((int64_t)p->niter * p->nb + p->nb > 2048)
+        return set_err(ctx, BSG_ERR_UNSUPPORTED, "bsg_lanczos: niter*nb above 2048 (projected matrix too large)");
+    if ((int64_t)p->nkeep > ctx->dim) return set_err(ctx, BSG_ERR_ARG, "bsg_lanczos: nkeep > dim");
+    int st = cuda_check(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+    if (st) return st;
+    Lz L;
+    L.ctx = ctx;
+    L.s = ctx->stream;
+    L.n = ctx->dim;
+    L.nb = p->nb;
+    L.prec = p->matvec_prec;
+    const int niter_eff = (int)std::min<int64_t>(p->niter, (ctx->dim + p->nb - 1) / p->nb + 1);
+    bsg_lanczos_params pp = *p;
+    pp.niter = std::max(2, niter_eff);
+    const int maxcol = pp.niter * L.nb + L.nb;
+    const int N = maxcol;
+    const size_t vb = sizeof(double) * (size_t)L.n;
+    size_t need = vb * ((size_t)maxcol + 2 * L.nb + (size_t)std::max(L.nb, pp.nkeep + pp.nthick_add + 1)) +
+                  2 * (size_t)L.n * L.nb * (L.prec == 4 ? 4 : 8);
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    if (need > fr) return set_err(ctx, BSG_ERR_NOMEM, "bsg_lanczos: history does not fit in device memory");
+    const int G = dot_grid(L.n);
+    const int ktmp = std::max(L.nb, pp.nkeep + std::max(pp.nthick_add, 0) + 1);
+    if ((st = dev_alloc(ctx, L.hist, vb * maxcol)) || (st = dev_alloc(ctx, L.W, vb * L.nb)) ||
+        (st = dev_alloc(ctx, L.tmp, vb * ktmp)) ||
+        (st = dev_alloc(ctx, L.X, (size_t)L.n * L.nb * (L.prec == 4 ? 4 : 8))) ||
+        (st = dev_alloc(ctx, L.Y, (size_t)L.n * L.nb * (L.prec == 4 ? 4 : 8))) ||
+        (st = dev_alloc(ctx, L.partial, sizeof(double) * (size_t)4096 * G)) ||
+        (st = dev_alloc(ctx, L.coef, sizeof(double) * (size_t)maxcol * L.nb)) ||
+        (st = dev_alloc(ctx, L.sqp, sizeof(double) * 16 * 592)) || (st = dev_alloc(ctx, L.sq, sizeof(double) * 16)) ||
+        (st = dev_alloc(ctx, L.Adev, sizeof(double) * (size_t)N * N)) ||
+        (st = dev_alloc(ctx, L.Vtmp, sizeof(double) * (size_t)N * N)) ||
+        (st = dev_alloc(ctx, L.Zdev, sizeof(double) * (size_t)N * N)) || (st = dev_alloc(ctx, L.wdev, sizeof(double) * N)) ||
+        (st = dev_alloc(ctx, L.stat, sizeof(int) * 4)) || (st = dev_alloc(ctx, L.al, sizeof(double) * N)) ||
+        (st = dev_alloc(ctx, L.bt, sizeof(double) * N)) || (st = dev_alloc(ctx, L.ev, sizeof(double) * N)) ||
+        (st = dev_alloc(ctx, L.M, sizeof(double) * 16 * 16))) {
+        // fall through to cleanup
+    }
+    if (!st) {
+        cudaEventCreate(&L.e0);
+        cudaEventCreate(&L.e1);
+        cudaEvent_t t0, t1;
+        cudaEventCreate(&t0);
+        cudaEventCreate(&t1);
+        cudaEventRecord(t0, L.s);
+        st = run(L, &pp, pivot, evals, evecs, rep);
+        cudaEventRecord(t1, L.s);
+        cudaEventSynchronize(t1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, t0, t1);
+        if (rep) rep->t_total_ms = ms;
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        cudaEventDestroy(L.e0);
+        cudaEventDestroy(L.e1);
+    }
+    DevBuf *bufs[] = {&L.hist, &L.W, &L.X, &L.Y, &L.tmp, &L.partial, &L.coef, &L.sqp, &L.sq, &L.Adev,
+                      &L.Vtmp, &L.Zdev, &L.wdev, &L.stat, &L.al, &L.bt, &L.ev, &L.M};
+    cudaStreamSynchronize(L.s);
+    for (DevBuf *b : bufs) dev_free(*b);
+    return st;
+}

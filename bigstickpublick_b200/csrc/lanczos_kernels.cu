@@ -1,0 +1,457 @@
+// FP64 device kernels for the Lanczos loop.
+//
+//   k_multidot      C = A^T B for a few tall vectors (alpha, Gram-Schmidt
+//                   coefficients, block overlaps): dot_product8 /
+//                   br_orthogonalize's dot phase (src/breorthog.f90:658-891)
+//   k_sub_gemv      W -= H C (the subtract phase of br_orthogonalize and the
+//                   alpha projection of br_remove_prev_overlap)
+//   k_transform     out = V Y (br_transform_basis, src/breorthog.f90:1211-1243)
+//   k_jacobi        dense symmetric eigenproblem of the projected matrix in one
+//                   CTA (replaces the vendored DSYEV, src/blanczoslib.f90:226-258)
+//   k_bisect_arrow  lowest eigenvalues of the arrowhead-tridiagonal projected
+//                   matrix of scalar Lanczos by Sturm counting (replaces the
+//                   DSYEV 'N' / DSTEGR calls made for the convergence test)
+//   k_pack/k_unpack history columns <-> interleaved applyH vectors
+//
+// All reductions are two-pass with a fixed grid and fixed summation order, so
+// every coefficient is bitwise repeatable.
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "lanczos_kernels.h"
+
+namespace bsg {
+
+constexpr int kDotThreads = 256;
+constexpr int kDotTile = 512;      // rows per tile
+constexpr int kMaxPairsPerThread = 16;
+
+// C[p] partials: pairs p = a*nB + b, a < nA, b < nB; A, B column-major with
+// leading dimension ld (vector j at base + j*ld).  partial[p * gridDim.x + blockIdx.x].
+__global__ void __launch_bounds__(kDotThreads) k_multidot(const double *__restrict__ A, int nA,
+                                                         const double *__restrict__ B, int nB,
+                                                         int64_t n, int64_t ld, double *__restrict__ partial) {
+    extern __shared__ double sB[];  // [kDotTile][nB]
+    const int npairs = nA * nB;
+    double acc[kMaxPairsPerThread];
+#pragma unroll
+    for (int k = 0; k < kMaxPairsPerThread; ++k) acc[k] = 0.0;
+    for (int64_t t0 = (int64_t)blockIdx.x * kDotTile; t0 < n; t0 += (int64_t)gridDim.x * kDotTile) {
+        const int rows = (int)((n - t0) < kDotTile ? (n - t0) : kDotTile);
+        __syncthreads();
+        for (int e = threadIdx.x; e < rows * nB; e += kDotThreads) {
+            const int r = e % rows, b = e / rows;
+            sB[r * nB + b] = B[(int64_t)b * ld + t0 + r];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kMaxPairsPerThread; ++k) {
+            const int p = threadIdx.x + k * kDotThreads;
+            if (p >= npairs) break;
+            const int a = p / nB, b = p - a * nB;
+            const double *__restrict__ col = A + (int64_t)a * ld + t0;
+            double s = 0.0;
+            for (int r = 0; r < rows; ++r) s = fma(__ldg(col + r), sB[r * nB + b], s);
+            acc[k] += s;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < kMaxPairsPerThread; ++k) {
+        const int p = threadIdx.x + k * kDotThreads;
+        if (p < npairs) partial[(int64_t)p * gridDim.x + blockIdx.x] = acc[k];
+    }
+}
+
+// out[p] = sum over g of partial[p*G + g] (fixed order); one thread per p
+__global__ void k_reduce_partials(const double *__restrict__ partial, int npairs, int G, double *__restrict__ out) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npairs) return;
+    double s = 0.0;
+    for (int g = 0; g < G; ++g) s += partial[(int64_t)p * G + g];
+    out[p] = s;
+}
+
+// W[b] -= sum_j H[j] * C[j*nB + b]   (j < k), fused sum of squares of the
+// result per column when sq != nullptr (partials per block, nB entries)
+__global__ void __launch_bounds__(256) k_sub_gemv(const double *__restrict__ H, int k, const double *__restrict__ C,
+                                                  double *__restrict__ W, int nB, int64_t n, int64_t ld,
+                                                  double *__restrict__ sq) {
+    extern __shared__ double sC[];  // [k*nB] then [8][nB] warp sums
+    for (int e = threadIdx.x; e < k * nB; e += blockDim.x) sC[e] = C[e];
+    __syncthreads();
+    double sqacc[16];
+    for (int b = 0; b < 16; ++b) sqacc[b] = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double acc[16];
+        for (int b = 0; b < nB; ++b) acc[b] = 0.0;
+        for (int j = 0; j < k; ++j) {
+            const double h = __ldg(H + (int64_t)j * ld + i);
+            for (int b = 0; b < nB; ++b) acc[b] = fma(h, sC[j * nB + b], acc[b]);
+        }
+        for (int b = 0; b < nB; ++b) {
+            const double w = W[(int64_t)b * ld + i] - acc[b];
+            W[(int64_t)b * ld + i] = w;
+            sqacc[b] = fma(w, w, sqacc[b]);
+        }
+    }
+    if (!sq) return;
+    double *red = sC + k * nB;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int b = 0; b < nB; ++b) {
+        double v = sqacc[b];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[warp * nB + b] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < nB) {
+        double v = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[w * nB + threadIdx.x];
+        sq[(int64_t)threadIdx.x * gridDim.x + blockIdx.x] = v;
+    }
+}
+
+// out[l] = sum_j V[j] * Y[j*ldy + l], l < K (K <= 16 per launch)
+__global__ void __launch_bounds__(256) k_transform(const double *__restrict__ V, int m, const double *__restrict__ Y,
+                                                   int ldy, int K, double *__restrict__ out, int64_t n, int64_t ld,
+                                                   int64_t ldo) {
+    extern __shared__ double sY[];  // [m][K]
+    for (int e = threadIdx.x; e < m * K; e += blockDim.x) {
+        const int j = e / K, l = e - j * K;
+        sY[e] = Y[(int64_t)j * ldy + l];
+    }
+    __syncthreads();
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double acc[16];
+        for (int l = 0; l < K; ++l) acc[l] = 0.0;
+        for (int j = 0; j < m; ++j) {
+            const double v = __ldg(V + (int64_t)j * ld + i);
+            for (int l = 0; l < K; ++l) acc[l] = fma(v, sY[j * K + l], acc[l]);
+        }
+        for (int l = 0; l < K; ++l) out[(int64_t)l * ldo + i] = acc[l];
+    }
+}
+
+// y[b] = s[b] * x[b] (scale columns), x and y may alias
+__global__ void k_scale_cols(const double *__restrict__ x, double *y, const double *__restrict__ s, int nB,
+                             int64_t n, int64_t ld) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        for (int b = 0; b < nB; ++b) y[(int64_t)b * ld + i] = x[(int64_t)b * ld + i] * s[b];
+}
+
+// interleaved applyH vector from nB history columns (fp64 -> T)
+template <typename T>
+__global__ void k_pack(const double *__restrict__ V, int nB, int64_t n, int64_t ld, T *__restrict__ x) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n * nB; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = e / nB;
+        const int b = (int)(e - s * nB);
+        x[e] = (T)V[(int64_t)b * ld + s];
+    }
+}
+template <typename T>
+__global__ void k_unpack(const T *__restrict__ y, int nB, int64_t n, int64_t ld, double *__restrict__ W) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n * nB; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = e / nB;
+        const int b = (int)(e - s * nB);
+        W[(int64_t)b * ld + s] = (double)y[e];
+    }
+}
+
+// ------------------------------------------------------------- Jacobi -----
+// Cyclic two-sided Jacobi with a round-robin (tournament) ordering: every
+// round rotates n/2 disjoint (p,q) pairs in parallel.  A (n x n, row-major,
+// symmetric) is overwritten; on exit w holds the eigenvalues in ascending
+// order and Z (n x n, column j = eigenvector j) the eigenvectors.
+// Bounded: at most max_sweeps sweeps; *status = 1 if not converged.
+__global__ void __launch_bounds__(1024) k_jacobi(int n, double *__restrict__ A, double *__restrict__ Vtmp,
+                                                 double *__restrict__ w, double *__restrict__ Z, int max_sweeps,
+                                                 int *__restrict__ status) {
+    extern __shared__ double sh[];
+    const int m = n + (n & 1);                 // even size, index n is a dummy
+    double *cs = sh;                           // [m/2] c
+    double *sn = sh + m / 2;                   // [m/2] s
+    int *pp = reinterpret_cast<int *>(sh + m); // [m/2] p, [m/2] q, [m] order
+    int *qq = pp + m / 2;
+    int *ord = qq + m / 2;
+    __shared__ double red[32];
+    __shared__ int done;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int e = tid; e < n * n; e += nt) Vtmp[e] = ((e / n) == (e % n)) ? 1.0 : 0.0;
+    for (int e = tid; e < m; e += nt) ord[e] = e;
+    __syncthreads();
+    // scale of the matrix (Frobenius norm squared)
+    double fro = 0.0;
+    for (int e = tid; e < n * n; e += nt) fro += A[e] * A[e];
+    for (int o = 16; o > 0; o >>= 1) fro += __shfl_down_sync(0xffffffffu, fro, o);
+    if ((tid & 31) == 0) red[tid >> 5] = fro;
+    __syncthreads();
+    if (tid == 0) {
+        double s = 0.0;
+        for (int k = 0; k < (nt + 31) / 32; ++k) s += red[k];
+        red[0] = s;
+    }
+    __syncthreads();
+    const double tol2 = red[0] * 1e-30;
+    __syncthreads();
+    int sweep = 0;
+    for (; sweep < max_sweeps; ++sweep) {
+        double off = 0.0;
+        for (int e = tid; e < n * n; e += nt) {
+            const int i = e / n, j = e % n;
+            if (i != j) off += A[e] * A[e];
+        }
+        for (int o = 16; o > 0; o >>= 1) off += __shfl_down_sync(0xffffffffu, off, o);
+        __syncthreads();
+        if ((tid & 31) == 0) red[tid >> 5] = off;
+        __syncthreads();
+        if (tid == 0) {
+            double s = 0.0;
+            for (int k = 0; k < (nt + 31) / 32; ++k) s += red[k];
+            done = (s <= tol2) ? 1 : 0;
+        }
+        __syncthreads();
+        if (done) break;
+        for (int round = 0; round < m - 1; ++round) {
+            // pairs from the current ordering: (ord[k], ord[m-1-k])
+            for (int k = tid; k < m / 2; k += nt) {
+                int p = ord[k], q = ord[m - 1 - k];
+                if (p > q) { const int t = p; p = q; q = t; }
+                double c = 1.0, s = 0.0;
+                if (q < n) {
+                    const double apq = A[p * n + q];
+                    if (apq != 0.0) {
+                        const double theta = (A[q * n + q] - A[p * n + p]) / (2.0 * apq);
+                        const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                        c = 1.0 / sqrt(t * t + 1.0);
+                        s = t * c;
+                    }
+                }
+                pp[k] = p;
+                qq[k] = q;
+                cs[k] = c;
+                sn[k] = s;
+            }
+            __syncthreads();
+            // columns: A <- A J, Z <- Z J
+            for (int e = tid; e < (m / 2) * n; e += nt) {
+                const int k = e / n, i = e % n;
+                const int p = pp[k], q = qq[k];
+                if (q >= n || sn[k] == 0.0) continue;
+                const double c = cs[k], s = sn[k];
+                const double aip = A[i * n + p], aiq = A[i * n + q];
+                A[i * n + p] = c * aip - s * aiq;
+                A[i * n + q] = s * aip + c * aiq;
+                const double vip = Vtmp[i * n + p], viq = Vtmp[i * n + q];
+                Vtmp[i * n + p] = c * vip - s * viq;
+                Vtmp[i * n + q] = s * vip + c * viq;
+            }
+            __syncthreads();
+            // rows: A <- J^T A
+            for (int e = tid; e < (m / 2) * n; e += nt) {
+                const int k = e / n, j = e % n;
+                const int p = pp[k], q = qq[k];
+                if (q >= n || sn[k] == 0.0) continue;
+                const double c = cs[k], s = sn[k];
+                const double apj = A[p * n + j], aqj = A[q * n + j];
+                A[p * n + j] = c * apj - s * aqj;
+                A[q * n + j] = s * apj + c * aqj;
+            }
+            __syncthreads();
+            for (int k = tid; k < m / 2; k += nt) {
+                const int p = pp[k], q = qq[k];
+                if (q < n && sn[k] != 0.0) {
+                    A[p * n + q] = 0.0;
+                    A[q * n + p] = 0.0;
+                }
+            }
+            // next ordering: ord[0] fixed, the rest rotates by one
+            __syncthreads();
+            if (tid == 0) {
+                const int last = ord[m - 1];
+                for (int k = m - 1; k > 1; --k) ord[k] = ord[k - 1];
+                ord[1] = last;
+            }
+            __syncthreads();
+        }
+    }
+    if (tid == 0 && status) *status = (sweep >= max_sweeps) ? 1 : 0;
+    // ascending order by rank (ties broken by index)
+    for (int i = tid; i < n; i += nt) {
+        const double di = A[i * n + i];
+        int r = 0;
+        for (int j = 0; j < n; ++j) {
+            const double dj = A[j * n + j];
+            r += (dj < di || (dj == di && j < i)) ? 1 : 0;
+        }
+        w[r] = di;
+        for (int row = 0; row < n; ++row) Z[(int64_t)row * n + r] = Vtmp[row * n + i];
+    }
+}
+
+// ---------------------------------------------------------- bisection ----
+// number of eigenvalues below x of the symmetric arrowhead-tridiagonal T:
+// T(i,i) = al[i]; T(i,k) = bt[i] for i < k (arrow, k = nthick);
+// T(i,i+1) = bt[i] for k <= i < n-1.  Sylvester inertia of LDL^T(T - xI)
+// eliminating the arrow diagonal first.
+__device__ int sturm_count(int n, int k, const double *__restrict__ al, const double *__restrict__ bt,
+                           double x, double pivmin) {
+    int cnt = 0;
+    double schur = 0.0;
+    for (int i = 0; i < k; ++i) {
+        double d = al[i] - x;
+        if (fabs(d) < pivmin) d = -pivmin;
+        if (d < 0) ++cnt;
+        schur += bt[i] * bt[i] / d;
+    }
+    double d = al[k] - x - schur;
+    if (fabs(d) < pivmin) d = -pivmin;
+    if (d < 0) ++cnt;
+    for (int i = k + 1; i < n; ++i) {
+        const double b = bt[i - 1];
+        d = al[i] - x - b * b / d;
+        if (fabs(d) < pivmin) d = -pivmin;
+        if (d < 0) ++cnt;
+    }
+    return cnt;
+}
+
+// one warp per wanted eigenvalue index j: multisection with 32 shifts a round
+__global__ void k_bisect_arrow(int n, int k, const double *__restrict__ al, const double *__restrict__ bt,
+                               int nwant, double glo, double ghi, double *__restrict__ ev) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= nwant) return;
+    const int j = warp;  // find the (j+1)-th smallest eigenvalue
+    double lo = glo, hi = ghi;
+    const double scale = fmax(fabs(glo), fabs(ghi));
+    const double pivmin = fmax(1e-300, 1e-290 * scale * scale);
+    for (int round = 0; round < 40; ++round) {
+        if (hi - lo <= 2.2e-16 * fmax(fabs(lo), fabs(hi)) + 1e-300) break;
+        const double x = lo + (hi - lo) * (double)(lane + 1) / 33.0;
+        const int c = sturm_count(n, k, al, bt, x, pivmin);
+        // lanes whose shift has count <= j lie at or below the eigenvalue
+        const unsigned below = __ballot_sync(0xffffffffu, c <= j);
+        const int nb = __popc(below);  // shifts 0..nb-1 are below
+        const double nlo = (nb == 0) ? lo : lo + (hi - lo) * (double)nb / 33.0;
+        const double nhi = (nb == 32) ? hi : lo + (hi - lo) * (double)(nb + 1) / 33.0;
+        lo = nlo;
+        hi = nhi;
+    }
+    if (lane == 0) ev[j] = 0.5 * (lo + hi);
+}
+
+// seeded pseudo-random normal columns (SplitMix64 of (seed, column, row) and
+// Box-Muller), for block pivots and random restarts
+__device__ __forceinline__ uint64_t splitmix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+__global__ void k_random_cols(double *W, int nB, int64_t n, int64_t ld, uint64_t seed) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        for (int b = 0; b < nB; ++b) {
+            const uint64_t h = splitmix64(seed ^ splitmix64(((uint64_t)b << 48) ^ (uint64_t)i));
+            const uint64_t h2 = splitmix64(h);
+            const double u1 = ((double)(h >> 11) + 1.0) * (1.0 / 9007199254740992.0);
+            const double u2 = (double)(h2 >> 11) * (1.0 / 9007199254740992.0);
+            W[(int64_t)b * ld + i] = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+        }
+}
+
+// ------------------------------------------------------------- launchers --
+cudaError_t random_cols(double *W, int nB, int64_t n, int64_t ld, uint64_t seed, cudaStream_t s) {
+    k_random_cols<<<592, 256, 0, s>>>(W, nB, n, ld, seed);
+    return cudaGetLastError();
+}
+
+int dot_grid(int64_t n) {
+    int64_t tiles = (n + kDotTile - 1) / kDotTile;
+    return (int)(tiles < 592 ? (tiles > 0 ? tiles : 1) : 592);
+}
+
+cudaError_t multidot(const double *A, int nA, const double *B, int nB, int64_t n, int64_t ld, double *partial,
+                     double *out, cudaStream_t s) {
+    const int npairs = nA * nB;
+    if (npairs <= 0) return cudaSuccess;
+    const int G = dot_grid(n);
+    for (int a0 = 0; a0 < nA;) {
+        // chunk nA so that pairs fit the per-thread accumulators
+        const int maxa = (kDotThreads * kMaxPairsPerThread) / nB;
+        const int na = (nA - a0) < maxa ? (nA - a0) : maxa;
+        const size_t smem = sizeof(double) * kDotTile * nB;
+        k_multidot<<<G, kDotThreads, smem, s>>>(A + (int64_t)a0 * ld, na, B, nB, n, ld, partial);
+        k_reduce_partials<<<(na * nB + 127) / 128, 128, 0, s>>>(partial, na * nB, G, out + (int64_t)a0 * nB);
+        a0 += na;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t sub_gemv(const double *H, int k, const double *C, double *W, int nB, int64_t n, int64_t ld,
+                     double *sq_partial, double *sq_out, cudaStream_t s) {
+    const int G = 592;
+    // process at most 512 history columns per launch (shared memory)
+    for (int j0 = 0; j0 < k || (k == 0 && j0 == 0);) {
+        const int kk = (k - j0) < 512 ? (k - j0) : 512;
+        const bool last = (j0 + kk >= k);
+        const size_t smem = sizeof(double) * ((size_t)kk * nB + 8 * nB);
+        k_sub_gemv<<<G, 256, smem, s>>>(H + (int64_t)j0 * ld, kk, C + (int64_t)j0 * nB, W, nB, n, ld,
+                                         last ? sq_partial : nullptr);
+        j0 += kk;
+        if (k == 0) break;
+    }
+    if (sq_partial && sq_out) k_reduce_partials<<<1, 32, 0, s>>>(sq_partial, nB, G, sq_out);
+    return cudaGetLastError();
+}
+
+cudaError_t transform(const double *V, int m, const double *Y, int ldy, int K, double *out, int64_t n, int64_t ld,
+                      int64_t ldo, cudaStream_t s) {
+    for (int l0 = 0; l0 < K; l0 += 16) {
+        const int kk = (K - l0) < 16 ? (K - l0) : 16;
+        // Y rows in chunks that fit shared memory: accumulate over row chunks
+        if ((size_t)m * kk * sizeof(double) > 160 * 1024) return cudaErrorInvalidValue;
+        const size_t smem = sizeof(double) * (size_t)m * kk;
+        cudaFuncSetAttribute(k_transform, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+        k_transform<<<592, 256, smem, s>>>(V, m, Y + l0, ldy, kk, out + (int64_t)l0 * ldo, n, ld, ldo);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t scale_cols(const double *x, double *y, const double *sc, int nB, int64_t n, int64_t ld, cudaStream_t s) {
+    k_scale_cols<<<592, 256, 0, s>>>(x, y, sc, nB, n, ld);
+    return cudaGetLastError();
+}
+
+cudaError_t pack(const double *V, int nB, int64_t n, int64_t ld, void *x, int prec, cudaStream_t s) {
+    if (prec == 4)
+        k_pack<float><<<1184, 256, 0, s>>>(V, nB, n, ld, (float *)x);
+    else
+        k_pack<double><<<1184, 256, 0, s>>>(V, nB, n, ld, (double *)x);
+    return cudaGetLastError();
+}
+
+cudaError_t unpack(const void *y, int nB, int64_t n, int64_t ld, double *W, int prec, cudaStream_t s) {
+    if (prec == 4)
+        k_unpack<float><<<1184, 256, 0, s>>>((const float *)y, nB, n, ld, W);
+    else
+        k_unpack<double><<<1184, 256, 0, s>>>((const double *)y, nB, n, ld, W);
+    return cudaGetLastError();
+}
+
+cudaError_t jacobi(int n, double *A, double *Vtmp, double *w, double *Z, int *status, cudaStream_t s) {
+    const int m = n + (n & 1);
+    const size_t smem = sizeof(double) * m + sizeof(int) * 2 * m;
+    cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(smem + 1024));
+    k_jacobi<<<1, 1024, smem, s>>>(n, A, Vtmp, w, Z, 60, status);
+    return cudaGetLastError();
+}
+
+cudaError_t bisect_arrow(int n, int k, const double *al, const double *bt, int nwant, double glo, double ghi,
+                         double *ev, cudaStream_t s) {
+    if (nwant <= 0) return cudaSuccess;
+    const int threads = 32 * nwant;
+    k_bisect_arrow<<<(threads + 255) / 256, 256, 0, s>>>(n, k, al, bt, nwant, glo, ghi, ev);
+    return cudaGetLastError();
+}
+
+}  // namespace bsg

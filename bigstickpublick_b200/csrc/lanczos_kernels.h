@@ -1,0 +1,27 @@
+// Launchers of the FP64 Lanczos kernels (lanczos_kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace bsg {
+int dot_grid(int64_t n);
+// out[a*nB + b] = A_a . B_b   (partial: scratch of nA*nB*dot_grid(n) doubles)
+cudaError_t multidot(const double *A, int nA, const double *B, int nB, int64_t n, int64_t ld, double *partial,
+                     double *out, cudaStream_t s);
+// W_b -= sum_j H_j C[j*nB+b]; optional column sums of squares of the result
+// (sq_partial: nB*592 doubles, sq_out: nB doubles)
+cudaError_t sub_gemv(const double *H, int k, const double *C, double *W, int nB, int64_t n, int64_t ld,
+                     double *sq_partial, double *sq_out, cudaStream_t s);
+// out_l = sum_j V_j Y[j*ldy + l], l < K
+cudaError_t transform(const double *V, int m, const double *Y, int ldy, int K, double *out, int64_t n, int64_t ld,
+                      int64_t ldo, cudaStream_t s);
+cudaError_t scale_cols(const double *x, double *y, const double *sc, int nB, int64_t n, int64_t ld, cudaStream_t s);
+cudaError_t pack(const double *V, int nB, int64_t n, int64_t ld, void *x, int prec, cudaStream_t s);
+cudaError_t unpack(const void *y, int nB, int64_t n, int64_t ld, double *W, int prec, cudaStream_t s);
+// dense symmetric eigenproblem (n x n row-major A, destroyed); Z row-major,
+// column j = eigenvector of w[j] (ascending)
+cudaError_t jacobi(int n, double *A, double *Vtmp, double *w, double *Z, int *status, cudaStream_t s);
+// lowest nwant eigenvalues of the arrowhead-tridiagonal matrix
+cudaError_t bisect_arrow(int n, int k, const double *al, const double *bt, int nwant, double glo, double ghi,
+                         double *ev, cudaStream_t s);
+}  // namespace bsg

@@ -1,3 +1,2 @@
 #include "bsg_internal.h"
-extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *, const double *, double *, double *, bsg_report *) { return bsg::set_err(ctx, BSG_ERR_UNSUPPORTED, "lanczos not built"); }
 extern "C" int bsg_grad(bsg_ctx *ctx, const double *, int, double *, double *, double *, double *, double *) { return bsg::set_err(ctx, BSG_ERR_UNSUPPORTED, "grad not built"); }

@@ -1,0 +1,107 @@
+"""Device Lanczos (lanczos_p / lanczos_block with thick restart) against
+exact diagonalization and the oracle's numpy restatement."""
+import numpy as np
+import pytest
+
+from bigstickpublick_b200 import model
+import oracle
+from oracle import lanczos as olz
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def sd22():
+    from bigstickpublick_b200.engine import Hamiltonian
+    T = model.build_tables(model.sd_model(2, 2, seed=1))
+    H = Hamiltonian(T)
+    exact = np.linalg.eigvalsh(oracle.dense_from_applyh(T))
+    return T, H, exact
+
+
+def generic_pivot(n, nb=1, seed=5):
+    # no proton-neutron exchange symmetry, unlike the uniform pivot
+    return np.random.default_rng(seed).standard_normal(n * nb)
+
+
+def test_fp64_matches_exact(sd22):
+    T, H, exact = sd22
+    ev, _, rep = H.lanczos(nkeep=10, niter=300, matvec_prec=8, converge_tol=1e-13,
+                           pivot=generic_pivot(T.dim))
+    rel = np.abs(ev - exact[:10]) / np.abs(exact[:10])
+    assert rel.max() < 1e-10, (rel, rep)
+
+
+def test_uniform_pivot_reaches_exchange_symmetric_states(sd22):
+    """N = Z, isospin-conserving H: the uniform pivot (the reference's option 0)
+    only reaches states with nonzero overlap; those eigenvalues must agree."""
+    T, H, exact = sd22
+    Hd = oracle.dense_from_applyh(T)
+    w, Z = np.linalg.eigh(Hd)
+    u = np.ones(T.dim) / np.sqrt(T.dim)
+    reach = w[np.abs(Z.T @ u) > 1e-8]
+    ev, _, rep = H.lanczos(nkeep=3, niter=200, matvec_prec=8, converge_tol=1e-13)
+    assert np.abs(ev - reach[:3]).max() / np.abs(reach[:3]).max() < 1e-10
+
+
+def test_fp64_matches_oracle_lanczos(sd22):
+    T, H, exact = sd22
+    ev, _, rep = H.lanczos(nkeep=10, niter=100, matvec_prec=8, fixed_iter=True)
+    ref, _, _ = olz.lanczos(T, nkeep=10, niter=100, fixed_iter=True)
+    assert np.abs(ev - ref).max() / np.abs(ref).max() < 1e-10
+
+
+def test_mixed_precision_error_bound(sd22):
+    T, H, exact = sd22
+    ev, _, rep = H.lanczos(nkeep=10, niter=300, matvec_prec=4, converge_tol=1e-10,
+                           pivot=generic_pivot(T.dim))
+    rel = np.abs(ev - exact[:10]) / np.abs(exact[:10])
+    assert rel.max() < 1e-6, rel
+
+
+def test_eigenvectors(sd22):
+    T, H, exact = sd22
+    ev, vecs, rep = H.lanczos(nkeep=5, niter=300, matvec_prec=8, want_vectors=True, converge_tol=1e-13,
+                              pivot=generic_pivot(T.dim))
+    assert vecs.shape == (T.dim, 5)
+    for k in range(5):
+        v = vecs[:, k]
+        r = oracle.applyh(T, v) - ev[k] * v
+        assert abs(np.linalg.norm(v) - 1) < 1e-8
+        assert np.linalg.norm(r) < 1e-6 * abs(ev[k])
+
+
+def test_thick_restart_converges(sd22):
+    T, H, exact = sd22
+    ev, _, rep = H.lanczos(nkeep=5, niter=40, nthick_add=10, max_restarts=80, matvec_prec=8,
+                           converge_tol=1e-9, pivot=generic_pivot(T.dim))
+    assert rep["restarts"] >= 1, rep
+    rel = np.abs(ev - exact[:5]) / np.abs(exact[:5])
+    assert rel.max() < 1e-9, (rel, rep)
+
+
+def test_thick_restart_matches_oracle(sd22):
+    T, H, exact = sd22
+    kw = dict(nkeep=5, niter=30, nthick_add=5, max_restarts=3, converge_tol=1e-30)
+    ev, _, rep = H.lanczos(matvec_prec=8, **kw)
+    ref, _, orep = olz.lanczos(T, tol=1e-30, **{k: v for k, v in kw.items() if k != "converge_tol"})
+    assert rep["restarts"] == orep["restarts"] == 3
+    assert np.abs(ev - ref).max() / np.abs(ref).max() < 1e-10, (ev, ref)
+
+
+@pytest.mark.parametrize("nb", [2, 4, 8])
+def test_block_lanczos(sd22, nb):
+    T, H, exact = sd22
+    ev, vecs, rep = H.lanczos(nkeep=8, niter=max(20, 160 // nb), nb=nb, matvec_prec=8, want_vectors=True,
+                              converge_tol=1e-10)
+    rel = np.abs(ev - exact[:8]) / np.abs(exact[:8])
+    assert rel.max() < 1e-9, (nb, rel, rep)
+
+
+def test_block_thick_restart(sd22):
+    T, H, exact = sd22
+    ev, _, rep = H.lanczos(nkeep=6, niter=12, nb=4, nthick_add=6, max_restarts=60, matvec_prec=4,
+                           converge_tol=1e-8)
+    assert rep["restarts"] >= 1
+    rel = np.abs(ev - exact[:6]) / np.abs(exact[:6])
+    assert rel.max() < 1e-6, (rel, rep)
