@@ -32,22 +32,21 @@ def test_fp64_matches_exact(sd22):
     assert rel.max() < 1e-10, (rel, rep)
 
 
-def test_uniform_pivot_reaches_exchange_symmetric_states(sd22):
-    """N = Z, isospin-conserving H: the uniform pivot (the reference's option 0)
-    only reaches states with nonzero overlap; those eigenvalues must agree."""
+def test_uniform_pivot_ground_state(sd22):
+    """The reference's option-0 pivot (uniform 1/sqrt(dim)) is symmetric under
+    proton-neutron exchange for N = Z; the ground state lies in its class.
+    (Round-off slowly seeds the other class, so only the ground state is a
+    well-posed comparison.)"""
     T, H, exact = sd22
-    Hd = oracle.dense_from_applyh(T)
-    w, Z = np.linalg.eigh(Hd)
-    u = np.ones(T.dim) / np.sqrt(T.dim)
-    reach = w[np.abs(Z.T @ u) > 1e-8]
-    ev, _, rep = H.lanczos(nkeep=3, niter=200, matvec_prec=8, converge_tol=1e-13)
-    assert np.abs(ev - reach[:3]).max() / np.abs(reach[:3]).max() < 1e-10
+    ev, _, rep = H.lanczos(nkeep=1, niter=120, matvec_prec=8, converge_tol=1e-13)
+    assert abs(ev[0] - exact[0]) / abs(exact[0]) < 1e-10
 
 
 def test_fp64_matches_oracle_lanczos(sd22):
     T, H, exact = sd22
-    ev, _, rep = H.lanczos(nkeep=10, niter=100, matvec_prec=8, fixed_iter=True)
-    ref, _, _ = olz.lanczos(T, nkeep=10, niter=100, fixed_iter=True)
+    piv = generic_pivot(T.dim)
+    ev, _, rep = H.lanczos(nkeep=10, niter=100, matvec_prec=8, fixed_iter=True, pivot=piv)
+    ref, _, _ = olz.lanczos(T, nkeep=10, niter=100, fixed_iter=True, pivot=piv)
     assert np.abs(ev - ref).max() / np.abs(ref).max() < 1e-10
 
 
@@ -83,8 +82,9 @@ def test_thick_restart_converges(sd22):
 def test_thick_restart_matches_oracle(sd22):
     T, H, exact = sd22
     kw = dict(nkeep=5, niter=30, nthick_add=5, max_restarts=3, converge_tol=1e-30)
-    ev, _, rep = H.lanczos(matvec_prec=8, **kw)
-    ref, _, orep = olz.lanczos(T, tol=1e-30, **{k: v for k, v in kw.items() if k != "converge_tol"})
+    piv = generic_pivot(T.dim)
+    ev, _, rep = H.lanczos(matvec_prec=8, pivot=piv, **kw)
+    ref, _, orep = olz.lanczos(T, tol=1e-30, pivot=piv, **{k: v for k, v in kw.items() if k != "converge_tol"})
     assert rep["restarts"] == orep["restarts"] == 3
     assert np.abs(ev - ref).max() / np.abs(ref).max() < 1e-10, (ev, ref)
 
@@ -92,7 +92,7 @@ def test_thick_restart_matches_oracle(sd22):
 @pytest.mark.parametrize("nb", [2, 4, 8])
 def test_block_lanczos(sd22, nb):
     T, H, exact = sd22
-    ev, vecs, rep = H.lanczos(nkeep=8, niter=max(20, 160 // nb), nb=nb, matvec_prec=8, want_vectors=True,
+    ev, vecs, rep = H.lanczos(nkeep=8, niter={2: 150, 4: 100, 8: 60}[nb], nb=nb, matvec_prec=8, want_vectors=True,
                               converge_tol=1e-10)
     rel = np.abs(ev - exact[:8]) / np.abs(exact[:8])
     assert rel.max() < 1e-9, (nb, rel, rep)
