@@ -254,8 +254,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_rows(const RowArgs a, const T *
 
 template <typename T, int NB, int ITEMS>
 static int launch_one(bsg_ctx *ctx, const T *vin, T *vout, int ld, int v0, int accumulate,
-                      cudaStream_t s) {
-    const TileSet *ts = get_tiles(ctx, 32 * ITEMS);
+                      cudaStream_t s, TileLookup lookup) {
+    const TileSet *ts = lookup ? lookup(ctx, 32 * ITEMS) : get_tiles(ctx, 32 * ITEMS);
     if (!ts) return ctx->last_error.empty() ? BSG_ERR_NOMEM : BSG_ERR_CUDA;
     if (ts->ntiles == 0) return BSG_OK;
     RowArgs a = ctx->args;
@@ -285,40 +285,42 @@ static int launch_one(bsg_ctx *ctx, const T *vin, T *vout, int ld, int v0, int a
 // tile width: 32*ITEMS positions, ITEMS the smallest power of two covering the
 // median row, capped so that ITEMS*NB accumulators stay in registers
 template <typename T, int NB>
-static int launch_nb(bsg_ctx *ctx, const T *vin, T *vout, int ld, int v0, int accumulate, cudaStream_t s) {
+static int launch_nb(bsg_ctx *ctx, const T *vin, T *vout, int ld, int v0, int accumulate, cudaStream_t s,
+                     TileLookup lk) {
     constexpr int cap = NB >= 8 ? 1 : (NB == 4 ? 2 : (NB == 2 ? 4 : 8));
     int items = 1;
     while (items < cap && 32 * items < ctx->median_rowlen) items *= 2;
-    if (items >= 8 && cap >= 8) return launch_one<T, NB, (cap >= 8 ? 8 : 1)>(ctx, vin, vout, ld, v0, accumulate, s);
-    if (items >= 4 && cap >= 4) return launch_one<T, NB, (cap >= 4 ? 4 : 1)>(ctx, vin, vout, ld, v0, accumulate, s);
-    if (items >= 2 && cap >= 2) return launch_one<T, NB, (cap >= 2 ? 2 : 1)>(ctx, vin, vout, ld, v0, accumulate, s);
-    return launch_one<T, NB, 1>(ctx, vin, vout, ld, v0, accumulate, s);
+    if (items >= 8 && cap >= 8) return launch_one<T, NB, (cap >= 8 ? 8 : 1)>(ctx, vin, vout, ld, v0, accumulate, s, lk);
+    if (items >= 4 && cap >= 4) return launch_one<T, NB, (cap >= 4 ? 4 : 1)>(ctx, vin, vout, ld, v0, accumulate, s, lk);
+    if (items >= 2 && cap >= 2) return launch_one<T, NB, (cap >= 2 ? 2 : 1)>(ctx, vin, vout, ld, v0, accumulate, s, lk);
+    return launch_one<T, NB, 1>(ctx, vin, vout, ld, v0, accumulate, s, lk);
 }
 
 template <typename T>
-static int launch_typed(bsg_ctx *ctx, const T *vin, T *vout, int nb, int accumulate, cudaStream_t s) {
+static int launch_typed(bsg_ctx *ctx, const T *vin, T *vout, int nb, int accumulate, cudaStream_t s,
+                        TileLookup lk) {
     switch (nb) {
-    case 1: return launch_nb<T, 1>(ctx, vin, vout, nb, 0, accumulate, s);
-    case 2: return launch_nb<T, 2>(ctx, vin, vout, nb, 0, accumulate, s);
-    case 4: return launch_nb<T, 4>(ctx, vin, vout, nb, 0, accumulate, s);
-    case 8: return launch_nb<T, 8>(ctx, vin, vout, nb, 0, accumulate, s);
-    case 16: return launch_nb<T, 16>(ctx, vin, vout, nb, 0, accumulate, s);
+    case 1: return launch_nb<T, 1>(ctx, vin, vout, nb, 0, accumulate, s, lk);
+    case 2: return launch_nb<T, 2>(ctx, vin, vout, nb, 0, accumulate, s, lk);
+    case 4: return launch_nb<T, 4>(ctx, vin, vout, nb, 0, accumulate, s, lk);
+    case 8: return launch_nb<T, 8>(ctx, vin, vout, nb, 0, accumulate, s, lk);
+    case 16: return launch_nb<T, 16>(ctx, vin, vout, nb, 0, accumulate, s, lk);
     default: {
         // other block sizes: one column pass per vector (strided layout)
         int st = BSG_OK;
-        for (int v0 = 0; v0 < nb && st == BSG_OK; ++v0) st = launch_nb<T, 1>(ctx, vin, vout, nb, v0, accumulate, s);
+        for (int v0 = 0; v0 < nb && st == BSG_OK; ++v0) st = launch_nb<T, 1>(ctx, vin, vout, nb, v0, accumulate, s, lk);
         return st;
     }
     }
 }
 
 int launch_applyh(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec, int accumulate,
-                  cudaStream_t s) {
+                  cudaStream_t s, TileLookup lk) {
     if (ctx->args.max_nbd > 8192)
         return set_err(ctx, BSG_ERR_UNSUPPORTED, "a neutron sector jump has more than 8192 distinct (b,d) pairs");
     if (prec == BSG_PREC_FP32)
-        return launch_typed<float>(ctx, (const float *)vin, (float *)vout, nb, accumulate, s);
-    return launch_typed<double>(ctx, (const double *)vin, (double *)vout, nb, accumulate, s);
+        return launch_typed<float>(ctx, (const float *)vin, (float *)vout, nb, accumulate, s, lk);
+    return launch_typed<double>(ctx, (const double *)vin, (double *)vout, nb, accumulate, s, lk);
 }
 
 }  // namespace bsg

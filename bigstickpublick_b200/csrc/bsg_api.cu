@@ -61,15 +61,13 @@ int upload(bsg_ctx *ctx, DevBuf &b, const void *src, size_t bytes) {
     return BSG_OK;
 }
 
-const TileSet *get_tiles(bsg_ctx *ctx, int tp) {
-    auto it = ctx->tiles.find(tp);
-    if (it != ctx->tiles.end()) return &it->second;
+void build_tile_list(const bsg_ctx *ctx, int tp, std::vector<Tile> &tiles) {
     // tiles of tp positions, heaviest rows first (longest-processing-time order)
     std::vector<int32_t> order(ctx->nrows);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(),
                      [&](int32_t x, int32_t y) { return ctx->h_work[x] > ctx->h_work[y]; });
-    std::vector<Tile> tiles;
+    tiles.clear();
     for (int32_t r : order)
         for (int32_t p0 = 0; p0 < ctx->h_rowlen[r]; p0 += tp) {
             Tile t;
@@ -79,6 +77,13 @@ const TileSet *get_tiles(bsg_ctx *ctx, int tp) {
             t.pad = 0;
             tiles.push_back(t);
         }
+}
+
+const TileSet *get_tiles(bsg_ctx *ctx, int tp) {
+    auto it = ctx->tiles.find(tp);
+    if (it != ctx->tiles.end()) return &it->second;
+    std::vector<Tile> tiles;
+    build_tile_list(ctx, tp, tiles);
     TileSet ts;
     if (upload(ctx, ts.buf, tiles.data(), tiles.size() * sizeof(Tile))) return nullptr;
     ts.ntiles = (int32_t)tiles.size();

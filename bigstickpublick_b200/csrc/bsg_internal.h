@@ -157,6 +157,11 @@ int dev_alloc(bsg_ctx *ctx, DevBuf &b, size_t bytes);
 void dev_free(DevBuf &b);
 int upload(bsg_ctx *ctx, DevBuf &b, const void *src, size_t bytes);
 const TileSet *get_tiles(bsg_ctx *ctx, int tp);
+// row tiles of width tp in longest-processing-time order (host list)
+void build_tile_list(const bsg_ctx *ctx, int tp, std::vector<Tile> &tiles);
+// where applyH finds its row tiles; nullptr = the context's own (built and
+// cached on first use)
+typedef const TileSet *(*TileLookup)(bsg_ctx *ctx, int tp);
 int launch_applyh(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec, int accumulate,
-                  cudaStream_t s);
+                  cudaStream_t s, TileLookup lookup = nullptr);
 }  // namespace bsg

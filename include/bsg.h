@@ -167,6 +167,20 @@ int  bsg_applyh(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec, int
 int  bsg_applyh_stream(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec,
                        int flags, void *cuda_stream);
 
+/* ---- applyH on host vectors with no device allocation.  No counterpart in
+ *      the reference.  For callers that cannot allocate device memory when
+ *      they need a matvec (code running under CUDA stream capture, where
+ *      cudaMalloc is not allowed; hosts whose device memory is a fixed pool
+ *      owned by another component): vin/vout are staged through one static
+ *      __device__ array instead of buffers allocated on first use.  Each
+ *      vector (dim*nb*element size) must fit in BSG_NOALLOC_MAX_VECTOR_BYTES,
+ *      else BSG_ERR_ARG.  The first call on a device looks up the array's
+ *      address; make it before any stream capture.  All calls in the process
+ *      share the array: calls that overlap on the GPU race.  Same semantics as
+ *      bsg_applyh otherwise (host pointers only, BSG_ACCUMULATE honoured). ---- */
+#define BSG_NOALLOC_MAX_VECTOR_BYTES (8u << 20)
+int  bsg_applyh_noalloc(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec, int flags);
+
 /* ---- Lanczos: replaces lanczos_p (src/blanczosmain.f90:1413) and
  *      lanczos_block (:1804) with thick restart; everything stays on the
  *      device.  evals[nkeep]; evecs (host, fp64, dim x nkeep column-major) or
