@@ -122,6 +122,31 @@ def alg_bytes(stats, tables, nb, s):
     return nops * nb * 3 * s + jb + tables.dim * nb * 2 * s, nops
 
 
+def reduce_max(x, dist, device=None):
+    """Max over ranks of a per-rank time (the slowest replica sets the pace)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(steps, world, max_seconds):
+    """Whole-job rate: every rank runs `steps` matvecs on its own replica."""
+    return world * steps / max_seconds
+
+
+def table_checksum(tables):
+    """Digest of every table array: replicas must run identical workloads."""
+    import hashlib
+    h = hashlib.sha256()
+    for k in sorted(tables.a):
+        h.update(k.encode())
+        h.update(np.ascontiguousarray(tables.a[k]).tobytes())
+    return h.hexdigest()
+
+
 def cpu_baseline(tables, nb, prec, budget_s=10.0, nthreads=None):
     import oracle
     dt = np.float32 if prec == 4 else np.float64
@@ -259,12 +284,8 @@ def main():
     warm_ms = w0.elapsed_time(w1) / args.steps
     clocks = sampler.stop()
 
-    total_ms = float(sum(kern_ms))
-    if dist is not None:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * args.steps / (total_ms / 1e3)
+    total_ms = reduce_max(float(sum(kern_ms)), dist, device="cuda")
+    value = replica_rate(args.steps, world, total_ms / 1e3)
 
     # ---- end to end through the C ABI with pinned host buffers
     hin = torch.empty(shape, dtype=dt, pin_memory=True)
@@ -277,12 +298,8 @@ def main():
     t0 = time.perf_counter()
     for _ in range(args.steps):
         H.applyh(hin_np, hout_np)  # H2D copy, kernel, D2H copy, synchronize
-    e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = world * args.steps / e2e_s
+    e2e_s = reduce_max(time.perf_counter() - t0, dist, device="cuda")
+    e2e = replica_rate(args.steps, world, e2e_s)
     vbytes = tables.dim * nb * s_bytes
 
     peaks, peak_kind = load_peaks()

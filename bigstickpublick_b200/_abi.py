@@ -177,5 +177,9 @@ def gpu_lib():
         lib.bsg_grad.restype = C.c_int
         lib.bsg_get_stats.argtypes = [vp, C.POINTER(BsgStats)]
         lib.bsg_get_stats.restype = C.c_int
+        lib.bsg_validate_tables.argtypes = [C.POINTER(BsgTables), C.c_char_p, C.c_size_t]
+        lib.bsg_validate_tables.restype = C.c_int
+        lib.bsg_applyh_noalloc.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_int]
+        lib.bsg_applyh_noalloc.restype = C.c_int
         _gpu = lib
     return _gpu

@@ -121,7 +121,7 @@ void csr_by_out(const std::vector<int32_t> &out, const std::vector<Rec> &recs, i
     for (size_t k = 0; k < recs.size(); ++k) sorted[fill[out[k]]++] = recs[k];
 }
 
-int derive(bsg_ctx *ctx, const bsg_tables *t) {
+int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
     Validator V{ctx, ""};
     // ---- basic presence and sizes
     if (t->dimbasis <= 0 || t->nsd_p <= 0 || t->nsd_n <= 0)
@@ -526,6 +526,7 @@ int derive(bsg_ctx *ctx, const bsg_tables *t) {
         ctx->h_work[r] = (int32_t)std::min<int64_t>(w, INT32_MAX);
     }
 
+    if (!do_upload) return BSG_OK;
     // ---- upload: raw tables (unchanged) and derived layouts
     auto up = [&](DevBuf &b, const void *src, size_t bytes) { return upload(ctx, b, src, bytes); };
     int st = 0;
@@ -687,6 +688,24 @@ int bsg_create(const bsg_tables *t, const bsg_config *cfg, bsg_ctx **out) {
     ctx->stats.kernel_launches_per_matvec = 1;
     *out = ctx;
     return BSG_OK;
+}
+
+int bsg_validate_tables(const bsg_tables *t, char *msg, size_t len) {
+    if (msg && len) msg[0] = 0;
+    if (!t) return BSG_ERR_ARG;
+    bsg_ctx *ctx = new (std::nothrow) bsg_ctx();
+    if (!ctx) return BSG_ERR_NOMEM;
+    ctx->t = *t;
+    ctx->dim = t->dimbasis;
+    int st;
+    try {
+        st = derive(ctx, t, false);
+    } catch (const std::bad_alloc &) {
+        st = set_err(ctx, BSG_ERR_NOMEM, "host allocation failed while validating");
+    }
+    if (msg && len) std::snprintf(msg, len, "%s", ctx->last_error.c_str());
+    delete ctx;
+    return st;
 }
 
 int bsg_destroy(bsg_ctx *ctx) {

@@ -30,6 +30,16 @@ def _is_torch(x):
     return type(x).__module__.startswith("torch")
 
 
+def validate_tables(tables):
+    """Run bsg_create's table validator on the host (no GPU needed).
+    Returns (status, message); status 0 means valid."""
+    lib = _abi.gpu_lib()
+    t = tables.as_ctypes()
+    buf = C.create_string_buffer(512)
+    st = lib.bsg_validate_tables(C.byref(t), buf, 512)
+    return st, buf.value.decode()
+
+
 class Hamiltonian:
     def __init__(self, tables, device=0, max_nb=16, validate=True):
         self.lib = _abi.gpu_lib()

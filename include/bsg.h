@@ -152,6 +152,11 @@ typedef struct bsg_report {
 /* ---- lifecycle ---- */
 int  bsg_create(const bsg_tables *t, const bsg_config *cfg, bsg_ctx **out);
 int  bsg_destroy(bsg_ctx *ctx);
+/* the validator bsg_create runs, on the host only (no GPU needed): every
+ * index of every table checked against its array (the reference's own checks
+ * are check_opbundle_bounds, src/bparallel_opbundles.f90:1232-1286, and the
+ * range asserts of src/bapplyhlibOMP.f90:1968-1972); msg gets the reason */
+int  bsg_validate_tables(const bsg_tables *t, char *msg, size_t len);
 const char *bsg_strerror(int status);
 /* copies the latched message of the last failing call on ctx */
 int  bsg_last_error(const bsg_ctx *ctx, char *buf, size_t len);

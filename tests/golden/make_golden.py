@@ -1,0 +1,69 @@
+"""Regenerate tests/golden/mg25.json from the reference's own example files.
+
+Reads (from the reference checkout given as argv[1], default /root/reference):
+  examples/sd/sd.sps            orbits (isospin format)
+  examples/sd/usdb.int          USDB interaction (63 TBMEs + 3 SPEs)
+  examples/sd/input.mg25ref     4 protons, 5 neutrons, 2Jz = 1, scaling 1 18 25 0.3
+  examples/sd/input.mg25altwfn  same nucleus, scaling 0 1 1 1 (xspe = 0)
+  examples/sd/output/mg25ref.res, mg25alt.res   10 lowest energies, J, T (5 decimals)
+and writes the numbers as JSON.  Run once in a checkout that has the reference;
+the JSON is what the tests read (the reference is not needed at test time).
+"""
+import json
+import os
+import re
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from bigstickpublick_b200 import model  # noqa: E402
+
+
+def read_res(path):
+    states = []
+    lines = open(path).read().splitlines()
+    for i, ln in enumerate(lines):
+        if "State" in ln and "E" in ln and "Ex" in ln:
+            for row in lines[i + 1:]:
+                f = row.split()
+                if len(f) != 5 or not f[0].isdigit():
+                    break
+                states.append({"n": int(f[0]), "E": float(f[1]), "Ex": float(f[2]), "J": float(f[3]),
+                               "T": float(f[4])})
+            break
+    m = re.search(r"(\d+)\s+iterations", open(path).read())
+    return states, int(m.group(1)) if m else None
+
+
+def read_input(path):
+    toks = [ln.split("!")[0].split() for ln in open(path)]
+    toks = [t for t in toks if t]
+    # d / name / sps / "Z N" / 2Jz / n / int / scaling / end / ld / nkeep niter
+    zn = [int(x) for x in toks[3][:2]]
+    jz2 = int(toks[4][0])
+    scaling = [float(x) for x in toks[7][:4]]
+    nkeep, niter = (int(x) for x in toks[10][:2])
+    return {"np": zn[0], "nn": zn[1], "jz2": jz2, "scaling": scaling, "nkeep": nkeep, "niter": niter}
+
+
+def main():
+    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ex = os.path.join(ref, "examples", "sd")
+    orbits = model.read_sps(os.path.join(ex, "sd.sps"))
+    spe, tbme = model.read_int(os.path.join(ex, "usdb.int"), len(orbits))
+    out = {"source": "examples/sd of the BIGSTICK reference (sd.sps, usdb.int, input.mg25*, output/*.res)",
+           "orbits": orbits, "spe": spe, "tbme": tbme, "runs": {}}
+    for name, inp in (("mg25ref", "input.mg25ref"), ("mg25alt", "input.mg25altwfn")):
+        states, iters = read_res(os.path.join(ex, "output", name + ".res"))
+        run = read_input(os.path.join(ex, inp))
+        run.update({"states": states, "reference_iterations": iters,
+                    "res_file": f"examples/sd/output/{name}.res"})
+        out["runs"][name] = run
+    with open(os.path.join(HERE, "mg25.json"), "w") as f:
+        json.dump(out, f, indent=1)
+    print("wrote", os.path.join(HERE, "mg25.json"))
+
+
+if __name__ == "__main__":
+    main()
