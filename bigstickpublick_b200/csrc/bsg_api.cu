@@ -202,6 +202,7 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
     std::vector<PNRec> pnrec_all;
     std::vector<NNRec> nnrec_all;
     std::vector<int32_t> nnrec_op_all;
+    std::vector<int8_t> nnrec_ph_all;
     std::vector<BDPair> bd_all;
     auto get_nop = [&](int kind, int dir, int64_t x0, int64_t x1, int32_t &id) -> int {
         NKey k{kind, dir, x0, x1};
@@ -255,6 +256,7 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
         } else {
             std::vector<NNRec> recs(n);
             std::vector<int32_t> ops(n);
+            std::vector<int8_t> phs(n);
             for (int64_t x = x0; x <= x1; ++x) {
                 const int64_t isd = t->n2b_isd[x - 1], fsd = t->n2b_fsd[x - 1];
                 if (isd < 1 || fsd < 1 || isd > ctx->max_rowlen || fsd > ctx->max_rowlen)
@@ -271,6 +273,7 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
                 r.me = xme;
                 recs[x - x0] = r;
                 ops[x - x0] = opl;
+                phs[x - x0] = (int8_t)ph;
                 maxin = std::max(maxin, r.in);
                 maxout = std::max(maxout, out[x - x0]);
             }
@@ -279,6 +282,9 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
             csr_by_out(out, recs, maxout + 1, ptr, sorted);
             std::vector<int32_t> sorted_ops;
             csr_by_out(out, ops, maxout + 1, ptr, sorted_ops);
+            std::vector<int8_t> sorted_phs;
+            csr_by_out(out, phs, maxout + 1, ptr, sorted_phs);
+            nnrec_ph_all.insert(nnrec_ph_all.end(), sorted_phs.begin(), sorted_phs.end());
             op.rec_base = (int64_t)nnrec_all.size();
             op.ptr_base = (int64_t)nptr_all.size();
             op.nout = maxout + 1;
@@ -296,6 +302,7 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
     // ---- contributions per row
     std::vector<std::pair<int32_t, PPContrib>> pp;
     std::vector<int32_t> pp_op_tmp;
+    std::vector<int8_t> pp_ph_tmp;
     std::vector<std::pair<int32_t, NNContrib>> nn;
     std::vector<std::pair<int32_t, PNContrib>> pn;
     std::vector<std::pair<int32_t, SPEContrib>> spe;
@@ -338,6 +345,7 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
                 c.hi = hi;
                 pp.push_back({rf, c});
                 pp_op_tmp.push_back(opl);
+                pp_ph_tmp.push_back((int8_t)ph);
             }
             ops[1] += (px1 - px0 + 1) * (nx1 - nx0 + 1);
         } else if (op == BSG_OP_NN) {
@@ -509,7 +517,11 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
     std::vector<SPEContrib> h_spe;
     by_slot(pp, w_pp, ctx->h_pp_ptr, ctx->h_pp, &pp_perm);
     ctx->h_pp_op.resize(pp_perm.size());
-    for (size_t k = 0; k < pp_perm.size(); ++k) ctx->h_pp_op[k] = pp_op_tmp[pp_perm[k]];
+    ctx->h_pp_ph.resize(pp_perm.size());
+    for (size_t k = 0; k < pp_perm.size(); ++k) {
+        ctx->h_pp_op[k] = pp_op_tmp[pp_perm[k]];
+        ctx->h_pp_ph[k] = pp_ph_tmp[pp_perm[k]];
+    }
     by_slot(nn, w_nn, ctx->h_nn_ptr, ctx->h_nn, nullptr);
     by_slot(pn, w_pn, ctx->h_pn_ptr, ctx->h_pn, nullptr);
     by_slot(spe, w_spe, spe_ptr, h_spe, nullptr);
@@ -575,6 +587,8 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
         (st = up(ctx->nspe, nspe.data(), 4 * nspe.size())) ||
         (st = up(ctx->pp_op, ctx->h_pp_op.data(), 4 * ctx->h_pp_op.size())) ||
         (st = up(ctx->nnrec_op, nnrec_op_all.data(), 4 * nnrec_op_all.size())) ||
+        (st = up(ctx->nnrec_ph, nnrec_ph_all.data(), nnrec_ph_all.size())) ||
+        (st = up(ctx->pp_ph, ctx->h_pp_ph.data(), ctx->h_pp_ph.size())) ||
         (st = up(ctx->hmatpp_d, t->hmatpp, 4 * (size_t)t->nmatpp)) ||
         (st = up(ctx->hmatnn_d, t->hmatnn, 4 * (size_t)t->nmatnn)))
         return st;
@@ -620,7 +634,8 @@ void free_ctx(bsg_ctx *ctx) {
     for (auto &b : ctx->raw) dev_free(b);
     DevBuf *bufs[] = {&ctx->row_off, &ctx->pp_ptr, &ctx->nn_ptr, &ctx->pn_ptr, &ctx->spe_ptr, &ctx->pp, &ctx->nn,
                       &ctx->pn, &ctx->spe, &ctx->nops, &ctx->nptr, &ctx->pnrec, &ctx->nnrec, &ctx->bd, &ctx->hmatpn,
-                      &ctx->cpn, &ctx->dpn, &ctx->nspe, &ctx->pp_op, &ctx->nnrec_op, &ctx->hmatpp_d,
+                      &ctx->cpn, &ctx->dpn, &ctx->nspe, &ctx->pp_op, &ctx->nnrec_op, &ctx->nnrec_ph, &ctx->pp_ph,
+                      &ctx->hmatpp_d,
                       &ctx->hmatnn_d, &ctx->scratch_in, &ctx->scratch_out};
     for (DevBuf *b : bufs) dev_free(*b);
     for (auto &kv : ctx->tiles) dev_free(kv.second.buf);

@@ -139,11 +139,12 @@ struct bsg_ctx {
     std::vector<int32_t> h_pp_ptr, h_nn_ptr, h_pn_ptr;
     std::vector<bsg::PPContrib> h_pp;
     std::vector<int32_t> h_pp_op;        // hmatpp label of each PP contribution
+    std::vector<int8_t> h_pp_ph;         // jump phase of each PP contribution
     std::vector<bsg::NNContrib> h_nn;
     std::vector<bsg::PNContrib> h_pn;
     std::vector<bsg::NOp> h_nops;
     std::vector<int32_t> h_nnrec_op;     // hmatnn label of each NN record
-    bsg::DevBuf pp_op, nnrec_op;
+    bsg::DevBuf pp_op, nnrec_op, nnrec_ph, pp_ph;
     bsg_stats stats{};
     // scratch vectors for host-pointer applyh
     bsg::DevBuf scratch_in, scratch_out;

@@ -298,3 +298,35 @@ def sd_model(np_, nn, seed=None, jz2=0, interaction=None, spe_scale=1.0, tbme_sc
 def pf_model(np_, nn, seed, jz2=0):
     spe, tb = synthetic_interaction(PF_ORBITS, seed)
     return ModelSpec(PF_ORBITS, np_, nn, jz2, 1, spe, tb, 1.0, 1.0)
+
+
+def chain_rule(tables, dhmat):
+    """Gradient of one eigenvalue with respect to the coupled interaction.
+
+    dhmat: {'pp','nn','pn'} arrays dE/dhmat(label) (from Hamiltonian.grad, one
+    state), plus 'spe_p'/'spe_n' (dE/dpspe_h, dE/dnspe_h) when the tables use
+    SPE bundles.  Returns (dE/dV for every line of the interaction file in
+    spec.tbme order, dE/de for every orbit's SPE) through the builder's
+    uncoupling coefficients (src/btbme.f90:1209-1551, src/btbmepn.f90:177-587,
+    SPE subsumption src/bsppot.f90:39-238).
+    """
+    spec = tables.extra["spec"]
+    jac = tables.extra["jacobian"]
+    g_tb = np.zeros(max(1, len(spec.tbme)))
+    g_spe = np.zeros(len(spec.orbits))
+    for nm in ("pp", "nn", "pn"):
+        jt, js = jac[nm]
+        d = np.asarray(dhmat[nm], dtype=np.float64)
+        if d.size:
+            g_tb += d @ jt
+            g_spe += d @ js
+    if tables.s["call_spe"] and "spe_p" in dhmat:
+        # pspe_h(ip) = spe_scale * sum of occupied orbit SPEs
+        for key, orbk, bits in (("spe_p", "sp_orb_p", "sd_bits_p"), ("spe_n", "sp_orb_n", "sd_bits_n")):
+            orb = tables.extra[orbk]
+            b = tables.extra[bits]
+            d = np.asarray(dhmat[key], dtype=np.float64)
+            for q in range(len(orb)):
+                occ = ((b >> np.uint64(q)) & np.uint64(1)).astype(bool)
+                g_spe[orb[q]] += spec.spe_scale * d[occ].sum()
+    return g_tb[:len(spec.tbme)], g_spe

@@ -42,6 +42,8 @@ def lib():
         L.oracle_applyh_omp.restype = C.c_int
         L.oracle_count_ops.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
         L.oracle_count_ops.restype = None
+        L.oracle_density.argtypes = [C.c_void_p] + [C.c_void_p] * 6
+        L.oracle_density.restype = C.c_int
         _LIB = L
     return _LIB
 
@@ -84,6 +86,21 @@ def count_ops(tables):
     p, keep = _tp(tables)
     lib().oracle_count_ops(p, ops)
     return tuple(int(x) for x in ops)
+
+
+def density(tables, psi):
+    """dE/dhmat for a normalized eigenvector psi (restated two-body densities):
+    dict with 'pp', 'nn', 'pn' (and 'spe_p', 'spe_n' when call_spe)."""
+    psi = np.ascontiguousarray(psi, dtype=np.float64)
+    s = tables.s
+    out = {"pp": np.zeros(s["nmatpp"]), "nn": np.zeros(s["nmatnn"]), "pn": np.zeros(s["nmatpn"]),
+           "spe_p": np.zeros(s["nsd_p"]), "spe_n": np.zeros(s["nsd_n"])}
+    p, keep = _tp(tables)
+    st = lib().oracle_density(p, psi.ctypes.data, out["pp"].ctypes.data, out["nn"].ctypes.data,
+                              out["pn"].ctypes.data, out["spe_p"].ctypes.data, out["spe_n"].ctypes.data)
+    if st != 0:
+        raise RuntimeError(f"oracle_density status {st}")
+    return out
 
 
 def dense_from_applyh(tables, prec=8):

@@ -284,3 +284,62 @@ void oracle_count_ops(const bsg_tables *t, int64_t *ops /* [4]: spe, pp, nn, pn 
         }
     }
 }
+
+/* Two-body densities with both vectors equal to psi (FP64), the traversal of
+ * applyh{PP,NN,PN}bundled_den (src/bdenslib4.f90:129-729): for every bundle
+ * and every jump pair, dmat(label) += psi(f) * psi(i) * phase.  With the
+ * Hamiltonian's own bundles this is dE/dhmat(label) (Hellmann-Feynman). SPE
+ * bundles give d/dpspe_h and d/dnspe_h.  Outputs are accumulated (caller
+ * zeroes them). */
+int oracle_density(const bsg_tables *t, const double *psi, double *dpp, double *dnn, double *dpn,
+                   double *dspe_p, double *dspe_n) {
+    if (!t || !psi) return BSG_ERR_ARG;
+    for (int64_t ib = 0; ib < t->nbundles; ++ib) {
+        const int op = t->optype[ib], hc = t->hchar[ib];
+        const int64_t px0 = t->pxstart[ib], px1 = t->pxend[ib];
+        const int64_t nx0 = t->nxstart[ib], nx1 = t->nxend[ib];
+        const int64_t cs = t->cstride[ib] > 0 ? t->cstride[ib] : 1;
+        if (op == BSG_OP_PP) {
+            const int64_t *s1 = hc == 'b' ? t->p2b_fsd : t->p2b_isd;
+            const int64_t *s2 = hc == 'b' ? t->p2b_isd : t->p2b_fsd;
+            for (int64_t x = px0; x <= px1; ++x) {
+                double s = 0.0;
+                for (int64_t csd = nx0; csd <= nx1; csd += cs) {
+                    const int64_t nsd = t->nstart[csd - 1];
+                    s += psi[s2[x - 1] + nsd - 1] * psi[s1[x - 1] + nsd - 1];
+                }
+                dpp[t->p2b_op[x - 1] - 1] += s * t->p2b_phase[x - 1];
+            }
+        } else if (op == BSG_OP_NN) {
+            const int64_t *s1 = hc == 'b' ? t->n2b_fsd : t->n2b_isd;
+            const int64_t *s2 = hc == 'b' ? t->n2b_isd : t->n2b_fsd;
+            for (int64_t csd = px0; csd <= px1; csd += cs) {
+                const int64_t psd = t->pstart[csd - 1];
+                for (int64_t x = nx0; x <= nx1; ++x)
+                    dnn[t->n2b_op[x - 1] - 1] += psi[s2[x - 1] + psd - 1] * psi[s1[x - 1] + psd - 1] * t->n2b_phase[x - 1];
+            }
+        } else if (op == BSG_OP_PN) {
+            for (int64_t pj = px0; pj <= px1; ++pj) {
+                const int a = t->p1b_cop[pj - 1], c = t->p1b_dop[pj - 1];
+                for (int64_t nj = nx0; nj <= nx1; ++nj) {
+                    const int b = t->n1b_cop[nj - 1], d = t->n1b_dop[nj - 1];
+                    const int64_t lab = CPN(t, b, a) + DPN(t, d, c);
+                    const int64_t sf = t->n1b_fsd[nj - 1] + t->p1b_fsd[pj - 1];
+                    const int64_t si = t->n1b_isd[nj - 1] + t->p1b_isd[pj - 1];
+                    dpn[lab - 1] += psi[sf - 1] * psi[si - 1] * t->p1b_phase[pj - 1] * t->n1b_phase[nj - 1];
+                }
+            }
+        } else if (op == BSG_OP_SPE && dspe_p && dspe_n) {
+            for (int64_t ip = px0; ip <= px1; ++ip) {
+                int64_t statef = t->pstart[ip - 1] + t->nstart[nx0 - 1];
+                for (int64_t in = nx0; in <= nx1; ++in) {
+                    const double p2 = psi[statef - 1] * psi[statef - 1];
+                    dspe_p[ip - 1] += p2;
+                    dspe_n[in - 1] += p2;
+                    ++statef;
+                }
+            }
+        }
+    }
+    return BSG_OK;
+}

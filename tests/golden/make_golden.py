@@ -36,6 +36,28 @@ def read_res(path):
     return states, int(m.group(1)) if m else None
 
 
+def read_diag_density(path):
+    """Jt=0, Tt=0 one-body densities rho(a,b) of the blocks whose initial and
+    final state coincide: {state: [[a, b, rho_T0, rho_T1], ...], 'J2': 2J}"""
+    lines = open(path).read().splitlines()
+    out = {}
+    i = 0
+    while i < len(lines):
+        m = re.match(r"\s*Initial state #\s+(\d+).*2xJ, 2xT =\s+(\d+)\s+(\d+)", lines[i])
+        if m and i + 1 < len(lines):
+            f = re.match(r"\s*Final state\s+#\s+(\d+)", lines[i + 1])
+            if f and f.group(1) == m.group(1) and "Jt =   0, Tt = 0" in lines[i + 2]:
+                rows = []
+                for row in lines[i + 3:]:
+                    t = row.split()
+                    if len(t) != 4 or not t[0].isdigit():
+                        break
+                    rows.append([int(t[0]), int(t[1]), float(t[2]), float(t[3])])
+                out[m.group(1)] = {"J2": int(m.group(2)), "T2": int(m.group(3)), "rho": rows}
+        i += 1
+    return out
+
+
 def read_input(path):
     toks = [ln.split("!")[0].split() for ln in open(path)]
     toks = [t for t in toks if t]
@@ -58,7 +80,8 @@ def main():
         states, iters = read_res(os.path.join(ex, "output", name + ".res"))
         run = read_input(os.path.join(ex, inp))
         run.update({"states": states, "reference_iterations": iters,
-                    "res_file": f"examples/sd/output/{name}.res"})
+                    "res_file": f"examples/sd/output/{name}.res",
+                    "density_jt0": read_diag_density(os.path.join(ex, "output", name + ".res"))})
         out["runs"][name] = run
     with open(os.path.join(HERE, "mg25.json"), "w") as f:
         json.dump(out, f, indent=1)
