@@ -177,6 +177,51 @@ def traffic_from_profile(workload, nb, prec):
         return None
 
 
+def lanczos_leg(H, tables, args):
+    """The eigenvalue side of the metric: FP64 vs mixed (FP32 applyH, FP64
+    Lanczos) on the same workload and pivot, lowest 10 states, fixed
+    iteration count; relative eigenvalue error of mixed vs FP64 and the
+    iterations per second of each.  For the pf 4p4n workload also the block
+    (nb = 8) mixed run with thick restart keeping 20 vectors."""
+    import torch
+    rng = np.random.default_rng(11)
+    piv = rng.standard_normal(tables.dim)
+    out = {}
+    niter = args.lanczos_iters
+    runs = {}
+    for name, prec in (("fp64", 8), ("mixed", 4)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ev, _, rep = H.lanczos(nkeep=10, niter=niter, matvec_prec=prec, fixed_iter=True, pivot=piv)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        runs[name] = (ev, rep, el)
+        out[name] = {"iterations": rep["total_iterations"], "its_per_s": rep["total_iterations"] / el,
+                     "wall_s": el, "t_matvec_ms": rep["t_matvec_ms"], "t_reorth_ms": rep["t_reorth_ms"],
+                     "t_eig_ms": rep["t_eig_ms"], "lowest": [float(x) for x in ev[:3]]}
+    e64, e32 = runs["fp64"][0], runs["mixed"][0]
+    out["mixed_vs_fp64_max_rel_eig_err"] = float(np.max(np.abs(e32 - e64) / np.abs(e64)))
+    out["speedup_its_per_s"] = out["mixed"]["its_per_s"] / out["fp64"]["its_per_s"]
+    out["config"] = f"{niter} iterations, lowest 10, fixed iteration count, seeded generic pivot"
+    if args.block_leg:
+        nb = 8
+        pivb = rng.standard_normal(tables.dim * nb)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        evb, _, repb = H.lanczos(nkeep=10, niter=args.block_iters, nb=nb, nthick_add=10, max_restarts=args.block_restarts,
+                                 matvec_prec=4, converge_tol=1e-9, pivot=pivb)
+        torch.cuda.synchronize()
+        elb = time.perf_counter() - t0
+        out["block_mixed"] = {"nb": nb, "keep": 20, "iterations": repb["total_iterations"], "restarts": repb["restarts"],
+                              "vector_matvecs_per_s": repb["total_iterations"] * nb / elb, "wall_s": elb,
+                              "max_rel_eig_err_vs_fp64": float(np.max(np.abs(evb - e64) / np.abs(e64))),
+                              "converged": repb["converged"], "t_matvec_ms": repb["t_matvec_ms"],
+                              "t_reorth_ms": repb["t_reorth_ms"], "t_eig_ms": repb["t_eig_ms"]}
+        out["block_vs_fp64_vector_matvec_rate"] = out["block_mixed"]["vector_matvecs_per_s"] / out["fp64"]["its_per_s"]
+        out["fp64"]["vector_matvecs_per_s"] = out["fp64"]["its_per_s"]
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -221,6 +266,11 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=3.0)
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-lanczos", action="store_true")
+    ap.add_argument("--lanczos-iters", type=int, default=300)
+    ap.add_argument("--block-leg", action="store_true")
+    ap.add_argument("--block-iters", type=int, default=20)
+    ap.add_argument("--block-restarts", type=int, default=30)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -322,6 +372,8 @@ def main():
         "clocks": clocks,
         "warm_l2_matvec_per_s": world / (warm_ms / 1e3),
     }
+    if rank == 0 and not args.no_lanczos:
+        line["lanczos"] = lanczos_leg(H, tables, args)
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, cores, n, el = cpu_baseline(tables, nb, prec, budget_s=args.cpu_budget)
         line["cpu_baseline"] = {"value": rate, "unit": "matvec/s", "cores": cores, "kind": "port",

@@ -53,7 +53,7 @@ struct Lz {
     int64_t n;
     int nb, prec;
     int maxcol;      // history columns
-    DevBuf hist, W, X, Y, tmp, partial, coef, sqp, sq, Adev, Vtmp, Zdev, wdev, stat, al, bt, ev, M;
+    DevBuf hist, W, X, Y, tmp, partial, coef, sqp, sq, Adev, Vtmp, Zdev, wdev, stat, al, bt, ev, M, tau, ework;
     std::vector<double> T;  // host projected matrix (maxcol x maxcol), row-major
     float t_mv = 0, t_ort = 0, t_eig = 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -80,57 +80,53 @@ float elapsed(Lz &L) {
     return ms;
 }
 
-// dense symmetric eigenproblem of T[0:m,0:m] on the device; evals (host) and
-// optionally eigenvectors (host, row-major m x m, column j = vector j)
-int eig_dense(Lz &L, int m, std::vector<double> &w, std::vector<double> *Z) {
-    std::vector<double> A((size_t)m * m);
-    for (int i = 0; i < m; ++i)
-        for (int j = 0; j < m; ++j) A[(size_t)i * m + j] = 0.5 * (L.Tm(i, j) + L.Tm(j, i));
-    cudaEventRecord(L.e0, L.s);
-    CK(cudaMemcpyAsync(L.Adev.p, A.data(), sizeof(double) * m * m, cudaMemcpyHostToDevice, L.s));
-    CK(jacobi(m, (double *)L.Adev.p, (double *)L.Vtmp.p, (double *)L.wdev.p, (double *)L.Zdev.p, (int *)L.stat.p, L.s));
-    w.resize(m);
-    CK(cudaMemcpyAsync(w.data(), L.wdev.p, sizeof(double) * m, cudaMemcpyDeviceToHost, L.s));
-    int st = 0;
-    CK(cudaMemcpyAsync(&st, L.stat.p, sizeof(int), cudaMemcpyDeviceToHost, L.s));
-    if (Z) {
-        Z->resize((size_t)m * m);
-        CK(cudaMemcpyAsync(Z->data(), L.Zdev.p, sizeof(double) * m * m, cudaMemcpyDeviceToHost, L.s));
-    }
-    cudaEventRecord(L.e1, L.s);
-    CK(cudaStreamSynchronize(L.s));
-    L.t_eig += elapsed(L);
-    if (st) return set_err(L.ctx, BSG_ERR_NOT_CONVERGED, "Jacobi eigensolver did not converge");
-    return BSG_OK;
-}
-
-// lowest nwant eigenvalues of the scalar projected matrix (arrow k, size m)
-int eig_arrow(Lz &L, int m, int k, int nwant, std::vector<double> &e) {
-    std::vector<double> al(m), bt(std::max(m, 1), 0.0);
-    for (int i = 0; i < m; ++i) al[i] = L.Tm(i, i);
-    for (int i = 0; i < k; ++i) bt[i] = L.Tm(k, i);
-    for (int i = k; i + 1 < m; ++i) bt[i] = L.Tm(i + 1, i);
-    // Gershgorin bounds
+// Lowest `want` eigenpairs of the projected matrix T[0:m,0:m] on the device.
+// Scalar Lanczos: T is arrowhead-tridiagonal (arrow of size k) -> Sturm
+// bisection + inverse iteration.  Block Lanczos: T is dense (band + arrow) ->
+// Householder tridiagonalization first, then the same, then the reflectors.
+// w (host) gets the eigenvalues; Z (host, column-major m x want) the vectors.
+int eig_lowest(Lz &L, int m, int k, int want, std::vector<double> &w, std::vector<double> *Z) {
+    want = std::min(want, m);
     double glo = 1e300, ghi = -1e300;
     for (int i = 0; i < m; ++i) {
         double r = 0.0;
-        if (i < k) r = std::fabs(bt[i]);
-        if (i == k) for (int j = 0; j < k; ++j) r += std::fabs(bt[j]);
-        if (i >= k && i + 1 < m) r += std::fabs(bt[i]);
-        if (i > k) r += std::fabs(bt[i - 1]);
-        glo = std::min(glo, al[i] - r);
-        ghi = std::max(ghi, al[i] + r);
+        for (int j = 0; j < m; ++j)
+            if (j != i) r += std::fabs(L.Tm(i, j));
+        glo = std::min(glo, L.Tm(i, i) - r);
+        ghi = std::max(ghi, L.Tm(i, i) + r);
     }
-    const double pad = 1e-12 * std::max(std::fabs(glo), std::fabs(ghi)) + 1e-300;
+    const double scale = std::max(std::fabs(glo), std::fabs(ghi));
+    const double pad = 1e-12 * scale + 1e-300;
     glo -= pad;
     ghi += pad;
-    nwant = std::min(nwant, m);
     cudaEventRecord(L.e0, L.s);
-    CK(cudaMemcpyAsync(L.al.p, al.data(), sizeof(double) * m, cudaMemcpyHostToDevice, L.s));
-    CK(cudaMemcpyAsync(L.bt.p, bt.data(), sizeof(double) * m, cudaMemcpyHostToDevice, L.s));
-    CK(bisect_arrow(m, k, (const double *)L.al.p, (const double *)L.bt.p, nwant, glo, ghi, (double *)L.ev.p, L.s));
-    e.resize(nwant);
-    CK(cudaMemcpyAsync(e.data(), L.ev.p, sizeof(double) * nwant, cudaMemcpyDeviceToHost, L.s));
+    int kk = k;
+    if (L.nb == 1) {
+        std::vector<double> al(m), bt(std::max(m, 1), 0.0);
+        for (int i = 0; i < m; ++i) al[i] = L.Tm(i, i);
+        for (int i = 0; i < k; ++i) bt[i] = L.Tm(k, i);
+        for (int i = k; i + 1 < m; ++i) bt[i] = L.Tm(i + 1, i);
+        CK(cudaMemcpyAsync(L.al.p, al.data(), sizeof(double) * m, cudaMemcpyHostToDevice, L.s));
+        CK(cudaMemcpyAsync(L.bt.p, bt.data(), sizeof(double) * m, cudaMemcpyHostToDevice, L.s));
+    } else {
+        std::vector<double> A((size_t)m * m);
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < m; ++j) A[(size_t)i * m + j] = 0.5 * (L.Tm(i, j) + L.Tm(j, i));
+        CK(cudaMemcpyAsync(L.Adev.p, A.data(), sizeof(double) * m * m, cudaMemcpyHostToDevice, L.s));
+        CK(tridiag(m, (double *)L.Adev.p, (double *)L.al.p, (double *)L.bt.p, (double *)L.Vtmp.p, (double *)L.tau.p,
+                   (double *)L.ework.p, L.s));
+        kk = 0;
+    }
+    CK(bisect_arrow(m, kk, (const double *)L.al.p, (const double *)L.bt.p, want, glo, ghi, (double *)L.wdev.p, L.s));
+    w.resize(want);
+    CK(cudaMemcpyAsync(w.data(), L.wdev.p, sizeof(double) * want, cudaMemcpyDeviceToHost, L.s));
+    if (Z) {
+        CK(inverse_iter_arrow(m, kk, (const double *)L.al.p, (const double *)L.bt.p, (const double *)L.wdev.p, want,
+                              scale, (double *)L.Zdev.p, (double *)L.ework.p + 2 * (size_t)m, L.s));
+        if (L.nb > 1) CK(apply_q(m, want, (const double *)L.Vtmp.p, (const double *)L.tau.p, (double *)L.Zdev.p, L.s));
+        Z->resize((size_t)m * want);
+        CK(cudaMemcpyAsync(Z->data(), L.Zdev.p, sizeof(double) * m * want, cudaMemcpyDeviceToHost, L.s));
+    }
     cudaEventRecord(L.e1, L.s);
     CK(cudaStreamSynchronize(L.s));
     L.t_eig += elapsed(L);
@@ -320,13 +316,7 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
         // ---- eigenvalues and convergence (convergence_test option 0)
         if (cur >= niter * nb) finished = true;
         if (!p->fixed_iter && mT > ncheck && mT < (int64_t)n) {
-            if (nb == 1)
-                ST(eig_arrow(L, mT, karrow, ncheck, e));
-            else {
-                std::vector<double> w;
-                ST(eig_dense(L, mT, w, nullptr));
-                e.assign(w.begin(), w.begin() + std::min<int>(ncheck, mT));
-            }
+            ST(eig_lowest(L, mT, karrow, ncheck, e, nullptr));
             if ((int)eold.size() == (int)e.size()) {
                 double ed = 0.0;
                 for (size_t j = 0; j < e.size(); ++j) ed += std::fabs(eold[j] - e[j]);
@@ -348,8 +338,8 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
             }
             const int m = mT - nb;           // projected matrix without its last block
             const int k = std::min(nthick, m - 1);
-            std::vector<double> w, Z;
-            ST(eig_dense(L, m, w, &Z));
+            std::vector<double> w, Z;          // Z column-major m x k
+            ST(eig_lowest(L, m, karrow, k, w, &Z));
             // coupling rows: beta_prev block between block [m-nb, m) and [m, m+nb)
             std::vector<double> bp((size_t)nb * nb);
             for (int a = 0; a < nb; ++a)
@@ -358,7 +348,7 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
             cudaEventRecord(L.e0, L.s);
             std::vector<double> Yk((size_t)m * k);
             for (int j = 0; j < m; ++j)
-                for (int l = 0; l < k; ++l) Yk[(size_t)j * k + l] = Z[(size_t)j * m + l];
+                for (int l = 0; l < k; ++l) Yk[(size_t)j * k + l] = Z[(size_t)l * m + j];
             DevBuf Yd;
             ST(upload(ctx, Yd, Yk.data(), sizeof(double) * Yk.size()));
             cudaError_t te = transform(L.col(0), m, (const double *)Yd.p, k, k, (double *)L.tmp.p, n, n, n, L.s);
@@ -376,7 +366,7 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
             for (int a = 0; a < nb; ++a)
                 for (int i = 0; i < k; ++i) {
                     double c_ = 0.0;
-                    for (int c = 0; c < nb; ++c) c_ += bp[(size_t)a * nb + c] * Z[(size_t)(m - nb + c) * m + i];
+                    for (int c = 0; c < nb; ++c) c_ += bp[(size_t)a * nb + c] * Z[(size_t)i * m + (m - nb + c)];
                     L.Tm(k + a, i) = c_;
                     L.Tm(i, k + a) = c_;
                 }
@@ -390,14 +380,14 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
     }
 
     // ---- final Ritz pairs of T[0:mT] (lanczos_output, src/blanczoslib.f90:1268)
-    std::vector<double> w, Z;
-    ST(eig_dense(L, mT, w, evecs ? &Z : nullptr));
+    std::vector<double> w, Z;          // Z column-major mT x nk
     const int nk = std::min(nkeep, mT);
+    ST(eig_lowest(L, mT, karrow, nk, w, evecs ? &Z : nullptr));
     for (int j = 0; j < nkeep; ++j) evals[j] = (j < nk) ? w[j] : NAN;
     if (evecs) {
         std::vector<double> Yk((size_t)mT * nk);
         for (int j = 0; j < mT; ++j)
-            for (int l = 0; l < nk; ++l) Yk[(size_t)j * nk + l] = Z[(size_t)j * mT + l];
+            for (int l = 0; l < nk; ++l) Yk[(size_t)j * nk + l] = Z[(size_t)l * mT + j];
         DevBuf Yd, out;
         ST(upload(ctx, Yd, Yk.data(), sizeof(double) * Yk.size()));
         int st2 = dev_alloc(ctx, out, sizeof(double) * (size_t)n * nk);
@@ -431,7 +421,8 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
                            double *evecs, bsg_report *rep) {
     if (!ctx) return BSG_ERR_ARG;
     if (!p || !evals) return set_err(ctx, BSG_ERR_ARG, "bsg_lanczos: null argument");
-    if (p->nb < 1 || p->nb > 16 || p->nkeep < 1 || p->niter < 2 ||
+    if ((p->nb != 1 && p->nb != 2 && p->nb != 4 && p->nb != 8 && p->nb != 16) || p->nkeep < 1 || p->niter < 2 ||
+        p->nkeep + std::max(p->nthick_add, 0) > 128 ||
         (p->matvec_prec != BSG_PREC_FP32 && p->matvec_prec != BSG_PREC_FP64))
         return set_err(ctx, BSG_ERR_ARG, "bsg_lanczos: bad parameters");
     if ((int64_t)p->niter * p->nb + p->nb > 2048)
@@ -470,7 +461,8 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
         (st = dev_alloc(ctx, L.Zdev, sizeof(double) * (size_t)N * N)) || (st = dev_alloc(ctx, L.wdev, sizeof(double) * N)) ||
         (st = dev_alloc(ctx, L.stat, sizeof(int) * 4)) || (st = dev_alloc(ctx, L.al, sizeof(double) * N)) ||
         (st = dev_alloc(ctx, L.bt, sizeof(double) * N)) || (st = dev_alloc(ctx, L.ev, sizeof(double) * N)) ||
-        (st = dev_alloc(ctx, L.M, sizeof(double) * 16 * 16))) {
+        (st = dev_alloc(ctx, L.M, sizeof(double) * 16 * 16)) || (st = dev_alloc(ctx, L.tau, sizeof(double) * N)) ||
+        (st = dev_alloc(ctx, L.ework, sizeof(double) * ((size_t)2 * N + (size_t)6 * N * std::min(N, 128))))) {
         // fall through to cleanup
     }
     if (!st) {
@@ -492,7 +484,7 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
         cudaEventDestroy(L.e1);
     }
     DevBuf *bufs[] = {&L.hist, &L.W, &L.X, &L.Y, &L.tmp, &L.partial, &L.coef, &L.sqp, &L.sq, &L.Adev,
-                      &L.Vtmp, &L.Zdev, &L.wdev, &L.stat, &L.al, &L.bt, &L.ev, &L.M};
+                      &L.Vtmp, &L.Zdev, &L.wdev, &L.stat, &L.al, &L.bt, &L.ev, &L.M, &L.tau, &L.ework};
     cudaStreamSynchronize(L.s);
     for (DevBuf *b : bufs) dev_free(*b);
     return st;

@@ -25,88 +25,114 @@ namespace bsg {
 
 constexpr int kDotThreads = 256;
 constexpr int kDotTile = 512;      // rows per tile
-constexpr int kMaxPairsPerThread = 16;
 
 // C[p] partials: pairs p = a*nB + b, a < nA, b < nB; A, B column-major with
-// leading dimension ld (vector j at base + j*ld).  partial[p * gridDim.x + blockIdx.x].
+// leading dimension ld (vector j at base + j*ld).  Each CTA walks row chunks
+// (grid-stride); the chunk of B is staged in shared memory, warp w takes
+// vectors a = w, w+8, ... and reads them coalesced, lanes keep NB partial
+// sums, a warp reduction adds them into the CTA's shared accumulator (each
+// (a,b) owned by one warp), and the CTA writes partial[p * gridDim.x + cta].
+template <int NB>
 __global__ void __launch_bounds__(kDotThreads) k_multidot(const double *__restrict__ A, int nA,
-                                                         const double *__restrict__ B, int nB,
-                                                         int64_t n, int64_t ld, double *__restrict__ partial) {
-    extern __shared__ double sB[];  // [kDotTile][nB]
-    const int npairs = nA * nB;
-    double acc[kMaxPairsPerThread];
-#pragma unroll
-    for (int k = 0; k < kMaxPairsPerThread; ++k) acc[k] = 0.0;
+                                                         const double *__restrict__ B, int64_t n, int64_t ld,
+                                                         double *__restrict__ partial) {
+    extern __shared__ double sm[];
+    double *sB = sm;                       // [kDotTile][NB]
+    double *sAcc = sm + kDotTile * NB;     // [nA][NB]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = kDotThreads / 32;
+    for (int e = threadIdx.x; e < nA * NB; e += kDotThreads) sAcc[e] = 0.0;
     for (int64_t t0 = (int64_t)blockIdx.x * kDotTile; t0 < n; t0 += (int64_t)gridDim.x * kDotTile) {
         const int rows = (int)((n - t0) < kDotTile ? (n - t0) : kDotTile);
         __syncthreads();
-        for (int e = threadIdx.x; e < rows * nB; e += kDotThreads) {
-            const int r = e % rows, b = e / rows;
-            sB[r * nB + b] = B[(int64_t)b * ld + t0 + r];
+        for (int e = threadIdx.x; e < rows * NB; e += kDotThreads) {
+            const int b = e / rows, r = e - b * rows;
+            sB[r * NB + b] = B[(int64_t)b * ld + t0 + r];
         }
         __syncthreads();
-#pragma unroll
-        for (int k = 0; k < kMaxPairsPerThread; ++k) {
-            const int p = threadIdx.x + k * kDotThreads;
-            if (p >= npairs) break;
-            const int a = p / nB, b = p - a * nB;
+        for (int a = warp; a < nA; a += nw) {
             const double *__restrict__ col = A + (int64_t)a * ld + t0;
-            double s = 0.0;
-            for (int r = 0; r < rows; ++r) s = fma(__ldg(col + r), sB[r * nB + b], s);
-            acc[k] += s;
+            double acc[NB];
+#pragma unroll
+            for (int b = 0; b < NB; ++b) acc[b] = 0.0;
+            for (int r = lane; r < rows; r += 32) {
+                const double x = __ldg(col + r);
+#pragma unroll
+                for (int b = 0; b < NB; ++b) acc[b] = fma(x, sB[r * NB + b], acc[b]);
+            }
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                double v = acc[b];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0) sAcc[a * NB + b] += v;
+            }
         }
     }
-#pragma unroll
-    for (int k = 0; k < kMaxPairsPerThread; ++k) {
-        const int p = threadIdx.x + k * kDotThreads;
-        if (p < npairs) partial[(int64_t)p * gridDim.x + blockIdx.x] = acc[k];
-    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < nA * NB; e += kDotThreads) partial[(int64_t)e * gridDim.x + blockIdx.x] = sAcc[e];
 }
 
-// out[p] = sum over g of partial[p*G + g] (fixed order); one thread per p
+// out[p] = sum over g of partial[p*G + g]: one warp per p, lanes take g = lane,
+// lane+32, ... in order and a fixed shuffle tree combines them
 __global__ void k_reduce_partials(const double *__restrict__ partial, int npairs, int G, double *__restrict__ out) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if (p >= npairs) return;
     double s = 0.0;
-    for (int g = 0; g < G; ++g) s += partial[(int64_t)p * G + g];
-    out[p] = s;
+    for (int g = lane; g < G; g += 32) s += partial[(int64_t)p * G + g];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) out[p] = s;
 }
 
 // W[b] -= sum_j H[j] * C[j*nB + b]   (j < k), fused sum of squares of the
-// result per column when sq != nullptr (partials per block, nB entries)
+// result per column when sq != nullptr (partials per block, NB entries)
+template <int NB>
 __global__ void __launch_bounds__(256) k_sub_gemv(const double *__restrict__ H, int k, const double *__restrict__ C,
-                                                  double *__restrict__ W, int nB, int64_t n, int64_t ld,
+                                                  double *__restrict__ W, int64_t n, int64_t ld,
                                                   double *__restrict__ sq) {
-    extern __shared__ double sC[];  // [k*nB] then [8][nB] warp sums
-    for (int e = threadIdx.x; e < k * nB; e += blockDim.x) sC[e] = C[e];
+    extern __shared__ double sC[];  // [k*NB] then [8][NB] warp sums
+    for (int e = threadIdx.x; e < k * NB; e += blockDim.x) sC[e] = C[e];
     __syncthreads();
-    double sqacc[16];
-    for (int b = 0; b < 16; ++b) sqacc[b] = 0.0;
+    double sqacc[NB];
+#pragma unroll
+    for (int b = 0; b < NB; ++b) sqacc[b] = 0.0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        double acc[16];
-        for (int b = 0; b < nB; ++b) acc[b] = 0.0;
-        for (int j = 0; j < k; ++j) {
-            const double h = __ldg(H + (int64_t)j * ld + i);
-            for (int b = 0; b < nB; ++b) acc[b] = fma(h, sC[j * nB + b], acc[b]);
+        double acc[NB];
+#pragma unroll
+        for (int b = 0; b < NB; ++b) acc[b] = 0.0;
+        int j = 0;
+        for (; j + 1 < k; j += 2) {
+            const double h0 = __ldg(H + (int64_t)j * ld + i), h1 = __ldg(H + (int64_t)(j + 1) * ld + i);
+#pragma unroll
+            for (int b = 0; b < NB; ++b) acc[b] = fma(h1, sC[(j + 1) * NB + b], fma(h0, sC[j * NB + b], acc[b]));
         }
-        for (int b = 0; b < nB; ++b) {
+        if (j < k) {
+            const double h0 = __ldg(H + (int64_t)j * ld + i);
+#pragma unroll
+            for (int b = 0; b < NB; ++b) acc[b] = fma(h0, sC[j * NB + b], acc[b]);
+        }
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
             const double w = W[(int64_t)b * ld + i] - acc[b];
             W[(int64_t)b * ld + i] = w;
             sqacc[b] = fma(w, w, sqacc[b]);
         }
     }
     if (!sq) return;
-    double *red = sC + k * nB;
+    double *red = sC + k * NB;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int b = 0; b < nB; ++b) {
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
         double v = sqacc[b];
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-        if (lane == 0) red[warp * nB + b] = v;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) red[warp * NB + b] = v;
     }
     __syncthreads();
-    if (threadIdx.x < nB) {
+    if (threadIdx.x < NB) {
         double v = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[w * nB + threadIdx.x];
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[w * NB + threadIdx.x];
         sq[(int64_t)threadIdx.x * gridDim.x + blockIdx.x] = v;
     }
 }
@@ -359,6 +385,263 @@ __global__ void k_random_cols(double *W, int nB, int64_t n, int64_t ld, uint64_t
         }
 }
 
+// ---------------------------------------------------- inverse iteration ---
+// Eigenvectors of the arrowhead-tridiagonal T (see sturm_count) for given
+// eigenvalues: one thread per vector, three steps of inverse iteration
+// (T - theta) x_{new} = x / |x|.  The arrow rows i < k are eliminated into
+// row k (Schur complement), the remaining tridiagonal block is factored by
+// Gaussian elimination with partial pivoting (the dgttrf/dgttrs scheme), and
+// the arrow unknowns are recovered by back substitution.  Tiny pivots are
+// replaced by +-pivmin.  work: 6*n doubles per vector.
+__device__ void arrow_solve(int n, int k, const double *__restrict__ al, const double *__restrict__ bt, double th,
+                            double pivmin, double *x, double *w) {
+    const int m = n - k;
+    double *dl = w, *d = w + n, *du = w + 2 * n, *du2 = w + 3 * n, *b = w + 4 * n;
+    int *piv = reinterpret_cast<int *>(w + 5 * n);
+    // Schur complement of the arrow block into row k
+    double sdiag = 0.0, srhs = 0.0;
+    for (int i = 0; i < k; ++i) {
+        double di = al[i] - th;
+        if (fabs(di) < pivmin) di = (di < 0 ? -pivmin : pivmin);
+        sdiag += bt[i] * bt[i] / di;
+        srhs += bt[i] * x[i] / di;
+    }
+    for (int i = 0; i < m; ++i) {
+        d[i] = al[k + i] - th;
+        b[i] = x[k + i];
+        if (i + 1 < m) { dl[i] = bt[k + i]; du[i] = bt[k + i]; }
+        du2[i] = 0.0;
+    }
+    d[0] -= sdiag;
+    b[0] -= srhs;
+    // factor with partial pivoting
+    for (int i = 0; i + 1 < m; ++i) {
+        if (fabs(d[i]) >= fabs(dl[i])) {
+            piv[i] = i;
+            if (fabs(d[i]) < pivmin) d[i] = (d[i] < 0 ? -pivmin : pivmin);
+            const double f = dl[i] / d[i];
+            dl[i] = f;
+            d[i + 1] -= f * du[i];
+        } else {
+            piv[i] = i + 1;
+            const double f = d[i] / dl[i];
+            d[i] = dl[i];
+            dl[i] = f;
+            const double t = du[i];
+            du[i] = d[i + 1];
+            d[i + 1] = t - f * d[i + 1];
+            if (i + 2 < m) {
+                du2[i] = du[i + 1];
+                du[i + 1] = -f * du[i + 1];
+            }
+        }
+    }
+    if (fabs(d[m - 1]) < pivmin) d[m - 1] = (d[m - 1] < 0 ? -pivmin : pivmin);
+    // forward: L
+    for (int i = 0; i + 1 < m; ++i) {
+        if (piv[i] == i) {
+            b[i + 1] -= dl[i] * b[i];
+        } else {
+            const double t = b[i];
+            b[i] = b[i + 1];
+            b[i + 1] = t - dl[i] * b[i + 1];
+        }
+    }
+    // back: U
+    b[m - 1] /= d[m - 1];
+    if (m > 1) b[m - 2] = (b[m - 2] - du[m - 2] * b[m - 1]) / d[m - 2];
+    for (int i = m - 3; i >= 0; --i) b[i] = (b[i] - du[i] * b[i + 1] - du2[i] * b[i + 2]) / d[i];
+    // arrow unknowns
+    const double xk = b[0];
+    for (int i = 0; i < k; ++i) {
+        double di = al[i] - th;
+        if (fabs(di) < pivmin) di = (di < 0 ? -pivmin : pivmin);
+        x[i] = (x[i] - bt[i] * xk) / di;
+    }
+    for (int i = 0; i < m; ++i) x[k + i] = b[i];
+}
+
+__global__ void k_inverse_iter_arrow(int n, int k, const double *__restrict__ al, const double *__restrict__ bt,
+                                     const double *__restrict__ ev, int nvec, double scale, double *__restrict__ Z,
+                                     double *__restrict__ work) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nvec) return;
+    double *x = Z + (int64_t)j * n;  // column j (column-major n x nvec)
+    double *w = work + (int64_t)j * 6 * n;
+    const double pivmin = fmax(1e-300, 2.2e-16 * scale);
+    // deterministic start vector with components in every direction
+    for (int i = 0; i < n; ++i) x[i] = 1.0 + 0.5 * sin(0.7 * (double)(i + 1) + 1.3 * (double)(j + 1));
+    for (int it = 0; it < 3; ++it) {
+        double nrm = 0.0;
+        for (int i = 0; i < n; ++i) nrm += x[i] * x[i];
+        nrm = 1.0 / sqrt(nrm);
+        for (int i = 0; i < n; ++i) x[i] *= nrm;
+        arrow_solve(n, k, al, bt, ev[j], pivmin, x, w);
+    }
+    double nrm = 0.0;
+    for (int i = 0; i < n; ++i) nrm += x[i] * x[i];
+    nrm = 1.0 / sqrt(nrm);
+    for (int i = 0; i < n; ++i) x[i] *= nrm;
+}
+
+// modified Gram-Schmidt of the nvec columns of Z (column-major n x nvec), in
+// order, in one CTA (keeps nearly degenerate inverse-iteration vectors
+// orthogonal)
+__global__ void k_mgs(int n, int nvec, double *__restrict__ Z) {
+    __shared__ double red[32];
+    __shared__ double coef;
+    for (int j = 0; j < nvec; ++j) {
+        double *zj = Z + (int64_t)j * n;
+        for (int i2 = 0; i2 < j; ++i2) {
+            const double *zi = Z + (int64_t)i2 * n;
+            double s = 0.0;
+            for (int r = threadIdx.x; r < n; r += blockDim.x) s += zi[r] * zj[r];
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double t = 0.0;
+                for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+                coef = t;
+            }
+            __syncthreads();
+            const double c = coef;
+            for (int r = threadIdx.x; r < n; r += blockDim.x) zj[r] -= c * zi[r];
+            __syncthreads();
+        }
+        double s = 0.0;
+        for (int r = threadIdx.x; r < n; r += blockDim.x) s += zj[r] * zj[r];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+            coef = 1.0 / sqrt(t);
+        }
+        __syncthreads();
+        const double c = coef;
+        for (int r = threadIdx.x; r < n; r += blockDim.x) zj[r] *= c;
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------ Householder tridiagonal --
+// In one CTA: A (n x n row-major, symmetric, lower part used) is reduced to
+// tridiagonal form Q^T A Q (the dsytd2 scheme): d[0:n] diagonal, e[0:n-1]
+// subdiagonal; reflector j is stored in V[j*n + (j+1 .. n-1)] with tau[j].
+// work: 2*n doubles.
+__global__ void __launch_bounds__(1024) k_tridiag(int n, double *__restrict__ A, double *__restrict__ d,
+                                                  double *__restrict__ e, double *__restrict__ V,
+                                                  double *__restrict__ tau, double *__restrict__ work) {
+    __shared__ double red[32];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    double *p = work, *v = work + n;
+    auto block_sum = [&](double x) -> double {
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        __syncthreads();
+        if ((tid & 31) == 0) red[tid >> 5] = x;
+        __syncthreads();
+        double t = 0.0;
+        for (int w = 0; w < (nt + 31) / 32; ++w) t += red[w];
+        return t;
+    };
+    for (int j = 0; j + 2 < n; ++j) {
+        const int m = n - j - 1;  // length of the column below the diagonal
+        // x = A[j+1:, j]
+        double ss = 0.0;
+        for (int i = tid; i < m; i += nt) {
+            const double xi = A[(j + 1 + i) * n + j];
+            ss += (i > 0) ? xi * xi : 0.0;
+        }
+        const double sigma = block_sum(ss);  // sum of squares without x0
+        const double x0 = A[(j + 1) * n + j];
+        double alpha, t_;
+        if (sigma == 0.0) {
+            t_ = 0.0;
+            alpha = x0;
+        } else {
+            const double nrm = sqrt(x0 * x0 + sigma);
+            alpha = (x0 <= 0.0) ? nrm : -nrm;
+            const double v0 = x0 - alpha;
+            t_ = -v0 / alpha;             // tau = (alpha - x0)/alpha
+            for (int i = tid; i < m; i += nt) v[i] = (i == 0) ? 1.0 : A[(j + 1 + i) * n + j] / v0;
+        }
+        if (tid == 0) {
+            d[j] = A[j * n + j];
+            e[j] = alpha;
+            tau[j] = t_;
+        }
+        __syncthreads();
+        if (t_ == 0.0) {
+            for (int i = tid; i < m; i += nt) V[(int64_t)j * n + j + 1 + i] = (i == 0) ? 1.0 : 0.0;
+            __syncthreads();
+            continue;
+        }
+        for (int i = tid; i < m; i += nt) V[(int64_t)j * n + j + 1 + i] = v[i];
+        // p = tau * A22 v: one warp per row, coalesced over the row
+        {
+            const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
+            for (int r = warp; r < m; r += nw) {
+                const double *row = A + (int64_t)(j + 1 + r) * n + (j + 1);
+                double s2 = 0.0;
+                for (int c = lane; c < m; c += 32) s2 += row[c] * v[c];
+                for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+                if (lane == 0) p[r] = t_ * s2;
+            }
+        }
+        __syncthreads();
+        double pv = 0.0;
+        for (int i = tid; i < m; i += nt) pv += p[i] * v[i];
+        const double K = 0.5 * t_ * block_sum(pv);
+        // w = p - K v ; A22 -= v w^T + w v^T
+        for (int i = tid; i < m; i += nt) p[i] -= K * v[i];
+        __syncthreads();
+        for (int e2 = tid; e2 < m * m; e2 += nt) {
+            const int r = e2 / m, c = e2 - r * m;
+            A[(j + 1 + r) * n + (j + 1 + c)] -= v[r] * p[c] + p[r] * v[c];
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        if (n >= 2) {
+            d[n - 2] = A[(n - 2) * n + (n - 2)];
+            e[n - 2] = A[(n - 1) * n + (n - 2)];
+        }
+        d[n - 1] = A[(n - 1) * n + (n - 1)];
+    }
+}
+
+// Z (n x nvec column-major) <- Q Z with Q = H_0 H_1 ... H_{n-3}
+__global__ void k_apply_q(int n, int nvec, const double *__restrict__ V, const double *__restrict__ tau,
+                          double *__restrict__ Z) {
+    const int col = blockIdx.x;
+    if (col >= nvec) return;
+    double *z = Z + (int64_t)col * n;
+    __shared__ double red[32];
+    __shared__ double coef;
+    for (int j = n - 3; j >= 0; --j) {
+        const double t_ = tau[j];
+        if (t_ == 0.0) continue;
+        const double *v = V + (int64_t)j * n + j + 1;
+        const int m = n - j - 1;
+        double s = 0.0;
+        for (int i = threadIdx.x; i < m; i += blockDim.x) s += v[i] * z[j + 1 + i];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+            coef = t_ * t;
+        }
+        __syncthreads();
+        const double c = coef;
+        for (int i = threadIdx.x; i < m; i += blockDim.x) z[j + 1 + i] -= c * v[i];
+        __syncthreads();
+    }
+}
+
 // ------------------------------------------------------------- launchers --
 cudaError_t random_cols(double *W, int nB, int64_t n, int64_t ld, uint64_t seed, cudaStream_t s) {
     k_random_cols<<<592, 256, 0, s>>>(W, nB, n, ld, seed);
@@ -370,38 +653,64 @@ int dot_grid(int64_t n) {
     return (int)(tiles < 592 ? (tiles > 0 ? tiles : 1) : 592);
 }
 
-cudaError_t multidot(const double *A, int nA, const double *B, int nB, int64_t n, int64_t ld, double *partial,
-                     double *out, cudaStream_t s) {
-    const int npairs = nA * nB;
-    if (npairs <= 0) return cudaSuccess;
+template <int NB>
+static cudaError_t multidot_nb(const double *A, int nA, const double *B, int64_t n, int64_t ld, double *partial,
+                               double *out, cudaStream_t s) {
     const int G = dot_grid(n);
+    const int maxa = 4096 / NB;  // shared accumulator of at most 4096 doubles
     for (int a0 = 0; a0 < nA;) {
-        // chunk nA so that pairs fit the per-thread accumulators
-        const int maxa = (kDotThreads * kMaxPairsPerThread) / nB;
         const int na = (nA - a0) < maxa ? (nA - a0) : maxa;
-        const size_t smem = sizeof(double) * kDotTile * nB;
-        k_multidot<<<G, kDotThreads, smem, s>>>(A + (int64_t)a0 * ld, na, B, nB, n, ld, partial);
-        k_reduce_partials<<<(na * nB + 127) / 128, 128, 0, s>>>(partial, na * nB, G, out + (int64_t)a0 * nB);
+        const size_t smem = sizeof(double) * ((size_t)kDotTile * NB + (size_t)na * NB);
+        cudaFuncSetAttribute(k_multidot<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_multidot<NB><<<G, kDotThreads, smem, s>>>(A + (int64_t)a0 * ld, na, B, n, ld, partial);
+        k_reduce_partials<<<(na * NB * 32 + 255) / 256, 256, 0, s>>>(partial, na * NB, G, out + (int64_t)a0 * NB);
         a0 += na;
     }
     return cudaGetLastError();
 }
 
-cudaError_t sub_gemv(const double *H, int k, const double *C, double *W, int nB, int64_t n, int64_t ld,
-                     double *sq_partial, double *sq_out, cudaStream_t s) {
+cudaError_t multidot(const double *A, int nA, const double *B, int nB, int64_t n, int64_t ld, double *partial,
+                     double *out, cudaStream_t s) {
+    if (nA <= 0 || nB <= 0) return cudaSuccess;
+    switch (nB) {
+    case 1: return multidot_nb<1>(A, nA, B, n, ld, partial, out, s);
+    case 2: return multidot_nb<2>(A, nA, B, n, ld, partial, out, s);
+    case 4: return multidot_nb<4>(A, nA, B, n, ld, partial, out, s);
+    case 8: return multidot_nb<8>(A, nA, B, n, ld, partial, out, s);
+    case 16: return multidot_nb<16>(A, nA, B, n, ld, partial, out, s);
+    default:
+        return cudaErrorInvalidValue;
+    }
+}
+
+template <int NB>
+static cudaError_t sub_gemv_nb(const double *H, int k, const double *C, double *W, int64_t n, int64_t ld,
+                               double *sq_partial, double *sq_out, cudaStream_t s) {
     const int G = 592;
-    // process at most 512 history columns per launch (shared memory)
-    for (int j0 = 0; j0 < k || (k == 0 && j0 == 0);) {
+    int j0 = 0;
+    do {
         const int kk = (k - j0) < 512 ? (k - j0) : 512;
         const bool last = (j0 + kk >= k);
-        const size_t smem = sizeof(double) * ((size_t)kk * nB + 8 * nB);
-        k_sub_gemv<<<G, 256, smem, s>>>(H + (int64_t)j0 * ld, kk, C + (int64_t)j0 * nB, W, nB, n, ld,
-                                         last ? sq_partial : nullptr);
+        const size_t smem = sizeof(double) * ((size_t)kk * NB + 8 * NB);
+        cudaFuncSetAttribute(k_sub_gemv<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(smem + 256));
+        k_sub_gemv<NB><<<G, 256, smem, s>>>(H + (int64_t)j0 * ld, kk, C + (int64_t)j0 * NB, W, n, ld,
+                                             last ? sq_partial : nullptr);
         j0 += kk;
-        if (k == 0) break;
-    }
-    if (sq_partial && sq_out) k_reduce_partials<<<1, 32, 0, s>>>(sq_partial, nB, G, sq_out);
+    } while (j0 < k);
+    if (sq_partial && sq_out) k_reduce_partials<<<(NB * 32 + 255) / 256, 256, 0, s>>>(sq_partial, NB, G, sq_out);
     return cudaGetLastError();
+}
+
+cudaError_t sub_gemv(const double *H, int k, const double *C, double *W, int nB, int64_t n, int64_t ld,
+                     double *sq_partial, double *sq_out, cudaStream_t s) {
+    switch (nB) {
+    case 1: return sub_gemv_nb<1>(H, k, C, W, n, ld, sq_partial, sq_out, s);
+    case 2: return sub_gemv_nb<2>(H, k, C, W, n, ld, sq_partial, sq_out, s);
+    case 4: return sub_gemv_nb<4>(H, k, C, W, n, ld, sq_partial, sq_out, s);
+    case 8: return sub_gemv_nb<8>(H, k, C, W, n, ld, sq_partial, sq_out, s);
+    case 16: return sub_gemv_nb<16>(H, k, C, W, n, ld, sq_partial, sq_out, s);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t transform(const double *V, int m, const double *Y, int ldy, int K, double *out, int64_t n, int64_t ld,
@@ -443,6 +752,25 @@ cudaError_t jacobi(int n, double *A, double *Vtmp, double *w, double *Z, int *st
     const size_t smem = sizeof(double) * m + sizeof(int) * 2 * m;
     cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(smem + 1024));
     k_jacobi<<<1, 1024, smem, s>>>(n, A, Vtmp, w, Z, 60, status);
+    return cudaGetLastError();
+}
+
+cudaError_t inverse_iter_arrow(int n, int k, const double *al, const double *bt, const double *ev, int nvec,
+                               double scale, double *Z, double *work, cudaStream_t s) {
+    if (nvec <= 0) return cudaSuccess;
+    k_inverse_iter_arrow<<<(nvec + 31) / 32, 32, 0, s>>>(n, k, al, bt, ev, nvec, scale, Z, work);
+    k_mgs<<<1, 256, 0, s>>>(n, nvec, Z);
+    return cudaGetLastError();
+}
+
+cudaError_t tridiag(int n, double *A, double *d, double *e, double *V, double *tau, double *work, cudaStream_t s) {
+    k_tridiag<<<1, 1024, 0, s>>>(n, A, d, e, V, tau, work);
+    return cudaGetLastError();
+}
+
+cudaError_t apply_q(int n, int nvec, const double *V, const double *tau, double *Z, cudaStream_t s) {
+    if (n < 3 || nvec <= 0) return cudaSuccess;
+    k_apply_q<<<nvec, 256, 0, s>>>(n, nvec, V, tau, Z);
     return cudaGetLastError();
 }
 

@@ -24,4 +24,13 @@ cudaError_t jacobi(int n, double *A, double *Vtmp, double *w, double *Z, int *st
 // lowest nwant eigenvalues of the arrowhead-tridiagonal matrix
 cudaError_t bisect_arrow(int n, int k, const double *al, const double *bt, int nwant, double glo, double ghi,
                          double *ev, cudaStream_t s);
+// eigenvectors (columns of Z, column-major n x nvec) of the arrowhead-
+// tridiagonal matrix for the given eigenvalues; work: 6*n*nvec doubles
+cudaError_t inverse_iter_arrow(int n, int k, const double *al, const double *bt, const double *ev, int nvec,
+                               double scale, double *Z, double *work, cudaStream_t s);
+// Householder reduction of a dense symmetric matrix (row-major, destroyed)
+// to tridiagonal d/e with reflectors V/tau; work: 2*n doubles
+cudaError_t tridiag(int n, double *A, double *d, double *e, double *V, double *tau, double *work, cudaStream_t s);
+// Z <- Q Z for the reflectors of tridiag
+cudaError_t apply_q(int n, int nvec, const double *V, const double *tau, double *Z, cudaStream_t s);
 }  // namespace bsg
