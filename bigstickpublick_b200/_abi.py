@@ -181,5 +181,23 @@ def gpu_lib():
         lib.bsg_validate_tables.restype = C.c_int
         lib.bsg_applyh_noalloc.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_int]
         lib.bsg_applyh_noalloc.restype = C.c_int
+        lib.bsg_batch_create.argtypes = [C.c_int, C.POINTER(C.POINTER(BsgTables)), C.POINTER(BsgConfig), C.POINTER(vp)]
+        lib.bsg_batch_create.restype = C.c_int
+        lib.bsg_batch_destroy.argtypes = [vp]
+        lib.bsg_batch_destroy.restype = C.c_int
+        lib.bsg_batch_last_error.argtypes = [vp, C.c_char_p, C.c_size_t]
+        lib.bsg_batch_last_error.restype = C.c_int
+        lib.bsg_batch_dims.argtypes = [vp, i64p]
+        lib.bsg_batch_dims.restype = C.c_int
+        lib.bsg_batch_system.argtypes = [vp, C.c_int, C.POINTER(vp)]
+        lib.bsg_batch_system.restype = C.c_int
+        lib.bsg_batch_applyh.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.c_int, vp]
+        lib.bsg_batch_applyh.restype = C.c_int
+        lib.bsg_batch_autotune.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]
+        lib.bsg_batch_autotune.restype = C.c_int
+        lib.bsg_batch_set_tuning.argtypes = [vp, C.c_int, C.c_int]
+        lib.bsg_batch_set_tuning.restype = C.c_int
+        lib.bsg_batch_lanczos.argtypes = [vp, C.POINTER(BsgLanczosParams), f64p, C.POINTER(f64p), C.POINTER(BsgReport)]
+        lib.bsg_batch_lanczos.restype = C.c_int
         _gpu = lib
     return _gpu

@@ -16,240 +16,19 @@
 // (hmat * phase, src/bapplyhlibOMP.f90:1093-1095, :1269-1272) and promoted
 // to the vector type; FP32 vectors accumulate in FP32, FP64 vectors in FP64.
 
-#include "bsg_internal.h"
+#include "applyh_tile.cuh"
 
 namespace bsg {
 
-template <typename T, int NB, bool FULL>
-struct Vec {
-    // load NB consecutive elements of vector data starting at p
-    static __device__ __forceinline__ void load(const T *__restrict__ p, T (&x)[NB]) {
-#pragma unroll
-        for (int v = 0; v < NB; ++v) x[v] = __ldg(p + v);
-    }
-};
-template <>
-struct Vec<float, 4, true> {
-    static __device__ __forceinline__ void load(const float *__restrict__ p, float (&x)[4]) {
-        const float4 a = __ldg(reinterpret_cast<const float4 *>(p));
-        x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
-    }
-};
-template <>
-struct Vec<float, 8, true> {
-    static __device__ __forceinline__ void load(const float *__restrict__ p, float (&x)[8]) {
-        const float4 a = __ldg(reinterpret_cast<const float4 *>(p));
-        const float4 b = __ldg(reinterpret_cast<const float4 *>(p) + 1);
-        x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
-        x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
-    }
-};
-template <>
-struct Vec<float, 16, true> {
-    static __device__ __forceinline__ void load(const float *__restrict__ p, float (&x)[16]) {
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const float4 a = __ldg(reinterpret_cast<const float4 *>(p) + k);
-            x[4 * k] = a.x; x[4 * k + 1] = a.y; x[4 * k + 2] = a.z; x[4 * k + 3] = a.w;
-        }
-    }
-};
-template <>
-struct Vec<float, 2, true> {
-    static __device__ __forceinline__ void load(const float *__restrict__ p, float (&x)[2]) {
-        const float2 a = __ldg(reinterpret_cast<const float2 *>(p));
-        x[0] = a.x; x[1] = a.y;
-    }
-};
-template <int NB>
-struct VecD2 {
-    static __device__ __forceinline__ void load(const double *__restrict__ p, double (&x)[NB]) {
-#pragma unroll
-        for (int k = 0; k < NB / 2; ++k) {
-            const double2 a = __ldg(reinterpret_cast<const double2 *>(p) + k);
-            x[2 * k] = a.x; x[2 * k + 1] = a.y;
-        }
-    }
-};
-template <> struct Vec<double, 2, true> : VecD2<2> {};
-template <> struct Vec<double, 4, true> : VecD2<4> {};
-template <> struct Vec<double, 8, true> : VecD2<8> {};
-template <> struct Vec<double, 16, true> : VecD2<16> {};
-
-constexpr int kWarps = kRowWarps;
-
-__host__ __device__ constexpr size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
-
-// One CTA = one tile of one output row: positions pos0 + lane + 32*i.  Warp w
-// handles the contributions assigned to slot (row, w) at setup (balanced by
-// estimated work) and accumulates in registers; the eight partial sums are
-// added in fixed warp order at the end, so the result does not depend on
-// scheduling.
-// ld: elements between consecutive states (the block size nb); v0: first
-// vector column handled by this launch; FULL: ld == NB and aligned base.
-// mstride: floats of per-warp shared memory for the PN matrix-element table.
 template <typename T, int NB, int ITEMS, bool FULL>
 __global__ void __launch_bounds__(kWarps * 32) k_rows(const RowArgs a, const T *__restrict__ vin,
                                                       T *__restrict__ vout, const int ld, const int v0,
                                                       const int mstride) {
     extern __shared__ __align__(16) unsigned char smem[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
     float *__restrict__ Mw = reinterpret_cast<float *>(smem) + (size_t)warp * mstride;
     T *__restrict__ part = reinterpret_cast<T *>(smem + align16(sizeof(float) * (size_t)kWarps * mstride));
-
-    const Tile tile = a.tiles[blockIdx.x];
-    const int row = tile.row;
-    const int64_t roff = a.row_off[row];
-
-    T acc[ITEMS][NB];
-    int pos[ITEMS];
-    bool valid[ITEMS];
-#pragma unroll
-    for (int i = 0; i < ITEMS; ++i) {
-        const int local = lane + 32 * i;
-        pos[i] = tile.pos0 + local;
-        valid[i] = local < tile.npos;
-#pragma unroll
-        for (int v = 0; v < NB; ++v) acc[i][v] = T(0);
-    }
-
-    // ---- PP: out[pos] += me * in[q_off + pos]   (src/bapplyhlibOMP.f90:1068-1241)
-    {
-        const int slot = row * kWarps + warp;
-        const int c1 = a.pp_ptr[slot + 1];
-        for (int c = a.pp_ptr[slot]; c < c1; ++c) {
-            const PPContrib pc = a.pp[c];
-            const T me = (T)pc.me;
-#pragma unroll
-            for (int i = 0; i < ITEMS; ++i) {
-                if (valid[i] && pos[i] >= pc.lo && pos[i] <= pc.hi) {
-                    T x[NB];
-                    Vec<T, NB, FULL>::load(vin + (size_t)(pc.q_off + pos[i]) * ld + v0, x);
-#pragma unroll
-                    for (int v = 0; v < NB; ++v) acc[i][v] += me * x[v];
-                }
-            }
-        }
-    }
-    // ---- NN: out[pos] += sum r.me * in[row + r.in]   (:1012-1066)
-    {
-        const int slot = row * kWarps + warp;
-        const int c1 = a.nn_ptr[slot + 1];
-        const T *__restrict__ src = vin + (size_t)roff * ld + v0;
-        for (int c = a.nn_ptr[slot]; c < c1; ++c) {
-            const NOp op = a.nops[a.nn[c].nop];
-            const int32_t *__restrict__ ptr = a.nptr + op.ptr_base;
-            const int2 *__restrict__ rec = reinterpret_cast<const int2 *>(a.nnrec + op.rec_base);
-#pragma unroll
-            for (int i = 0; i < ITEMS; ++i) {
-                if (!valid[i] || pos[i] >= op.nout) continue;
-                const int k0 = __ldg(ptr + pos[i]), k1 = __ldg(ptr + pos[i] + 1);
-                int k = k0;
-                for (; k + 1 < k1; k += 2) {
-                    const int2 r0 = __ldg(rec + k), r1 = __ldg(rec + k + 1);
-                    T x0[NB], x1[NB];
-                    Vec<T, NB, FULL>::load(src + (size_t)r0.x * ld, x0);
-                    Vec<T, NB, FULL>::load(src + (size_t)r1.x * ld, x1);
-                    const T m0 = (T)__int_as_float(r0.y), m1 = (T)__int_as_float(r1.y);
-#pragma unroll
-                    for (int v = 0; v < NB; ++v) { acc[i][v] += m0 * x0[v]; acc[i][v] += m1 * x1[v]; }
-                }
-                if (k < k1) {
-                    const int2 r0 = __ldg(rec + k);
-                    T x0[NB];
-                    Vec<T, NB, FULL>::load(src + (size_t)r0.x * ld, x0);
-                    const T m0 = (T)__int_as_float(r0.y);
-#pragma unroll
-                    for (int v = 0; v < NB; ++v) acc[i][v] += m0 * x0[v];
-                }
-            }
-        }
-    }
-    // ---- PN: out[pos] += sum hmatpn(cpn(b,a)+dpn(d,c))*php*phn * in[q_off + r.in]  (:1242-1442)
-    // The warp first tabulates hmatpn(cpn(b,a)+dpn(d,c))*php for the proton
-    // jump's (a,c) and every distinct neutron (b,d) of the operator; a record
-    // then costs one shared load, the neutron phase is its sign bit.
-    {
-        const int slot = row * kWarps + warp;
-        const int c1 = a.pn_ptr[slot + 1];
-        for (int c = a.pn_ptr[slot]; c < c1; ++c) {
-            const PNContrib pc = a.pn[c];
-            const NOp op = a.nops[pc.nop];
-            const int acol = pc.acol * a.ld_cpn, ccol = pc.ccol * a.ld_cpn;
-            for (int k = lane; k < op.nbd; k += 32) {
-                const BDPair bd = a.bd[op.bd_base + k];
-                const int idx = __ldg(a.cpn + bd.b + acol) + __ldg(a.dpn + bd.d + ccol);
-                float xme = __ldg(a.hmatpn + idx - 1);
-                Mw[k] = xme * pc.php;
-            }
-            __syncwarp();
-            const int32_t *__restrict__ ptr = a.nptr + op.ptr_base;
-            const int2 *__restrict__ rec = reinterpret_cast<const int2 *>(a.pnrec + op.rec_base);
-            const T *__restrict__ src = vin + (size_t)pc.q_off * ld + v0;
-#pragma unroll
-            for (int i = 0; i < ITEMS; ++i) {
-                if (!valid[i] || pos[i] >= op.nout) continue;
-                const int k0 = __ldg(ptr + pos[i]), k1 = __ldg(ptr + pos[i] + 1);
-                int k = k0;
-                for (; k + 1 < k1; k += 2) {
-                    const int2 r0 = __ldg(rec + k), r1 = __ldg(rec + k + 1);
-                    T x0[NB], x1[NB];
-                    Vec<T, NB, FULL>::load(src + (size_t)r0.x * ld, x0);
-                    Vec<T, NB, FULL>::load(src + (size_t)r1.x * ld, x1);
-                    // neutron phase: int8 at bits 16..23, its sign moved to bit 31
-                    const float f0 = __int_as_float(__float_as_int(Mw[r0.y & 0xffff]) ^ ((r0.y << 8) & 0x80000000));
-                    const float f1 = __int_as_float(__float_as_int(Mw[r1.y & 0xffff]) ^ ((r1.y << 8) & 0x80000000));
-                    const T m0 = (T)f0, m1 = (T)f1;
-#pragma unroll
-                    for (int v = 0; v < NB; ++v) { acc[i][v] += m0 * x0[v]; acc[i][v] += m1 * x1[v]; }
-                }
-                if (k < k1) {
-                    const int2 r0 = __ldg(rec + k);
-                    T x0[NB];
-                    Vec<T, NB, FULL>::load(src + (size_t)r0.x * ld, x0);
-                    const float f0 = __int_as_float(__float_as_int(Mw[r0.y & 0xffff]) ^ ((r0.y << 8) & 0x80000000));
-                    const T m0 = (T)f0;
-#pragma unroll
-                    for (int v = 0; v < NB; ++v) acc[i][v] += m0 * x0[v];
-                }
-            }
-            __syncwarp();
-        }
-    }
-    // ---- SPE: out[pos] += (pspe + nspe) * in[pos]   (:988-1011)
-    {
-        const int slot = row * kWarps + warp;
-        const int c1 = a.spe_ptr[slot + 1];
-        for (int c = a.spe_ptr[slot]; c < c1; ++c) {
-            const SPEContrib sc = a.spe[c];
-#pragma unroll
-            for (int i = 0; i < ITEMS; ++i) {
-                if (valid[i] && pos[i] >= sc.lo && pos[i] <= sc.hi) {
-                    const float e = sc.pspe + __ldg(a.nspe + sc.n0 + (pos[i] - sc.lo));
-                    T x[NB];
-                    Vec<T, NB, FULL>::load(vin + (size_t)(roff + pos[i]) * ld + v0, x);
-#pragma unroll
-                    for (int v = 0; v < NB; ++v) acc[i][v] += x[v] * (T)e;
-                }
-            }
-        }
-    }
-    // ---- fixed-order reduction over the warps, single write per element
-    constexpr int TP = 32 * ITEMS;
-#pragma unroll
-    for (int i = 0; i < ITEMS; ++i)
-#pragma unroll
-        for (int v = 0; v < NB; ++v) part[((size_t)warp * TP + lane + 32 * i) * NB + v] = acc[i][v];
-    __syncthreads();
-    const int nel = tile.npos * NB;
-    for (int e = threadIdx.x; e < nel; e += kWarps * 32) {
-        T s = part[e];
-#pragma unroll
-        for (int w = 1; w < kWarps; ++w) s += part[(size_t)w * TP * NB + e];
-        const int lp = e / NB, v = e - lp * NB;
-        T *o = vout + (size_t)(roff + tile.pos0 + lp) * ld + v0 + v;
-        *o = a.accumulate ? *o + s : s;
-    }
+    row_tile<T, NB, ITEMS, FULL>(a, a.tiles[blockIdx.x], vin, vout, ld, v0, Mw, part);
 }
 
 template <typename T, int NB, int ITEMS>

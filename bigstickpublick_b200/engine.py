@@ -161,3 +161,112 @@ class Hamiltonian:
                                sn.ctypes.data_as(_abi.f64p) if sn is not None else None)
         self._check(st, "bsg_grad")
         return out
+
+
+class _SystemView(Hamiltonian):
+    """A Hamiltonian bound to one system of a Batch (the batch owns it)."""
+
+    def __init__(self, lib, handle, tables):
+        self.lib = lib
+        self.tables = tables
+        self.h = handle
+        self.dim = tables.dim
+
+    def close(self):
+        self.h = None
+
+
+class Batch:
+    """Many independent Hamiltonians (bsg_batch_*): one persistent launch
+    applies all of them; Lanczos runs lock-step with one captured CUDA graph
+    per iteration.
+
+    tune_cache: JSON file mapping a batch signature to the autotuned
+    (tile width, CTAs per SM); read if present, written after autotuning."""
+
+    def __init__(self, tables_list, device=0, autotune=False, tune_cache=None):
+        self.lib = _abi.gpu_lib()
+        self.tables = list(tables_list)
+        self._ct = [t.as_ctypes() for t in self.tables]
+        arr = (C.POINTER(_abi.BsgTables) * len(self._ct))(*[C.pointer(t) for t in self._ct])
+        cfg = _abi.BsgConfig(device, 16, 1, 0)
+        h = C.c_void_p()
+        st = self.lib.bsg_batch_create(len(self._ct), arr, C.byref(cfg), C.byref(h))
+        if st != 0:
+            raise BsgError(st, "bsg_batch_create failed")
+        self.h = h
+        self.dims = [t.dim for t in self.tables]
+        self.tuning = None
+        sig = self.signature()
+        cache = {}
+        if tune_cache:
+            import json
+            import os
+            if os.path.exists(tune_cache):
+                cache = json.load(open(tune_cache))
+        if sig in cache:
+            items, ctas = cache[sig]["items"], cache[sig]["ctas_per_sm"]
+            self._check(self.lib.bsg_batch_set_tuning(self.h, items, ctas), "bsg_batch_set_tuning")
+            self.tuning = dict(cache[sig], source="cache")
+        elif autotune:
+            self.tuning = self.autotune()
+            if tune_cache:
+                import json
+                cache[sig] = {k: v for k, v in self.tuning.items() if k != "source"}
+                with open(tune_cache, "w") as f:
+                    json.dump(cache, f, indent=1)
+
+    def signature(self):
+        import hashlib
+        h = hashlib.sha256()
+        for t in self.tables:
+            h.update(str((t.dim, t.s["np1b"], t.s["np2b"], t.s["nn1b"], t.s["nn2b"])).encode())
+        return h.hexdigest()[:16]
+
+    def _check(self, st, what):
+        if st != 0:
+            buf = C.create_string_buffer(512)
+            self.lib.bsg_batch_last_error(self.h, buf, 512)
+            raise BsgError(st, f"{what}: {buf.value.decode()}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.bsg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def system(self, s):
+        ctx = C.c_void_p()
+        self._check(self.lib.bsg_batch_system(self.h, s, C.byref(ctx)), "bsg_batch_system")
+        return _SystemView(self.lib, ctx, self.tables[s])
+
+    def autotune(self):
+        it, cps, ms = C.c_int(), C.c_int(), C.c_double()
+        self._check(self.lib.bsg_batch_autotune(self.h, C.byref(it), C.byref(cps), C.byref(ms)), "autotune")
+        return {"items": it.value, "ctas_per_sm": cps.value, "ms": ms.value, "source": "autotune"}
+
+    def applyh(self, vins, vouts, stream=None):
+        """vins/vouts: lists of contiguous CUDA tensors (float32 or float64)."""
+        import torch
+        prec = 4 if vins[0].dtype == torch.float32 else 8
+        vi = (C.c_void_p * len(vins))(*[v.data_ptr() for v in vins])
+        vo = (C.c_void_p * len(vouts))(*[v.data_ptr() for v in vouts])
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        self._check(self.lib.bsg_batch_applyh(self.h, vi, vo, prec, C.c_void_p(s)), "bsg_batch_applyh")
+
+    def lanczos(self, nkeep=5, niter=150, matvec_prec=8, want_vectors=False):
+        p = _abi.BsgLanczosParams()
+        p.nkeep, p.niter, p.nb, p.matvec_prec, p.fixed_iter = nkeep, niter, 1, matvec_prec, 1
+        ev = np.zeros(len(self.tables) * nkeep)
+        vecs = [np.zeros((nkeep, d)) for d in self.dims] if want_vectors else None
+        vp = (_abi.f64p * len(self.tables))(*[v.ctypes.data_as(_abi.f64p) for v in vecs]) if vecs else None
+        rep = _abi.BsgReport()
+        self._check(self.lib.bsg_batch_lanczos(self.h, C.byref(p), ev.ctypes.data_as(_abi.f64p), vp, C.byref(rep)),
+                    "bsg_batch_lanczos")
+        report = {k: getattr(rep, k) for k, _ in rep._fields_}
+        return ev.reshape(len(self.tables), nkeep), ([v.T.copy() for v in vecs] if vecs else None), report

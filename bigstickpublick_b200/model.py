@@ -330,3 +330,18 @@ def chain_rule(tables, dhmat):
                 occ = ((b >> np.uint64(q)) & np.uint64(1)).astype(bool)
                 g_spe[orb[q]] += spec.spe_scale * d[occ].sum()
     return g_tb[:len(spec.tbme)], g_spe
+
+
+def batch_member(seed):
+    """One Hamiltonian of the seeded sd-shell batch: valence Z and N drawn
+    uniformly in 2..8 from a SplitMix64 stream of `seed`, then the synthetic
+    isospin interaction continued from the same stream (SPEs -3.9/-3.2/+2.1
+    MeV); 2Jz = 0 for even A, 1 for odd A."""
+    rng = SplitMix64(seed)
+    np_ = rng.randint(2, 8)
+    nn = rng.randint(2, 8)
+    tb = []
+    for k in canonical_tbme_keys(SD_ORBITS):
+        tb.append(k + (float(np.float32(float("%.8e" % rng.normal()))),))
+    spe = [float(np.float32(float("%.8e" % s))) for s in SD_SYNTH_SPE]
+    return ModelSpec(SD_ORBITS, np_, nn, (np_ + nn) % 2, 1, spe, tb)

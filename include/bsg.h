@@ -202,6 +202,29 @@ int  bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const double *pivot_
 int  bsg_grad(bsg_ctx *ctx, const double *evecs, int nstates,
               double *dpp, double *dnn, double *dpn, double *dspe_p, double *dspe_n);
 
+/* ---- batched systems: many independent Hamiltonians of uneven dimension
+ *      (the reference runs one per process).  bsg_batch_applyh applies all of
+ *      them in one persistent launch whose CTAs pull (system, row tile) work
+ *      items heaviest first; vin[s]/vout[s] are device pointers of dim_s
+ *      elements.  bsg_batch_lanczos runs lock-step scalar Lanczos on all
+ *      systems for exactly p->niter iterations (uniform pivots, full
+ *      classical Gram-Schmidt reorthogonalization) with each iteration
+ *      captured once as a CUDA graph and replayed; evals[s*nkeep + k];
+ *      evecs NULL or n host pointers of dim_s*nkeep doubles.  The tile width
+ *      and CTA residency of the batched kernel come from bsg_batch_autotune
+ *      (timed on the device) or bsg_batch_set_tuning. ---- */
+typedef struct bsg_batch bsg_batch;
+int  bsg_batch_create(int n, const bsg_tables *const *tables, const bsg_config *cfg, bsg_batch **out);
+int  bsg_batch_destroy(bsg_batch *b);
+int  bsg_batch_last_error(const bsg_batch *b, char *buf, size_t len);
+int  bsg_batch_dims(const bsg_batch *b, int64_t *dims);
+int  bsg_batch_system(const bsg_batch *b, int s, bsg_ctx **ctx);
+int  bsg_batch_applyh(bsg_batch *b, const void *const *vin, void *const *vout, int prec, void *cuda_stream);
+int  bsg_batch_autotune(bsg_batch *b, int *items, int *ctas_per_sm, double *best_ms);
+int  bsg_batch_set_tuning(bsg_batch *b, int items, int ctas_per_sm);
+int  bsg_batch_lanczos(bsg_batch *b, const bsg_lanczos_params *p, double *evals, double *const *evecs,
+                       bsg_report *rep);
+
 /* ---- introspection used by tests and the benchmark ---- */
 typedef struct bsg_stats {
     int64_t n_ops_pp, n_ops_nn, n_ops_pn, n_ops_spe;  /* inner-loop updates / matvec */
