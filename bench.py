@@ -222,6 +222,51 @@ def lanczos_leg(H, tables, args):
     return out
 
 
+def batch_leg(args):
+    """Config 4: 256 sd-shell Hamiltonians (seeds 1000..1255, valence Z and N
+    uniform in 2..8), one persistent launch per batched matvec, lock-step
+    Lanczos with one captured graph per iteration, then the adjoint gradient
+    of the lowest 5 eigenvalues of every system with respect to its 63 TBMEs
+    and 3 SPEs."""
+    import torch
+    from bigstickpublick_b200 import model
+    from bigstickpublick_b200.engine import Batch
+    t0 = time.perf_counter()
+    tabs = [model.build_tables(model.batch_member(s)) for s in range(1000, 1000 + args.batch_n)]
+    t_build = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    cache = os.path.join(ROOT, "profiles", "batch_tuning.json") if args.tune_cache else None
+    b = Batch(tabs, autotune=True, tune_cache=cache)
+    t_create = time.perf_counter() - t0
+    dims = [t.dim for t in tabs]
+    vin = [torch.randn(d, dtype=torch.float32, device="cuda") for d in dims]
+    vout = [torch.empty_like(v) for v in vin]
+    for _ in range(3):
+        b.applyh(vin, vout)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(20):
+        b.applyh(vin, vout)
+    e1.record()
+    torch.cuda.synchronize()
+    mv_ms = e0.elapsed_time(e1) / 20
+    ev, vecs, rep = b.lanczos(nkeep=5, niter=args.batch_iters, matvec_prec=8, want_vectors=True)
+    t0 = time.perf_counter()
+    grads = []
+    for s, t in enumerate(tabs):
+        g = b.system(s).grad(vecs[s])
+        grads.append([model.chain_rule(t, {k: v[i] for k, v in g.items()}) for i in range(5)])
+    t_grad = time.perf_counter() - t0
+    b.close()
+    return {"systems": len(tabs), "dims_min": min(dims), "dims_max": max(dims), "dims_sum": int(sum(dims)),
+            "tuning": b.tuning, "build_s": t_build, "create_s": t_create,
+            "batched_matvec_ms": mv_ms, "system_matvecs_per_s": len(tabs) / (mv_ms / 1e3),
+            "lanczos_iters": args.batch_iters, "lanczos_graph_ms": rep["t_matvec_ms"],
+            "lanczos_eig_ms": rep["t_eig_ms"], "grad_s_all_systems_5_states": t_grad,
+            "ground_states_first4": [float(x) for x in ev[:4, 0]]}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -271,6 +316,10 @@ def main():
     ap.add_argument("--block-leg", action="store_true")
     ap.add_argument("--block-iters", type=int, default=20)
     ap.add_argument("--block-restarts", type=int, default=30)
+    ap.add_argument("--batch-leg", action="store_true")
+    ap.add_argument("--batch-n", type=int, default=256)
+    ap.add_argument("--batch-iters", type=int, default=150)
+    ap.add_argument("--tune-cache", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -374,6 +423,8 @@ def main():
     }
     if rank == 0 and not args.no_lanczos:
         line["lanczos"] = lanczos_leg(H, tables, args)
+    if rank == 0 and args.batch_leg:
+        line["batch"] = batch_leg(args)
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, cores, n, el = cpu_baseline(tables, nb, prec, budget_s=args.cpu_budget)
         line["cpu_baseline"] = {"value": rate, "unit": "matvec/s", "cores": cores, "kind": "port",

@@ -476,7 +476,8 @@ int bsg_batch_applyh(bsg_batch *b, const void *const *vin, void *const *vout, in
     cudaSetDevice(b->device);
     int st = set_vectors(b, vin, vout);
     if (st) return st;
-    return launch_batch(b, prec, stream ? (cudaStream_t)stream : b->stream);
+    // stream: the caller's cudaStream_t; NULL is the legacy default stream
+    return launch_batch(b, prec, (cudaStream_t)stream);
 }
 
 // autotuner: time the batched matvec for each tile width and CTA residency,

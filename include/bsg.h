@@ -206,7 +206,7 @@ int  bsg_grad(bsg_ctx *ctx, const double *evecs, int nstates,
  *      (the reference runs one per process).  bsg_batch_applyh applies all of
  *      them in one persistent launch whose CTAs pull (system, row tile) work
  *      items heaviest first; vin[s]/vout[s] are device pointers of dim_s
- *      elements.  bsg_batch_lanczos runs lock-step scalar Lanczos on all
+ *      elements, launched on cuda_stream (NULL: the legacy default stream).  bsg_batch_lanczos runs lock-step scalar Lanczos on all
  *      systems for exactly p->niter iterations (uniform pivots, full
  *      classical Gram-Schmidt reorthogonalization) with each iteration
  *      captured once as a CUDA graph and replayed; evals[s*nkeep + k];
