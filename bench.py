@@ -267,6 +267,61 @@ def batch_leg(args):
             "ground_states_first4": [float(x) for x in ev[:4, 0]]}
 
 
+def large_leg(args):
+    """Config 5: pf shell 6p6n, 2Jz = 0 (M-scheme dim 109,954,620), seeded
+    synthetic pf interaction; FP32 applyH rate, thick-restart mixed-precision
+    Lanczos for the lowest 5 states (FP64 history and reorthogonalization),
+    adjoint gradient of the ground state w.r.t. all 195 TBMEs and 4 SPEs,
+    everything resident in device memory."""
+    import torch
+    from bigstickpublick_b200 import model
+    from bigstickpublick_b200.engine import Hamiltonian
+    t0 = time.perf_counter()
+    T = model.build_tables(model.pf_model(6, 6, seed=5))
+    t_build = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    H = Hamiltonian(T)
+    t_create = time.perf_counter() - t0
+    st = H.stats()
+    x = torch.randn(T.dim, dtype=torch.float32, device="cuda")
+    y = torch.empty_like(x)
+    H.applyh(x, y)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(3):
+        H.applyh(x, y)
+    e1.record()
+    torch.cuda.synchronize()
+    mv_s = e0.elapsed_time(e1) / 3 / 1e3
+    balg, nops = alg_bytes(st, T, 1, 4)
+    peaks, _ = load_peaks()
+    del x, y
+    t0 = time.perf_counter()
+    ev, vecs, rep = H.lanczos(nkeep=5, niter=args.large_iters, nthick_add=15, max_restarts=args.large_restarts,
+                              matvec_prec=4, converge_tol=args.large_tol, want_vectors=True)
+    t_lz = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    g = H.grad(vecs[:, :1])
+    gtb, gspe = model.chain_rule(T, {k: v[0] for k, v in g.items()})
+    t_grad = time.perf_counter() - t0
+    spec = T.extra["spec"]
+    euler = float(np.array([t[6] for t in spec.tbme]) @ gtb + np.array(spec.spe) @ gspe)
+    free, total = torch.cuda.mem_get_info()
+    H.close()
+    return {"dim": T.dim, "ops_per_matvec": nops, "build_s": t_build, "create_s": t_create,
+            "matvec_fp32_s": mv_s, "matvec_alg_GBps": balg / mv_s / 1e9,
+            "matvec_roofline_frac": balg / mv_s / 1e9 / peaks["hbm_gbs"],
+            "lanczos": {"evals": [float(v) for v in ev], "restarts": rep["restarts"],
+                        "total_iterations": rep["total_iterations"], "converged": rep["converged"],
+                        "wall_s": t_lz, "t_matvec_ms": rep["t_matvec_ms"], "t_reorth_ms": rep["t_reorth_ms"],
+                        "t_eig_ms": rep["t_eig_ms"], "converge_tol": args.large_tol,
+                        "basis": f"{args.large_iters} vectors, thick restart keeping 20"},
+            "grad_ground_state_s": t_grad, "euler_identity_rel_err": abs(euler - ev[0]) / abs(ev[0]),
+            "grad_tbme_norm": float(np.linalg.norm(gtb)), "grad_spe": [float(v) for v in gspe],
+            "device_mem_total_GB": total / 1e9}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -320,6 +375,10 @@ def main():
     ap.add_argument("--batch-n", type=int, default=256)
     ap.add_argument("--batch-iters", type=int, default=150)
     ap.add_argument("--tune-cache", action="store_true")
+    ap.add_argument("--large-leg", action="store_true")
+    ap.add_argument("--large-iters", type=int, default=60)
+    ap.add_argument("--large-restarts", type=int, default=20)
+    ap.add_argument("--large-tol", type=float, default=1e-4)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -425,6 +484,8 @@ def main():
         line["lanczos"] = lanczos_leg(H, tables, args)
     if rank == 0 and args.batch_leg:
         line["batch"] = batch_leg(args)
+    if rank == 0 and args.large_leg:
+        line["large"] = large_leg(args)
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, cores, n, el = cpu_baseline(tables, nb, prec, budget_s=args.cpu_budget)
         line["cpu_baseline"] = {"value": rate, "unit": "matvec/s", "cores": cores, "kind": "port",
