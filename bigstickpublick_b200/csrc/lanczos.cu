@@ -56,7 +56,21 @@ struct Lz {
     DevBuf hist, W, X, Y, tmp, partial, coef, sqp, sq, Adev, Vtmp, Zdev, wdev, stat, al, bt, ev, M, tau, ework;
     std::vector<double> T;  // host projected matrix (maxcol x maxcol), row-major
     float t_mv = 0, t_ort = 0, t_eig = 0;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
+    // pinned staging for the per-step scalars read on the host (alpha block,
+    // residual sums of squares): device->host copies into it stay
+    // asynchronous, so a step synchronizes with the device once
+    double *hpin = nullptr;
+    static constexpr int kPinAlpha = 0, kPinSq = 256, kPinW = 512;  // then al, bt: maxcol each
+    double *pin_w() { return hpin + kPinW; }
+    double *pin_al() { return hpin + kPinW + maxcol; }
+    double *pin_bt() { return hpin + kPinW + 2 * (size_t)maxcol; }
+    size_t pin_doubles() const { return kPinW + 3 * (size_t)maxcol; }
+    // side stream for the convergence test of the scalar recursion, which
+    // then overlaps the next step's applyH
+    cudaStream_t s2 = nullptr;
+    cudaEvent_t econv = nullptr;
+    DevBuf al2, bt2, w2;
 
     double *col(int j) { return (double *)hist.p + (int64_t)j * n; }
     double &Tm(int i, int j) { return T[(size_t)i * maxcol + j]; }
@@ -85,9 +99,10 @@ float elapsed(Lz &L) {
 // bisection + inverse iteration.  Block Lanczos: T is dense (band + arrow) ->
 // Householder tridiagonalization first, then the same, then the reflectors.
 // w (host) gets the eigenvalues; Z (host, column-major m x want) the vectors.
-int eig_lowest(Lz &L, int m, int k, int want, std::vector<double> &w, std::vector<double> *Z) {
-    want = std::min(want, m);
-    double glo = 1e300, ghi = -1e300;
+// Gershgorin interval of T[0:m,0:m], padded; scale = max |end point|
+void gershgorin(Lz &L, int m, double &glo, double &ghi, double &scale) {
+    glo = 1e300;
+    ghi = -1e300;
     for (int i = 0; i < m; ++i) {
         double r = 0.0;
         for (int j = 0; j < m; ++j)
@@ -95,17 +110,29 @@ int eig_lowest(Lz &L, int m, int k, int want, std::vector<double> &w, std::vecto
         glo = std::min(glo, L.Tm(i, i) - r);
         ghi = std::max(ghi, L.Tm(i, i) + r);
     }
-    const double scale = std::max(std::fabs(glo), std::fabs(ghi));
+    scale = std::max(std::fabs(glo), std::fabs(ghi));
     const double pad = 1e-12 * scale + 1e-300;
     glo -= pad;
     ghi += pad;
+}
+
+// diagonal al[0:m] and arrow/sub-diagonal bt[0:m] of the scalar projected matrix
+void arrow_inputs(Lz &L, int m, int k, double *al, double *bt) {
+    for (int i = 0; i < m; ++i) al[i] = L.Tm(i, i);
+    for (int i = 0; i < m; ++i) bt[i] = 0.0;
+    for (int i = 0; i < k; ++i) bt[i] = L.Tm(k, i);
+    for (int i = k; i + 1 < m; ++i) bt[i] = L.Tm(i + 1, i);
+}
+
+int eig_lowest(Lz &L, int m, int k, int want, std::vector<double> &w, std::vector<double> *Z) {
+    want = std::min(want, m);
+    double glo, ghi, scale;
+    gershgorin(L, m, glo, ghi, scale);
     cudaEventRecord(L.e0, L.s);
     int kk = k;
     if (L.nb == 1) {
         std::vector<double> al(m), bt(std::max(m, 1), 0.0);
-        for (int i = 0; i < m; ++i) al[i] = L.Tm(i, i);
-        for (int i = 0; i < k; ++i) bt[i] = L.Tm(k, i);
-        for (int i = k; i + 1 < m; ++i) bt[i] = L.Tm(i + 1, i);
+        arrow_inputs(L, m, k, al.data(), bt.data());
         CK(cudaMemcpyAsync(L.al.p, al.data(), sizeof(double) * m, cudaMemcpyHostToDevice, L.s));
         CK(cudaMemcpyAsync(L.bt.p, bt.data(), sizeof(double) * m, cudaMemcpyHostToDevice, L.s));
     } else {
@@ -133,13 +160,37 @@ int eig_lowest(Lz &L, int m, int k, int want, std::vector<double> &w, std::vecto
     return BSG_OK;
 }
 
+// Queue the lowest `want` eigenvalues of the scalar projected matrix
+// T[0:m,0:m] on the side stream (pinned inputs and result, no host wait);
+// eig_collect() waits for them.
+int eig_queue(Lz &L, int m, int k, int want) {
+    want = std::min(want, m);
+    double glo, ghi, scale;
+    gershgorin(L, m, glo, ghi, scale);
+    arrow_inputs(L, m, k, L.pin_al(), L.pin_bt());
+    CK(cudaMemcpyAsync(L.al2.p, L.pin_al(), sizeof(double) * m, cudaMemcpyHostToDevice, L.s2));
+    CK(cudaMemcpyAsync(L.bt2.p, L.pin_bt(), sizeof(double) * m, cudaMemcpyHostToDevice, L.s2));
+    CK(bisect_arrow(m, k, (const double *)L.al2.p, (const double *)L.bt2.p, want, glo, ghi, (double *)L.w2.p, L.s2));
+    CK(cudaMemcpyAsync(L.pin_w(), L.w2.p, sizeof(double) * want, cudaMemcpyDeviceToHost, L.s2));
+    CK(cudaEventRecord(L.econv, L.s2));
+    return BSG_OK;
+}
+
+int eig_collect(Lz &L, int want, std::vector<double> &w) {
+    CK(cudaEventSynchronize(L.econv));
+    w.assign(L.pin_w(), L.pin_w() + want);
+    return BSG_OK;
+}
+
 // classical Gram-Schmidt of W (nb columns) against history columns [0, k);
-// optional column sums of squares into host sq
-int cgs(Lz &L, int k, std::vector<double> *sq) {
+// optional column sums of squares into host sq (synchronizes), or left in
+// L.sq on the device (sq_on_device)
+int cgs(Lz &L, int k, std::vector<double> *sq, bool sq_on_device = false) {
     double *C = (double *)L.coef.p;
+    const bool want_sq = sq || sq_on_device;
     if (k > 0) CK(multidot(L.col(0), k, (const double *)L.W.p, L.nb, L.n, L.n, (double *)L.partial.p, C, L.s));
-    CK(sub_gemv(L.col(0), k, C, (double *)L.W.p, L.nb, L.n, L.n, sq ? (double *)L.sqp.p : nullptr,
-                sq ? (double *)L.sq.p : nullptr, L.s));
+    CK(sub_gemv(L.col(0), k, C, (double *)L.W.p, L.nb, L.n, L.n, want_sq ? (double *)L.sqp.p : nullptr,
+                want_sq ? (double *)L.sq.p : nullptr, L.s));
     if (sq) {
         sq->resize(L.nb);
         CK(cudaMemcpyAsync(sq->data(), L.sq.p, sizeof(double) * L.nb, cudaMemcpyDeviceToHost, L.s));
@@ -237,28 +288,47 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
     bool finished = false, converged = false;
     std::vector<double> eold, e;
     int iter = 0;         // block iterations in this cycle (the reference's iter)
+    struct {
+        bool active = false;
+        int want = 0, iter = 0, total = 0, rnd = 0, cur = 0, mT = 0;
+    } pend;               // convergence test queued on the side stream
     while (!finished) {
         ++iter;
         ++total;
         // ---- W = H V
         CK(pack(L.col(cur), nb, n, n, L.X.p, L.prec, L.s));
-        cudaEventRecord(L.e0, L.s);
+        CK(cudaEventRecord(L.e0, L.s));
         ST(launch_applyh(ctx, L.X.p, L.Y.p, nb, L.prec, 0, L.s));
-        cudaEventRecord(L.e1, L.s);
+        CK(cudaEventRecord(L.e1, L.s));
         CK(unpack(L.Y.p, nb, n, n, (double *)L.W.p, L.prec, L.s));
         ++matvecs;
-        L.t_mv += elapsed(L);
-        // ---- alpha = V^T W ; W -= V alpha ; CGS against [0, cur)
-        cudaEventRecord(L.e0, L.s);
+        // ---- alpha = V^T W ; W -= V alpha ; CGS against [0, cur), all queued
+        // without a host round trip; the scalar recursion also normalizes
+        // the residual on the device (V_{i+1} = W / |W|), which the
+        // safeguards below redo in the rare steps where they trigger
         CK(multidot(L.col(cur), nb, (const double *)L.W.p, nb, n, n, (double *)L.partial.p, (double *)L.coef.p, L.s));
-        std::vector<double> alpha((size_t)nb * nb);
-        CK(cudaMemcpyAsync(alpha.data(), L.coef.p, sizeof(double) * nb * nb, cudaMemcpyDeviceToHost, L.s));
+        CK(cudaMemcpyAsync(L.hpin + Lz::kPinAlpha, L.coef.p, sizeof(double) * nb * nb, cudaMemcpyDeviceToHost, L.s));
         CK(sub_gemv(L.col(cur), nb, (const double *)L.coef.p, (double *)L.W.p, nb, n, n, nullptr, nullptr, L.s));
-        ST(cgs(L, cur, &sq));
+        ST(cgs(L, cur, nullptr, true));
+        CK(cudaMemcpyAsync(L.hpin + Lz::kPinSq, L.sq.p, sizeof(double) * nb, cudaMemcpyDeviceToHost, L.s));
+        if (nb == 1) CK(normalize_col((const double *)L.W.p, L.col(cur + 1), (const double *)L.sq.p, n, L.s));
+        CK(cudaEventRecord(L.e2, L.s));
+        CK(cudaEventSynchronize(L.e2));
+        {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, L.e0, L.e1);
+            L.t_mv += ms;
+            cudaEventElapsedTime(&ms, L.e1, L.e2);
+            L.t_ort += ms;
+        }
+        std::vector<double> alpha(L.hpin + Lz::kPinAlpha, L.hpin + Lz::kPinAlpha + (size_t)nb * nb);
+        sq.assign(L.hpin + Lz::kPinSq, L.hpin + Lz::kPinSq + nb);
+        cudaEventRecord(L.e0, L.s);
         // ---- scalar beta checks (src/blanczosmain.f90:1634-1660)
-        if (nb == 1 && iter > 1 && beta_prev > 0.0) {
+        if (nb == 1) {
             const double b = std::sqrt(std::max(sq[0], 0.0));
-            if (b < 1e-4 * beta_prev) {
+            beta.assign(1, b);
+            if (iter > 1 && beta_prev > 0.0 && b < 1e-4 * beta_prev) {
                 // random restart: keep the tiny beta, continue from a random
                 // direction orthogonal to the whole history
                 CK(random_cols((double *)L.W.p, 1, n, n, p->seed + 7919ull * (uint64_t)(rnd + 1), L.s));
@@ -267,13 +337,11 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
                 ++rnd;
                 std::vector<double> b2;
                 ST(next_block(L, cur + 1, sq, b2, lmin, lmax));
-                beta.assign(1, b);
-                goto stored;
-            } else if (b < 0.1 * beta_prev) {
+            } else if (iter > 1 && beta_prev > 0.0 && b < 0.1 * beta_prev) {
                 ST(cgs(L, cur + 1, &sq));  // second full pass, v_i included
+                ST(next_block(L, cur + 1, sq, beta, lmin, lmax));
             }
-        }
-        if (nb > 1) {
+        } else {
             // block: guard against a rank-deficient residual block
             ST(next_block(L, cur + nb, sq, beta, lmin, lmax));
             if (lmin <= 1e-20 * std::max(lmax, 1.0)) {
@@ -292,10 +360,7 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
                 ST(next_block(L, cur + nb, sq, beta, lmin, lmax));
                 ++rnd;
             }
-        } else {
-            ST(next_block(L, cur + 1, sq, beta, lmin, lmax));
         }
-    stored:
         cudaEventRecord(L.e1, L.s);
         CK(cudaStreamSynchronize(L.s));
         L.t_ort += elapsed(L);
@@ -314,19 +379,49 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
         mT = cur + nb;
         cur += nb;
         // ---- eigenvalues and convergence (convergence_test option 0)
+        auto conv_test = [&](const std::vector<double> &ev_) {
+            bool hit = false;
+            if ((int)eold.size() == (int)ev_.size()) {
+                double ed = 0.0;
+                for (size_t j = 0; j < ev_.size(); ++j) ed += std::fabs(eold[j] - ev_[j]);
+                ed = ed / std::sqrt((double)ev_.size() + 1.0) * (1.0 + restarts);
+                hit = ed < tol;
+            }
+            eold = ev_;
+            return hit;
+        };
+        if (pend.active) {
+            // the previous step's test ran beside this step's applyH; if it
+            // converged, this step is discarded and the run ends where the
+            // reference's would
+            pend.active = false;
+            ST(eig_collect(L, pend.want, e));
+            if (conv_test(e)) {
+                iter = pend.iter;
+                total = pend.total;
+                rnd = pend.rnd;
+                cur = pend.cur;
+                mT = pend.mT;
+                finished = converged = true;
+                break;
+            }
+        }
         if (cur >= niter * nb) finished = true;
         if (!p->fixed_iter && mT > ncheck && mT < (int64_t)n) {
-            ST(eig_lowest(L, mT, karrow, ncheck, e, nullptr));
-            if ((int)eold.size() == (int)e.size()) {
-                double ed = 0.0;
-                for (size_t j = 0; j < e.size(); ++j) ed += std::fabs(eold[j] - e[j]);
-                ed = ed / std::sqrt((double)e.size() + 1.0) * (1.0 + restarts);
-                if (ed < tol) {
-                    finished = true;
-                    converged = true;
-                }
+            const bool restart_due = thick && !finished && cur + nb > (niter - 1) * nb;
+            if (nb == 1 && !finished && !restart_due) {
+                ST(eig_queue(L, mT, karrow, ncheck));
+                pend.active = true;
+                pend.want = std::min(ncheck, mT);
+                pend.iter = iter;
+                pend.total = total;
+                pend.rnd = rnd;
+                pend.cur = cur;
+                pend.mT = mT;
+            } else {
+                ST(eig_lowest(L, mT, karrow, ncheck, e, nullptr));
+                if (conv_test(e)) finished = converged = true;
             }
-            eold = e;
         }
         if (mT >= (int64_t)n) { finished = true; converged = true; }  // Krylov space exhausted
         if (p->fixed_iter && finished) converged = true;
@@ -465,9 +560,19 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
         (st = dev_alloc(ctx, L.ework, sizeof(double) * ((size_t)2 * N + (size_t)6 * N * std::min(N, 128))))) {
         // fall through to cleanup
     }
+    L.maxcol = maxcol;
+    if (!st && ((st = dev_alloc(ctx, L.al2, sizeof(double) * N)) || (st = dev_alloc(ctx, L.bt2, sizeof(double) * N)) ||
+                (st = dev_alloc(ctx, L.w2, sizeof(double) * N)))) {
+        // fall through to cleanup
+    }
+    if (!st) st = cuda_check(ctx, cudaHostAlloc((void **)&L.hpin, sizeof(double) * L.pin_doubles(), cudaHostAllocDefault),
+                             "cudaHostAlloc (Lanczos staging)");
+    if (!st) st = cuda_check(ctx, cudaStreamCreateWithFlags(&L.s2, cudaStreamNonBlocking), "cudaStreamCreate");
     if (!st) {
         cudaEventCreate(&L.e0);
         cudaEventCreate(&L.e1);
+        cudaEventCreate(&L.e2);
+        cudaEventCreateWithFlags(&L.econv, cudaEventDisableTiming);
         cudaEvent_t t0, t1;
         cudaEventCreate(&t0);
         cudaEventCreate(&t1);
@@ -482,10 +587,18 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
         cudaEventDestroy(t1);
         cudaEventDestroy(L.e0);
         cudaEventDestroy(L.e1);
+        cudaEventDestroy(L.e2);
     }
+    if (L.s2) {
+        cudaStreamSynchronize(L.s2);
+        cudaStreamDestroy(L.s2);
+    }
+    if (L.econv) cudaEventDestroy(L.econv);
     DevBuf *bufs[] = {&L.hist, &L.W, &L.X, &L.Y, &L.tmp, &L.partial, &L.coef, &L.sqp, &L.sq, &L.Adev,
-                      &L.Vtmp, &L.Zdev, &L.wdev, &L.stat, &L.al, &L.bt, &L.ev, &L.M, &L.tau, &L.ework};
+                      &L.Vtmp, &L.Zdev, &L.wdev, &L.stat, &L.al, &L.bt, &L.ev, &L.M, &L.tau, &L.ework,
+                      &L.al2, &L.bt2, &L.w2};
     cudaStreamSynchronize(L.s);
     for (DevBuf *b : bufs) dev_free(*b);
+    if (L.hpin) cudaFreeHost(L.hpin);
     return st;
 }

@@ -165,6 +165,17 @@ __global__ void k_scale_cols(const double *__restrict__ x, double *y, const doub
         for (int b = 0; b < nB; ++b) y[(int64_t)b * ld + i] = x[(int64_t)b * ld + i] * s[b];
 }
 
+// y = x / sqrt(sq[0]) when sq[0] > 0 (nothing written otherwise): the
+// scalar normalization of the residual, with the norm left on the device
+__global__ void k_normalize_col(const double *__restrict__ x, double *__restrict__ y, const double *__restrict__ sq,
+                                int64_t n) {
+    const double q = sq[0];
+    if (!(q > 0.0)) return;
+    const double inv = 1.0 / sqrt(q);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] = x[i] * inv;
+}
+
 // interleaved applyH vector from nB history columns (fp64 -> T)
 template <typename T>
 __global__ void k_pack(const double *__restrict__ V, int nB, int64_t n, int64_t ld, T *__restrict__ x) {
@@ -360,6 +371,9 @@ __global__ void k_bisect_arrow(int n, int k, const double *__restrict__ al, cons
         const int nb = __popc(below);  // shifts 0..nb-1 are below
         const double nlo = (nb == 0) ? lo : lo + (hi - lo) * (double)nb / 33.0;
         const double nhi = (nb == 32) ? hi : lo + (hi - lo) * (double)(nb + 1) / 33.0;
+        // an interval a few ulps wide no longer shrinks: every shift rounds
+        // onto an end point
+        if (nlo == lo && nhi == hi) break;
         lo = nlo;
         hi = nhi;
     }
@@ -728,6 +742,11 @@ cudaError_t transform(const double *V, int m, const double *Y, int ldy, int K, d
 
 cudaError_t scale_cols(const double *x, double *y, const double *sc, int nB, int64_t n, int64_t ld, cudaStream_t s) {
     k_scale_cols<<<592, 256, 0, s>>>(x, y, sc, nB, n, ld);
+    return cudaGetLastError();
+}
+
+cudaError_t normalize_col(const double *x, double *y, const double *sq, int64_t n, cudaStream_t s) {
+    k_normalize_col<<<592, 256, 0, s>>>(x, y, sq, n);
     return cudaGetLastError();
 }
 

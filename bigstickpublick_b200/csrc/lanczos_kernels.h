@@ -16,6 +16,8 @@ cudaError_t sub_gemv(const double *H, int k, const double *C, double *W, int nB,
 cudaError_t transform(const double *V, int m, const double *Y, int ldy, int K, double *out, int64_t n, int64_t ld,
                       int64_t ldo, cudaStream_t s);
 cudaError_t scale_cols(const double *x, double *y, const double *sc, int nB, int64_t n, int64_t ld, cudaStream_t s);
+// y = x / sqrt(sq[0]) if sq[0] > 0, else y untouched (sq on the device)
+cudaError_t normalize_col(const double *x, double *y, const double *sq, int64_t n, cudaStream_t s);
 cudaError_t pack(const double *V, int nB, int64_t n, int64_t ld, void *x, int prec, cudaStream_t s);
 cudaError_t unpack(const void *y, int nB, int64_t n, int64_t ld, double *W, int prec, cudaStream_t s);
 // dense symmetric eigenproblem (n x n row-major A, destroyed); Z row-major,

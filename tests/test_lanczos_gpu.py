@@ -79,6 +79,24 @@ def test_thick_restart_converges(sd22):
     assert rel.max() < 1e-9, (rel, rep)
 
 
+@pytest.mark.parametrize("kw", [dict(nkeep=5, niter=200),
+                                dict(nkeep=5, niter=30, nthick_add=10, max_restarts=40)])
+def test_convergence_stop_matches_oracle(sd22, kw):
+    """The convergence test of a step runs beside the next step's applyH;
+    the run must still stop at the same step as the reference's order (the
+    oracle's stop step is the same for tol within +-2 %, so round-off cannot
+    move it)."""
+    T, H, exact = sd22
+    piv = generic_pivot(T.dim)
+    ev, _, rep = H.lanczos(matvec_prec=8, converge_tol=1e-6, pivot=piv, **kw)
+    ref, _, orep = olz.lanczos(T, tol=1e-6, pivot=piv, **kw)
+    assert rep["converged"] == 1
+    assert rep["total_iterations"] == orep["total_iterations"], (rep, orep)
+    assert rep["restarts"] == orep["restarts"]
+    assert rep["iterations"] == orep["iterations"]
+    assert np.abs(ev - ref).max() < 1e-9 * np.abs(ref).max()
+
+
 def test_thick_restart_matches_oracle(sd22):
     T, H, exact = sd22
     kw = dict(nkeep=5, niter=30, nthick_add=5, max_restarts=3, converge_tol=1e-30)
