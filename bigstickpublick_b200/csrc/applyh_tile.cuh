@@ -76,8 +76,12 @@ __host__ __device__ constexpr size_t align16(size_t x) { return (x + 15) & ~size
 // mstride: floats of per-warp shared memory for the PN matrix-element table.
 template <typename T, int NB, int ITEMS, bool FULL>
 __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, const T *__restrict__ vin,
-                                         T *__restrict__ vout, const int ld, const int v0,
+                                         T *__restrict__ vout, const int ld_, const int v0_,
                                          float *__restrict__ Mw, T *__restrict__ part) {
+    // dense layout: the stride is the compile-time block size and the column
+    // offset is zero, so gather addresses need no runtime multiply
+    const int ld = FULL ? NB : ld_;
+    const int v0 = FULL ? 0 : v0_;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int row = tile.row;
     const int64_t roff = a.row_off[row];
