@@ -235,7 +235,7 @@ def batch_leg(args):
     tabs = [model.build_tables(model.batch_member(s)) for s in range(1000, 1000 + args.batch_n)]
     t_build = time.perf_counter() - t0
     t0 = time.perf_counter()
-    cache = os.path.join(ROOT, "profiles", "batch_tuning.json") if args.tune_cache else None
+    cache = os.path.join(ROOT, ".tune_cache", "batch_tuning.json") if args.tune_cache else None
     b = Batch(tabs, autotune=True, tune_cache=cache)
     t_create = time.perf_counter() - t0
     dims = [t.dim for t in tabs]

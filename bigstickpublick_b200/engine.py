@@ -14,6 +14,8 @@ Errors raise ``BsgError`` with the status name and the latched message; there
 is no CPU fallback anywhere on this path.
 """
 import ctypes as C
+import json
+import os
 
 import numpy as np
 
@@ -200,8 +202,6 @@ class Batch:
         sig = self.signature()
         cache = {}
         if tune_cache:
-            import json
-            import os
             if os.path.exists(tune_cache):
                 cache = json.load(open(tune_cache))
         if sig in cache:
@@ -211,8 +211,8 @@ class Batch:
         elif autotune:
             self.tuning = self.autotune()
             if tune_cache:
-                import json
                 cache[sig] = {k: v for k, v in self.tuning.items() if k != "source"}
+                os.makedirs(os.path.dirname(os.path.abspath(tune_cache)), exist_ok=True)
                 with open(tune_cache, "w") as f:
                     json.dump(cache, f, indent=1)
 
