@@ -95,8 +95,10 @@ static int launch_typed(bsg_ctx *ctx, const T *vin, T *vout, int nb, int accumul
 
 int launch_applyh(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec, int accumulate,
                   cudaStream_t s, TileLookup lk) {
-    if (ctx->args.max_nbd > 8192)
-        return set_err(ctx, BSG_ERR_UNSUPPORTED, "a neutron sector jump has more than 8192 distinct (b,d) pairs");
+    // the 8 per-warp PN tables must fit in shared memory beside the partial
+    // sums (227 KB per CTA; 32 KB of partial sums at nb = 16, FP64)
+    if (ctx->args.max_nbd > 5120)
+        return set_err(ctx, BSG_ERR_UNSUPPORTED, "a neutron sector jump has more than 5120 distinct (b,d) pairs");
     if (prec == BSG_PREC_FP32)
         return launch_typed<float>(ctx, (const float *)vin, (float *)vout, nb, accumulate, s, lk);
     return launch_typed<double>(ctx, (const double *)vin, (double *)vout, nb, accumulate, s, lk);

@@ -8,7 +8,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/bsg.h"
+#include "bsg.h"
 
 namespace bsg {
 

@@ -166,6 +166,11 @@ extern "C" int bsg_grad(bsg_ctx *ctx, const double *evecs, int nstates, double *
     g.dspe_p = spe ? (double *)gsp.p : nullptr;
     g.dspe_n = spe ? (double *)gsn.p : nullptr;
     const int mstride = (a.max_nbd + 1) & ~1;
+    // 8 per-warp FP64 tables within the 227 KB of shared memory per CTA
+    if (a.max_nbd > 3392) {
+        dev_free(psi); dev_free(gpp); dev_free(gnn); dev_free(gpn); dev_free(gsp); dev_free(gsn);
+        return set_err(ctx, BSG_ERR_UNSUPPORTED, "bsg_grad: a neutron sector jump has more than 3392 distinct (b,d) pairs");
+    }
     const size_t smem = sizeof(double) * (size_t)kGradWarps * (mstride > 0 ? mstride : 2);
     cudaStream_t s = ctx->stream;
     cudaError_t e = cudaFuncSetAttribute(k_grad<ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

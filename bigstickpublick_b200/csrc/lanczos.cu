@@ -71,6 +71,9 @@ struct Lz {
     cudaStream_t s2 = nullptr;
     cudaEvent_t econv = nullptr;
     DevBuf al2, bt2, w2;
+    // block recursion: dense projected matrix (pinned), Householder work
+    double *pinA = nullptr;
+    DevBuf Adev2, Vtmp2, tau2, ework2;
 
     double *col(int j) { return (double *)hist.p + (int64_t)j * n; }
     double &Tm(int i, int j) { return T[(size_t)i * maxcol + j]; }
@@ -167,10 +170,20 @@ int eig_queue(Lz &L, int m, int k, int want) {
     want = std::min(want, m);
     double glo, ghi, scale;
     gershgorin(L, m, glo, ghi, scale);
-    arrow_inputs(L, m, k, L.pin_al(), L.pin_bt());
-    CK(cudaMemcpyAsync(L.al2.p, L.pin_al(), sizeof(double) * m, cudaMemcpyHostToDevice, L.s2));
-    CK(cudaMemcpyAsync(L.bt2.p, L.pin_bt(), sizeof(double) * m, cudaMemcpyHostToDevice, L.s2));
-    CK(bisect_arrow(m, k, (const double *)L.al2.p, (const double *)L.bt2.p, want, glo, ghi, (double *)L.w2.p, L.s2));
+    int kk = k;
+    if (L.nb == 1) {
+        arrow_inputs(L, m, k, L.pin_al(), L.pin_bt());
+        CK(cudaMemcpyAsync(L.al2.p, L.pin_al(), sizeof(double) * m, cudaMemcpyHostToDevice, L.s2));
+        CK(cudaMemcpyAsync(L.bt2.p, L.pin_bt(), sizeof(double) * m, cudaMemcpyHostToDevice, L.s2));
+    } else {
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < m; ++j) L.pinA[(size_t)i * m + j] = 0.5 * (L.Tm(i, j) + L.Tm(j, i));
+        CK(cudaMemcpyAsync(L.Adev2.p, L.pinA, sizeof(double) * m * m, cudaMemcpyHostToDevice, L.s2));
+        CK(tridiag(m, (double *)L.Adev2.p, (double *)L.al2.p, (double *)L.bt2.p, (double *)L.Vtmp2.p,
+                   (double *)L.tau2.p, (double *)L.ework2.p, L.s2));
+        kk = 0;
+    }
+    CK(bisect_arrow(m, kk, (const double *)L.al2.p, (const double *)L.bt2.p, want, glo, ghi, (double *)L.w2.p, L.s2));
     CK(cudaMemcpyAsync(L.pin_w(), L.w2.p, sizeof(double) * want, cudaMemcpyDeviceToHost, L.s2));
     CK(cudaEventRecord(L.econv, L.s2));
     return BSG_OK;
@@ -409,7 +422,7 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
         if (cur >= niter * nb) finished = true;
         if (!p->fixed_iter && mT > ncheck && mT < (int64_t)n) {
             const bool restart_due = thick && !finished && cur + nb > (niter - 1) * nb;
-            if (nb == 1 && !finished && !restart_due) {
+            if (!finished && !restart_due) {
                 ST(eig_queue(L, mT, karrow, ncheck));
                 pend.active = true;
                 pend.want = std::min(ncheck, mT);
@@ -565,6 +578,15 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
                 (st = dev_alloc(ctx, L.w2, sizeof(double) * N)))) {
         // fall through to cleanup
     }
+    if (!st && L.nb > 1 &&
+        ((st = dev_alloc(ctx, L.Adev2, sizeof(double) * (size_t)N * N)) ||
+         (st = dev_alloc(ctx, L.Vtmp2, sizeof(double) * (size_t)N * N)) || (st = dev_alloc(ctx, L.tau2, sizeof(double) * N)) ||
+         (st = dev_alloc(ctx, L.ework2, sizeof(double) * 2 * (size_t)N)))) {
+        // fall through to cleanup
+    }
+    if (!st && L.nb > 1)
+        st = cuda_check(ctx, cudaHostAlloc((void **)&L.pinA, sizeof(double) * (size_t)N * N, cudaHostAllocDefault),
+                        "cudaHostAlloc (Lanczos projected matrix)");
     if (!st) st = cuda_check(ctx, cudaHostAlloc((void **)&L.hpin, sizeof(double) * L.pin_doubles(), cudaHostAllocDefault),
                              "cudaHostAlloc (Lanczos staging)");
     if (!st) st = cuda_check(ctx, cudaStreamCreateWithFlags(&L.s2, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -596,9 +618,10 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
     if (L.econv) cudaEventDestroy(L.econv);
     DevBuf *bufs[] = {&L.hist, &L.W, &L.X, &L.Y, &L.tmp, &L.partial, &L.coef, &L.sqp, &L.sq, &L.Adev,
                       &L.Vtmp, &L.Zdev, &L.wdev, &L.stat, &L.al, &L.bt, &L.ev, &L.M, &L.tau, &L.ework,
-                      &L.al2, &L.bt2, &L.w2};
+                      &L.al2, &L.bt2, &L.w2, &L.Adev2, &L.Vtmp2, &L.tau2, &L.ework2};
     cudaStreamSynchronize(L.s);
     for (DevBuf *b : bufs) dev_free(*b);
     if (L.hpin) cudaFreeHost(L.hpin);
+    if (L.pinA) cudaFreeHost(L.pinA);
     return st;
 }

@@ -17,6 +17,7 @@
 // every coefficient is bitwise repeatable.
 
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <stdint.h>
 
 #include "lanczos_kernels.h"
@@ -27,49 +28,88 @@ constexpr int kDotThreads = 256;
 constexpr int kDotTile = 512;      // rows per tile
 
 // C[p] partials: pairs p = a*nB + b, a < nA, b < nB; A, B column-major with
-// leading dimension ld (vector j at base + j*ld).  Each CTA walks row chunks
-// (grid-stride); the chunk of B is staged in shared memory, warp w takes
-// vectors a = w, w+8, ... and reads them coalesced, lanes keep NB partial
-// sums, a warp reduction adds them into the CTA's shared accumulator (each
-// (a,b) owned by one warp), and the CTA writes partial[p * gridDim.x + cta].
+// leading dimension ld (vector j at base + j*ld).  CTA (x, y) walks the row
+// chunks x, x + gridDim.x, ... and the A vectors of chunk y (short vectors
+// spread the A vectors over gridDim.y CTAs).  The chunk of B is staged in
+// shared memory, column-major so that lanes read consecutive rows; warp w
+// takes its vectors (two at a time for NB >= 4, halving the shared loads per
+// multiply-add) and reads them coalesced, lanes keep NB partial sums per
+// vector, and a warp reduction adds them into the CTA's shared accumulator
+// (each (a,b) owned by one warp, added in chunk order).  The CTA writes
+// partial[p * gridDim.x + x] for its vectors.
 template <int NB>
 __global__ void __launch_bounds__(kDotThreads) k_multidot(const double *__restrict__ A, int nA,
                                                          const double *__restrict__ B, int64_t n, int64_t ld,
                                                          double *__restrict__ partial) {
     extern __shared__ double sm[];
-    double *sB = sm;                       // [kDotTile][NB]
+    double *sB = sm;                       // [NB][kDotTile]
     double *sAcc = sm + kDotTile * NB;     // [nA][NB]
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = kDotThreads / 32;
+    const int per = (nA + gridDim.y - 1) / gridDim.y;
+    const int a_lo = blockIdx.y * per, a_hi = min(nA, a_lo + per);
+    constexpr int PAIR = NB >= 4 ? 2 : 1;
     for (int e = threadIdx.x; e < nA * NB; e += kDotThreads) sAcc[e] = 0.0;
     for (int64_t t0 = (int64_t)blockIdx.x * kDotTile; t0 < n; t0 += (int64_t)gridDim.x * kDotTile) {
         const int rows = (int)((n - t0) < kDotTile ? (n - t0) : kDotTile);
         __syncthreads();
         for (int e = threadIdx.x; e < rows * NB; e += kDotThreads) {
             const int b = e / rows, r = e - b * rows;
-            sB[r * NB + b] = B[(int64_t)b * ld + t0 + r];
+            sB[b * kDotTile + r] = B[(int64_t)b * ld + t0 + r];
         }
         __syncthreads();
-        for (int a = warp; a < nA; a += nw) {
-            const double *__restrict__ col = A + (int64_t)a * ld + t0;
-            double acc[NB];
+        for (int a = a_lo + warp * PAIR; a < a_hi; a += nw * PAIR) {
+            const bool two = PAIR == 2 && a + 1 < a_hi;
+            const double *__restrict__ col0 = A + (int64_t)a * ld + t0;
+            const double *__restrict__ col1 = two ? col0 + ld : col0;
+            double acc0[NB], acc1[NB];
 #pragma unroll
-            for (int b = 0; b < NB; ++b) acc[b] = 0.0;
-            for (int r = lane; r < rows; r += 32) {
-                const double x = __ldg(col + r);
+            for (int b = 0; b < NB; ++b) acc0[b] = acc1[b] = 0.0;
+            // four rows per lane and step, loads first (the sum stays in row order)
+            int r = lane;
+            for (; r + 96 < rows; r += 128) {
+                double x0[4], x1[4];
 #pragma unroll
-                for (int b = 0; b < NB; ++b) acc[b] = fma(x, sB[r * NB + b], acc[b]);
+                for (int u = 0; u < 4; ++u) {
+                    x0[u] = __ldg(col0 + r + 32 * u);
+                    x1[u] = PAIR == 2 ? __ldg(col1 + r + 32 * u) : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+#pragma unroll
+                    for (int b = 0; b < NB; ++b) {
+                        const double y = sB[b * kDotTile + r + 32 * u];
+                        acc0[b] = fma(x0[u], y, acc0[b]);
+                        if (PAIR == 2) acc1[b] = fma(x1[u], y, acc1[b]);
+                    }
+            }
+            for (; r < rows; r += 32) {
+                const double x0 = __ldg(col0 + r);
+                const double x1 = PAIR == 2 ? __ldg(col1 + r) : 0.0;
+#pragma unroll
+                for (int b = 0; b < NB; ++b) {
+                    const double y = sB[b * kDotTile + r];
+                    acc0[b] = fma(x0, y, acc0[b]);
+                    if (PAIR == 2) acc1[b] = fma(x1, y, acc1[b]);
+                }
             }
 #pragma unroll
             for (int b = 0; b < NB; ++b) {
-                double v = acc[b];
+                double v = acc0[b];
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
                 if (lane == 0) sAcc[a * NB + b] += v;
+                if (PAIR == 2) {
+                    double u = acc1[b];
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) u += __shfl_xor_sync(0xffffffffu, u, o);
+                    if (lane == 0 && two) sAcc[(a + 1) * NB + b] += u;
+                }
             }
         }
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < nA * NB; e += kDotThreads) partial[(int64_t)e * gridDim.x + blockIdx.x] = sAcc[e];
+    for (int e = a_lo * NB + threadIdx.x; e < a_hi * NB; e += kDotThreads)
+        partial[(int64_t)e * gridDim.x + blockIdx.x] = sAcc[e];
 }
 
 // out[p] = sum over g of partial[p*G + g]: one warp per p, lanes take g = lane,
@@ -138,8 +178,10 @@ __global__ void __launch_bounds__(256) k_sub_gemv(const double *__restrict__ H, 
 }
 
 // out[l] = sum_j V[j] * Y[j*ldy + l], l < K (K <= 16 per launch)
+// K is a template parameter so that the K accumulators live in registers
+template <int K>
 __global__ void __launch_bounds__(256) k_transform(const double *__restrict__ V, int m, const double *__restrict__ Y,
-                                                   int ldy, int K, double *__restrict__ out, int64_t n, int64_t ld,
+                                                   int ldy, double *__restrict__ out, int64_t n, int64_t ld,
                                                    int64_t ldo) {
     extern __shared__ double sY[];  // [m][K]
     for (int e = threadIdx.x; e < m * K; e += blockDim.x) {
@@ -148,12 +190,21 @@ __global__ void __launch_bounds__(256) k_transform(const double *__restrict__ V,
     }
     __syncthreads();
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        double acc[16];
+        double acc[K];
+#pragma unroll
         for (int l = 0; l < K; ++l) acc[l] = 0.0;
-        for (int j = 0; j < m; ++j) {
-            const double v = __ldg(V + (int64_t)j * ld + i);
-            for (int l = 0; l < K; ++l) acc[l] = fma(v, sY[j * K + l], acc[l]);
+        int j = 0;
+        for (; j + 1 < m; j += 2) {
+            const double v0 = __ldg(V + (int64_t)j * ld + i), v1 = __ldg(V + (int64_t)(j + 1) * ld + i);
+#pragma unroll
+            for (int l = 0; l < K; ++l) acc[l] = fma(v1, sY[(j + 1) * K + l], fma(v0, sY[j * K + l], acc[l]));
         }
+        if (j < m) {
+            const double v0 = __ldg(V + (int64_t)j * ld + i);
+#pragma unroll
+            for (int l = 0; l < K; ++l) acc[l] = fma(v0, sY[j * K + l], acc[l]);
+        }
+#pragma unroll
         for (int l = 0; l < K; ++l) out[(int64_t)l * ldo + i] = acc[l];
     }
 }
@@ -674,9 +725,12 @@ static cudaError_t multidot_nb(const double *A, int nA, const double *B, int64_t
     const int maxa = 4096 / NB;  // shared accumulator of at most 4096 doubles
     for (int a0 = 0; a0 < nA;) {
         const int na = (nA - a0) < maxa ? (nA - a0) : maxa;
+        // short vectors (fewer row chunks than 4 CTAs per SM): spread the A
+        // vectors over more CTAs, at least 8 vectors each
+        const int gy = std::max(1, std::min((592 + G - 1) / G, na / 8));
         const size_t smem = sizeof(double) * ((size_t)kDotTile * NB + (size_t)na * NB);
         cudaFuncSetAttribute(k_multidot<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_multidot<NB><<<G, kDotThreads, smem, s>>>(A + (int64_t)a0 * ld, na, B, n, ld, partial);
+        k_multidot<NB><<<dim3(G, gy), kDotThreads, smem, s>>>(A + (int64_t)a0 * ld, na, B, n, ld, partial);
         k_reduce_partials<<<(na * NB * 32 + 255) / 256, 256, 0, s>>>(partial, na * NB, G, out + (int64_t)a0 * NB);
         a0 += na;
     }
@@ -734,8 +788,21 @@ cudaError_t transform(const double *V, int m, const double *Y, int ldy, int K, d
         // Y rows in chunks that fit shared memory: accumulate over row chunks
         if ((size_t)m * kk * sizeof(double) > 160 * 1024) return cudaErrorInvalidValue;
         const size_t smem = sizeof(double) * (size_t)m * kk;
-        cudaFuncSetAttribute(k_transform, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-        k_transform<<<592, 256, smem, s>>>(V, m, Y + l0, ldy, kk, out + (int64_t)l0 * ldo, n, ld, ldo);
+        cudaError_t e = cudaSuccess;
+        switch (kk) {
+#define BSG_TRANSFORM_CASE(KT)                                                                              \
+    case KT:                                                                                                \
+        e = cudaFuncSetAttribute(k_transform<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024); \
+        if (e == cudaSuccess)                                                                               \
+            k_transform<KT><<<592, 256, smem, s>>>(V, m, Y + l0, ldy, out + (int64_t)l0 * ldo, n, ld, ldo); \
+        break;
+            BSG_TRANSFORM_CASE(1) BSG_TRANSFORM_CASE(2) BSG_TRANSFORM_CASE(3) BSG_TRANSFORM_CASE(4)
+            BSG_TRANSFORM_CASE(5) BSG_TRANSFORM_CASE(6) BSG_TRANSFORM_CASE(7) BSG_TRANSFORM_CASE(8)
+            BSG_TRANSFORM_CASE(9) BSG_TRANSFORM_CASE(10) BSG_TRANSFORM_CASE(11) BSG_TRANSFORM_CASE(12)
+            BSG_TRANSFORM_CASE(13) BSG_TRANSFORM_CASE(14) BSG_TRANSFORM_CASE(15) BSG_TRANSFORM_CASE(16)
+#undef BSG_TRANSFORM_CASE
+        }
+        if (e != cudaSuccess) return e;
     }
     return cudaGetLastError();
 }
