@@ -326,6 +326,14 @@ def large_leg(args):
             "device_mem_total_GB": total / 1e9}
 
 
+def workload_config(args, tables, world):
+    """The `config` object of both arms' JSON lines."""
+    return {"workload": args.workload, "dim": tables.dim, "nb": args.nb,
+            "interaction": "seeded synthetic isospin TBMEs N(0,1) MeV",
+            "l2": "flushed (256 MiB write) before every timed matvec; kernel timed alone",
+            "parallelism": f"replicas x{world}"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -348,7 +356,7 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_total / max(1, n_total),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if args.prec == 4 else "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "nb": args.nb, "dim": tables.dim},
+        "config": workload_config(args, tables, int(os.environ.get("WORLD_SIZE", "1"))),
         "cpu_baseline": {"value": value, "unit": "matvec/s", "cores": nthreads, "kind": "port",
                          "sample": f"{n_total} matvecs over {t_total:.1f} s (reference is Fortran; "
                                    "no Fortran compiler in the image)"},
@@ -472,10 +480,7 @@ def main():
         "metric": METRIC, "value": value, "unit": "matvec/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32" if prec == 4 else "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "dim": tables.dim, "nb": nb,
-                   "interaction": "seeded synthetic isospin TBMEs N(0,1) MeV",
-                   "l2": "flushed (256 MiB write) before every timed matvec; kernel timed alone",
-                   "parallelism": f"replicas x{world}"},
+        "config": workload_config(args, tables, world),
         "e2e": {"value": e2e, "unit": "matvec/s", "h2d_bytes_per_step": vbytes, "d2h_bytes_per_step": vbytes},
         "gpu_launches": args.steps * st["kernel_launches_per_matvec"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
