@@ -449,6 +449,37 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
         return x.second.nop < y.second.nop;
     });
     auto nrec_of = [&](int32_t id) -> int64_t { return nptr_all[nops[id].ptr_base + nops[id].nout]; };
+    // ---- sliced records: per operator, output positions in slices of 32;
+    // a slice holds its longest position's count of 32-record rows, record k
+    // of lane l at row k (padding rows hold {0, 0} and are never read)
+    std::vector<int2> sell_all;
+    std::vector<int32_t> slice_off_all;
+    for (NOp &op : nops) {
+        op.sell_base = (int64_t)sell_all.size();
+        op.slice_base = (int64_t)slice_off_all.size();
+        const int32_t *ptr = nptr_all.data() + op.ptr_base;
+        const int nslice = (op.nout + 31) / 32;
+        int64_t off = 0;
+        for (int sl = 0; sl < nslice; ++sl) {
+            int32_t width = 0;
+            for (int l = 0; l < 32 && 32 * sl + l < op.nout; ++l)
+                width = std::max(width, ptr[32 * sl + l + 1] - ptr[32 * sl + l]);
+            if (off > INT32_MAX) return V.fail("a neutron operator has more than 2^31 sliced records");
+            slice_off_all.push_back((int32_t)off);
+            const size_t row0 = sell_all.size();
+            sell_all.resize(row0 + (size_t)32 * width, make_int2(0, 0));
+            for (int l = 0; l < 32 && 32 * sl + l < op.nout; ++l)
+                for (int32_t k = ptr[32 * sl + l]; k < ptr[32 * sl + l + 1]; ++k) {
+                    int2 r;
+                    if (op.kind == 1)
+                        std::memcpy(&r, &pnrec_all[op.rec_base + k], sizeof(int2));
+                    else
+                        std::memcpy(&r, &nnrec_all[op.rec_base + k], sizeof(int2));
+                    sell_all[row0 + (size_t)32 * (k - ptr[32 * sl + l]) + l] = r;
+                }
+            off += (int64_t)32 * width;
+        }
+    }
     const int W = kRowWarps;
     std::vector<uint8_t> w_pp(pp.size()), w_nn(nn.size()), w_pn(pn.size()), w_spe(spe.size());
     {
@@ -582,6 +613,8 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
         (st = up(ctx->nptr, nptr_all.data(), 4 * nptr_all.size())) ||
         (st = up(ctx->pnrec, pnrec_all.data(), sizeof(PNRec) * pnrec_all.size())) ||
         (st = up(ctx->nnrec, nnrec_all.data(), sizeof(NNRec) * nnrec_all.size())) ||
+        (st = up(ctx->sell, sell_all.data(), sizeof(int2) * sell_all.size())) ||
+        (st = up(ctx->slice_off, slice_off_all.data(), 4 * slice_off_all.size())) ||
         (st = up(ctx->bd, bd_all.data(), sizeof(BDPair) * bd_all.size())) ||
         (st = up(ctx->cpn, cpn32.data(), 4 * cpn32.size())) || (st = up(ctx->dpn, dpn32.data(), 4 * dpn32.size())) ||
         (st = up(ctx->nspe, nspe.data(), 4 * nspe.size())) ||
@@ -596,7 +629,8 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
                                          sizeof(PPContrib) * ctx->h_pp.size() + sizeof(NNContrib) * ctx->h_nn.size() +
                                          sizeof(PNContrib) * ctx->h_pn.size() + sizeof(SPEContrib) * h_spe.size() +
                                          sizeof(NOp) * nops.size() + 4 * nptr_all.size() +
-                                         sizeof(PNRec) * pnrec_all.size() + sizeof(NNRec) * nnrec_all.size());
+                                         sizeof(PNRec) * pnrec_all.size() + sizeof(NNRec) * nnrec_all.size() +
+                                         sizeof(int2) * sell_all.size() + 4 * slice_off_all.size());
     ctx->stats.n_rows = nrows;
     ctx->stats.n_contrib = (int64_t)(ctx->h_pp.size() + ctx->h_nn.size() + ctx->h_pn.size() + h_spe.size());
 
@@ -614,6 +648,8 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
     a.nptr = (const int32_t *)ctx->nptr.p;
     a.pnrec = (const PNRec *)ctx->pnrec.p;
     a.nnrec = (const NNRec *)ctx->nnrec.p;
+    a.sell = (const int2 *)ctx->sell.p;
+    a.slice_off = (const int32_t *)ctx->slice_off.p;
     a.bd = (const BDPair *)ctx->bd.p;
     int32_t max_nbd = 0;
     for (auto &o : nops) max_nbd = std::max(max_nbd, o.nbd);
@@ -633,7 +669,8 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
 void free_ctx(bsg_ctx *ctx) {
     for (auto &b : ctx->raw) dev_free(b);
     DevBuf *bufs[] = {&ctx->row_off, &ctx->pp_ptr, &ctx->nn_ptr, &ctx->pn_ptr, &ctx->spe_ptr, &ctx->pp, &ctx->nn,
-                      &ctx->pn, &ctx->spe, &ctx->nops, &ctx->nptr, &ctx->pnrec, &ctx->nnrec, &ctx->bd, &ctx->hmatpn,
+                      &ctx->pn, &ctx->spe, &ctx->nops, &ctx->nptr, &ctx->pnrec, &ctx->nnrec, &ctx->bd, &ctx->sell,
+                      &ctx->slice_off, &ctx->hmatpn,
                       &ctx->cpn, &ctx->dpn, &ctx->nspe, &ctx->pp_op, &ctx->nnrec_op, &ctx->nnrec_ph, &ctx->pp_ph,
                       &ctx->hmatpp_d,
                       &ctx->hmatnn_d, &ctx->scratch_in, &ctx->scratch_out};

@@ -54,6 +54,12 @@ struct NOp {
     int32_t kind;       // 0 = NN (me records), 1 = PN (label records)
     int32_t bd_base;    // PN: first entry of its distinct (b,d) list
     int32_t nbd;        // PN: number of distinct (b,d) neutron label pairs
+    // sliced copy of the records for the row kernels: output positions in
+    // slices of 32; record k of position 32*s + l sits at
+    // sell[sell_base + slice_off[slice_base + s] + 32*k + l], so the lanes of
+    // a warp read adjacent records
+    int64_t sell_base;
+    int64_t slice_base;
 };
 // PN record: input position, index of its (b,d) pair in the operator's
 // distinct-pair list, neutron jump phase
@@ -90,6 +96,8 @@ struct RowArgs {
     const int32_t *nptr;          // pointer arrays of all neutron ops
     const PNRec *pnrec;
     const NNRec *nnrec;
+    const int2 *sell;             // sliced PN / NN records (see NOp)
+    const int32_t *slice_off;
     const BDPair *bd;
     const float *hmatpn;
     const int32_t *cpn, *dpn;     // cpnpair/dpnpair as int32 (validated)
@@ -126,7 +134,7 @@ struct bsg_ctx {
     // raw tables on the device (byte-identical copies)
     std::vector<bsg::DevBuf> raw;
     // derived
-    bsg::DevBuf row_off, pp_ptr, nn_ptr, pn_ptr, spe_ptr, pp, nn, pn, spe, nops, nptr, pnrec, nnrec, bd;
+    bsg::DevBuf row_off, pp_ptr, nn_ptr, pn_ptr, spe_ptr, pp, nn, pn, spe, nops, nptr, pnrec, nnrec, bd, sell, slice_off;
     bsg::DevBuf hmatpn, cpn, dpn, nspe, hmatpp_d, hmatnn_d;
     bsg::RowArgs args{};
     std::map<int, bsg::TileSet> tiles;   // tile size -> tiles
