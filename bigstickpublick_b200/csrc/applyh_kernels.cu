@@ -16,19 +16,45 @@
 // (hmat * phase, src/bapplyhlibOMP.f90:1093-1095, :1269-1272) and promoted
 // to the vector type; FP32 vectors accumulate in FP32, FP64 vectors in FP64.
 
+#include <type_traits>
+
 #include "applyh_tile.cuh"
 
 namespace bsg {
 
 template <typename T, int NB, int ITEMS, bool FULL>
-__global__ void __launch_bounds__(kWarps * 32) k_rows(const RowArgs a, const T *__restrict__ vin,
-                                                      T *__restrict__ vout, const int ld, const int v0,
-                                                      const int mstride) {
+__device__ __forceinline__ void rows_body(const RowArgs &a, const T *__restrict__ vin, T *__restrict__ vout,
+                                          const int ld, const int v0, const int mstride) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int warp = threadIdx.x >> 5;
     float *__restrict__ Mw = reinterpret_cast<float *>(smem) + (size_t)warp * mstride;
     T *__restrict__ part = reinterpret_cast<T *>(smem + align16(sizeof(float) * (size_t)kWarps * mstride));
     row_tile<T, NB, ITEMS, FULL>(a, a.tiles[blockIdx.x], vin, vout, ld, v0, Mw, part);
+}
+
+template <typename T, int NB, int ITEMS, bool FULL>
+__global__ void __launch_bounds__(kWarps * 32) k_rows(const RowArgs a, const T *__restrict__ vin,
+                                                      T *__restrict__ vout, const int ld, const int v0,
+                                                      const int mstride) {
+    rows_body<T, NB, ITEMS, FULL>(a, vin, vout, ld, v0, mstride);
+}
+
+// single FP32 vectors: at most 40 registers, so that 6 CTAs of 256 threads
+// stay resident per SM to hide the gather latency (measured faster than the
+// compiler's own choice of 48 registers on the sliced walk)
+template <int ITEMS, bool FULL>
+__global__ void __launch_bounds__(kWarps * 32, 6) k_rows_f1(const RowArgs a, const float *__restrict__ vin,
+                                                            float *__restrict__ vout, const int ld, const int v0,
+                                                            const int mstride) {
+    rows_body<float, 1, ITEMS, FULL>(a, vin, vout, ld, v0, mstride);
+}
+
+template <typename T, int NB, int ITEMS, bool FULL>
+constexpr auto rows_kernel() {
+    if constexpr (std::is_same<T, float>::value && NB == 1)
+        return k_rows_f1<ITEMS, FULL>;
+    else
+        return k_rows<T, NB, ITEMS, FULL>;
 }
 
 template <typename T, int NB, int ITEMS>
@@ -49,11 +75,11 @@ static int launch_one(bsg_ctx *ctx, const T *vin, T *vout, int ld, int v0, int a
     const bool full = (ld == NB) && ((reinterpret_cast<uintptr_t>(vin) & 15u) == 0);
     cudaError_t e;
     if (full) {
-        auto k = k_rows<T, NB, ITEMS, true>;
+        auto k = rows_kernel<T, NB, ITEMS, true>();
         e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e == cudaSuccess) k<<<ts->ntiles, kWarps * 32, smem, s>>>(a, vin, vout, ld, v0, mstride);
     } else {
-        auto k = k_rows<T, NB, ITEMS, false>;
+        auto k = rows_kernel<T, NB, ITEMS, false>();
         e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e == cudaSuccess) k<<<ts->ntiles, kWarps * 32, smem, s>>>(a, vin, vout, ld, v0, mstride);
     }

@@ -65,18 +65,19 @@ template <> struct Vec<double, 16, true> : VecD2<16> {};
 constexpr int kWarps = kRowWarps;
 
 // Record k of an output position is read at column[kRecStride * k].  Blocks
-// of vectors (NB >= 2) walk the sliced copy, where the lanes of a warp read
-// adjacent records (tiles start on multiples of 32, so pos & 31 == lane);
-// single vectors walk the position-sorted records, which costs fewer
-// registers and serves the short rows of small spaces better.  Both give the
-// records of a position in the same order.
-template <int NB> constexpr int kRecStride = NB >= 2 ? 32 : 1;
+// of vectors and single FP32 vectors walk the sliced copy, where the lanes of
+// a warp read adjacent records (tiles start on multiples of 32, so
+// pos & 31 == lane); single FP64 vectors walk the position-sorted records,
+// which fits their register budget.  Both give the records of a position in
+// the same order.
+template <typename T, int NB> constexpr bool kSliced = NB >= 2 || sizeof(T) == 4;
+template <typename T, int NB> constexpr int kRecStride = kSliced<T, NB> ? 32 : 1;
 // the column base and the range of k for one output position; csr = the
 // operator's position-sorted records, [k0, k1) this position's range there
-template <int NB>
+template <typename T, int NB>
 __device__ __forceinline__ void record_column(const RowArgs &a, const NOp &op, const int2 *csr, int k0, int k1,
                                               int pos, int lane, const int2 *&col, int &k, int &kend) {
-    if constexpr (NB >= 2) {
+    if constexpr (kSliced<T, NB>) {
         col = a.sell + op.sell_base + __ldg(a.slice_off + op.slice_base + (pos >> 5)) + lane;
         k = 0;
         kend = k1 - k0;
@@ -154,9 +155,9 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
                 const int k0 = __ldg(ptr + pos[i]), k1 = __ldg(ptr + pos[i] + 1);
                 const int2 *col;
                 int k, n;
-                record_column<NB>(a, op, rec, k0, k1, pos[i], lane, col, k, n);
+                record_column<T, NB>(a, op, rec, k0, k1, pos[i], lane, col, k, n);
                 for (; k + 1 < n; k += 2) {
-                    const int2 r0 = __ldg(col + kRecStride<NB> * k), r1 = __ldg(col + kRecStride<NB> * (k + 1));
+                    const int2 r0 = __ldg(col + kRecStride<T, NB> * k), r1 = __ldg(col + kRecStride<T, NB> * (k + 1));
                     T x0[NB], x1[NB];
                     Vec<T, NB, FULL>::load(src + (size_t)r0.x * ld, x0);
                     Vec<T, NB, FULL>::load(src + (size_t)r1.x * ld, x1);
@@ -165,7 +166,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
                     for (int v = 0; v < NB; ++v) { acc[i][v] += m0 * x0[v]; acc[i][v] += m1 * x1[v]; }
                 }
                 if (k < n) {
-                    const int2 r0 = __ldg(col + kRecStride<NB> * k);
+                    const int2 r0 = __ldg(col + kRecStride<T, NB> * k);
                     T x0[NB];
                     Vec<T, NB, FULL>::load(src + (size_t)r0.x * ld, x0);
                     const T m0 = (T)__int_as_float(r0.y);
@@ -202,9 +203,9 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
                 const int k0 = __ldg(ptr + pos[i]), k1 = __ldg(ptr + pos[i] + 1);
                 const int2 *col;
                 int k, n;
-                record_column<NB>(a, op, rec, k0, k1, pos[i], lane, col, k, n);
+                record_column<T, NB>(a, op, rec, k0, k1, pos[i], lane, col, k, n);
                 for (; k + 1 < n; k += 2) {
-                    const int2 r0 = __ldg(col + kRecStride<NB> * k), r1 = __ldg(col + kRecStride<NB> * (k + 1));
+                    const int2 r0 = __ldg(col + kRecStride<T, NB> * k), r1 = __ldg(col + kRecStride<T, NB> * (k + 1));
                     T x0[NB], x1[NB];
                     Vec<T, NB, FULL>::load(src + (size_t)r0.x * ld, x0);
                     Vec<T, NB, FULL>::load(src + (size_t)r1.x * ld, x1);
@@ -216,7 +217,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
                     for (int v = 0; v < NB; ++v) { acc[i][v] += m0 * x0[v]; acc[i][v] += m1 * x1[v]; }
                 }
                 if (k < n) {
-                    const int2 r0 = __ldg(col + kRecStride<NB> * k);
+                    const int2 r0 = __ldg(col + kRecStride<T, NB> * k);
                     T x0[NB];
                     Vec<T, NB, FULL>::load(src + (size_t)r0.x * ld, x0);
                     const float f0 = __int_as_float(__float_as_int(Mw[r0.y & 0xffff]) ^ ((r0.y << 8) & 0x80000000));
