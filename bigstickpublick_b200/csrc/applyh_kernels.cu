@@ -74,13 +74,20 @@ static int launch_one(bsg_ctx *ctx, const T *vin, T *vout, int ld, int v0, int a
     // the base pointer is 16-byte aligned
     const bool full = (ld == NB) && ((reinterpret_cast<uintptr_t>(vin) & 15u) == 0);
     cudaError_t e;
+    auto allow = [&](const void *fn) -> cudaError_t {
+        size_t &cur = ctx->smem_allowed[fn];
+        if (cur >= smem) return cudaSuccess;
+        const cudaError_t r = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (r == cudaSuccess) cur = smem;
+        return r;
+    };
     if (full) {
         auto k = rows_kernel<T, NB, ITEMS, true>();
-        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = allow((const void *)k);
         if (e == cudaSuccess) k<<<ts->ntiles, kWarps * 32, smem, s>>>(a, vin, vout, ld, v0, mstride);
     } else {
         auto k = rows_kernel<T, NB, ITEMS, false>();
-        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = allow((const void *)k);
         if (e == cudaSuccess) k<<<ts->ntiles, kWarps * 32, smem, s>>>(a, vin, vout, ld, v0, mstride);
     }
     if (e != cudaSuccess) return cuda_check(ctx, e, "applyh smem attribute");

@@ -138,6 +138,9 @@ struct bsg_ctx {
     bsg::DevBuf hmatpn, cpn, dpn, nspe, hmatpp_d, hmatnn_d;
     bsg::RowArgs args{};
     std::map<int, bsg::TileSet> tiles;   // tile size -> tiles
+    // largest dynamic shared memory already allowed per kernel function (the
+    // attribute is set once per size, not on every launch)
+    std::map<const void *, size_t> smem_allowed;
     std::vector<int32_t> h_rowlen;
     std::vector<bsg::BDPair> h_bd;
     std::vector<bsg::PNRec> h_pnrec;
