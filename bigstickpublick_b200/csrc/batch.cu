@@ -27,6 +27,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <numeric>
+#include <type_traits>
 #include <vector>
 
 #include "applyh_tile.cuh"
@@ -64,9 +65,8 @@ struct BChunk {
 constexpr int kChunk = 2048;
 
 template <typename T, int ITEMS>
-__global__ void __launch_bounds__(kWarps * 32) k_rows_batch(const BatchSys *__restrict__ sys,
-                                                            const BatchItem *__restrict__ items, int nitems,
-                                                            int *__restrict__ counter, int mstride) {
+__device__ __forceinline__ void rows_batch_body(const BatchSys *__restrict__ sys, const BatchItem *__restrict__ items,
+                                                int nitems, int *__restrict__ counter, int mstride) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_item;
     const int warp = threadIdx.x >> 5;
@@ -83,6 +83,32 @@ __global__ void __launch_bounds__(kWarps * 32) k_rows_batch(const BatchSys *__re
         row_tile<T, 1, ITEMS, false>(S->a, S->a.tiles[w.tile], (const T *)S->vin, (T *)S->vout, 1, 0, Mw, part);
         __syncthreads();
     }
+}
+
+template <typename T, int ITEMS>
+__global__ void __launch_bounds__(kWarps * 32) k_rows_batch(const BatchSys *__restrict__ sys,
+                                                            const BatchItem *__restrict__ items, int nitems,
+                                                            int *__restrict__ counter, int mstride) {
+    rows_batch_body<T, ITEMS>(sys, items, nitems, counter, mstride);
+}
+
+// FP32: capped at 40 registers so that 6 CTAs of 256 threads stay resident
+// per SM; the system descriptors come from global memory, and the compiler's
+// own choice (64 registers, 4 CTAs) was measured slower than the spills the
+// cap costs
+template <int ITEMS>
+__global__ void __launch_bounds__(kWarps * 32, 6) k_rows_batch_f32(const BatchSys *__restrict__ sys,
+                                                                   const BatchItem *__restrict__ items, int nitems,
+                                                                   int *__restrict__ counter, int mstride) {
+    rows_batch_body<float, ITEMS>(sys, items, nitems, counter, mstride);
+}
+
+template <typename T, int ITEMS>
+constexpr auto batch_rows_kernel() {
+    if constexpr (std::is_same<T, float>::value)
+        return k_rows_batch_f32<ITEMS>;
+    else
+        return k_rows_batch<T, ITEMS>;
 }
 
 // ---- lock-step Lanczos kernels (iteration index `it` read from device)
@@ -369,11 +395,12 @@ int set_vectors(bsg_batch *b, const void *const *vin, void *const *vout) {
 template <typename T, int ITEMS>
 int launch_batch_t(bsg_batch *b, cudaStream_t s) {
     const size_t smem = align16(sizeof(float) * (size_t)kWarps * b->mstride) + sizeof(T) * (size_t)kWarps * 32 * ITEMS;
-    cudaError_t e = cudaFuncSetAttribute(k_rows_batch<T, ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    auto kern = batch_rows_kernel<T, ITEMS>();
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess) e = cudaMemsetAsync(b->counter.p, 0, sizeof(int), s);
     if (e == cudaSuccess) {
         const int grid = std::max(1, std::min(b->nitems, b->nsm * b->ctas_per_sm));
-        k_rows_batch<T, ITEMS><<<grid, kWarps * 32, smem, s>>>((const BatchSys *)b->sys.p, (const BatchItem *)b->work.p,
+        kern<<<grid, kWarps * 32, smem, s>>>((const BatchSys *)b->sys.p, (const BatchItem *)b->work.p,
                                                                 b->nitems, (int *)b->counter.p, b->mstride);
         e = cudaGetLastError();
     }
