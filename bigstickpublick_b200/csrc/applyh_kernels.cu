@@ -39,20 +39,28 @@ __global__ void __launch_bounds__(kWarps * 32) k_rows(const RowArgs a, const T *
     rows_body<T, NB, ITEMS, FULL>(a, vin, vout, ld, v0, mstride);
 }
 
-// single FP32 vectors: at most 40 registers, so that 6 CTAs of 256 threads
-// stay resident per SM to hide the gather latency (measured faster than the
-// compiler's own choice of 48 registers on the sliced walk)
+// single vectors: at most 40 registers, so that 6 CTAs of 256 threads stay
+// resident per SM to hide the gather latency (measured faster than the
+// compiler's own choice of 48 registers, the small spills included)
 template <int ITEMS, bool FULL>
 __global__ void __launch_bounds__(kWarps * 32, 6) k_rows_f1(const RowArgs a, const float *__restrict__ vin,
                                                             float *__restrict__ vout, const int ld, const int v0,
                                                             const int mstride) {
     rows_body<float, 1, ITEMS, FULL>(a, vin, vout, ld, v0, mstride);
 }
+template <int ITEMS, bool FULL>
+__global__ void __launch_bounds__(kWarps * 32, 6) k_rows_d1(const RowArgs a, const double *__restrict__ vin,
+                                                            double *__restrict__ vout, const int ld, const int v0,
+                                                            const int mstride) {
+    rows_body<double, 1, ITEMS, FULL>(a, vin, vout, ld, v0, mstride);
+}
 
 template <typename T, int NB, int ITEMS, bool FULL>
 constexpr auto rows_kernel() {
     if constexpr (std::is_same<T, float>::value && NB == 1)
         return k_rows_f1<ITEMS, FULL>;
+    else if constexpr (std::is_same<T, double>::value && NB == 1)
+        return k_rows_d1<ITEMS, FULL>;
     else
         return k_rows<T, NB, ITEMS, FULL>;
 }
@@ -99,7 +107,9 @@ static int launch_one(bsg_ctx *ctx, const T *vin, T *vout, int ld, int v0, int a
 template <typename T, int NB>
 static int launch_nb(bsg_ctx *ctx, const T *vin, T *vout, int ld, int v0, int accumulate, cudaStream_t s,
                      TileLookup lk) {
-    constexpr int cap = NB >= 8 ? 1 : (NB == 4 ? 2 : (NB == 2 ? 4 : 8));
+    // nb = 8 measured fastest at two positions per lane (pf 4p4n: 5.10 ms at
+    // one, 4.86 at two, 5.08 at four)
+    constexpr int cap = NB >= 16 ? 1 : (NB >= 4 ? 2 : (NB == 2 ? 4 : 8));
     int items = 1;
     while (items < cap && 32 * items < ctx->median_rowlen) items *= 2;
     if (items >= 8 && cap >= 8) return launch_one<T, NB, (cap >= 8 ? 8 : 1)>(ctx, vin, vout, ld, v0, accumulate, s, lk);

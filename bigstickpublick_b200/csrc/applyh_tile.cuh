@@ -64,13 +64,12 @@ template <> struct Vec<double, 16, true> : VecD2<16> {};
 
 constexpr int kWarps = kRowWarps;
 
-// Record k of an output position is read at column[kRecStride * k].  Blocks
-// of vectors and single FP32 vectors walk the sliced copy, where the lanes of
-// a warp read adjacent records (tiles start on multiples of 32, so
-// pos & 31 == lane); single FP64 vectors walk the position-sorted records,
-// which fits their register budget.  Both give the records of a position in
-// the same order.
-template <typename T, int NB> constexpr bool kSliced = NB >= 2 || sizeof(T) == 4;
+// Record k of an output position is read at column[kRecStride * k].  The row
+// kernels walk the sliced copy, where the lanes of a warp read adjacent
+// records (tiles start on multiples of 32, so pos & 31 == lane).  The
+// position-sorted walk (stride 1) gives the records of a position in the same
+// order and stays available for other traversals.
+template <typename T, int NB> constexpr bool kSliced = true;
 template <typename T, int NB> constexpr int kRecStride = kSliced<T, NB> ? 32 : 1;
 // the column base and the range of k for one output position; csr = the
 // operator's position-sorted records, [k0, k1) this position's range there

@@ -12,7 +12,8 @@
 //     (br_remove_prev_overlap / grab_alpha_blockv2); one classical
 //     Gram-Schmidt pass against every earlier history vector
 //     (br_orthogonalize(1) / compute_W); scalar: beta = |W|, V_{i+1} = W/beta
-//     (br_normalize); block: S = W^T W = U L U^T, beta = L^1/2 U^T,
+//     (br_normalize); block: S = W^T W = U L U^T (nb x nb, decomposed on
+//     the host like the reference's DSYEV), beta = L^1/2 U^T,
 //     V_{i+1} = W U L^-1/2 (spectral_decomp, src/bblock_algebra.f90:684-856);
 //   * beta collapse (beta < 1e-4 beta_prev) -> random restart against the
 //     history (random_restart_with_history, src/breorthog.f90:1471-1482);
@@ -20,8 +21,8 @@
 //     (src/blanczosmain.f90:1634-1660);
 //   * projected matrix: tridiagonal / band plus the arrow left by thick
 //     restart (src/blanczoslib.f90:195-221); its lowest eigenvalues for the
-//     convergence test come from Sturm bisection (scalar) or Jacobi (block)
-//     on the device;
+//     convergence test come from Sturm bisection on the device, after a
+//     Householder reduction of the band for the block recursion;
 //   * convergence_test option 0 (src/blanczoslib.f90:2660-2800): mean energy
 //     change over ncheck states, scaled by (1+restarts)/sqrt(ncheck+1),
 //     below converge_tol;
@@ -54,14 +55,17 @@ struct Lz {
     int nb, prec;
     int maxcol;      // history columns
     DevBuf hist, W, X, Y, tmp, partial, coef, sqp, sq, Adev, Vtmp, Zdev, wdev, stat, al, bt, ev, M, tau, ework;
+    DevBuf Ydev;     // Ritz coefficients of a thick restart (maxcol x 128)
     std::vector<double> T;  // host projected matrix (maxcol x maxcol), row-major
     float t_mv = 0, t_ort = 0, t_eig = 0;
-    cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr, e4 = nullptr;
     // pinned staging for the per-step scalars read on the host (alpha block,
     // residual sums of squares): device->host copies into it stay
     // asynchronous, so a step synchronizes with the device once
     double *hpin = nullptr;
-    static constexpr int kPinAlpha = 0, kPinSq = 256, kPinW = 512;  // then al, bt: maxcol each
+    // alpha block, residual norms, W^T W and the block coefficients (nb <= 16
+    // each), then the convergence test's eigenvalues, diagonal and arrow
+    static constexpr int kPinAlpha = 0, kPinSq = 256, kPinS = 272, kPinM = 528, kPinW = 784;
     double *pin_w() { return hpin + kPinW; }
     double *pin_al() { return hpin + kPinW + maxcol; }
     double *pin_bt() { return hpin + kPinW + 2 * (size_t)maxcol; }
@@ -212,6 +216,84 @@ int cgs(Lz &L, int k, std::vector<double> *sq, bool sq_on_device = false) {
     return BSG_OK;
 }
 
+// Eigen-decomposition of a small symmetric matrix (n <= 16, row-major A) by
+// cyclic Jacobi rotations (Golub & Van Loan, Matrix Computations, 8.5):
+// w ascending, Z row-major with column j the eigenvector of w[j].  The block
+// recursion needs it once per step for W^T W; on the host it costs
+// microseconds and no round trip to the device.
+void host_sym_eig(int n, std::vector<double> A, std::vector<double> &w, std::vector<double> &Z) {
+    std::vector<double> V((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i) V[(size_t)i * n + i] = 1.0;
+    for (int sweep = 0; sweep < 64; ++sweep) {
+        double off = 0.0, diag = 0.0;
+        for (int i = 0; i < n; ++i) {
+            diag += A[(size_t)i * n + i] * A[(size_t)i * n + i];
+            for (int j = i + 1; j < n; ++j) off += A[(size_t)i * n + j] * A[(size_t)i * n + j];
+        }
+        if (off <= 1e-32 * diag || off == 0.0) break;
+        for (int p = 0; p < n - 1; ++p)
+            for (int q = p + 1; q < n; ++q) {
+                const double apq = A[(size_t)p * n + q];
+                if (apq == 0.0) continue;
+                const double app = A[(size_t)p * n + p], aqq = A[(size_t)q * n + q];
+                const double theta = (aqq - app) / (2.0 * apq);
+                const double t = (theta >= 0.0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+                const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+                for (int k = 0; k < n; ++k) {  // columns p, q
+                    const double akp = A[(size_t)k * n + p], akq = A[(size_t)k * n + q];
+                    A[(size_t)k * n + p] = c * akp - sn * akq;
+                    A[(size_t)k * n + q] = sn * akp + c * akq;
+                }
+                for (int k = 0; k < n; ++k) {  // rows p, q
+                    const double apk = A[(size_t)p * n + k], aqk = A[(size_t)q * n + k];
+                    A[(size_t)p * n + k] = c * apk - sn * aqk;
+                    A[(size_t)q * n + k] = sn * apk + c * aqk;
+                }
+                A[(size_t)p * n + q] = A[(size_t)q * n + p] = 0.0;
+                for (int k = 0; k < n; ++k) {
+                    const double vkp = V[(size_t)k * n + p], vkq = V[(size_t)k * n + q];
+                    V[(size_t)k * n + p] = c * vkp - sn * vkq;
+                    V[(size_t)k * n + q] = sn * vkp + c * vkq;
+                }
+            }
+    }
+    std::vector<int> idx(n);
+    for (int i = 0; i < n; ++i) idx[i] = i;
+    std::sort(idx.begin(), idx.end(), [&](int x, int y) { return A[(size_t)x * n + x] < A[(size_t)y * n + y]; });
+    w.resize(n);
+    Z.assign((size_t)n * n, 0.0);
+    for (int j = 0; j < n; ++j) {
+        w[j] = A[(size_t)idx[j] * n + idx[j]];
+        for (int k = 0; k < n; ++k) Z[(size_t)k * n + j] = V[(size_t)k * n + idx[j]];
+    }
+}
+
+// Block step from S = W^T W on the host: S = U L U^T, beta = L^1/2 U^T,
+// V_{next} = W U L^-1/2 written to history column `dst`.  The coefficients go
+// through pinned memory; nothing waits for the device.
+int block_finish(Lz &L, int dst, const double *Shost, std::vector<double> &beta, double &lmin, double &lmax) {
+    const int nb = L.nb;
+    std::vector<double> A((size_t)nb * nb), w, Z;
+    for (int i = 0; i < nb; ++i)
+        for (int j = 0; j < nb; ++j) A[(size_t)i * nb + j] = 0.5 * (Shost[(size_t)i * nb + j] + Shost[(size_t)j * nb + i]);
+    host_sym_eig(nb, A, w, Z);
+    lmin = w[0];
+    lmax = w[nb - 1];
+    beta.assign((size_t)nb * nb, 0.0);
+    double *Mh = L.hpin + Lz::kPinM;
+    for (int a = 0; a < nb; ++a) {
+        const double l = std::max(w[a], 0.0);
+        const double sl = std::sqrt(l), il = (l > 0.0) ? 1.0 / sl : 0.0;
+        for (int c = 0; c < nb; ++c) {
+            beta[(size_t)a * nb + c] = sl * Z[(size_t)c * nb + a];  // (L^1/2 U^T)[a][c] = sqrt(l_a) U[c][a]
+            Mh[(size_t)c * nb + a] = Z[(size_t)c * nb + a] * il;     // (U L^-1/2)[c][a]
+        }
+    }
+    CK(cudaMemcpyAsync(L.M.p, Mh, sizeof(double) * nb * nb, cudaMemcpyHostToDevice, L.s));
+    CK(transform((const double *)L.W.p, nb, (const double *)L.M.p, nb, nb, L.col(dst), L.n, L.n, L.n, L.s));
+    return BSG_OK;
+}
+
 // V_{next} (nb columns at history column `dst`) from W: scalar normalization
 // or the block spectral decomposition; returns the beta block (nb x nb,
 // row-major beta[a][c]) and the smallest overlap eigenvalue
@@ -228,37 +310,12 @@ int next_block(Lz &L, int dst, const std::vector<double> &sq, std::vector<double
         CK(scale_cols((const double *)L.W.p, L.col(dst), (const double *)L.M.p, 1, L.n, L.n, L.s));
         return BSG_OK;
     }
-    // S = W^T W -> U L U^T
+    // S = W^T W, then the decomposition on the host
     CK(multidot((const double *)L.W.p, nb, (const double *)L.W.p, nb, L.n, L.n, (double *)L.partial.p,
                 (double *)L.coef.p, L.s));
-    std::vector<double> S((size_t)nb * nb);
-    CK(cudaMemcpyAsync(S.data(), L.coef.p, sizeof(double) * nb * nb, cudaMemcpyDeviceToHost, L.s));
+    CK(cudaMemcpyAsync(L.hpin + Lz::kPinS, L.coef.p, sizeof(double) * nb * nb, cudaMemcpyDeviceToHost, L.s));
     CK(cudaStreamSynchronize(L.s));
-    std::vector<double> A((size_t)nb * nb), w, Z;
-    for (int i = 0; i < nb; ++i)
-        for (int j = 0; j < nb; ++j) A[(size_t)i * nb + j] = 0.5 * (S[(size_t)i * nb + j] + S[(size_t)j * nb + i]);
-    CK(cudaMemcpyAsync(L.Adev.p, A.data(), sizeof(double) * nb * nb, cudaMemcpyHostToDevice, L.s));
-    CK(jacobi(nb, (double *)L.Adev.p, (double *)L.Vtmp.p, (double *)L.wdev.p, (double *)L.Zdev.p, (int *)L.stat.p, L.s));
-    w.resize(nb);
-    Z.resize((size_t)nb * nb);
-    CK(cudaMemcpyAsync(w.data(), L.wdev.p, sizeof(double) * nb, cudaMemcpyDeviceToHost, L.s));
-    CK(cudaMemcpyAsync(Z.data(), L.Zdev.p, sizeof(double) * nb * nb, cudaMemcpyDeviceToHost, L.s));
-    CK(cudaStreamSynchronize(L.s));
-    lmin = w[0];
-    lmax = w[nb - 1];
-    // beta = L^1/2 U^T ; M = U L^-1/2
-    std::vector<double> Mh((size_t)nb * nb);
-    for (int a = 0; a < nb; ++a) {
-        const double l = std::max(w[a], 0.0);
-        const double sl = std::sqrt(l), il = (l > 0.0) ? 1.0 / sl : 0.0;
-        for (int c = 0; c < nb; ++c) {
-            beta[(size_t)a * nb + c] = sl * Z[(size_t)c * nb + a];  // (L^1/2 U^T)[a][c] = sqrt(l_a) U[c][a]
-            Mh[(size_t)c * nb + a] = Z[(size_t)c * nb + a] * il;     // (U L^-1/2)[c][a]
-        }
-    }
-    CK(cudaMemcpyAsync(L.M.p, Mh.data(), sizeof(double) * nb * nb, cudaMemcpyHostToDevice, L.s));
-    CK(transform((const double *)L.W.p, nb, (const double *)L.M.p, nb, nb, L.col(dst), L.n, L.n, L.n, L.s));
-    return BSG_OK;
+    return block_finish(L, dst, L.hpin + Lz::kPinS, beta, lmin, lmax);
 }
 
 int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, double *evecs, bsg_report *rep) {
@@ -275,11 +332,9 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
 
     // ---- pivot block into history columns [0, nb)
     if (pivot) {
-        std::vector<double> hp((size_t)n * nb);
-        for (int64_t s_ = 0; s_ < n; ++s_)
-            for (int b = 0; b < nb; ++b) hp[(size_t)b * n + s_] = pivot[(size_t)s_ * nb + b];
-        CK(cudaMemcpyAsync(L.W.p, hp.data(), sizeof(double) * n * nb, cudaMemcpyHostToDevice, L.s));
-        CK(cudaStreamSynchronize(L.s));
+        // the interleaved pivot block as given, split into columns on the device
+        CK(cudaMemcpyAsync(L.tmp.p, pivot, sizeof(double) * n * nb, cudaMemcpyHostToDevice, L.s));
+        CK(unpack(L.tmp.p, nb, n, n, (double *)L.W.p, BSG_PREC_FP64, L.s));
     } else if (nb == 1) {
         std::vector<double> hp(n, 1.0 / std::sqrt((double)n));
         CK(cudaMemcpyAsync(L.W.p, hp.data(), sizeof(double) * n, cudaMemcpyHostToDevice, L.s));
@@ -300,6 +355,7 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
     double beta_prev = -1.0;
     bool finished = false, converged = false;
     std::vector<double> eold, e;
+    bool post_pending = false;  // e3 -> e4 of the last step not yet accounted
     int iter = 0;         // block iterations in this cycle (the reference's iter)
     struct {
         bool active = false;
@@ -324,7 +380,14 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
         CK(sub_gemv(L.col(cur), nb, (const double *)L.coef.p, (double *)L.W.p, nb, n, n, nullptr, nullptr, L.s));
         ST(cgs(L, cur, nullptr, true));
         CK(cudaMemcpyAsync(L.hpin + Lz::kPinSq, L.sq.p, sizeof(double) * nb, cudaMemcpyDeviceToHost, L.s));
-        if (nb == 1) CK(normalize_col((const double *)L.W.p, L.col(cur + 1), (const double *)L.sq.p, n, L.s));
+        if (nb == 1) {
+            CK(normalize_col((const double *)L.W.p, L.col(cur + 1), (const double *)L.sq.p, n, L.s));
+        } else {
+            // W^T W for the block step, read back with alpha and the norms
+            CK(multidot((const double *)L.W.p, nb, (const double *)L.W.p, nb, n, n, (double *)L.partial.p,
+                        (double *)L.coef.p, L.s));
+            CK(cudaMemcpyAsync(L.hpin + Lz::kPinS, L.coef.p, sizeof(double) * nb * nb, cudaMemcpyDeviceToHost, L.s));
+        }
         CK(cudaEventRecord(L.e2, L.s));
         CK(cudaEventSynchronize(L.e2));
         {
@@ -333,10 +396,15 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
             L.t_mv += ms;
             cudaEventElapsedTime(&ms, L.e1, L.e2);
             L.t_ort += ms;
+            if (post_pending) {  // the previous step's work after its synchronization
+                cudaEventElapsedTime(&ms, L.e3, L.e4);
+                L.t_ort += ms;
+                post_pending = false;
+            }
         }
         std::vector<double> alpha(L.hpin + Lz::kPinAlpha, L.hpin + Lz::kPinAlpha + (size_t)nb * nb);
         sq.assign(L.hpin + Lz::kPinSq, L.hpin + Lz::kPinSq + nb);
-        cudaEventRecord(L.e0, L.s);
+        cudaEventRecord(L.e3, L.s);
         // ---- scalar beta checks (src/blanczosmain.f90:1634-1660)
         if (nb == 1) {
             const double b = std::sqrt(std::max(sq[0], 0.0));
@@ -356,7 +424,7 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
             }
         } else {
             // block: guard against a rank-deficient residual block
-            ST(next_block(L, cur + nb, sq, beta, lmin, lmax));
+            ST(block_finish(L, cur + nb, L.hpin + Lz::kPinS, beta, lmin, lmax));
             if (lmin <= 1e-20 * std::max(lmax, 1.0)) {
                 CK(random_cols((double *)L.tmp.p, nb, n, n, p->seed + 104729ull * (uint64_t)(rnd + 1), L.s));
                 const double eps = 1e-7 * std::sqrt(std::max(lmax, 1e-30));
@@ -374,9 +442,10 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
                 ++rnd;
             }
         }
-        cudaEventRecord(L.e1, L.s);
-        CK(cudaStreamSynchronize(L.s));
-        L.t_ort += elapsed(L);
+        // no wait here: the host goes on with the projected matrix while the
+        // device finishes the step; its time is read at the next sync
+        CK(cudaEventRecord(L.e4, L.s));
+        post_pending = true;
         // ---- projected matrix
         for (int a = 0; a < nb; ++a)
             for (int c = 0; c < nb; ++c) {
@@ -457,16 +526,12 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
             std::vector<double> Yk((size_t)m * k);
             for (int j = 0; j < m; ++j)
                 for (int l = 0; l < k; ++l) Yk[(size_t)j * k + l] = Z[(size_t)l * m + j];
-            DevBuf Yd;
-            ST(upload(ctx, Yd, Yk.data(), sizeof(double) * Yk.size()));
-            cudaError_t te = transform(L.col(0), m, (const double *)Yd.p, k, k, (double *)L.tmp.p, n, n, n, L.s);
-            if (te == cudaSuccess)
-                te = cudaMemcpyAsync(L.col(0), L.tmp.p, sizeof(double) * n * k, cudaMemcpyDeviceToDevice, L.s);
-            if (te == cudaSuccess)
-                te = cudaMemcpyAsync(L.col(k), L.col(m), sizeof(double) * n * nb, cudaMemcpyDeviceToDevice, L.s);
-            cudaStreamSynchronize(L.s);
-            dev_free(Yd);
-            CK(te);
+            // Y (m x k <= maxcol x 128) through the solve's own buffer: no
+            // allocation per restart
+            CK(cudaMemcpyAsync(L.Ydev.p, Yk.data(), sizeof(double) * Yk.size(), cudaMemcpyHostToDevice, L.s));
+            CK(transform(L.col(0), m, (const double *)L.Ydev.p, k, k, (double *)L.tmp.p, n, n, n, L.s));
+            CK(cudaMemcpyAsync(L.col(0), L.tmp.p, sizeof(double) * n * k, cudaMemcpyDeviceToDevice, L.s));
+            CK(cudaMemcpyAsync(L.col(k), L.col(m), sizeof(double) * n * nb, cudaMemcpyDeviceToDevice, L.s));
             cudaEventRecord(L.e1, L.s);
             L.t_ort += elapsed(L);
             std::fill(L.T.begin(), L.T.end(), 0.0);
@@ -487,6 +552,12 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
         }
     }
 
+    if (post_pending) {
+        CK(cudaEventSynchronize(L.e4));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, L.e3, L.e4);
+        L.t_ort += ms;
+    }
     // ---- final Ritz pairs of T[0:mT] (lanczos_output, src/blanczoslib.f90:1268)
     std::vector<double> w, Z;          // Z column-major mT x nk
     const int nk = std::min(nkeep, mT);
@@ -575,7 +646,8 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
     }
     L.maxcol = maxcol;
     if (!st && ((st = dev_alloc(ctx, L.al2, sizeof(double) * N)) || (st = dev_alloc(ctx, L.bt2, sizeof(double) * N)) ||
-                (st = dev_alloc(ctx, L.w2, sizeof(double) * N)))) {
+                (st = dev_alloc(ctx, L.w2, sizeof(double) * N)) ||
+                (st = dev_alloc(ctx, L.Ydev, sizeof(double) * (size_t)N * 128)))) {
         // fall through to cleanup
     }
     if (!st && L.nb > 1 &&
@@ -594,6 +666,8 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
         cudaEventCreate(&L.e0);
         cudaEventCreate(&L.e1);
         cudaEventCreate(&L.e2);
+        cudaEventCreate(&L.e3);
+        cudaEventCreate(&L.e4);
         cudaEventCreateWithFlags(&L.econv, cudaEventDisableTiming);
         cudaEvent_t t0, t1;
         cudaEventCreate(&t0);
@@ -610,6 +684,8 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
         cudaEventDestroy(L.e0);
         cudaEventDestroy(L.e1);
         cudaEventDestroy(L.e2);
+        cudaEventDestroy(L.e3);
+        cudaEventDestroy(L.e4);
     }
     if (L.s2) {
         cudaStreamSynchronize(L.s2);
@@ -618,7 +694,7 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
     if (L.econv) cudaEventDestroy(L.econv);
     DevBuf *bufs[] = {&L.hist, &L.W, &L.X, &L.Y, &L.tmp, &L.partial, &L.coef, &L.sqp, &L.sq, &L.Adev,
                       &L.Vtmp, &L.Zdev, &L.wdev, &L.stat, &L.al, &L.bt, &L.ev, &L.M, &L.tau, &L.ework,
-                      &L.al2, &L.bt2, &L.w2, &L.Adev2, &L.Vtmp2, &L.tau2, &L.ework2};
+                      &L.al2, &L.bt2, &L.w2, &L.Adev2, &L.Vtmp2, &L.tau2, &L.ework2, &L.Ydev};
     cudaStreamSynchronize(L.s);
     for (DevBuf *b : bufs) dev_free(*b);
     if (L.hpin) cudaFreeHost(L.hpin);

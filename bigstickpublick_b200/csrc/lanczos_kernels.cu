@@ -6,8 +6,6 @@
 //   k_sub_gemv      W -= H C (the subtract phase of br_orthogonalize and the
 //                   alpha projection of br_remove_prev_overlap)
 //   k_transform     out = V Y (br_transform_basis, src/breorthog.f90:1211-1243)
-//   k_jacobi        dense symmetric eigenproblem of the projected matrix in one
-//                   CTA (replaces the vendored DSYEV, src/blanczoslib.f90:226-258)
 //   k_bisect_arrow  lowest eigenvalues of the arrowhead-tridiagonal projected
 //                   matrix of scalar Lanczos by Sturm counting (replaces the
 //                   DSYEV 'N' / DSTEGR calls made for the convergence test)
@@ -37,7 +35,7 @@ constexpr int kDotTile = 512;      // rows per tile
 // vector, and a warp reduction adds them into the CTA's shared accumulator
 // (each (a,b) owned by one warp, added in chunk order).  The CTA writes
 // partial[p * gridDim.x + x] for its vectors.
-template <int NB>
+template <int NB, int PAIR>
 __global__ void __launch_bounds__(kDotThreads) k_multidot(const double *__restrict__ A, int nA,
                                                          const double *__restrict__ B, int64_t n, int64_t ld,
                                                          double *__restrict__ partial) {
@@ -47,7 +45,6 @@ __global__ void __launch_bounds__(kDotThreads) k_multidot(const double *__restri
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = kDotThreads / 32;
     const int per = (nA + gridDim.y - 1) / gridDim.y;
     const int a_lo = blockIdx.y * per, a_hi = min(nA, a_lo + per);
-    constexpr int PAIR = NB >= 4 ? 2 : 1;
     for (int e = threadIdx.x; e < nA * NB; e += kDotThreads) sAcc[e] = 0.0;
     for (int64_t t0 = (int64_t)blockIdx.x * kDotTile; t0 < n; t0 += (int64_t)gridDim.x * kDotTile) {
         const int rows = (int)((n - t0) < kDotTile ? (n - t0) : kDotTile);
@@ -242,137 +239,6 @@ __global__ void k_unpack(const T *__restrict__ y, int nB, int64_t n, int64_t ld,
         const int64_t s = e / nB;
         const int b = (int)(e - s * nB);
         W[(int64_t)b * ld + s] = (double)y[e];
-    }
-}
-
-// ------------------------------------------------------------- Jacobi -----
-// Cyclic two-sided Jacobi with a round-robin (tournament) ordering: every
-// round rotates n/2 disjoint (p,q) pairs in parallel.  A (n x n, row-major,
-// symmetric) is overwritten; on exit w holds the eigenvalues in ascending
-// order and Z (n x n, column j = eigenvector j) the eigenvectors.
-// Bounded: at most max_sweeps sweeps; *status = 1 if not converged.
-__global__ void __launch_bounds__(1024) k_jacobi(int n, double *__restrict__ A, double *__restrict__ Vtmp,
-                                                 double *__restrict__ w, double *__restrict__ Z, int max_sweeps,
-                                                 int *__restrict__ status) {
-    extern __shared__ double sh[];
-    const int m = n + (n & 1);                 // even size, index n is a dummy
-    double *cs = sh;                           // [m/2] c
-    double *sn = sh + m / 2;                   // [m/2] s
-    int *pp = reinterpret_cast<int *>(sh + m); // [m/2] p, [m/2] q, [m] order
-    int *qq = pp + m / 2;
-    int *ord = qq + m / 2;
-    __shared__ double red[32];
-    __shared__ int done;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    for (int e = tid; e < n * n; e += nt) Vtmp[e] = ((e / n) == (e % n)) ? 1.0 : 0.0;
-    for (int e = tid; e < m; e += nt) ord[e] = e;
-    __syncthreads();
-    // scale of the matrix (Frobenius norm squared)
-    double fro = 0.0;
-    for (int e = tid; e < n * n; e += nt) fro += A[e] * A[e];
-    for (int o = 16; o > 0; o >>= 1) fro += __shfl_down_sync(0xffffffffu, fro, o);
-    if ((tid & 31) == 0) red[tid >> 5] = fro;
-    __syncthreads();
-    if (tid == 0) {
-        double s = 0.0;
-        for (int k = 0; k < (nt + 31) / 32; ++k) s += red[k];
-        red[0] = s;
-    }
-    __syncthreads();
-    const double tol2 = red[0] * 1e-30;
-    __syncthreads();
-    int sweep = 0;
-    for (; sweep < max_sweeps; ++sweep) {
-        double off = 0.0;
-        for (int e = tid; e < n * n; e += nt) {
-            const int i = e / n, j = e % n;
-            if (i != j) off += A[e] * A[e];
-        }
-        for (int o = 16; o > 0; o >>= 1) off += __shfl_down_sync(0xffffffffu, off, o);
-        __syncthreads();
-        if ((tid & 31) == 0) red[tid >> 5] = off;
-        __syncthreads();
-        if (tid == 0) {
-            double s = 0.0;
-            for (int k = 0; k < (nt + 31) / 32; ++k) s += red[k];
-            done = (s <= tol2) ? 1 : 0;
-        }
-        __syncthreads();
-        if (done) break;
-        for (int round = 0; round < m - 1; ++round) {
-            // pairs from the current ordering: (ord[k], ord[m-1-k])
-            for (int k = tid; k < m / 2; k += nt) {
-                int p = ord[k], q = ord[m - 1 - k];
-                if (p > q) { const int t = p; p = q; q = t; }
-                double c = 1.0, s = 0.0;
-                if (q < n) {
-                    const double apq = A[p * n + q];
-                    if (apq != 0.0) {
-                        const double theta = (A[q * n + q] - A[p * n + p]) / (2.0 * apq);
-                        const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-                        c = 1.0 / sqrt(t * t + 1.0);
-                        s = t * c;
-                    }
-                }
-                pp[k] = p;
-                qq[k] = q;
-                cs[k] = c;
-                sn[k] = s;
-            }
-            __syncthreads();
-            // columns: A <- A J, Z <- Z J
-            for (int e = tid; e < (m / 2) * n; e += nt) {
-                const int k = e / n, i = e % n;
-                const int p = pp[k], q = qq[k];
-                if (q >= n || sn[k] == 0.0) continue;
-                const double c = cs[k], s = sn[k];
-                const double aip = A[i * n + p], aiq = A[i * n + q];
-                A[i * n + p] = c * aip - s * aiq;
-                A[i * n + q] = s * aip + c * aiq;
-                const double vip = Vtmp[i * n + p], viq = Vtmp[i * n + q];
-                Vtmp[i * n + p] = c * vip - s * viq;
-                Vtmp[i * n + q] = s * vip + c * viq;
-            }
-            __syncthreads();
-            // rows: A <- J^T A
-            for (int e = tid; e < (m / 2) * n; e += nt) {
-                const int k = e / n, j = e % n;
-                const int p = pp[k], q = qq[k];
-                if (q >= n || sn[k] == 0.0) continue;
-                const double c = cs[k], s = sn[k];
-                const double apj = A[p * n + j], aqj = A[q * n + j];
-                A[p * n + j] = c * apj - s * aqj;
-                A[q * n + j] = s * apj + c * aqj;
-            }
-            __syncthreads();
-            for (int k = tid; k < m / 2; k += nt) {
-                const int p = pp[k], q = qq[k];
-                if (q < n && sn[k] != 0.0) {
-                    A[p * n + q] = 0.0;
-                    A[q * n + p] = 0.0;
-                }
-            }
-            // next ordering: ord[0] fixed, the rest rotates by one
-            __syncthreads();
-            if (tid == 0) {
-                const int last = ord[m - 1];
-                for (int k = m - 1; k > 1; --k) ord[k] = ord[k - 1];
-                ord[1] = last;
-            }
-            __syncthreads();
-        }
-    }
-    if (tid == 0 && status) *status = (sweep >= max_sweeps) ? 1 : 0;
-    // ascending order by rank (ties broken by index)
-    for (int i = tid; i < n; i += nt) {
-        const double di = A[i * n + i];
-        int r = 0;
-        for (int j = 0; j < n; ++j) {
-            const double dj = A[j * n + j];
-            r += (dj < di || (dj == di && j < i)) ? 1 : 0;
-        }
-        w[r] = di;
-        for (int row = 0; row < n; ++row) Z[(int64_t)row * n + r] = Vtmp[row * n + i];
     }
 }
 
@@ -729,8 +595,15 @@ static cudaError_t multidot_nb(const double *A, int nA, const double *B, int64_t
         // vectors over more CTAs, at least 8 vectors each
         const int gy = std::max(1, std::min((592 + G - 1) / G, na / 8));
         const size_t smem = sizeof(double) * ((size_t)kDotTile * NB + (size_t)na * NB);
-        cudaFuncSetAttribute(k_multidot<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_multidot<NB><<<dim3(G, gy), kDotThreads, smem, s>>>(A + (int64_t)a0 * ld, na, B, n, ld, partial);
+        // two A vectors per warp pass halve the shared loads per multiply-add
+        // for NB >= 4, once there are enough vectors to keep all 8 warps busy
+        if (NB >= 4 && na >= 16) {
+            cudaFuncSetAttribute(k_multidot<NB, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            k_multidot<NB, 2><<<dim3(G, gy), kDotThreads, smem, s>>>(A + (int64_t)a0 * ld, na, B, n, ld, partial);
+        } else {
+            cudaFuncSetAttribute(k_multidot<NB, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            k_multidot<NB, 1><<<dim3(G, gy), kDotThreads, smem, s>>>(A + (int64_t)a0 * ld, na, B, n, ld, partial);
+        }
         k_reduce_partials<<<(na * NB * 32 + 255) / 256, 256, 0, s>>>(partial, na * NB, G, out + (int64_t)a0 * NB);
         a0 += na;
     }
@@ -830,14 +703,6 @@ cudaError_t unpack(const void *y, int nB, int64_t n, int64_t ld, double *W, int 
         k_unpack<float><<<1184, 256, 0, s>>>((const float *)y, nB, n, ld, W);
     else
         k_unpack<double><<<1184, 256, 0, s>>>((const double *)y, nB, n, ld, W);
-    return cudaGetLastError();
-}
-
-cudaError_t jacobi(int n, double *A, double *Vtmp, double *w, double *Z, int *status, cudaStream_t s) {
-    const int m = n + (n & 1);
-    const size_t smem = sizeof(double) * m + sizeof(int) * 2 * m;
-    cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(smem + 1024));
-    k_jacobi<<<1, 1024, smem, s>>>(n, A, Vtmp, w, Z, 60, status);
     return cudaGetLastError();
 }
 

@@ -20,9 +20,6 @@ cudaError_t scale_cols(const double *x, double *y, const double *sc, int nB, int
 cudaError_t normalize_col(const double *x, double *y, const double *sq, int64_t n, cudaStream_t s);
 cudaError_t pack(const double *V, int nB, int64_t n, int64_t ld, void *x, int prec, cudaStream_t s);
 cudaError_t unpack(const void *y, int nB, int64_t n, int64_t ld, double *W, int prec, cudaStream_t s);
-// dense symmetric eigenproblem (n x n row-major A, destroyed); Z row-major,
-// column j = eigenvector of w[j] (ascending)
-cudaError_t jacobi(int n, double *A, double *Vtmp, double *w, double *Z, int *status, cudaStream_t s);
 // lowest nwant eigenvalues of the arrowhead-tridiagonal matrix
 cudaError_t bisect_arrow(int n, int k, const double *al, const double *bt, int nwant, double glo, double ghi,
                          double *ev, cudaStream_t s);
