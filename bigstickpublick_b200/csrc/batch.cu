@@ -111,6 +111,20 @@ constexpr auto batch_rows_kernel() {
         return k_rows_batch<T, ITEMS>;
 }
 
+// Y[j*nk + l] = Z[l*m + j]: Ritz coefficients from the inverse iteration's
+// column-major layout to the layout of the basis transform
+__global__ void k_transpose_small(const double *__restrict__ Z, int m, int nk, double *__restrict__ Y) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m * nk; e += gridDim.x * blockDim.x) {
+        const int j = e / nk, l = e - j * nk;
+        Y[e] = Z[(size_t)l * m + j];
+    }
+}
+cudaError_t transpose_small(const double *Z, int m, int nk, double *Y, cudaStream_t s) {
+    const int total = m * nk;
+    k_transpose_small<<<(total + 255) / 256, 256, 0, s>>>(Z, m, nk, Y);
+    return cudaGetLastError();
+}
+
 // ---- lock-step Lanczos kernels (iteration index `it` read from device)
 template <typename T>
 __global__ void k_bpack(const BLz *__restrict__ L, const BChunk *__restrict__ ch, int nch, const int *__restrict__ itp,
@@ -712,27 +726,29 @@ int bsg_batch_lanczos(bsg_batch *b, const bsg_lanczos_params *p, double *evals, 
         if (cudaEventSynchronize(e1) != cudaSuccess) st = berr(b, BSG_ERR_CUDA, "batched Lanczos failed");
         cudaEventElapsedTime(&loop_ms, e0, e1);
     }
-    // ---- projected tridiagonal matrices: eigenpairs on the device
+    // ---- projected tridiagonal matrices: eigenpairs on the device.  Every
+    // system's solve is queued on one stream without host round trips (alpha
+    // and beta are read where the loop left them, eigenvalues and Ritz vectors
+    // collect in device arrays); one synchronization, then the copies out.
     float eig_ms = 0.f;
     if (!st) {
         std::vector<double> abh((size_t)2 * n * niter);
-        cudaMemcpy(abh.data(), ab.p, 8 * abh.size(), cudaMemcpyDeviceToHost);
-        if (const char *dump = std::getenv("BSG_BATCH_DUMP_AB")) {
-            if (FILE *f = std::fopen(dump, "wb")) {
-                std::fwrite(abh.data(), 8, abh.size(), f);
-                std::fclose(f);
-            }
-        }
-        DevBuf al, bt, ev, Z, wk, Yd, outv;
+        if (cudaMemcpy(abh.data(), ab.p, 8 * abh.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+            st = berr(b, BSG_ERR_CUDA, "batched Lanczos: reading alpha/beta failed");
         const int nk = std::min(p->nkeep, niter);
-        if ((st = dev_alloc(c0, al, 8 * (size_t)niter)) || (st = dev_alloc(c0, bt, 8 * (size_t)niter)) ||
-            (st = dev_alloc(c0, ev, 8 * (size_t)nk)) || (st = dev_alloc(c0, Z, 8 * (size_t)niter * nk)) ||
-            (st = dev_alloc(c0, wk, 8 * (size_t)6 * niter * nk)) || (st = dev_alloc(c0, Yd, 8 * (size_t)niter * nk))) {
+        const bool vecs = evecs != nullptr;
+        int64_t tot_dim = 0;
+        for (int s = 0; s < n; ++s) tot_dim += b->dims[s];
+        DevBuf evd, Z, wk, Yd, outv;
+        if (!st && ((st = dev_alloc(c0, evd, 8 * (size_t)n * nk)) || (st = dev_alloc(c0, Z, 8 * (size_t)niter * nk)) ||
+                    (st = dev_alloc(c0, wk, 8 * (size_t)6 * niter * nk)) || (st = dev_alloc(c0, Yd, 8 * (size_t)niter * nk)) ||
+                    (vecs && (st = dev_alloc(c0, outv, 8 * (size_t)tot_dim * nk))))) {
             st = berr(b, st, "eigen workspace allocation failed");
         }
         cudaEventRecord(e0, s0);
-        std::vector<double> w(nk), Zh((size_t)niter * nk), Yk((size_t)niter * nk);
-        for (int s = 0; s < n && !st; ++s) {
+        cudaError_t e = cudaSuccess;
+        int64_t off = 0;
+        for (int s = 0; s < n && !st && e == cudaSuccess; ++s) {
             const double *A = abh.data() + (size_t)s * niter, *B = abh.data() + (size_t)n * niter + (size_t)s * niter;
             double glo = 1e300, ghi = -1e300;
             for (int i = 0; i < niter; ++i) {
@@ -743,42 +759,37 @@ int bsg_batch_lanczos(bsg_batch *b, const bsg_lanczos_params *p, double *evals, 
             const double scale = std::max(std::fabs(glo), std::fabs(ghi));
             glo -= 1e-12 * scale + 1e-300;
             ghi += 1e-12 * scale + 1e-300;
-            cudaError_t e = cudaMemcpyAsync(al.p, A, 8 * niter, cudaMemcpyHostToDevice, s0);
-            if (e == cudaSuccess) e = cudaMemcpyAsync(bt.p, B, 8 * niter, cudaMemcpyHostToDevice, s0);
-            if (e == cudaSuccess) e = bisect_arrow(niter, 0, (const double *)al.p, (const double *)bt.p, nk, glo, ghi, (double *)ev.p, s0);
-            if (e == cudaSuccess) e = cudaMemcpyAsync(w.data(), ev.p, 8 * nk, cudaMemcpyDeviceToHost, s0);
-            if (e == cudaSuccess && evecs && evecs[s]) {
-                e = inverse_iter_arrow(niter, 0, (const double *)al.p, (const double *)bt.p, (const double *)ev.p, nk,
-                                       scale, (double *)Z.p, (double *)wk.p, s0);
-                // Z column-major niter x nk -> transform layout Y[j*nk + l]
-                if (e == cudaSuccess) e = cudaMemcpyAsync(Zh.data(), Z.p, 8 * Zh.size(), cudaMemcpyDeviceToHost, s0);
-                if (e == cudaSuccess) e = cudaStreamSynchronize(s0);
-                for (int j = 0; j < niter && e == cudaSuccess; ++j)
-                    for (int l = 0; l < nk; ++l) Yk[(size_t)j * nk + l] = Zh[(size_t)l * niter + j];
-                if (e == cudaSuccess) e = cudaMemcpyAsync(Yd.p, Yk.data(), 8 * Yk.size(), cudaMemcpyHostToDevice, s0);
-                if (e == cudaSuccess) {
-                    int st2 = dev_alloc(c0, outv, 8 * (size_t)b->dims[s] * nk);
-                    if (st2) e = cudaErrorMemoryAllocation;
-                }
+            const double *ald = (const double *)ab.p + (size_t)s * niter;
+            const double *btd = (const double *)ab.p + (size_t)n * niter + (size_t)s * niter;
+            double *evs = (double *)evd.p + (size_t)s * nk;
+            e = bisect_arrow(niter, 0, ald, btd, nk, glo, ghi, evs, s0);
+            if (e == cudaSuccess && vecs && evecs[s]) {
+                e = inverse_iter_arrow(niter, 0, ald, btd, evs, nk, scale, (double *)Z.p, (double *)wk.p, s0);
+                if (e == cudaSuccess) e = transpose_small((const double *)Z.p, niter, nk, (double *)Yd.p, s0);
                 if (e == cudaSuccess)
-                    e = transform(lz[s].hist, niter, (const double *)Yd.p, nk, nk, (double *)outv.p, b->dims[s], b->dims[s],
-                                  b->dims[s], s0);
-                if (e == cudaSuccess)
-                    e = cudaMemcpyAsync(evecs[s], outv.p, 8 * (size_t)b->dims[s] * nk, cudaMemcpyDeviceToHost, s0);
-                if (e == cudaSuccess) e = cudaStreamSynchronize(s0);
-                dev_free(outv);
+                    e = transform(lz[s].hist, niter, (const double *)Yd.p, nk, nk, (double *)outv.p + off * nk,
+                                  b->dims[s], b->dims[s], b->dims[s], s0);
             }
-            if (e == cudaSuccess) e = cudaStreamSynchronize(s0);
-            if (e != cudaSuccess) {
-                st = berr(b, BSG_ERR_CUDA, std::string("batched eigen-solve: ") + cudaGetErrorString(e));
-                break;
-            }
-            for (int k = 0; k < p->nkeep; ++k) evals[(size_t)s * p->nkeep + k] = k < nk ? w[k] : NAN;
+            off += b->dims[s];
         }
+        std::vector<double> w((size_t)n * nk);
+        if (!st && e == cudaSuccess) e = cudaMemcpyAsync(w.data(), evd.p, 8 * w.size(), cudaMemcpyDeviceToHost, s0);
+        if (!st && e == cudaSuccess) e = cudaStreamSynchronize(s0);
+        off = 0;
+        for (int s = 0; s < n && !st && e == cudaSuccess; ++s) {
+            if (vecs && evecs[s])
+                e = cudaMemcpy(evecs[s], (const double *)outv.p + off * nk, 8 * (size_t)b->dims[s] * nk,
+                               cudaMemcpyDeviceToHost);
+            off += b->dims[s];
+        }
+        if (!st && e != cudaSuccess) st = berr(b, BSG_ERR_CUDA, std::string("batched eigen-solve: ") + cudaGetErrorString(e));
+        if (!st)
+            for (int s = 0; s < n; ++s)
+                for (int k = 0; k < p->nkeep; ++k) evals[(size_t)s * p->nkeep + k] = k < nk ? w[(size_t)s * nk + k] : NAN;
         cudaEventRecord(e1, s0);
         cudaEventSynchronize(e1);
         cudaEventElapsedTime(&eig_ms, e0, e1);
-        DevBuf *bs2[] = {&al, &bt, &ev, &Z, &wk, &Yd};
+        DevBuf *bs2[] = {&evd, &Z, &wk, &Yd, &outv};
         for (DevBuf *x : bs2) dev_free(*x);
     }
     if (rep) {
