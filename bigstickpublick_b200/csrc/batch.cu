@@ -22,6 +22,8 @@
 // communication of any kind.
 
 #include <algorithm>
+#include <thread>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -451,13 +453,34 @@ int bsg_batch_create(int n, const bsg_tables *const *tables, const bsg_config *c
     b->n = n;
     b->device = cfg ? cfg->device : 0;
     int st = BSG_OK;
-    for (int s = 0; s < n && !st; ++s) {
-        bsg_ctx *c = nullptr;
-        st = bsg_create(tables[s], cfg, &c);
-        if (st) {
+    // the systems' set-ups (validation, derived layouts, uploads) are
+    // independent: host threads take them in turn
+    std::vector<bsg_ctx *> made(n, nullptr);
+    std::vector<int> stv(n, BSG_OK);
+    {
+        std::atomic<int> next{0};
+        auto worker = [&]() {
+            for (int s = next++; s < n; s = next++) stv[s] = bsg_create(tables[s], cfg, &made[s]);
+        };
+        const int nth = (int)std::max(1u, std::min<unsigned>(16u, std::min<unsigned>((unsigned)n, std::thread::hardware_concurrency())));
+        std::vector<std::thread> pool;
+        for (int t = 1; t < nth; ++t) pool.emplace_back(worker);
+        worker();
+        for (auto &th : pool) th.join();
+    }
+    for (int s = 0; s < n; ++s)
+        if (stv[s] != BSG_OK && !st) {
+            st = stv[s];
             b->last_error = "system " + std::to_string(s) + ": bsg_create failed";
-            break;
         }
+    if (st) {
+        for (bsg_ctx *c : made)
+            if (c) bsg_destroy(c);
+        delete b;
+        return st;
+    }
+    for (int s = 0; s < n; ++s) {
+        bsg_ctx *c = made[s];
         b->ctx.push_back(c);
         b->dims.push_back(c->dim);
         b->off.push_back(b->total);
