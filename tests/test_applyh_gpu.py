@@ -29,7 +29,7 @@ def built():
 
 @pytest.mark.parametrize("name", [c[0] for c in CASES])
 @pytest.mark.parametrize("prec", [8, 4])
-@pytest.mark.parametrize("nb", [1, 2, 3, 8])
+@pytest.mark.parametrize("nb", [1, 2, 3, 4, 8, 16])
 def test_applyh_matches_oracle(built, name, prec, nb):
     T, H = built[name]
     rng = np.random.default_rng(1234 + nb)
