@@ -63,6 +63,9 @@ struct Lz {
     // residual sums of squares): device->host copies into it stay
     // asynchronous, so a step synchronizes with the device once
     double *hpin = nullptr;
+    // X already holds the next step's block, written by the kernel that made
+    // it (the normalization or the block transform), so the step needs no pack
+    bool x_ready = false;
     // alpha block, residual norms, W^T W and the block coefficients (nb <= 16
     // each), then the convergence test's eigenvalues, diagonal and arrow
     static constexpr int kPinAlpha = 0, kPinSq = 256, kPinS = 272, kPinM = 528, kPinW = 784;
@@ -290,7 +293,9 @@ int block_finish(Lz &L, int dst, const double *Shost, std::vector<double> &beta,
         }
     }
     CK(cudaMemcpyAsync(L.M.p, Mh, sizeof(double) * nb * nb, cudaMemcpyHostToDevice, L.s));
-    CK(transform((const double *)L.W.p, nb, (const double *)L.M.p, nb, nb, L.col(dst), L.n, L.n, L.n, L.s));
+    CK(transform((const double *)L.W.p, nb, (const double *)L.M.p, nb, nb, L.col(dst), L.n, L.n, L.n, L.s, L.X.p,
+                 L.prec));
+    L.x_ready = true;
     return BSG_OK;
 }
 
@@ -365,7 +370,8 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
         ++iter;
         ++total;
         // ---- W = H V
-        CK(pack(L.col(cur), nb, n, n, L.X.p, L.prec, L.s));
+        if (!L.x_ready) CK(pack(L.col(cur), nb, n, n, L.X.p, L.prec, L.s));
+        L.x_ready = false;
         CK(cudaEventRecord(L.e0, L.s));
         ST(launch_applyh(ctx, L.X.p, L.Y.p, nb, L.prec, 0, L.s));
         CK(cudaEventRecord(L.e1, L.s));
@@ -381,7 +387,7 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
         ST(cgs(L, cur, nullptr, true));
         CK(cudaMemcpyAsync(L.hpin + Lz::kPinSq, L.sq.p, sizeof(double) * nb, cudaMemcpyDeviceToHost, L.s));
         if (nb == 1) {
-            CK(normalize_col((const double *)L.W.p, L.col(cur + 1), (const double *)L.sq.p, n, L.s));
+            CK(normalize_col((const double *)L.W.p, L.col(cur + 1), (const double *)L.sq.p, n, L.s, L.X.p, L.prec));
         } else {
             // W^T W for the block step, read back with alpha and the norms
             CK(multidot((const double *)L.W.p, nb, (const double *)L.W.p, nb, n, n, (double *)L.partial.p,
@@ -409,6 +415,7 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
         if (nb == 1) {
             const double b = std::sqrt(std::max(sq[0], 0.0));
             beta.assign(1, b);
+            L.x_ready = sq[0] > 0.0;  // the normalization wrote nothing otherwise
             if (iter > 1 && beta_prev > 0.0 && b < 1e-4 * beta_prev) {
                 // random restart: keep the tiny beta, continue from a random
                 // direction orthogonal to the whole history
@@ -418,9 +425,11 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
                 ++rnd;
                 std::vector<double> b2;
                 ST(next_block(L, cur + 1, sq, b2, lmin, lmax));
+                L.x_ready = false;
             } else if (iter > 1 && beta_prev > 0.0 && b < 0.1 * beta_prev) {
                 ST(cgs(L, cur + 1, &sq));  // second full pass, v_i included
                 ST(next_block(L, cur + 1, sq, beta, lmin, lmax));
+                L.x_ready = false;
             }
         } else {
             // block: guard against a rank-deficient residual block
@@ -547,6 +556,7 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
             mT = k;
             karrow = k;
             ++restarts;
+            L.x_ready = false;  // the continuation block was moved
             iter = k / nb;
             beta_prev = -1.0;
         }
@@ -634,7 +644,7 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
         (st = dev_alloc(ctx, L.Y, (size_t)L.n * L.nb * (L.prec == 4 ? 4 : 8))) ||
         (st = dev_alloc(ctx, L.partial, sizeof(double) * (size_t)4096 * G)) ||
         (st = dev_alloc(ctx, L.coef, sizeof(double) * (size_t)maxcol * L.nb)) ||
-        (st = dev_alloc(ctx, L.sqp, sizeof(double) * 16 * 592)) || (st = dev_alloc(ctx, L.sq, sizeof(double) * 16)) ||
+        (st = dev_alloc(ctx, L.sqp, sizeof(double) * 16 * kMaxDotGrid)) || (st = dev_alloc(ctx, L.sq, sizeof(double) * 16)) ||
         (st = dev_alloc(ctx, L.Adev, sizeof(double) * (size_t)N * N)) ||
         (st = dev_alloc(ctx, L.Vtmp, sizeof(double) * (size_t)N * N)) ||
         (st = dev_alloc(ctx, L.Zdev, sizeof(double) * (size_t)N * N)) || (st = dev_alloc(ctx, L.wdev, sizeof(double) * N)) ||

@@ -176,10 +176,12 @@ __global__ void __launch_bounds__(256) k_sub_gemv(const double *__restrict__ H, 
 
 // out[l] = sum_j V[j] * Y[j*ldy + l], l < K (K <= 16 per launch)
 // K is a template parameter so that the K accumulators live in registers
+// xpack (optional): the result also as the interleaved applyH input of the
+// next step (x[i*K + l], FP32 for xprec 4, FP64 for 8), as k_pack would make it
 template <int K>
 __global__ void __launch_bounds__(256) k_transform(const double *__restrict__ V, int m, const double *__restrict__ Y,
                                                    int ldy, double *__restrict__ out, int64_t n, int64_t ld,
-                                                   int64_t ldo) {
+                                                   int64_t ldo, void *__restrict__ xpack, int xprec) {
     extern __shared__ double sY[];  // [m][K]
     for (int e = threadIdx.x; e < m * K; e += blockDim.x) {
         const int j = e / K, l = e - j * K;
@@ -203,6 +205,15 @@ __global__ void __launch_bounds__(256) k_transform(const double *__restrict__ V,
         }
 #pragma unroll
         for (int l = 0; l < K; ++l) out[(int64_t)l * ldo + i] = acc[l];
+        if (xpack) {
+            if (xprec == 4) {
+#pragma unroll
+                for (int l = 0; l < K; ++l) static_cast<float *>(xpack)[i * K + l] = (float)acc[l];
+            } else {
+#pragma unroll
+                for (int l = 0; l < K; ++l) static_cast<double *>(xpack)[i * K + l] = acc[l];
+            }
+        }
     }
 }
 
@@ -215,13 +226,22 @@ __global__ void k_scale_cols(const double *__restrict__ x, double *y, const doub
 
 // y = x / sqrt(sq[0]) when sq[0] > 0 (nothing written otherwise): the
 // scalar normalization of the residual, with the norm left on the device
+// (xpack as for k_transform)
 __global__ void k_normalize_col(const double *__restrict__ x, double *__restrict__ y, const double *__restrict__ sq,
-                                int64_t n) {
+                                int64_t n, void *__restrict__ xpack, int xprec) {
     const double q = sq[0];
     if (!(q > 0.0)) return;
     const double inv = 1.0 / sqrt(q);
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        y[i] = x[i] * inv;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double v = x[i] * inv;
+        y[i] = v;
+        if (xpack) {
+            if (xprec == 4)
+                static_cast<float *>(xpack)[i] = (float)v;
+            else
+                static_cast<double *>(xpack)[i] = v;
+        }
+    }
 }
 
 // interleaved applyH vector from nB history columns (fp64 -> T)
@@ -581,13 +601,22 @@ cudaError_t random_cols(double *W, int nB, int64_t n, int64_t ld, uint64_t seed,
 
 int dot_grid(int64_t n) {
     int64_t tiles = (n + kDotTile - 1) / kDotTile;
-    return (int)(tiles < 592 ? (tiles > 0 ? tiles : 1) : 592);
+    return (int)(tiles < kMaxDotGrid ? (tiles > 0 ? tiles : 1) : kMaxDotGrid);
+}
+
+// CTAs of the streaming passes: single vectors at 40 registers fit 6 CTAs of
+// 256 per SM, and on long vectors (at least 592 row tiles) the extra loads in
+// flight were measured faster (pf 4p4n); blocks of vectors stay at 4 per SM
+template <int NB>
+static int stream_grid(int64_t n) {
+    return (NB == 1 && n >= (int64_t)592 * kDotTile) ? kMaxDotGrid : 592;
 }
 
 template <int NB>
 static cudaError_t multidot_nb(const double *A, int nA, const double *B, int64_t n, int64_t ld, double *partial,
                                double *out, cudaStream_t s) {
-    const int G = dot_grid(n);
+    const int64_t tiles = (n + kDotTile - 1) / kDotTile;
+    const int G = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, stream_grid<NB>(n)));
     const int maxa = 4096 / NB;  // shared accumulator of at most 4096 doubles
     for (int a0 = 0; a0 < nA;) {
         const int na = (nA - a0) < maxa ? (nA - a0) : maxa;
@@ -627,7 +656,7 @@ cudaError_t multidot(const double *A, int nA, const double *B, int nB, int64_t n
 template <int NB>
 static cudaError_t sub_gemv_nb(const double *H, int k, const double *C, double *W, int64_t n, int64_t ld,
                                double *sq_partial, double *sq_out, cudaStream_t s) {
-    const int G = 592;
+    const int G = stream_grid<NB>(n);
     int j0 = 0;
     do {
         const int kk = (k - j0) < 512 ? (k - j0) : 512;
@@ -655,7 +684,8 @@ cudaError_t sub_gemv(const double *H, int k, const double *C, double *W, int nB,
 }
 
 cudaError_t transform(const double *V, int m, const double *Y, int ldy, int K, double *out, int64_t n, int64_t ld,
-                      int64_t ldo, cudaStream_t s) {
+                      int64_t ldo, cudaStream_t s, void *xpack, int xprec) {
+    if (xpack && K > 16) return cudaErrorInvalidValue;  // the packed copy needs one pass
     for (int l0 = 0; l0 < K; l0 += 16) {
         const int kk = (K - l0) < 16 ? (K - l0) : 16;
         // Y rows in chunks that fit shared memory: accumulate over row chunks
@@ -667,7 +697,8 @@ cudaError_t transform(const double *V, int m, const double *Y, int ldy, int K, d
     case KT:                                                                                                \
         e = cudaFuncSetAttribute(k_transform<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024); \
         if (e == cudaSuccess)                                                                               \
-            k_transform<KT><<<592, 256, smem, s>>>(V, m, Y + l0, ldy, out + (int64_t)l0 * ldo, n, ld, ldo); \
+            k_transform<KT><<<592, 256, smem, s>>>(V, m, Y + l0, ldy, out + (int64_t)l0 * ldo, n, ld, ldo, \
+                                                    xpack, xprec);                                       \
         break;
             BSG_TRANSFORM_CASE(1) BSG_TRANSFORM_CASE(2) BSG_TRANSFORM_CASE(3) BSG_TRANSFORM_CASE(4)
             BSG_TRANSFORM_CASE(5) BSG_TRANSFORM_CASE(6) BSG_TRANSFORM_CASE(7) BSG_TRANSFORM_CASE(8)
@@ -685,8 +716,9 @@ cudaError_t scale_cols(const double *x, double *y, const double *sc, int nB, int
     return cudaGetLastError();
 }
 
-cudaError_t normalize_col(const double *x, double *y, const double *sq, int64_t n, cudaStream_t s) {
-    k_normalize_col<<<592, 256, 0, s>>>(x, y, sq, n);
+cudaError_t normalize_col(const double *x, double *y, const double *sq, int64_t n, cudaStream_t s, void *xpack,
+                          int xprec) {
+    k_normalize_col<<<592, 256, 0, s>>>(x, y, sq, n, xpack, xprec);
     return cudaGetLastError();
 }
 

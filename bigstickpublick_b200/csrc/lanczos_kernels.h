@@ -4,6 +4,8 @@
 #include <stdint.h>
 
 namespace bsg {
+// largest grid of the dot and update passes (partial buffers are sized by it)
+constexpr int kMaxDotGrid = 888;
 int dot_grid(int64_t n);
 // out[a*nB + b] = A_a . B_b   (partial: scratch of nA*nB*dot_grid(n) doubles)
 cudaError_t multidot(const double *A, int nA, const double *B, int nB, int64_t n, int64_t ld, double *partial,
@@ -13,11 +15,14 @@ cudaError_t multidot(const double *A, int nA, const double *B, int nB, int64_t n
 cudaError_t sub_gemv(const double *H, int k, const double *C, double *W, int nB, int64_t n, int64_t ld,
                      double *sq_partial, double *sq_out, cudaStream_t s);
 // out_l = sum_j V_j Y[j*ldy + l], l < K
+// xpack (optional, K <= 16): the result also as the interleaved applyH input
+// (FP32 for xprec 4, FP64 for 8), as pack() would make it
 cudaError_t transform(const double *V, int m, const double *Y, int ldy, int K, double *out, int64_t n, int64_t ld,
-                      int64_t ldo, cudaStream_t s);
+                      int64_t ldo, cudaStream_t s, void *xpack = nullptr, int xprec = 8);
 cudaError_t scale_cols(const double *x, double *y, const double *sc, int nB, int64_t n, int64_t ld, cudaStream_t s);
 // y = x / sqrt(sq[0]) if sq[0] > 0, else y untouched (sq on the device)
-cudaError_t normalize_col(const double *x, double *y, const double *sq, int64_t n, cudaStream_t s);
+cudaError_t normalize_col(const double *x, double *y, const double *sq, int64_t n, cudaStream_t s,
+                          void *xpack = nullptr, int xprec = 8);
 cudaError_t pack(const double *V, int nB, int64_t n, int64_t ld, void *x, int prec, cudaStream_t s);
 cudaError_t unpack(const void *y, int nB, int64_t n, int64_t ld, double *W, int prec, cudaStream_t s);
 // lowest nwant eigenvalues of the arrowhead-tridiagonal matrix
