@@ -22,52 +22,53 @@
 
 namespace bsg {
 
-template <typename T, int NB, int ITEMS, bool FULL>
+template <typename T, int NB, int ITEMS, bool FULL, int OUT>
 __device__ __forceinline__ void rows_body(const RowArgs &a, const T *__restrict__ vin, T *__restrict__ vout,
                                           const int ld, const int v0, const int mstride) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int warp = threadIdx.x >> 5;
     float *__restrict__ Mw = reinterpret_cast<float *>(smem) + (size_t)warp * mstride;
     T *__restrict__ part = reinterpret_cast<T *>(smem + align16(sizeof(float) * (size_t)kWarps * mstride));
-    row_tile<T, NB, ITEMS, FULL>(a, a.tiles[blockIdx.x], vin, vout, ld, v0, Mw, part);
+    row_tile<T, NB, ITEMS, FULL, OUT>(a, a.tiles[blockIdx.x], vin, vout, ld, v0, Mw, part);
 }
 
-template <typename T, int NB, int ITEMS, bool FULL>
+// OUT: store, accumulate, or FP64 columns (RowOut in applyh_tile.cuh)
+template <typename T, int NB, int ITEMS, bool FULL, int OUT>
 __global__ void __launch_bounds__(kWarps * 32) k_rows(const RowArgs a, const T *__restrict__ vin,
                                                       T *__restrict__ vout, const int ld, const int v0,
                                                       const int mstride) {
-    rows_body<T, NB, ITEMS, FULL>(a, vin, vout, ld, v0, mstride);
+    rows_body<T, NB, ITEMS, FULL, OUT>(a, vin, vout, ld, v0, mstride);
 }
 
 // single vectors: at most 40 registers, so that 6 CTAs of 256 threads stay
 // resident per SM to hide the gather latency (measured faster than the
 // compiler's own choice of 48 registers, the small spills included)
-template <int ITEMS, bool FULL>
+template <int ITEMS, bool FULL, int OUT>
 __global__ void __launch_bounds__(kWarps * 32, 6) k_rows_f1(const RowArgs a, const float *__restrict__ vin,
                                                             float *__restrict__ vout, const int ld, const int v0,
                                                             const int mstride) {
-    rows_body<float, 1, ITEMS, FULL>(a, vin, vout, ld, v0, mstride);
+    rows_body<float, 1, ITEMS, FULL, OUT>(a, vin, vout, ld, v0, mstride);
 }
-template <int ITEMS, bool FULL>
+template <int ITEMS, bool FULL, int OUT>
 __global__ void __launch_bounds__(kWarps * 32, 6) k_rows_d1(const RowArgs a, const double *__restrict__ vin,
                                                             double *__restrict__ vout, const int ld, const int v0,
                                                             const int mstride) {
-    rows_body<double, 1, ITEMS, FULL>(a, vin, vout, ld, v0, mstride);
+    rows_body<double, 1, ITEMS, FULL, OUT>(a, vin, vout, ld, v0, mstride);
 }
 
-template <typename T, int NB, int ITEMS, bool FULL>
+template <typename T, int NB, int ITEMS, bool FULL, int OUT>
 constexpr auto rows_kernel() {
     if constexpr (std::is_same<T, float>::value && NB == 1)
-        return k_rows_f1<ITEMS, FULL>;
+        return k_rows_f1<ITEMS, FULL, OUT>;
     else if constexpr (std::is_same<T, double>::value && NB == 1)
-        return k_rows_d1<ITEMS, FULL>;
+        return k_rows_d1<ITEMS, FULL, OUT>;
     else
-        return k_rows<T, NB, ITEMS, FULL>;
+        return k_rows<T, NB, ITEMS, FULL, OUT>;
 }
 
 template <typename T, int NB, int ITEMS>
 static int launch_one(bsg_ctx *ctx, const T *vin, T *vout, int ld, int v0, int accumulate,
-                      cudaStream_t s, TileLookup lookup) {
+                      cudaStream_t s, TileLookup lookup, double *cols) {
     const TileSet *ts = lookup ? lookup(ctx, 32 * ITEMS) : get_tiles(ctx, 32 * ITEMS);
     if (!ts) return ctx->last_error.empty() ? BSG_ERR_NOMEM : BSG_ERR_CUDA;
     if (ts->ntiles == 0) return BSG_OK;
@@ -75,6 +76,8 @@ static int launch_one(bsg_ctx *ctx, const T *vin, T *vout, int ld, int v0, int a
     a.tiles = (const Tile *)ts->buf.p;
     a.ntiles = ts->ntiles;
     a.accumulate = accumulate;
+    a.cols_out = cols;
+    a.cols_ld = ctx->dim;
     const int mstride = (a.max_nbd + 3) & ~3;
     const size_t smem = align16(sizeof(float) * (size_t)kWarps * mstride) +
                         sizeof(T) * (size_t)kWarps * 32 * ITEMS * NB;
@@ -89,15 +92,18 @@ static int launch_one(bsg_ctx *ctx, const T *vin, T *vout, int ld, int v0, int a
         if (r == cudaSuccess) cur = smem;
         return r;
     };
-    if (full) {
-        auto k = rows_kernel<T, NB, ITEMS, true>();
-        e = allow((const void *)k);
-        if (e == cudaSuccess) k<<<ts->ntiles, kWarps * 32, smem, s>>>(a, vin, vout, ld, v0, mstride);
-    } else {
-        auto k = rows_kernel<T, NB, ITEMS, false>();
-        e = allow((const void *)k);
-        if (e == cudaSuccess) k<<<ts->ntiles, kWarps * 32, smem, s>>>(a, vin, vout, ld, v0, mstride);
-    }
+    auto go = [&](auto k) -> cudaError_t {
+        cudaError_t r = allow((const void *)k);
+        if (r == cudaSuccess) k<<<ts->ntiles, kWarps * 32, smem, s>>>(a, vin, vout, ld, v0, mstride);
+        return r;
+    };
+    if (cols)
+        e = go(rows_kernel<T, NB, ITEMS, true, kColumns>());
+    else if (full)
+        e = accumulate ? go(rows_kernel<T, NB, ITEMS, true, kAccumulate>()) : go(rows_kernel<T, NB, ITEMS, true, kStore>());
+    else
+        e = accumulate ? go(rows_kernel<T, NB, ITEMS, false, kAccumulate>())
+                       : go(rows_kernel<T, NB, ITEMS, false, kStore>());
     if (e != cudaSuccess) return cuda_check(ctx, e, "applyh smem attribute");
     return cuda_check(ctx, cudaGetLastError(), "applyh kernel launch");
 }
@@ -106,16 +112,16 @@ static int launch_one(bsg_ctx *ctx, const T *vin, T *vout, int ld, int v0, int a
 // median row, capped so that ITEMS*NB accumulators stay in registers
 template <typename T, int NB>
 static int launch_nb(bsg_ctx *ctx, const T *vin, T *vout, int ld, int v0, int accumulate, cudaStream_t s,
-                     TileLookup lk) {
+                     TileLookup lk, double *cols = nullptr) {
     // nb = 8 measured fastest at two positions per lane (pf 4p4n: 5.10 ms at
     // one, 4.86 at two, 5.08 at four)
     constexpr int cap = NB >= 16 ? 1 : (NB >= 4 ? 2 : (NB == 2 ? 4 : 8));
     int items = 1;
     while (items < cap && 32 * items < ctx->median_rowlen) items *= 2;
-    if (items >= 8 && cap >= 8) return launch_one<T, NB, (cap >= 8 ? 8 : 1)>(ctx, vin, vout, ld, v0, accumulate, s, lk);
-    if (items >= 4 && cap >= 4) return launch_one<T, NB, (cap >= 4 ? 4 : 1)>(ctx, vin, vout, ld, v0, accumulate, s, lk);
-    if (items >= 2 && cap >= 2) return launch_one<T, NB, (cap >= 2 ? 2 : 1)>(ctx, vin, vout, ld, v0, accumulate, s, lk);
-    return launch_one<T, NB, 1>(ctx, vin, vout, ld, v0, accumulate, s, lk);
+    if (items >= 8 && cap >= 8) return launch_one<T, NB, (cap >= 8 ? 8 : 1)>(ctx, vin, vout, ld, v0, accumulate, s, lk, cols);
+    if (items >= 4 && cap >= 4) return launch_one<T, NB, (cap >= 4 ? 4 : 1)>(ctx, vin, vout, ld, v0, accumulate, s, lk, cols);
+    if (items >= 2 && cap >= 2) return launch_one<T, NB, (cap >= 2 ? 2 : 1)>(ctx, vin, vout, ld, v0, accumulate, s, lk, cols);
+    return launch_one<T, NB, 1>(ctx, vin, vout, ld, v0, accumulate, s, lk, cols);
 }
 
 template <typename T>
@@ -134,6 +140,33 @@ static int launch_typed(bsg_ctx *ctx, const T *vin, T *vout, int nb, int accumul
         return st;
     }
     }
+}
+
+int launch_applyh_cols(bsg_ctx *ctx, const void *vin, double *cols, int nb, int prec, cudaStream_t s) {
+    if (ctx->args.max_nbd > 5120)
+        return set_err(ctx, BSG_ERR_UNSUPPORTED, "a neutron sector jump has more than 5120 distinct (b,d) pairs");
+    if ((reinterpret_cast<uintptr_t>(vin) & 15u) != 0 || !cols)
+        return set_err(ctx, BSG_ERR_ARG, "applyH to columns: misaligned input or no output");
+    if (prec == BSG_PREC_FP32) {
+        const float *x = (const float *)vin;
+        switch (nb) {
+        case 1: return launch_nb<float, 1>(ctx, x, nullptr, 1, 0, 0, s, nullptr, cols);
+        case 2: return launch_nb<float, 2>(ctx, x, nullptr, 2, 0, 0, s, nullptr, cols);
+        case 4: return launch_nb<float, 4>(ctx, x, nullptr, 4, 0, 0, s, nullptr, cols);
+        case 8: return launch_nb<float, 8>(ctx, x, nullptr, 8, 0, 0, s, nullptr, cols);
+        case 16: return launch_nb<float, 16>(ctx, x, nullptr, 16, 0, 0, s, nullptr, cols);
+        }
+    } else {
+        const double *x = (const double *)vin;
+        switch (nb) {
+        case 1: return launch_nb<double, 1>(ctx, x, nullptr, 1, 0, 0, s, nullptr, cols);
+        case 2: return launch_nb<double, 2>(ctx, x, nullptr, 2, 0, 0, s, nullptr, cols);
+        case 4: return launch_nb<double, 4>(ctx, x, nullptr, 4, 0, 0, s, nullptr, cols);
+        case 8: return launch_nb<double, 8>(ctx, x, nullptr, 8, 0, 0, s, nullptr, cols);
+        case 16: return launch_nb<double, 16>(ctx, x, nullptr, 16, 0, 0, s, nullptr, cols);
+        }
+    }
+    return set_err(ctx, BSG_ERR_ARG, "applyH to columns: nb must be 1, 2, 4, 8 or 16");
 }
 
 int launch_applyh(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec, int accumulate,

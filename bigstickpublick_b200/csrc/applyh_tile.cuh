@@ -97,7 +97,13 @@ __host__ __device__ constexpr size_t align16(size_t x) { return (x + 15) & ~size
 // ld: elements between consecutive states (the block size nb); v0: first
 // vector column handled by this launch; FULL: ld == NB and aligned base.
 // mstride: floats of per-warp shared memory for the PN matrix-element table.
-template <typename T, int NB, int ITEMS, bool FULL>
+// what the tile does with its sums: store them, add them to the output, or
+// store them as FP64 columns (RowArgs::cols_out) for the Lanczos history.
+// Separate instantiations keep the common store free of the other modes'
+// registers.
+enum RowOut { kStore = 0, kAccumulate = 1, kColumns = 2 };
+
+template <typename T, int NB, int ITEMS, bool FULL, int OUT = kStore>
 __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, const T *__restrict__ vin,
                                          T *__restrict__ vout, const int ld_, const int v0_,
                                          float *__restrict__ Mw, T *__restrict__ part) {
@@ -254,13 +260,29 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
         for (int v = 0; v < NB; ++v) part[((size_t)warp * TP + lane + 32 * i) * NB + v] = acc[i][v];
     __syncthreads();
     const int nel = tile.npos * NB;
-    for (int e = threadIdx.x; e < nel; e += kWarps * 32) {
-        T s = part[e];
+    if constexpr (OUT == kColumns) {
+        // FP64 columns: consecutive threads take consecutive positions of one
+        // column (coalesced stores); each element summed as below
+        for (int e = threadIdx.x; e < nel; e += kWarps * 32) {
+            const int v = e / tile.npos, lp = e - v * tile.npos;
+            const int idx = lp * NB + v;
+            T s = part[idx];
 #pragma unroll
-        for (int w = 1; w < kWarps; ++w) s += part[(size_t)w * TP * NB + e];
-        const int lp = e / NB, v = e - lp * NB;
-        T *o = vout + (size_t)(roff + tile.pos0 + lp) * ld + v0 + v;
-        *o = a.accumulate ? *o + s : s;
+            for (int w = 1; w < kWarps; ++w) s += part[(size_t)w * TP * NB + idx];
+            a.cols_out[(size_t)(v0 + v) * a.cols_ld + roff + tile.pos0 + lp] = (double)s;
+        }
+    } else {
+        for (int e = threadIdx.x; e < nel; e += kWarps * 32) {
+            T s = part[e];
+#pragma unroll
+            for (int w = 1; w < kWarps; ++w) s += part[(size_t)w * TP * NB + e];
+            const int lp = e / NB, v = e - lp * NB;
+            T *o = vout + (size_t)(roff + tile.pos0 + lp) * ld + v0 + v;
+            if constexpr (OUT == kAccumulate)
+                *o = *o + s;
+            else
+                *o = s;
+        }
     }
 }
 

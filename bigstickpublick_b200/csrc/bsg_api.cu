@@ -654,6 +654,8 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
     int32_t max_nbd = 0;
     for (auto &o : nops) max_nbd = std::max(max_nbd, o.nbd);
     a.max_nbd = max_nbd;
+    a.cols_out = nullptr;  // set per launch by the Lanczos path only
+    a.cols_ld = 0;
     ctx->h_bd = bd_all;
     ctx->h_pnrec = pnrec_all;
     ctx->h_nptr = nptr_all;

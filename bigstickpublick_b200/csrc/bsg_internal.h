@@ -108,6 +108,11 @@ struct RowArgs {
     const Tile *tiles;
     int32_t ntiles;
     int32_t accumulate;
+    // optional: store the result as FP64 columns (column v at cols_out +
+    // v * cols_ld) instead of the interleaved output vector; the Lanczos
+    // history takes it directly
+    double *cols_out;
+    int64_t cols_ld;
 };
 
 struct DevBuf {
@@ -176,4 +181,7 @@ void build_tile_list(const bsg_ctx *ctx, int tp, std::vector<Tile> &tiles);
 typedef const TileSet *(*TileLookup)(bsg_ctx *ctx, int tp);
 int launch_applyh(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec, int accumulate,
                   cudaStream_t s, TileLookup lookup = nullptr);
+// H x for an interleaved input x (nb <= 16, dense and 16-byte aligned), the
+// result written as nb FP64 columns of length dim starting at cols
+int launch_applyh_cols(bsg_ctx *ctx, const void *vin, double *cols, int nb, int prec, cudaStream_t s);
 }  // namespace bsg

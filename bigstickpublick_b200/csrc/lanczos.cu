@@ -54,7 +54,7 @@ struct Lz {
     int64_t n;
     int nb, prec;
     int maxcol;      // history columns
-    DevBuf hist, W, X, Y, tmp, partial, coef, sqp, sq, Adev, Vtmp, Zdev, wdev, stat, al, bt, ev, M, tau, ework;
+    DevBuf hist, W, X, tmp, partial, coef, sqp, sq, Adev, Vtmp, Zdev, wdev, stat, al, bt, ev, M, tau, ework;
     DevBuf Ydev;     // Ritz coefficients of a thick restart (maxcol x 128)
     std::vector<double> T;  // host projected matrix (maxcol x maxcol), row-major
     float t_mv = 0, t_ort = 0, t_eig = 0;
@@ -373,9 +373,8 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
         if (!L.x_ready) CK(pack(L.col(cur), nb, n, n, L.X.p, L.prec, L.s));
         L.x_ready = false;
         CK(cudaEventRecord(L.e0, L.s));
-        ST(launch_applyh(ctx, L.X.p, L.Y.p, nb, L.prec, 0, L.s));
+        ST(launch_applyh_cols(ctx, L.X.p, (double *)L.W.p, nb, L.prec, L.s));  // W columns directly
         CK(cudaEventRecord(L.e1, L.s));
-        CK(unpack(L.Y.p, nb, n, n, (double *)L.W.p, L.prec, L.s));
         ++matvecs;
         // ---- alpha = V^T W ; W -= V alpha ; CGS against [0, cur), all queued
         // without a host round trip; the scalar recursion also normalizes
@@ -632,7 +631,7 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
     const int N = maxcol;
     const size_t vb = sizeof(double) * (size_t)L.n;
     size_t need = vb * ((size_t)maxcol + 2 * L.nb + (size_t)std::max(L.nb, pp.nkeep + pp.nthick_add + 1)) +
-                  2 * (size_t)L.n * L.nb * (L.prec == 4 ? 4 : 8);
+                  (size_t)L.n * L.nb * (L.prec == 4 ? 4 : 8);
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
     if (need > fr) return set_err(ctx, BSG_ERR_NOMEM, "bsg_lanczos: history does not fit in device memory");
@@ -641,7 +640,6 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
     if ((st = dev_alloc(ctx, L.hist, vb * maxcol)) || (st = dev_alloc(ctx, L.W, vb * L.nb)) ||
         (st = dev_alloc(ctx, L.tmp, vb * ktmp)) ||
         (st = dev_alloc(ctx, L.X, (size_t)L.n * L.nb * (L.prec == 4 ? 4 : 8))) ||
-        (st = dev_alloc(ctx, L.Y, (size_t)L.n * L.nb * (L.prec == 4 ? 4 : 8))) ||
         (st = dev_alloc(ctx, L.partial, sizeof(double) * (size_t)4096 * G)) ||
         (st = dev_alloc(ctx, L.coef, sizeof(double) * (size_t)maxcol * L.nb)) ||
         (st = dev_alloc(ctx, L.sqp, sizeof(double) * 16 * kMaxDotGrid)) || (st = dev_alloc(ctx, L.sq, sizeof(double) * 16)) ||
@@ -702,7 +700,7 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
         cudaStreamDestroy(L.s2);
     }
     if (L.econv) cudaEventDestroy(L.econv);
-    DevBuf *bufs[] = {&L.hist, &L.W, &L.X, &L.Y, &L.tmp, &L.partial, &L.coef, &L.sqp, &L.sq, &L.Adev,
+    DevBuf *bufs[] = {&L.hist, &L.W, &L.X, &L.tmp, &L.partial, &L.coef, &L.sqp, &L.sq, &L.Adev,
                       &L.Vtmp, &L.Zdev, &L.wdev, &L.stat, &L.al, &L.bt, &L.ev, &L.M, &L.tau, &L.ework,
                       &L.al2, &L.bt2, &L.w2, &L.Adev2, &L.Vtmp2, &L.tau2, &L.ework2, &L.Ydev};
     cudaStreamSynchronize(L.s);
