@@ -54,7 +54,7 @@ struct Lz {
     int64_t n;
     int nb, prec;
     int maxcol;      // history columns
-    DevBuf hist, W, X, tmp, partial, coef, sqp, sq, Adev, Vtmp, Zdev, wdev, stat, al, bt, ev, M, tau, ework;
+    DevBuf hist, W, X, tmp, partial, coef, sqp, sq, Adev, Vtmp, Zdev, wdev, al, bt, ev, M, tau, ework;
     DevBuf Ydev;     // Ritz coefficients of a thick restart (maxcol x 128)
     std::vector<double> T;  // host projected matrix (maxcol x maxcol), row-major
     float t_mv = 0, t_ort = 0, t_eig = 0;
@@ -646,7 +646,7 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
         (st = dev_alloc(ctx, L.Adev, sizeof(double) * (size_t)N * N)) ||
         (st = dev_alloc(ctx, L.Vtmp, sizeof(double) * (size_t)N * N)) ||
         (st = dev_alloc(ctx, L.Zdev, sizeof(double) * (size_t)N * N)) || (st = dev_alloc(ctx, L.wdev, sizeof(double) * N)) ||
-        (st = dev_alloc(ctx, L.stat, sizeof(int) * 4)) || (st = dev_alloc(ctx, L.al, sizeof(double) * N)) ||
+        (st = dev_alloc(ctx, L.al, sizeof(double) * N)) ||
         (st = dev_alloc(ctx, L.bt, sizeof(double) * N)) || (st = dev_alloc(ctx, L.ev, sizeof(double) * N)) ||
         (st = dev_alloc(ctx, L.M, sizeof(double) * 16 * 16)) || (st = dev_alloc(ctx, L.tau, sizeof(double) * N)) ||
         (st = dev_alloc(ctx, L.ework, sizeof(double) * ((size_t)2 * N + (size_t)6 * N * std::min(N, 128))))) {
@@ -701,7 +701,7 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
     }
     if (L.econv) cudaEventDestroy(L.econv);
     DevBuf *bufs[] = {&L.hist, &L.W, &L.X, &L.tmp, &L.partial, &L.coef, &L.sqp, &L.sq, &L.Adev,
-                      &L.Vtmp, &L.Zdev, &L.wdev, &L.stat, &L.al, &L.bt, &L.ev, &L.M, &L.tau, &L.ework,
+                      &L.Vtmp, &L.Zdev, &L.wdev, &L.al, &L.bt, &L.ev, &L.M, &L.tau, &L.ework,
                       &L.al2, &L.bt2, &L.w2, &L.Adev2, &L.Vtmp2, &L.tau2, &L.ework2, &L.Ydev};
     cudaStreamSynchronize(L.s);
     for (DevBuf *b : bufs) dev_free(*b);
