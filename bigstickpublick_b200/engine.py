@@ -165,6 +165,29 @@ class Hamiltonian:
         return out
 
 
+def angular_momentum_isospin(spec, vecs, device=0):
+    """J and T of the states `vecs` (dim x k, columns normalized, in the basis
+    of `spec`): <J^2> and <T^2> with the operators of model.jsq_spec /
+    model.tsq_spec applied by the engine in FP64, as lanczos_output reports
+    them.  Returns (J, T) arrays."""
+    from . import model
+    v = np.ascontiguousarray(np.asarray(vecs, dtype=np.float64))
+    if v.ndim == 1:
+        v = v[:, None]
+    out = []
+    for mk in (model.jsq_spec, model.tsq_spec):
+        T = model.build_tables(mk(spec))
+        if T.dim != v.shape[0]:
+            raise ValueError("vectors do not match the basis of the model")
+        H = Hamiltonian(T, device=device)
+        try:
+            ex = np.array([float(v[:, k] @ H.applyh(np.ascontiguousarray(v[:, k]))) for k in range(v.shape[1])])
+        finally:
+            H.close()
+        out.append(model.j_from_jsq(ex))
+    return out[0], out[1]
+
+
 class _SystemView(Hamiltonian):
     """A Hamiltonian bound to one system of a Batch (the batch owns it)."""
 

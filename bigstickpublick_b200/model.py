@@ -300,6 +300,40 @@ def pf_model(np_, nn, seed, jz2=0):
     return ModelSpec(PF_ORBITS, np_, nn, jz2, 1, spe, tb, 1.0, 1.0)
 
 
+def _pair_diagonal_keys(orbits):
+    return [k for k in canonical_tbme_keys(orbits) if k[0] == k[2] and k[1] == k[3]]
+
+
+def jsq_spec(spec: ModelSpec) -> ModelSpec:
+    """J^2 of the many-body space of `spec` as a two-body operator, in the
+    reference's own representation (a one-body part on the orbits plus
+    coupled J-T matrix elements; lanczos_output evaluates <J^2> the same way,
+    src/blanczoslib.f90:1023-1603):
+      J^2 = sum_i j_i^2 + sum_{i<j} 2 j_i.j_j,
+      one-body e_a = j_a(j_a+1),
+      <ab;JT| 2 j_1.j_2 |ab;JT> = J(J+1) - j_a(j_a+1) - j_b(j_b+1)  (diagonal).
+    Same orbits, particle numbers, 2Jz and parity, hence the same basis as H."""
+    def jj(o):
+        j = spec.orbits[o - 1][2] / 2.0
+        return j * (j + 1.0)
+    spe = [(o[2] / 2.0) * (o[2] / 2.0 + 1.0) for o in spec.orbits]
+    tb = [(a, b, c, d, J, T, J * (J + 1.0) - jj(a) - jj(b)) for (a, b, c, d, J, T) in _pair_diagonal_keys(spec.orbits)]
+    return ModelSpec(spec.orbits, spec.np_, spec.nn, spec.jz2, spec.parity, spe, tb, 1.0, 1.0)
+
+
+def tsq_spec(spec: ModelSpec) -> ModelSpec:
+    """T^2 like jsq_spec: one-body 3/4 per nucleon, pair elements
+    T(T+1) - 3/2 for every coupled pair."""
+    spe = [0.75] * len(spec.orbits)
+    tb = [(a, b, c, d, J, T, T * (T + 1.0) - 1.5) for (a, b, c, d, J, T) in _pair_diagonal_keys(spec.orbits)]
+    return ModelSpec(spec.orbits, spec.np_, spec.nn, spec.jz2, spec.parity, spe, tb, 1.0, 1.0)
+
+
+def j_from_jsq(x):
+    """J from <J^2> = J(J+1)."""
+    return 0.5 * (np.sqrt(1.0 + 4.0 * np.maximum(np.asarray(x, dtype=np.float64), 0.0)) - 1.0)
+
+
 def chain_rule(tables, dhmat):
     """Gradient of one eigenvalue with respect to the coupled interaction.
 

@@ -85,3 +85,21 @@ def test_two_particle_pn_spectrum_equals_coupled_jt_blocks():
         dense_h.coupled_two_body_spectrum(model.SD_ORBITS, spe, tb, 1)
     ref = np.sort([e for e, J in cs])
     assert np.abs(ev - ref).max() < 1e-5
+
+
+@pytest.mark.parametrize("np_,nn,jz", [(2, 2, 0), (1, 2, 1), (3, 2, 1)])
+def test_jsq_tsq_operator_spectra(np_, nn, jz):
+    """The J^2 and T^2 operators built through the uncoupling (model.jsq_spec,
+    model.tsq_spec) have spectra J(J+1), T(T+1) with J half-integer for odd A
+    and integer for even A, and T between |Tz| and A/2."""
+    base = model.sd_model(np_, nn, seed=1, jz2=jz)
+    a = np_ + nn
+    for mk, lo, hi in ((model.jsq_spec, None, None), (model.tsq_spec, abs(np_ - nn) / 2, a / 2)):
+        T = model.build_tables(mk(base))
+        M = oracle.dense_from_applyh(T)
+        x = model.j_from_jsq(np.linalg.eigvalsh(0.5 * (M + M.T)))
+        twice = np.round(2 * x)
+        assert np.abs(2 * x - twice).max() < 1e-5
+        assert np.all(twice % 2 == a % 2)
+        if lo is not None:
+            assert x.min() > lo - 1e-6 and x.max() < hi + 1e-6
