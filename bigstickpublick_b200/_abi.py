@@ -102,6 +102,17 @@ class BsgModelSpec(C.Structure):
     ]
 
 
+class BsgDensityTables(C.Structure):
+    _fields_ = [
+        ("np1b", C.c_int64), ("p1b_isd", i64p), ("p1b_fsd", i64p),
+        ("p1b_cop", i16p), ("p1b_dop", i16p), ("p1b_phase", i8p),
+        ("nn1b", C.c_int64), ("n1b_isd", i64p), ("n1b_fsd", i64p),
+        ("n1b_cop", i16p), ("n1b_dop", i16p), ("n1b_phase", i8p),
+        ("nbundles", C.c_int64), ("optype", i32p), ("hchar", i32p),
+        ("pxstart", i64p), ("pxend", i64p), ("nxstart", i64p), ("nxend", i64p), ("cstride", i64p),
+    ]
+
+
 class BsgHostTables(C.Structure):
     _fields_ = [
         ("t", BsgTables),
@@ -116,6 +127,7 @@ class BsgHostTables(C.Structure):
         ("sd_bits_p", u64p), ("sd_bits_n", u64p),
         ("npairs_pp", C.c_int64), ("npairs_nn", C.c_int64), ("npairs_pn", C.c_int64),
         ("priv", C.c_void_p),
+        ("dt", BsgDensityTables),
     ]
 
 
@@ -175,6 +187,8 @@ def gpu_lib():
         lib.bsg_lanczos.restype = C.c_int
         lib.bsg_grad.argtypes = [vp, f64p, C.c_int, f64p, f64p, f64p, f64p, f64p]
         lib.bsg_grad.restype = C.c_int
+        lib.bsg_density1b.argtypes = [vp, C.POINTER(BsgDensityTables), f64p, C.c_int, f64p, f64p]
+        lib.bsg_density1b.restype = C.c_int
         lib.bsg_get_stats.argtypes = [vp, C.POINTER(BsgStats)]
         lib.bsg_get_stats.restype = C.c_int
         lib.bsg_validate_tables.argtypes = [C.POINTER(BsgTables), C.c_char_p, C.c_size_t]

@@ -1,0 +1,326 @@
+// bsg_density1b: m-scheme one-body transition densities <f| a+_c a_d |i> for
+// every pair of a set of states, protons and neutrons, in one pass.
+//
+// The reference (src/bdenslib3.f90:14-311, driven by
+// master_density1b_bundled, src/bdenslib1.f90:1506-1607) walks P1B / N1B
+// opbundles: for each one-body jump it sums vec1(statei) * vec2(statef) over
+// the conjugate SDs of the other species (an arithmetic progression of basis
+// states) and adds the sum times the jump phase to p1bopme(cop, dop) (for 'b'
+// bundles the roles of the two states swap and the label is transposed).  It
+// handles one (initial, final) pair per call.
+//
+// Here the host turns every (bundle, jump) into a segment (first row on the
+// final-state side, first row on the initial-state side, stride, count,
+// phase), sorts the segments by output label and cuts each label's segments
+// into chunks of about the same number of rows.  One CTA per chunk stages
+// 64 rows of all states (interleaved, so a row of all states is contiguous)
+// in shared memory and accumulates the nstates x nstates products in FP64,
+// one (final, initial) pair per thread and pass; a second kernel sums the
+// chunks of each label in chunk order.  No atomics: bitwise repeatable.
+
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "bsg_internal.h"
+
+namespace bsg {
+
+namespace {
+
+constexpr int kDenThreads = 256;
+constexpr int kDenTile = 64;        // rows staged per pass
+constexpr int kDenMaxStates = 32;   // pairs per thread <= 4
+
+struct DSeg {
+    int64_t row_f, row_i;   // 0-based first rows: final-state side, initial-state side
+    int64_t step;           // row stride between consecutive conjugate SDs
+    int32_t cnt;            // conjugate SDs (rows) in this segment
+    int32_t item0;          // rows of the chunk before this segment
+    int32_t sign;           // jump phase
+    int32_t pad;
+};
+static_assert(sizeof(DSeg) == 40, "DSeg layout");
+
+struct DChunk {
+    int32_t seg0, seg1;     // segment range
+    int32_t nitems;         // rows in the chunk
+    int32_t label;          // output label (species-combined)
+};
+
+// [dim x ns] column-major -> [dim x ns] interleaved (row of all states contiguous)
+__global__ void k_interleave(const double *__restrict__ cols, double *__restrict__ x, int64_t dim, int ns) {
+    const int64_t n = dim * ns;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = e / ns;
+        const int k = (int)(e - row * ns);
+        x[e] = cols[(int64_t)k * dim + row];
+    }
+}
+
+__global__ void __launch_bounds__(kDenThreads) k_density_chunks(const DSeg *__restrict__ segs,
+                                                              const DChunk *__restrict__ chunks,
+                                                              const double *__restrict__ x, int ns,
+                                                              double *__restrict__ partial) {
+    __shared__ double s_f[kDenTile * kDenMaxStates];
+    __shared__ double s_i[kDenTile * kDenMaxStates];
+    __shared__ int64_t s_rf[kDenTile], s_ri[kDenTile];
+    __shared__ double s_sg[kDenTile];
+    const DChunk ch = chunks[blockIdx.x];
+    const int t = threadIdx.x;
+    const int np = ns * ns;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int base = 0; base < ch.nitems; base += kDenTile) {
+        if (t < kDenTile) {
+            const int item = base + t;
+            int64_t rf = -1, ri = -1;
+            double sg = 0.0;
+            if (item < ch.nitems) {
+                // last segment of the chunk whose item0 <= item
+                int lo = ch.seg0, hi = ch.seg1 - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (segs[mid].item0 <= item) lo = mid; else hi = mid - 1;
+                }
+                const DSeg sgm = segs[lo];
+                const int64_t c = item - sgm.item0;
+                rf = sgm.row_f + c * sgm.step;
+                ri = sgm.row_i + c * sgm.step;
+                sg = (double)sgm.sign;
+            }
+            s_rf[t] = rf;
+            s_ri[t] = ri;
+            s_sg[t] = sg;
+        }
+        __syncthreads();
+        const int nrow = min(kDenTile, ch.nitems - base);
+        for (int e = t; e < nrow * ns; e += kDenThreads) {
+            const int r = e / ns, k = e - r * ns;
+            s_f[k * kDenTile + r] = x[s_rf[r] * ns + k];
+            s_i[k * kDenTile + r] = s_sg[r] * x[s_ri[r] * ns + k];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int p = t + q * kDenThreads;
+            if (p < np) {
+                const int f = p / ns, i = p - f * ns;
+                const double *__restrict__ a = s_f + f * kDenTile;
+                const double *__restrict__ b = s_i + i * kDenTile;
+                double s = acc[q];
+                for (int r = 0; r < nrow; ++r) s = fma(a[r], b[r], s);
+                acc[q] = s;
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int p = t + q * kDenThreads;
+        if (p < np) partial[(int64_t)blockIdx.x * np + p] = acc[q];
+    }
+}
+
+// out[p * nlab + label] = sum over the label's chunks, in chunk order
+__global__ void k_density_reduce(const double *__restrict__ partial, const int32_t *__restrict__ lab_chunk0,
+                                 const int32_t *__restrict__ lab_ids, int np, double *__restrict__ out_p,
+                                 int nlab_p, double *__restrict__ out_n, int nlab_n) {
+    const int u = blockIdx.x;
+    const int c0 = lab_chunk0[u], c1 = lab_chunk0[u + 1];
+    const int label = lab_ids[u];
+    for (int p = threadIdx.x; p < np; p += blockDim.x) {
+        double s = 0.0;
+        for (int c = c0; c < c1; ++c) s += partial[(int64_t)c * np + p];
+        if (label < nlab_p) out_p[(int64_t)p * nlab_p + label] = s;
+        else out_n[(int64_t)p * nlab_n + (label - nlab_p)] = s;
+    }
+}
+
+struct RawSeg {
+    int32_t label;
+    int64_t row_f, row_i, step;
+    int64_t cnt;
+    int32_t sign;
+};
+
+}  // namespace
+
+}  // namespace bsg
+
+using namespace bsg;
+
+extern "C" int bsg_density1b(bsg_ctx *ctx, const bsg_density_tables *dt, const double *vecs, int nstates,
+                             double *p1bopme, double *n1bopme) {
+    if (!ctx) return BSG_ERR_ARG;
+    if (!dt || !vecs || !p1bopme || !n1bopme)
+        return set_err(ctx, BSG_ERR_ARG, "bsg_density1b: null argument");
+    if (nstates < 1 || nstates > kDenMaxStates)
+        return set_err(ctx, BSG_ERR_ARG, "bsg_density1b: nstates must be 1..32");
+    const int ns = nstates, np = ns * ns;
+    const int64_t dim = ctx->dim;
+    const int nl_p = ctx->t.nhsps_pl, nq_p = ctx->t.nhsps_pl + ctx->t.nhsps_pr;
+    const int nl_n = ctx->t.nhsps_nl, nq_n = ctx->t.nhsps_nl + ctx->t.nhsps_nr;
+    const int nlab_p = nq_p * nq_p, nlab_n = nq_n * nq_n;
+    std::memset(p1bopme, 0, sizeof(double) * (size_t)np * nlab_p);
+    std::memset(n1bopme, 0, sizeof(double) * (size_t)np * nlab_n);
+    int st = cuda_check(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+    if (st) return st;
+
+    // pstart / nstart (host copies of the uploaded tables)
+    std::vector<int64_t> pstart(ctx->t.nsd_p), nstart(ctx->t.nsd_n);
+    cudaError_t e = cudaMemcpy(pstart.data(), ctx->raw[0].p, 8 * pstart.size(), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(nstart.data(), ctx->raw[1].p, 8 * nstart.size(), cudaMemcpyDeviceToHost);
+    if ((st = cuda_check(ctx, e, "bsg_density1b: table copy"))) return st;
+
+    // ---- segments: one per (bundle, jump), validated
+    std::vector<RawSeg> raw;
+    auto comb = [](int lab, int nl, int nq) -> int {
+        if (lab < 0) return -lab <= nl ? -lab - 1 : -1;
+        return (lab > 0 && lab <= nq - nl) ? nl + lab - 1 : -1;
+    };
+    for (int64_t b = 0; b < dt->nbundles; ++b) {
+        const int op = dt->optype[b], hc = dt->hchar[b];
+        if (op != BSG_OP_P1B && op != BSG_OP_N1B)
+            return set_err(ctx, BSG_ERR_BAD_TABLE, "bsg_density1b: bundle " + std::to_string(b + 1) + " has an optype other than P1B/N1B");
+        if (hc != BSG_H_FWD && hc != BSG_H_BWD && hc != BSG_H_HERM)
+            return set_err(ctx, BSG_ERR_BAD_TABLE, "bsg_density1b: bad hchar in bundle " + std::to_string(b + 1));
+        const bool pro = op == BSG_OP_P1B;
+        const int64_t cs = dt->cstride[b];
+        const int64_t j0 = pro ? dt->pxstart[b] : dt->nxstart[b], j1 = pro ? dt->pxend[b] : dt->nxend[b];
+        const int64_t c0 = pro ? dt->nxstart[b] : dt->pxstart[b], c1 = pro ? dt->nxend[b] : dt->pxend[b];
+        const int64_t njumps = pro ? dt->np1b : dt->nn1b;
+        const int64_t nconj = pro ? ctx->t.nsd_n : ctx->t.nsd_p;
+        if (cs < 1 || j0 < 1 || j1 > njumps || c0 < 1 || c1 > nconj)
+            return set_err(ctx, BSG_ERR_OOB_INDEX, "bsg_density1b: bundle " + std::to_string(b + 1) + " range outside its table");
+        if (j1 < j0 || c1 < c0) continue;
+        const int64_t nc = (c1 + cs - c0) / cs;
+        int64_t first, step;
+        if (pro) {
+            // statei = isd + (nstart(c0 - cs + 1) - 1) + cs * k, k = 1..nc
+            const int64_t a = c0 - cs + 1;
+            if (a < 1) return set_err(ctx, BSG_ERR_OOB_INDEX, "bsg_density1b: P1B conjugate start below 1");
+            first = nstart[a - 1] - 1 + cs;   // + isd, 1-based
+            step = cs;
+        } else {
+            // statei = isd + pstart(c0) + pstride * (k - 1)
+            first = pstart[c0 - 1];
+            step = nc > 1 ? pstart[c0 - 1 + cs] - pstart[c0 - 1] : 0;
+        }
+        const int64_t *isd = pro ? dt->p1b_isd : dt->n1b_isd, *fsd = pro ? dt->p1b_fsd : dt->n1b_fsd;
+        const int16_t *cop = pro ? dt->p1b_cop : dt->n1b_cop, *dop = pro ? dt->p1b_dop : dt->n1b_dop;
+        const int8_t *ph = pro ? dt->p1b_phase : dt->n1b_phase;
+        const int nl = pro ? nl_p : nl_n, nq = pro ? nq_p : nq_n;
+        for (int64_t j = j0 - 1; j < j1; ++j) {
+            const int qc = comb(cop[j], nl, nq), qd = comb(dop[j], nl, nq);
+            if (qc < 0 || qd < 0)
+                return set_err(ctx, BSG_ERR_OOB_INDEX, "bsg_density1b: jump " + std::to_string(j + 1) + " label outside nhsps");
+            if (ph[j] != 1 && ph[j] != -1)
+                return set_err(ctx, BSG_ERR_BAD_TABLE, "bsg_density1b: jump " + std::to_string(j + 1) + " phase not +-1");
+            const int64_t ri = isd[j] + first - 1, rf = fsd[j] + first - 1;   // 0-based
+            const int64_t li = ri + step * (nc - 1), lf = rf + step * (nc - 1);
+            if (std::min({ri, rf, li, lf}) < 0 || std::max({ri, rf, li, lf}) >= dim)
+                return set_err(ctx, BSG_ERR_OOB_INDEX, "bsg_density1b: jump " + std::to_string(j + 1) + " reaches a state outside the basis");
+            RawSeg s;
+            const bool bwd = hc == BSG_H_BWD;
+            s.label = (pro ? 0 : nlab_p) + (bwd ? qd * nq + qc : qc * nq + qd);
+            s.row_f = bwd ? ri : rf;
+            s.row_i = bwd ? rf : ri;
+            s.step = step;
+            s.cnt = nc;
+            s.sign = ph[j];
+            raw.push_back(s);
+        }
+    }
+    std::stable_sort(raw.begin(), raw.end(), [](const RawSeg &a, const RawSeg &b) { return a.label < b.label; });
+    int64_t total = 0;
+    for (auto &s : raw) total += s.cnt;
+    if (total == 0) return BSG_OK;
+
+    // ---- chunks of about `per` rows, one label each
+    const int64_t per = std::max<int64_t>(1024, std::min<int64_t>(1 << 20, total / (148 * 16) + 1));
+    std::vector<DSeg> segs;
+    std::vector<DChunk> chunks;
+    std::vector<int32_t> lab_chunk0, lab_ids;
+    int cur_label = -1;
+    for (const RawSeg &r : raw) {
+        int64_t done = 0;
+        while (done < r.cnt) {
+            if (r.label != cur_label || chunks.back().nitems >= per) {
+                if (r.label != cur_label) {
+                    lab_chunk0.push_back((int32_t)chunks.size());
+                    lab_ids.push_back(r.label);
+                    cur_label = r.label;
+                }
+                DChunk c;
+                c.seg0 = c.seg1 = (int32_t)segs.size();
+                c.nitems = 0;
+                c.label = r.label;
+                chunks.push_back(c);
+            }
+            DChunk &c = chunks.back();
+            const int64_t take = std::min<int64_t>(r.cnt - done, per - c.nitems);
+            DSeg d;
+            d.row_f = r.row_f + done * r.step;
+            d.row_i = r.row_i + done * r.step;
+            d.step = r.step;
+            d.cnt = (int32_t)take;
+            d.item0 = c.nitems;
+            d.sign = r.sign;
+            d.pad = 0;
+            segs.push_back(d);
+            c.seg1 = (int32_t)segs.size();
+            c.nitems += (int32_t)take;
+            done += take;
+        }
+    }
+    lab_chunk0.push_back((int32_t)chunks.size());
+    if (chunks.size() > (size_t)INT32_MAX / 2 || segs.size() > (size_t)INT32_MAX / 2)
+        return set_err(ctx, BSG_ERR_UNSUPPORTED, "bsg_density1b: too many segments");
+
+    // ---- device work
+    DevBuf d_cols, d_x, d_segs, d_chunks, d_part, d_l0, d_lid, d_outp, d_outn;
+    auto release = [&]() {
+        dev_free(d_cols); dev_free(d_x); dev_free(d_segs); dev_free(d_chunks); dev_free(d_part);
+        dev_free(d_l0); dev_free(d_lid); dev_free(d_outp); dev_free(d_outn);
+    };
+    const size_t vbytes = sizeof(double) * (size_t)dim * ns;
+    if ((st = dev_alloc(ctx, d_cols, vbytes)) || (st = dev_alloc(ctx, d_x, vbytes)) ||
+        (st = upload(ctx, d_segs, segs.data(), sizeof(DSeg) * segs.size())) ||
+        (st = upload(ctx, d_chunks, chunks.data(), sizeof(DChunk) * chunks.size())) ||
+        (st = dev_alloc(ctx, d_part, sizeof(double) * (size_t)np * chunks.size())) ||
+        (st = upload(ctx, d_l0, lab_chunk0.data(), sizeof(int32_t) * lab_chunk0.size())) ||
+        (st = upload(ctx, d_lid, lab_ids.data(), sizeof(int32_t) * lab_ids.size())) ||
+        (st = dev_alloc(ctx, d_outp, sizeof(double) * (size_t)np * std::max(1, nlab_p))) ||
+        (st = dev_alloc(ctx, d_outn, sizeof(double) * (size_t)np * std::max(1, nlab_n)))) {
+        release();
+        return st;
+    }
+    cudaStream_t s = ctx->stream;
+    e = cudaMemcpyAsync(d_cols.p, vecs, vbytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_outp.p, 0, d_outp.bytes, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_outn.p, 0, d_outn.bytes, s);
+    if (e == cudaSuccess) {
+        k_interleave<<<148 * 8, 256, 0, s>>>((const double *)d_cols.p, (double *)d_x.p, dim, ns);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+        k_density_chunks<<<(unsigned)chunks.size(), kDenThreads, 0, s>>>(
+            (const DSeg *)d_segs.p, (const DChunk *)d_chunks.p, (const double *)d_x.p, ns, (double *)d_part.p);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+        k_density_reduce<<<(unsigned)lab_ids.size(), 256, 0, s>>>(
+            (const double *)d_part.p, (const int32_t *)d_l0.p, (const int32_t *)d_lid.p, np,
+            (double *)d_outp.p, nlab_p, (double *)d_outn.p, nlab_n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && nlab_p)
+        e = cudaMemcpyAsync(p1bopme, d_outp.p, sizeof(double) * (size_t)np * nlab_p, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && nlab_n)
+        e = cudaMemcpyAsync(n1bopme, d_outn.p, sizeof(double) * (size_t)np * nlab_n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    st = cuda_check(ctx, e, "bsg_density1b");
+    release();
+    return st;
+}

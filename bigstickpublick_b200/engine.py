@@ -164,6 +164,31 @@ class Hamiltonian:
         self._check(st, "bsg_grad")
         return out
 
+    def density1b(self, vecs, density_tables=None):
+        """m-scheme one-body transition densities of every pair of the states
+        `vecs` (dim x k, k <= 32): {'p': D_p, 'n': D_n} with
+        D[f, i, c, d] = <f| a+_c a_d |i>, c and d the combined s.p. indices of
+        the builder (``extra['sp_orb_p']`` etc.).  `density_tables`: a
+        ``bsg_density_tables`` (default: the builder's own, from these
+        tables)."""
+        v = np.asarray(vecs, dtype=np.float64)
+        if v.ndim == 1:
+            v = v[:, None]
+        if v.shape[0] != self.dim:
+            raise ValueError("vectors do not match the basis")
+        cols = np.ascontiguousarray(v.T)  # (k, dim): dim x k column-major
+        ns = cols.shape[0]
+        s = self.tables.s
+        nqp = int(s["nhsps_pl"] + s["nhsps_pr"])
+        nqn = int(s["nhsps_nl"] + s["nhsps_nr"])
+        dp = np.zeros((ns, ns, nqp, nqp))
+        dn = np.zeros((ns, ns, nqn, nqn))
+        dt = density_tables if density_tables is not None else self.tables.density_ctypes()
+        st = self.lib.bsg_density1b(self.h, C.byref(dt), cols.ctypes.data_as(_abi.f64p), ns,
+                                    dp.ctypes.data_as(_abi.f64p), dn.ctypes.data_as(_abi.f64p))
+        self._check(st, "bsg_density1b")
+        return {"p": dp, "n": dn}
+
 
 def angular_momentum_isospin(spec, vecs, device=0):
     """J and T of the states `vecs` (dim x k, columns normalized, in the basis

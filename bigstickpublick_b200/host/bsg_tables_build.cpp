@@ -495,6 +495,10 @@ struct Built {
     std::vector<int32_t> ps_jz, ps_par, ns_jz, ns_par, ps_conj;
     std::vector<int32_t> spo_p, spm_p, spo_n, spm_n;
     Pairs ppairs, npairs, pnpairs;
+    // one-body density jumps (Delta Jz = 0 sector jumps) and their bundles
+    Jumps1 dp1, dn1;
+    std::vector<int32_t> d_optype, d_hchar;
+    std::vector<int64_t> d_pxstart, d_pxend, d_nxstart, d_nxend, d_cstride;
     // chain-rule bookkeeping: per matrix element, list of (tbme line, coef)
     std::vector<std::vector<std::pair<int, double>>> jac_pp, jac_nn, jac_pn;
     std::vector<std::vector<std::pair<int, double>>> jspe_pp, jspe_nn, jspe_pn;
@@ -871,6 +875,52 @@ int build(const bsg_model_spec *s, Built &B) {
             if (sj.njumps > 0) B.n2sj.push_back(sj);
         }
 
+    // ---- one-body density jumps (set1bsectorjumps + master1bodyjumps for
+    // densities, src/bdenslib1.f90:190-213): every sector jump is -> fs
+    // (is >= fs) that keeps Jz, parity and the conjugate sector, all
+    // a+_i a_k with i, k of equal m, a+_k a_k included.  A proton jump range
+    // is paired with the conjugate neutron SDs (P1B), a neutron jump range
+    // with the conjugate proton SDs (N1B); is > fs also gets a 'b' bundle,
+    // which covers the reverse direction through the same jumps.
+    {
+        auto dadd = [&](int op, int hc, int64_t px0, int64_t px1, int64_t nx0, int64_t nx1) {
+            B.d_optype.push_back(op); B.d_hchar.push_back(hc);
+            B.d_pxstart.push_back(px0); B.d_pxend.push_back(px1);
+            B.d_nxstart.push_back(nx0); B.d_nxend.push_back(nx1);
+            B.d_cstride.push_back(1);
+        };
+        auto same_kind = [&](const SpeciesBasis &sb, int a, int b) {
+            return sb.sectors[a].jz2 == sb.sectors[b].jz2 && sb.sectors[a].pidx == sb.sectors[b].pidx;
+        };
+        if (s->np >= 1)
+            for (int is = 0; is < nps; ++is)
+                for (int fs = 0; fs <= is; ++fs) {
+                    if (!same_kind(B.pb, is, fs) || pconj[is] != pconj[fs]) continue;
+                    const int64_t j0 = (int64_t)B.dp1.isd.size();
+                    const int64_t nj = gen1(B.pb, B.pstart, is, fs, B.dp1);
+                    if (nj == 0) continue;
+                    const Sector &ns = B.nb.sectors[pconj[is]];
+                    dadd(BSG_OP_P1B, BSG_H_FWD, j0 + 1, j0 + nj, ns.xsdstart, ns.xsdend);
+                    if (is != fs) dadd(BSG_OP_P1B, BSG_H_BWD, j0 + 1, j0 + nj, ns.xsdstart, ns.xsdend);
+                }
+        // a proton SD combines with one neutron sector (no truncation), so
+        // a neutron sector jump shares its conjugate protons only with itself
+        if (s->nn >= 1)
+            for (int in = 0; in < nns; ++in) {
+                std::vector<int> psecs;
+                for (int ip = 0; ip < nps; ++ip)
+                    if (pconj[ip] == in) psecs.push_back(ip);
+                if (psecs.empty()) continue;
+                const int64_t j0 = (int64_t)B.dn1.isd.size();
+                const int64_t nj = gen1(B.nb, B.nstart, in, in, B.dn1);
+                if (nj == 0) continue;
+                for (int ip : psecs) {
+                    const Sector &ps = B.pb.sectors[ip];
+                    dadd(BSG_OP_N1B, BSG_H_FWD, ps.xsdstart, ps.xsdend, j0 + 1, j0 + nj);
+                }
+            }
+    }
+
     // ---- single-particle energies per SD when call_spe (makespeme)
     if (call_spe) {
         B.pspe_h.assign(nsdp, 0.0f);
@@ -1048,6 +1098,18 @@ int bsg_host_build(const bsg_model_spec *spec, bsg_host_tables **out) {
     h->npairs_pp = (int64_t)B->ppairs.list.size();
     h->npairs_nn = (int64_t)B->npairs.list.size();
     h->npairs_pn = (int64_t)B->pnpairs.list.size();
+    bsg_density_tables &d = h->dt;
+    d.np1b = (int64_t)B->dp1.isd.size();
+    d.p1b_isd = ptr_or_null(B->dp1.isd); d.p1b_fsd = ptr_or_null(B->dp1.fsd);
+    d.p1b_cop = ptr_or_null(B->dp1.cop); d.p1b_dop = ptr_or_null(B->dp1.dop); d.p1b_phase = ptr_or_null(B->dp1.phase);
+    d.nn1b = (int64_t)B->dn1.isd.size();
+    d.n1b_isd = ptr_or_null(B->dn1.isd); d.n1b_fsd = ptr_or_null(B->dn1.fsd);
+    d.n1b_cop = ptr_or_null(B->dn1.cop); d.n1b_dop = ptr_or_null(B->dn1.dop); d.n1b_phase = ptr_or_null(B->dn1.phase);
+    d.nbundles = (int64_t)B->d_optype.size();
+    d.optype = ptr_or_null(B->d_optype); d.hchar = ptr_or_null(B->d_hchar);
+    d.pxstart = ptr_or_null(B->d_pxstart); d.pxend = ptr_or_null(B->d_pxend);
+    d.nxstart = ptr_or_null(B->d_nxstart); d.nxend = ptr_or_null(B->d_nxend);
+    d.cstride = ptr_or_null(B->d_cstride);
     h->priv = B;
     *out = h;
     return BSG_OK;

@@ -179,6 +179,16 @@ _TABLE_FIELDS = [
     ("pxstart", "i8", "nbundles"), ("pxend", "i8", "nbundles"), ("nxstart", "i8", "nbundles"),
     ("nxend", "i8", "nbundles"), ("cstride", "i8", "nbundles"),
 ]
+# one-body density tables (bsg_density_tables): name, dtype, length field
+_DENSITY_FIELDS = [
+    ("p1b_isd", "i8", "np1b"), ("p1b_fsd", "i8", "np1b"), ("p1b_cop", "i2", "np1b"),
+    ("p1b_dop", "i2", "np1b"), ("p1b_phase", "i1", "np1b"),
+    ("n1b_isd", "i8", "nn1b"), ("n1b_fsd", "i8", "nn1b"), ("n1b_cop", "i2", "nn1b"),
+    ("n1b_dop", "i2", "nn1b"), ("n1b_phase", "i1", "nn1b"),
+    ("optype", "i4", "nbundles"), ("hchar", "i4", "nbundles"),
+    ("pxstart", "i8", "nbundles"), ("pxend", "i8", "nbundles"), ("nxstart", "i8", "nbundles"),
+    ("nxend", "i8", "nbundles"), ("cstride", "i8", "nbundles"),
+]
 _CTYPES = {"i1": C.c_int8, "i2": C.c_int16, "i4": C.c_int32, "i8": C.c_int64,
            "f4": C.c_float, "f8": C.c_double, "u8": C.c_uint64}
 
@@ -218,6 +228,19 @@ class Tables:
             else:
                 setattr(t, name, arr.ctypes.data_as(C.POINTER(_CTYPES[dt])))
         self._c = t
+        return t
+
+    def density_ctypes(self):
+        """``bsg_density_tables`` view of the one-body density jumps and
+        P1B/N1B bundles (pointers into ``extra['density']``)."""
+        d = self.extra["density"]
+        t = _abi.BsgDensityTables()
+        for k in ("np1b", "nn1b", "nbundles"):
+            setattr(t, k, int(d[k]))
+        for name, dt, _ in _DENSITY_FIELDS:
+            arr = d[name]
+            setattr(t, name, arr.ctypes.data_as(C.POINTER(_CTYPES[dt])) if arr.size else None)
+        self._dc = t
         return t
 
 
@@ -266,6 +289,11 @@ def build_tables(spec: ModelSpec) -> Tables:
             "sd_bits_p": _np_from(h.sd_bits_p, t.nsd_p, "u8"),
             "sd_bits_n": _np_from(h.sd_bits_n, t.nsd_n, "u8"),
         }
+        d = h.dt
+        dens = {"np1b": d.np1b, "nn1b": d.nn1b, "nbundles": d.nbundles}
+        for name, dt, nfield in _DENSITY_FIELDS:
+            dens[name] = _np_from(getattr(d, name), dens[nfield], dt)
+        extra["density"] = dens
         jac = {}
         ntb = max(1, len(spec.tbme))
         for kind, nm in ((0, "pp"), (1, "nn"), (2, "pn")):

@@ -202,6 +202,48 @@ int  bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const double *pivot_
 int  bsg_grad(bsg_ctx *ctx, const double *evecs, int nstates,
               double *dpp, double *dnn, double *dpn, double *dspe_p, double *dspe_n);
 
+/* ---- one-body densities: replaces master_density1b_bundled
+ *      (src/bdenslib1.f90:1506-1607), i.e. applyP1Bdenbundled_g and
+ *      applyN1Bdenbundled_g (src/bdenslib3.f90:14-311), for every pair of
+ *      nstates states in one call.  The tables are the one-body jumps that
+ *      master1bodyjumps builds for densities (Delta Jz = 0 sector jumps,
+ *      a+_c a_c included) in the jumpNbody arrays' types, bundled as the
+ *      reference's P1B / N1B opbundles:
+ *        P1B: jumps pxstart..pxend of p1b_*; conjugate neutron SDs
+ *             nxstart..nxend step cstride; statei = p1b_isd + nstart(...)
+ *             exactly as src/bdenslib3.f90:58-100 indexes it;
+ *        N1B: jumps nxstart..nxend of n1b_*; conjugate proton SDs
+ *             pxstart..pxend step cstride, pstride = pstart(pxstart+cstride)
+ *             - pstart(pxstart); statei = n1b_isd + pstart(pxstart) +
+ *             pstride*(k-1) (src/bdenslib3.f90:206-265).
+ *      hchar 'f'/'h' adds psi_f(statef) psi_i(statei) phase to (cop, dop);
+ *      'b' adds psi_f(statei) psi_i(statef) phase to (dop, cop).
+ *      vecs: host fp64, dim x nstates column-major, nstates <= 32.
+ *      Outputs (host fp64, zeroed first):
+ *        p1bopme[((f*nstates + i)*nqp + c)*nqp + d] = <f| a+_c a_d |i>
+ *      with nqp = nhsps_pl + nhsps_pr and c, d the combined s.p. index of a
+ *      signed label (-l -> l-1 for l = 1..nhsps_pl, +r -> nhsps_pl + r - 1);
+ *      n1bopme likewise with nqn = nhsps_nl + nhsps_nr.  The sum over each
+ *      label runs in a fixed order: results are bitwise repeatable. ---- */
+#define BSG_OP_P1B 5
+#define BSG_OP_N1B 6
+typedef struct bsg_density_tables {
+    int64_t np1b;
+    const int64_t *p1b_isd, *p1b_fsd;
+    const int16_t *p1b_cop, *p1b_dop;
+    const int8_t  *p1b_phase;
+    int64_t nn1b;
+    const int64_t *n1b_isd, *n1b_fsd;
+    const int16_t *n1b_cop, *n1b_dop;
+    const int8_t  *n1b_phase;
+    int64_t nbundles;
+    const int32_t *optype;             /* BSG_OP_P1B or BSG_OP_N1B           */
+    const int32_t *hchar;              /* 'f', 'b', 'h'                      */
+    const int64_t *pxstart, *pxend, *nxstart, *nxend, *cstride;
+} bsg_density_tables;
+int  bsg_density1b(bsg_ctx *ctx, const bsg_density_tables *dt, const double *vecs, int nstates,
+                   double *p1bopme, double *n1bopme);
+
 /* ---- batched systems: many independent Hamiltonians of uneven dimension
  *      (the reference runs one per process).  bsg_batch_applyh applies all of
  *      them in one persistent launch whose CTAs pull (system, row tile) work

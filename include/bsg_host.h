@@ -17,6 +17,9 @@
  *                    (iladd-1)*niradd + iradd; hermitian half isd >= fsd on
  *                    diagonal two-body blocks)
  *   opbundles        src/bparallel_opbundles.f90:36-708
+ *   density jumps    src/bdenslib1.f90:190-213 (set1bsectorjumps,
+ *                    master1bodyjumps) with P1B/N1B bundles as read by
+ *                    src/bdenslib3.f90:14-311
  *   jump sort        src/bsortjumpslib.f90:21-290 (shell sort, fixed strides)
  *   matrix elements  src/btbme.f90:1209-1551, src/btbmepn.f90:177-587,
  *                    src/binput_tbme.f90:898-2027, src/bsppot.f90:20-238
@@ -73,6 +76,9 @@ typedef struct bsg_host_tables {
     /* pair bookkeeping for the adjoint chain rule (coupled <- uncoupled) */
     int64_t npairs_pp, npairs_nn, npairs_pn;
     void *priv;                            /* builder internals            */
+    /* one-body density jumps and P1B/N1B bundles for bsg_density1b
+     * (master1bodyjumps for densities, src/bdenslib1.f90:190-213) */
+    bsg_density_tables dt;
 } bsg_host_tables;
 
 int  bsg_host_build(const bsg_model_spec *spec, bsg_host_tables **out);

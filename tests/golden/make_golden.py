@@ -5,7 +5,8 @@ Reads (from the reference checkout given as argv[1], default /root/reference):
   examples/sd/usdb.int          USDB interaction (63 TBMEs + 3 SPEs)
   examples/sd/input.mg25ref     4 protons, 5 neutrons, 2Jz = 1, scaling 1 18 25 0.3
   examples/sd/input.mg25altwfn  same nucleus, scaling 0 1 1 1 (xspe = 0)
-  examples/sd/output/mg25ref.res, mg25alt.res   10 lowest energies, J, T (5 decimals)
+  examples/sd/output/mg25ref.res, mg25alt.res   10 lowest energies, J, T (5 decimals) and
+                                                every one-body density block (5 decimals)
 and writes the numbers as JSON.  Run once in a checkout that has the reference;
 the JSON is what the tests read (the reference is not needed at test time).
 """
@@ -58,6 +59,38 @@ def read_diag_density(path):
     return out
 
 
+def read_all_densities(path):
+    """Every one-body density block the reference prints: initial and final
+    state (number, 2J, 2T), Jt, and the rows [a, b, rho_Tt=0, rho_Tt=1]."""
+    lines = open(path).read().splitlines()
+    blocks = []
+    i = 0
+    while i < len(lines):
+        m = re.match(r"\s*Initial state #\s+(\d+).*2xJ, 2xT =\s+(\d+)\s+(\d+)", lines[i])
+        f = re.match(r"\s*Final state\s+#\s+(\d+).*2xJ, 2xT =\s+(\d+)\s+(\d+)", lines[i + 1]) \
+            if m and i + 1 < len(lines) else None
+        if not f:
+            i += 1
+            continue
+        i += 2
+        while i < len(lines):
+            jt = re.match(r"\s*Jt =\s+(\d+), Tt = 0\s+1", lines[i])
+            if not jt:
+                break
+            rows = []
+            i += 1
+            while i < len(lines):
+                t = lines[i].split()
+                if len(t) != 4 or not t[0].isdigit():
+                    break
+                rows.append([int(t[0]), int(t[1]), float(t[2]), float(t[3])])
+                i += 1
+            blocks.append({"i": int(m.group(1)), "J2i": int(m.group(2)), "T2i": int(m.group(3)),
+                           "f": int(f.group(1)), "J2f": int(f.group(2)), "T2f": int(f.group(3)),
+                           "Jt": int(jt.group(1)), "rho": rows})
+    return blocks
+
+
 def read_input(path):
     toks = [ln.split("!")[0].split() for ln in open(path)]
     toks = [t for t in toks if t]
@@ -81,10 +114,12 @@ def main():
         run = read_input(os.path.join(ex, inp))
         run.update({"states": states, "reference_iterations": iters,
                     "res_file": f"examples/sd/output/{name}.res",
-                    "density_jt0": read_diag_density(os.path.join(ex, "output", name + ".res"))})
+                    "density_jt0": read_diag_density(os.path.join(ex, "output", name + ".res")),
+                    "densities": read_all_densities(os.path.join(ex, "output", name + ".res"))})
         out["runs"][name] = run
     with open(os.path.join(HERE, "mg25.json"), "w") as f:
-        json.dump(out, f, indent=1)
+        json.dump(out, f, separators=(",", ":"))
+        f.write("\n")
     print("wrote", os.path.join(HERE, "mg25.json"))
 
 

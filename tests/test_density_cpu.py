@@ -1,0 +1,142 @@
+"""One-body densities on the CPU: the builder's density jumps and P1B/N1B
+bundles against second quantization from the SD bits, and the Jt/Tt coupling
+(bigstickpublick_b200.densities, restating coupled_densities of
+src/bdensities.f90:69-181) against the properties the reference relies on:
+the particle-number sum rule it checks (src/bdenslib1.f90:300-330), the
+time-reversal relation it uses to fill f > i (src/bdenslib1.f90:350-362), and
+independence of the reduced densities from the Jz of the basis."""
+import numpy as np
+import pytest
+
+from bigstickpublick_b200 import densities as D
+from bigstickpublick_b200 import model
+import oracle
+from oracle import density1b as od
+
+SYSTEMS = [(2, 2, 0, "sd"), (3, 2, 1, "sd"), (1, 0, 1, "sd"), (0, 3, 3, "sd"), (2, 1, 1, "pf")]
+
+
+def _tables(np_, nn, jz, shell):
+    m = model.sd_model(np_, nn, seed=4, jz2=jz) if shell == "sd" else model.pf_model(np_, nn, seed=4, jz2=jz)
+    return model.build_tables(m)
+
+
+@pytest.mark.parametrize("np_,nn,jz,shell", SYSTEMS)
+def test_density_tables_match_second_quantization(np_, nn, jz, shell):
+    T = _tables(np_, nn, jz, shell)
+    X = np.random.default_rng(1).standard_normal((T.dim, 3))
+    Dp, Dn = od.bundled(T, X)
+    Bp, Bn = od.from_bits(T, X)
+    assert np.abs(Dp - Bp).max() < 1e-12 * max(1.0, np.abs(Bp).max())
+    assert np.abs(Dn - Bn).max() < 1e-12 * max(1.0, np.abs(Bn).max())
+    d = T.extra["density"]
+    assert set(np.unique(d["optype"]).tolist()) <= {5, 6}
+    # the reference indexes conjugate neutron SDs as consecutive nstart values
+    ex = T.extra
+    for i in range(len(ex["nsector_start"])):
+        ns = T.a["nstart"][ex["nsector_start"][i] - 1:ex["nsector_end"][i]]
+        assert (np.diff(ns) == 1).all()
+
+
+def test_cleb_known_values_and_orthogonality():
+    assert abs(D.cleb(1, 1, 1, -1, 0, 0) - np.sqrt(0.5)) < 1e-15
+    assert abs(D.cleb(1, -1, 1, 1, 0, 0) + np.sqrt(0.5)) < 1e-15
+    assert abs(D.cleb(2, 0, 2, 0, 4, 0) - np.sqrt(2.0 / 3.0)) < 1e-15
+    assert D.cleb(2, 0, 2, 0, 2, 0) == 0.0
+    j1, j2 = 5, 3
+    for J in range(abs(j1 - j2), j1 + j2 + 1, 2):
+        for Jp in range(abs(j1 - j2), j1 + j2 + 1, 2):
+            for M in range(-min(J, Jp), min(J, Jp) + 1, 2):
+                s = sum(D.cleb(j1, m1, j2, M - m1, J, M) * D.cleb(j1, m1, j2, M - m1, Jp, M)
+                        for m1 in range(-j1, j1 + 1, 2) if abs(M - m1) <= j2)
+                assert abs(s - (J == Jp)) < 1e-13
+
+
+def _states(spec, k):
+    T = model.build_tables(spec)
+    w, Z = np.linalg.eigh(oracle.dense_from_applyh(T))
+    Z = Z[:, :k]
+    Jq = model.build_tables(model.jsq_spec(spec))
+    Tq = model.build_tables(model.tsq_spec(spec))
+    J = [model.j_from_jsq(float(Z[:, i] @ oracle.applyh(Jq, Z[:, i]))) for i in range(k)]
+    Tv = [model.j_from_jsq(float(Z[:, i] @ oracle.applyh(Tq, Z[:, i]))) for i in range(k)]
+    Dp, Dn = od.bundled(T, Z)
+    return T, w[:k], J, Tv, D.reduced(T, {"p": Dp, "n": Dn}, J, Tv)
+
+
+def test_reduced_densities_sum_rule_time_reversal_and_jz_independence():
+    spe, tb = model.synthetic_interaction(model.SD_ORBITS, 7, spe=model.SD_SYNTH_SPE)
+    k = 8
+    runs = {jz: _states(model.ModelSpec(model.SD_ORBITS, 2, 1, jz, 1, spe, tb), k) for jz in (1, 3)}
+    T, w, J, Tv, red = runs[1]
+    orbj = [o[2] for o in model.SD_ORBITS]
+    # the number check of density1b_compute: sum_a rho_0(a,a) sqrt(2(2ja+1)) / sqrt((2J+1)(2T+1)) = N
+    for i in range(k):
+        b = red[(i + 1, i + 1)][0]
+        n = sum(b[a, a, 0] * np.sqrt(2 * (orbj[a] + 1)) for a in range(3)) / np.sqrt((2 * J[i] + 1) * (2 * Tv[i] + 1))
+        assert abs(n - 3.0) < 1e-6
+    # rho_K(a+b, i->f) = (-1)^(ja-jb+Ji-Jf+Ti-Tf) rho_K(b+a, f->i)
+    for (i, f), blocks in red.items():
+        J2i, J2f = round(2 * J[i - 1]), round(2 * J[f - 1])
+        T2i, T2f = round(2 * Tv[i - 1]), round(2 * Tv[f - 1])
+        for Jt, a in blocks.items():
+            b = red[(f, i)][Jt]
+            for x in range(3):
+                for y in range(3):
+                    ph = (-1) ** (((orbj[x] - orbj[y]) + (J2i - J2f) + (T2i - T2f)) // 2)
+                    assert np.abs(a[x, y] - ph * b[y, x]).max() < 1e-12
+    # the same states in the 2Jz = 3 basis give the same reduced densities
+    # (up to the sign of each eigenvector); float32 matrix elements break
+    # rotational invariance at 1e-7 of H, which moves the eigenvectors by
+    # about 1e-7 / (level spacing >= 0.04 MeV)
+    w3, red3 = runs[3][1], runs[3][4]
+    assert np.abs(w - w3).max() < 1e-5
+    for (i, f), blocks in red.items():
+        other = red3[(i, f)]
+        common = sorted(set(blocks) & set(other))
+        assert common
+        big = max(common, key=lambda jt: np.abs(blocks[jt]).max())
+        kk = np.unravel_index(np.argmax(np.abs(blocks[big])), blocks[big].shape)
+        sgn = np.sign(blocks[big][kk] * other[big][kk])
+        for Jt in common:
+            assert np.abs(blocks[Jt] - sgn * other[Jt]).max() < 5e-5, (i, f, Jt)
+
+
+def test_mg25ref_densities_from_oracle_equal_reference_res():
+    """The oracle chain alone (oracle matvec under ARPACK, oracle density
+    traversal, the coupling) against every density block of
+    examples/sd/output/mg25ref.res: pins the restatement before the GPU."""
+    import json
+    import os
+    from scipy.sparse.linalg import LinearOperator, eigsh
+    gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "mg25.json")))
+    r = gold["runs"]["mg25ref"]
+    ss, ts = model.ModelSpec.scaling(*r["scaling"])
+    orbits = [tuple(o) for o in gold["orbits"]]
+    spec = model.ModelSpec(orbits, r["np"], r["nn"], r["jz2"], 1, gold["spe"], [tuple(t) for t in gold["tbme"]], ss, ts)
+    T = model.build_tables(spec)
+    op = LinearOperator((T.dim, T.dim), dtype=np.float64,
+                        matvec=lambda v: oracle.applyh(T, np.ascontiguousarray(v, dtype=np.float64)))
+    w, Z = eigsh(op, k=10, which="SA", tol=1e-12, v0=np.ones(T.dim))
+    o = np.argsort(w)
+    w, Z = w[o], Z[:, o]
+    assert np.abs(w - np.array([s["E"] for s in r["states"]])).max() < 1.5e-5
+    Jq = model.build_tables(model.jsq_spec(spec))
+    Tq = model.build_tables(model.tsq_spec(spec))
+    J = [model.j_from_jsq(float(Z[:, i] @ oracle.applyh(Jq, Z[:, i]))) for i in range(10)]
+    Tv = [model.j_from_jsq(float(Z[:, i] @ oracle.applyh(Tq, Z[:, i]))) for i in range(10)]
+    Dp, Dn = od.bundled(T, Z)
+    red = D.reduced(T, {"p": Dp, "n": Dn}, J, Tv)
+    sign, big = {}, {}
+    for b in r["densities"]:
+        key = (min(b["i"], b["f"]), max(b["i"], b["f"]))
+        for a, c, t0, t1 in b["rho"]:
+            for tt, g in ((0, t0), (1, t1)):
+                if abs(g) > big.get(key, 0.0):
+                    big[key] = abs(g)
+                    sign[key] = np.sign(red[(b["i"], b["f"])][b["Jt"]][a - 1, c - 1, tt] * g)
+    assert len(r["densities"]) == 440
+    for b in r["densities"]:
+        ours = red[(b["i"], b["f"])][b["Jt"]] * sign[(min(b["i"], b["f"]), max(b["i"], b["f"]))]
+        for a, c, t0, t1 in b["rho"]:
+            assert abs(ours[a - 1, c - 1, 0] - t0) < 5e-5 and abs(ours[a - 1, c - 1, 1] - t1) < 5e-5
