@@ -230,6 +230,32 @@ def lanczos_leg(H, tables, args):
     return out
 
 
+def density_leg(H, tables, args, k=10, reps=5):
+    """One-body transition densities of every pair of k states (bsg_density1b):
+    device time of its kernels (CUDA events inside the call) and the call's
+    wall time with host vectors in and host densities out.  The work does not
+    depend on the vector values, so k seeded normalized vectors stand in for
+    eigenvectors."""
+    X = np.random.default_rng(5).standard_normal((tables.dim, k))
+    X /= np.linalg.norm(X, axis=0)
+    X = np.asfortranarray(X)
+    H.density1b(X)  # untimed: first use loads the kernels
+    dev, wall = [], []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        H.density1b(X)
+        wall.append(time.perf_counter() - t0)
+        dev.append(H.stats()["density_ms"])
+    st = H.stats()
+    rows = st["density_rows"]
+    kms = float(np.median(dev))
+    return {"states": k, "pairs": k * k, "rows": rows, "kernel_ms": kms, "e2e_ms": float(np.median(wall)) * 1e3,
+            "launches": st["density_launches"],
+            "fp64_gflop_per_s": 2.0 * rows * k * k / (kms * 1e-3) / 1e9,
+            "gathered_gb_per_s": rows * 2 * k * 8 / (kms * 1e-3) / 1e9,
+            "h2d_bytes": tables.dim * k * 8}
+
+
 def batch_leg(args):
     """Config 4: 256 sd-shell Hamiltonians (seeds 1000..1255, valence Z and N
     uniform in 2..8), one persistent launch per batched matvec, lock-step
@@ -383,6 +409,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-lanczos", action="store_true")
+    ap.add_argument("--no-density", action="store_true")
     ap.add_argument("--lanczos-iters", type=int, default=300)
     ap.add_argument("--block-leg", action="store_true")
     ap.add_argument("--block-iters", type=int, default=20)
@@ -495,6 +522,8 @@ def main():
     }
     if rank == 0 and not args.no_lanczos:
         line["lanczos"] = lanczos_leg(H, tables, args)
+    if rank == 0 and not args.no_density:
+        line["density"] = density_leg(H, tables, args)
     if rank == 0 and args.batch_leg:
         line["batch"] = batch_leg(args)
     if rank == 0 and args.large_leg:

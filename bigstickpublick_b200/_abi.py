@@ -81,6 +81,8 @@ class BsgStats(C.Structure):
         ("n_ops_spe", C.c_int64), ("jump_bytes", C.c_int64), ("derived_bytes", C.c_int64),
         ("n_rows", C.c_int64), ("n_contrib", C.c_int64),
         ("kernel_launches_per_matvec", C.c_int32), ("reserved", C.c_int32),
+        ("density_ms", C.c_double), ("density_rows", C.c_int64),
+        ("density_launches", C.c_int32), ("reserved2", C.c_int32),
     ]
 
 

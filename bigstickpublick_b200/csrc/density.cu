@@ -13,10 +13,10 @@
 // final-state side, first row on the initial-state side, stride, count,
 // phase), sorts the segments by output label and cuts each label's segments
 // into chunks of about the same number of rows.  One CTA per chunk stages
-// 64 rows of all states (interleaved, so a row of all states is contiguous)
-// in shared memory and accumulates the nstates x nstates products in FP64,
-// one (final, initial) pair per thread and pass; a second kernel sums the
-// chunks of each label in chunk order.  No atomics: bitwise repeatable.
+// up to 256 rows of all states (interleaved, so a row of all states is
+// contiguous) in shared memory and accumulates the nstates x nstates products
+// in FP64; a second kernel sums the chunks of each label in chunk order.  No
+// atomics: bitwise repeatable.
 
 #include <algorithm>
 #include <cstring>
@@ -30,7 +30,6 @@ namespace bsg {
 namespace {
 
 constexpr int kDenThreads = 256;
-constexpr int kDenTile = 64;        // rows staged per pass
 constexpr int kDenMaxStates = 32;   // pairs per thread <= 4
 
 struct DSeg {
@@ -59,66 +58,97 @@ __global__ void k_interleave(const double *__restrict__ cols, double *__restrict
     }
 }
 
+// rows of all states staged per pass: tile * ns doubles per side
+__host__ __device__ inline int den_tile(int ns) {
+    int t = (2048 / ns) / 32 * 32;
+    return t < 32 ? 32 : (t > kDenThreads ? kDenThreads : t);
+}
+// shared layout: s_f, s_i [ns rounded up to even][tile + 1] (odd stride: the
+// rows of different states fall in different banks), signs, row indices,
+// and the per-thread partial sums
+inline size_t den_smem(int ns) {
+    const int tile = den_tile(ns), nsp = (ns + 1) & ~1;
+    return sizeof(double) * (size_t)(2 * nsp * (tile + 1) + tile) + 2 * sizeof(int64_t) * tile +
+           sizeof(double) * 4 * kDenThreads;
+}
+
+// One CTA per chunk.  Per pass: the first `tile` threads map the next rows
+// of the chunk to (final row, initial row, sign), walking forward from the
+// segment the previous pass ended in; all threads stage those rows of every
+// state in shared memory; then each thread accumulates a 2 x 2 block of
+// (final, initial) pairs over its share of the rows: the h*h blocks
+// (h = ceil(ns/2)) take G = 256 / (h*h) row groups, summed in group order
+// at the end.
 __global__ void __launch_bounds__(kDenThreads) k_density_chunks(const DSeg *__restrict__ segs,
                                                               const DChunk *__restrict__ chunks,
                                                               const double *__restrict__ x, int ns,
                                                               double *__restrict__ partial) {
-    __shared__ double s_f[kDenTile * kDenMaxStates];
-    __shared__ double s_i[kDenTile * kDenMaxStates];
-    __shared__ int64_t s_rf[kDenTile], s_ri[kDenTile];
-    __shared__ double s_sg[kDenTile];
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int tile = den_tile(ns), ld = tile + 1;
+    const int h = (ns + 1) >> 1, nsp = 2 * h;
+    double *s_f = reinterpret_cast<double *>(smem);
+    double *s_i = s_f + nsp * ld;
+    double *s_sg = s_i + nsp * ld;
+    int64_t *s_rf = reinterpret_cast<int64_t *>(s_sg + tile);
+    int64_t *s_ri = s_rf + tile;
+    double *s_red = reinterpret_cast<double *>(s_ri + tile);
+    __shared__ int s_next;
     const DChunk ch = chunks[blockIdx.x];
     const int t = threadIdx.x;
-    const int np = ns * ns;
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int base = 0; base < ch.nitems; base += kDenTile) {
-        if (t < kDenTile) {
+    const int nbk = h * h, groups = kDenThreads / nbk;
+    const int g = t / nbk, bk = t - g * nbk;
+    const int f0 = 2 * (bk / h), i0 = 2 * (bk % h);
+    // the padding state (ns odd) stays zero
+    if (nsp != ns)
+        for (int r = t; r < ld; r += kDenThreads) { s_f[ns * ld + r] = 0.0; s_i[ns * ld + r] = 0.0; }
+    double a00 = 0.0, a01 = 0.0, a10 = 0.0, a11 = 0.0;
+    int seg = ch.seg0;
+    for (int base = 0; base < ch.nitems; base += tile) {
+        const int nrow = min(tile, ch.nitems - base);
+        if (t < nrow) {
             const int item = base + t;
-            int64_t rf = -1, ri = -1;
-            double sg = 0.0;
-            if (item < ch.nitems) {
-                // last segment of the chunk whose item0 <= item
-                int lo = ch.seg0, hi = ch.seg1 - 1;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (segs[mid].item0 <= item) lo = mid; else hi = mid - 1;
-                }
-                const DSeg sgm = segs[lo];
-                const int64_t c = item - sgm.item0;
-                rf = sgm.row_f + c * sgm.step;
-                ri = sgm.row_i + c * sgm.step;
-                sg = (double)sgm.sign;
-            }
-            s_rf[t] = rf;
-            s_ri[t] = ri;
-            s_sg[t] = sg;
+            int s = seg;
+            while (s + 1 < ch.seg1 && segs[s + 1].item0 <= item) ++s;
+            const DSeg sgm = segs[s];
+            const int64_t c = item - sgm.item0;
+            s_rf[t] = sgm.row_f + c * sgm.step;
+            s_ri[t] = sgm.row_i + c * sgm.step;
+            s_sg[t] = (double)sgm.sign;
+            if (t == nrow - 1) s_next = s;
         }
         __syncthreads();
-        const int nrow = min(kDenTile, ch.nitems - base);
+        seg = s_next;
         for (int e = t; e < nrow * ns; e += kDenThreads) {
             const int r = e / ns, k = e - r * ns;
-            s_f[k * kDenTile + r] = x[s_rf[r] * ns + k];
-            s_i[k * kDenTile + r] = s_sg[r] * x[s_ri[r] * ns + k];
+            s_f[k * ld + r] = x[s_rf[r] * ns + k];
+            s_i[k * ld + r] = s_sg[r] * x[s_ri[r] * ns + k];
         }
         __syncthreads();
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int p = t + q * kDenThreads;
-            if (p < np) {
-                const int f = p / ns, i = p - f * ns;
-                const double *__restrict__ a = s_f + f * kDenTile;
-                const double *__restrict__ b = s_i + i * kDenTile;
-                double s = acc[q];
-                for (int r = 0; r < nrow; ++r) s = fma(a[r], b[r], s);
-                acc[q] = s;
+        if (g < groups) {
+            const double *__restrict__ fa = s_f + f0 * ld, *__restrict__ fb = fa + ld;
+            const double *__restrict__ ia = s_i + i0 * ld, *__restrict__ ib = ia + ld;
+            for (int r = g; r < nrow; r += groups) {
+                const double x0 = fa[r], x1 = fb[r], y0 = ia[r], y1 = ib[r];
+                a00 = fma(x0, y0, a00);
+                a01 = fma(x0, y1, a01);
+                a10 = fma(x1, y0, a10);
+                a11 = fma(x1, y1, a11);
             }
         }
         __syncthreads();
     }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int p = t + q * kDenThreads;
-        if (p < np) partial[(int64_t)blockIdx.x * np + p] = acc[q];
+    s_red[4 * t + 0] = a00;
+    s_red[4 * t + 1] = a01;
+    s_red[4 * t + 2] = a10;
+    s_red[4 * t + 3] = a11;
+    __syncthreads();
+    const int np = ns * ns;
+    for (int p = t; p < np; p += kDenThreads) {
+        const int f = p / ns, i = p - f * ns;
+        const int b = (f >> 1) * h + (i >> 1), sub = ((f & 1) << 1) | (i & 1);
+        double v = 0.0;
+        for (int q = 0; q < groups; ++q) v += s_red[4 * (q * nbk + b) + sub];
+        partial[(int64_t)blockIdx.x * np + p] = v;
     }
 }
 
@@ -300,14 +330,19 @@ extern "C" int bsg_density1b(bsg_ctx *ctx, const bsg_density_tables *dt, const d
     e = cudaMemcpyAsync(d_cols.p, vecs, vbytes, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_outp.p, 0, d_outp.bytes, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_outn.p, 0, d_outn.bytes, s);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, s);
     if (e == cudaSuccess) {
         k_interleave<<<148 * 8, 256, 0, s>>>((const double *)d_cols.p, (double *)d_x.p, dim, ns);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) {
-        k_density_chunks<<<(unsigned)chunks.size(), kDenThreads, 0, s>>>(
-            (const DSeg *)d_segs.p, (const DChunk *)d_chunks.p, (const double *)d_x.p, ns, (double *)d_part.p);
-        e = cudaGetLastError();
+        const size_t sm = den_smem(ns);
+        e = cudaFuncSetAttribute(k_density_chunks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e == cudaSuccess) {
+            k_density_chunks<<<(unsigned)chunks.size(), kDenThreads, sm, s>>>(
+                (const DSeg *)d_segs.p, (const DChunk *)d_chunks.p, (const double *)d_x.p, ns, (double *)d_part.p);
+            e = cudaGetLastError();
+        }
     }
     if (e == cudaSuccess) {
         k_density_reduce<<<(unsigned)lab_ids.size(), 256, 0, s>>>(
@@ -315,11 +350,19 @@ extern "C" int bsg_density1b(bsg_ctx *ctx, const bsg_density_tables *dt, const d
             (double *)d_outp.p, nlab_p, (double *)d_outn.p, nlab_n);
         e = cudaGetLastError();
     }
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, s);
     if (e == cudaSuccess && nlab_p)
         e = cudaMemcpyAsync(p1bopme, d_outp.p, sizeof(double) * (size_t)np * nlab_p, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess && nlab_n)
         e = cudaMemcpyAsync(n1bopme, d_outn.p, sizeof(double) * (size_t)np * nlab_n, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    float ms = 0.0f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    if (e == cudaSuccess) {
+        ctx->stats.density_ms = ms;
+        ctx->stats.density_rows = total;
+        ctx->stats.density_launches = 3;
+    }
     st = cuda_check(ctx, e, "bsg_density1b");
     release();
     return st;

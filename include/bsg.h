@@ -276,6 +276,12 @@ typedef struct bsg_stats {
     int64_t n_contrib;         /* row contributions                            */
     int32_t kernel_launches_per_matvec;
     int32_t reserved;
+    /* last bsg_density1b: device time of its kernels (ms), rows summed
+     * (conjugate SDs over all jumps), launches */
+    double  density_ms;
+    int64_t density_rows;
+    int32_t density_launches;
+    int32_t reserved2;
 } bsg_stats;
 int  bsg_get_stats(const bsg_ctx *ctx, bsg_stats *st);
 
