@@ -233,7 +233,8 @@ def lanczos_leg(H, tables, args):
 def density_leg(H, tables, args, k=10, reps=5):
     """One-body transition densities of every pair of k states (bsg_density1b):
     device time of its kernels (CUDA events inside the call) and the call's
-    wall time with host vectors in and host densities out.  The work does not
+    wall time with host vectors in and host densities out; and a one-body
+    operator applied to the k vectors (bsg_apply1b, device time).  The work does not
     depend on the vector values, so k seeded normalized vectors stand in for
     eigenvectors."""
     X = np.random.default_rng(5).standard_normal((tables.dim, k))
@@ -249,11 +250,22 @@ def density_leg(H, tables, args, k=10, reps=5):
     st = H.stats()
     rows = st["density_rows"]
     kms = float(np.median(dev))
+    # the spin-like one-body operator (isoscalar, J = 1) on the same k vectors
+    nqp = int(tables.s["nhsps_pl"] + tables.s["nhsps_pr"])
+    nqn = int(tables.s["nhsps_nl"] + tables.s["nhsps_nr"])
+    rng = np.random.default_rng(6)
+    P, N = rng.standard_normal((nqp, nqp)), rng.standard_normal((nqn, nqn))
+    H.apply1b(P, N, X)
+    ams = []
+    for _ in range(reps):
+        H.apply1b(P, N, X)
+        ams.append(H.stats()["apply1b_ms"])
     return {"states": k, "pairs": k * k, "rows": rows, "kernel_ms": kms, "e2e_ms": float(np.median(wall)) * 1e3,
             "launches": st["density_launches"],
             "fp64_gflop_per_s": 2.0 * rows * k * k / (kms * 1e-3) / 1e9,
             "gathered_gb_per_s": rows * 2 * k * 8 / (kms * 1e-3) / 1e9,
-            "h2d_bytes": tables.dim * k * 8}
+            "h2d_bytes": tables.dim * k * 8,
+            "apply1b_ms": float(np.median(ams)), "apply1b_vectors": k}
 
 
 def batch_leg(args):

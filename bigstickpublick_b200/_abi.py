@@ -83,6 +83,7 @@ class BsgStats(C.Structure):
         ("kernel_launches_per_matvec", C.c_int32), ("reserved", C.c_int32),
         ("density_ms", C.c_double), ("density_rows", C.c_int64),
         ("density_launches", C.c_int32), ("reserved2", C.c_int32),
+        ("apply1b_ms", C.c_double),
     ]
 
 
@@ -191,6 +192,8 @@ def gpu_lib():
         lib.bsg_grad.restype = C.c_int
         lib.bsg_density1b.argtypes = [vp, C.POINTER(BsgDensityTables), f64p, C.c_int, f64p, f64p]
         lib.bsg_density1b.restype = C.c_int
+        lib.bsg_apply1b.argtypes = [vp, C.POINTER(BsgDensityTables), f64p, f64p, f64p, f64p, C.c_int]
+        lib.bsg_apply1b.restype = C.c_int
         lib.bsg_get_stats.argtypes = [vp, C.POINTER(BsgStats)]
         lib.bsg_get_stats.restype = C.c_int
         lib.bsg_validate_tables.argtypes = [C.POINTER(BsgTables), C.c_char_p, C.c_size_t]

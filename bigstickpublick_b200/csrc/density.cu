@@ -174,6 +174,140 @@ struct RawSeg {
     int32_t sign;
 };
 
+// One segment per (bundle, jump), every index checked: the rows of the
+// conjugate SDs are the arithmetic progressions the reference walks
+// (src/bdenslib3.f90:58-100 for P1B, :206-265 for N1B); 'b' bundles swap the
+// final and initial rows and transpose the label.  Labels are species-combined:
+// protons c*nqp + d, neutrons nqp^2 + c*nqn + d.
+int build_segments(bsg_ctx *ctx, const bsg_density_tables *dt, std::vector<RawSeg> &raw) {
+    const int64_t dim = ctx->dim;
+    const int nl_p = ctx->t.nhsps_pl, nq_p = ctx->t.nhsps_pl + ctx->t.nhsps_pr;
+    const int nl_n = ctx->t.nhsps_nl, nq_n = ctx->t.nhsps_nl + ctx->t.nhsps_nr;
+    const int nlab_p = nq_p * nq_p;
+    int st;
+    // pstart / nstart (host copies of the uploaded tables)
+    std::vector<int64_t> pstart(ctx->t.nsd_p), nstart(ctx->t.nsd_n);
+    cudaError_t e = cudaMemcpy(pstart.data(), ctx->raw[0].p, 8 * pstart.size(), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(nstart.data(), ctx->raw[1].p, 8 * nstart.size(), cudaMemcpyDeviceToHost);
+    if ((st = cuda_check(ctx, e, "density tables: table copy"))) return st;
+
+    // ---- segments: one per (bundle, jump), validated
+    auto comb = [](int lab, int nl, int nq) -> int {
+        if (lab < 0) return -lab <= nl ? -lab - 1 : -1;
+        return (lab > 0 && lab <= nq - nl) ? nl + lab - 1 : -1;
+    };
+    for (int64_t b = 0; b < dt->nbundles; ++b) {
+        const int op = dt->optype[b], hc = dt->hchar[b];
+        if (op != BSG_OP_P1B && op != BSG_OP_N1B)
+            return set_err(ctx, BSG_ERR_BAD_TABLE, "density tables: bundle " + std::to_string(b + 1) + " has an optype other than P1B/N1B");
+        if (hc != BSG_H_FWD && hc != BSG_H_BWD && hc != BSG_H_HERM)
+            return set_err(ctx, BSG_ERR_BAD_TABLE, "density tables: bad hchar in bundle " + std::to_string(b + 1));
+        const bool pro = op == BSG_OP_P1B;
+        const int64_t cs = dt->cstride[b];
+        const int64_t j0 = pro ? dt->pxstart[b] : dt->nxstart[b], j1 = pro ? dt->pxend[b] : dt->nxend[b];
+        const int64_t c0 = pro ? dt->nxstart[b] : dt->pxstart[b], c1 = pro ? dt->nxend[b] : dt->pxend[b];
+        const int64_t njumps = pro ? dt->np1b : dt->nn1b;
+        const int64_t nconj = pro ? ctx->t.nsd_n : ctx->t.nsd_p;
+        if (cs < 1 || j0 < 1 || j1 > njumps || c0 < 1 || c1 > nconj)
+            return set_err(ctx, BSG_ERR_OOB_INDEX, "density tables: bundle " + std::to_string(b + 1) + " range outside its table");
+        if (j1 < j0 || c1 < c0) continue;
+        const int64_t nc = (c1 + cs - c0) / cs;
+        int64_t first, step;
+        if (pro) {
+            // statei = isd + (nstart(c0 - cs + 1) - 1) + cs * k, k = 1..nc
+            const int64_t a = c0 - cs + 1;
+            if (a < 1) return set_err(ctx, BSG_ERR_OOB_INDEX, "density tables: P1B conjugate start below 1");
+            first = nstart[a - 1] - 1 + cs;   // + isd, 1-based
+            step = cs;
+        } else {
+            // statei = isd + pstart(c0) + pstride * (k - 1)
+            first = pstart[c0 - 1];
+            step = nc > 1 ? pstart[c0 - 1 + cs] - pstart[c0 - 1] : 0;
+        }
+        const int64_t *isd = pro ? dt->p1b_isd : dt->n1b_isd, *fsd = pro ? dt->p1b_fsd : dt->n1b_fsd;
+        const int16_t *cop = pro ? dt->p1b_cop : dt->n1b_cop, *dop = pro ? dt->p1b_dop : dt->n1b_dop;
+        const int8_t *ph = pro ? dt->p1b_phase : dt->n1b_phase;
+        const int nl = pro ? nl_p : nl_n, nq = pro ? nq_p : nq_n;
+        for (int64_t j = j0 - 1; j < j1; ++j) {
+            const int qc = comb(cop[j], nl, nq), qd = comb(dop[j], nl, nq);
+            if (qc < 0 || qd < 0)
+                return set_err(ctx, BSG_ERR_OOB_INDEX, "density tables: jump " + std::to_string(j + 1) + " label outside nhsps");
+            if (ph[j] != 1 && ph[j] != -1)
+                return set_err(ctx, BSG_ERR_BAD_TABLE, "density tables: jump " + std::to_string(j + 1) + " phase not +-1");
+            const int64_t ri = isd[j] + first - 1, rf = fsd[j] + first - 1;   // 0-based
+            const int64_t li = ri + step * (nc - 1), lf = rf + step * (nc - 1);
+            if (std::min({ri, rf, li, lf}) < 0 || std::max({ri, rf, li, lf}) >= dim)
+                return set_err(ctx, BSG_ERR_OOB_INDEX, "density tables: jump " + std::to_string(j + 1) + " reaches a state outside the basis");
+            RawSeg s;
+            const bool bwd = hc == BSG_H_BWD;
+            s.label = (pro ? 0 : nlab_p) + (bwd ? qd * nq + qc : qc * nq + qd);
+            s.row_f = bwd ? ri : rf;
+            s.row_i = bwd ? rf : ri;
+            s.step = step;
+            s.cnt = nc;
+            s.sign = ph[j];
+            raw.push_back(s);
+        }
+    }
+    return BSG_OK;
+}
+
+// ---- one-body operator application (applyP1Bopbundled_g /
+// applyN1Bopbundled_g, src/bdenslib3.f90:319-584): vout(statef) +=
+// pot(cop, dop) * phase * vin(statei), 'b' bundles the other way round.
+// Organised by output rows: the segments that write the same row progression
+// (same first row, stride and count: the jumps into one final SD of one
+// bundle) form a group; every row belongs to at most one group per species,
+// so each CTA owns its rows and sums its group's segments in a fixed order.
+struct AGroup {
+    int64_t out0, step;
+    int32_t cnt, seg0, seg1, pad;
+};
+struct ASeg {
+    int64_t in0;
+    double coef;
+};
+struct AItem {
+    int32_t group, c0;
+};
+constexpr int kApplyRows = 4;                       // rows per thread
+constexpr int kApplyChunk = kApplyRows * 256;       // rows per CTA
+
+__global__ void __launch_bounds__(256) k_apply1b(const AGroup *__restrict__ groups, const ASeg *__restrict__ segs,
+                                               const AItem *__restrict__ items, const double *__restrict__ vin,
+                                               double *__restrict__ vout, int64_t dim) {
+    __shared__ ASeg s_seg[128];
+    const AItem it = items[blockIdx.x];
+    const AGroup g = groups[it.group];
+    const double *__restrict__ x = vin + (int64_t)blockIdx.y * dim;
+    double *__restrict__ y = vout + (int64_t)blockIdx.y * dim;
+    int64_t c[kApplyRows];
+    bool ok[kApplyRows];
+    double acc[kApplyRows];
+#pragma unroll
+    for (int u = 0; u < kApplyRows; ++u) {
+        c[u] = (int64_t)it.c0 + threadIdx.x + 256 * u;
+        ok[u] = c[u] < g.cnt;
+        acc[u] = 0.0;
+    }
+    for (int s0 = g.seg0; s0 < g.seg1; s0 += 128) {
+        const int n = min(128, g.seg1 - s0);
+        __syncthreads();
+        if ((int)threadIdx.x < n) s_seg[threadIdx.x] = segs[s0 + threadIdx.x];
+        __syncthreads();
+        for (int q = 0; q < n; ++q) {
+            const int64_t b = s_seg[q].in0;
+            const double w = s_seg[q].coef;
+#pragma unroll
+            for (int u = 0; u < kApplyRows; ++u)
+                if (ok[u]) acc[u] = fma(w, x[b + c[u] * g.step], acc[u]);
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < kApplyRows; ++u)
+        if (ok[u]) y[g.out0 + c[u] * g.step] += acc[u];
+}
+
 }  // namespace
 
 }  // namespace bsg
@@ -189,79 +323,15 @@ extern "C" int bsg_density1b(bsg_ctx *ctx, const bsg_density_tables *dt, const d
         return set_err(ctx, BSG_ERR_ARG, "bsg_density1b: nstates must be 1..32");
     const int ns = nstates, np = ns * ns;
     const int64_t dim = ctx->dim;
-    const int nl_p = ctx->t.nhsps_pl, nq_p = ctx->t.nhsps_pl + ctx->t.nhsps_pr;
-    const int nl_n = ctx->t.nhsps_nl, nq_n = ctx->t.nhsps_nl + ctx->t.nhsps_nr;
+    const int nq_p = ctx->t.nhsps_pl + ctx->t.nhsps_pr, nq_n = ctx->t.nhsps_nl + ctx->t.nhsps_nr;
     const int nlab_p = nq_p * nq_p, nlab_n = nq_n * nq_n;
     std::memset(p1bopme, 0, sizeof(double) * (size_t)np * nlab_p);
     std::memset(n1bopme, 0, sizeof(double) * (size_t)np * nlab_n);
     int st = cuda_check(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
     if (st) return st;
 
-    // pstart / nstart (host copies of the uploaded tables)
-    std::vector<int64_t> pstart(ctx->t.nsd_p), nstart(ctx->t.nsd_n);
-    cudaError_t e = cudaMemcpy(pstart.data(), ctx->raw[0].p, 8 * pstart.size(), cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess) e = cudaMemcpy(nstart.data(), ctx->raw[1].p, 8 * nstart.size(), cudaMemcpyDeviceToHost);
-    if ((st = cuda_check(ctx, e, "bsg_density1b: table copy"))) return st;
-
-    // ---- segments: one per (bundle, jump), validated
     std::vector<RawSeg> raw;
-    auto comb = [](int lab, int nl, int nq) -> int {
-        if (lab < 0) return -lab <= nl ? -lab - 1 : -1;
-        return (lab > 0 && lab <= nq - nl) ? nl + lab - 1 : -1;
-    };
-    for (int64_t b = 0; b < dt->nbundles; ++b) {
-        const int op = dt->optype[b], hc = dt->hchar[b];
-        if (op != BSG_OP_P1B && op != BSG_OP_N1B)
-            return set_err(ctx, BSG_ERR_BAD_TABLE, "bsg_density1b: bundle " + std::to_string(b + 1) + " has an optype other than P1B/N1B");
-        if (hc != BSG_H_FWD && hc != BSG_H_BWD && hc != BSG_H_HERM)
-            return set_err(ctx, BSG_ERR_BAD_TABLE, "bsg_density1b: bad hchar in bundle " + std::to_string(b + 1));
-        const bool pro = op == BSG_OP_P1B;
-        const int64_t cs = dt->cstride[b];
-        const int64_t j0 = pro ? dt->pxstart[b] : dt->nxstart[b], j1 = pro ? dt->pxend[b] : dt->nxend[b];
-        const int64_t c0 = pro ? dt->nxstart[b] : dt->pxstart[b], c1 = pro ? dt->nxend[b] : dt->pxend[b];
-        const int64_t njumps = pro ? dt->np1b : dt->nn1b;
-        const int64_t nconj = pro ? ctx->t.nsd_n : ctx->t.nsd_p;
-        if (cs < 1 || j0 < 1 || j1 > njumps || c0 < 1 || c1 > nconj)
-            return set_err(ctx, BSG_ERR_OOB_INDEX, "bsg_density1b: bundle " + std::to_string(b + 1) + " range outside its table");
-        if (j1 < j0 || c1 < c0) continue;
-        const int64_t nc = (c1 + cs - c0) / cs;
-        int64_t first, step;
-        if (pro) {
-            // statei = isd + (nstart(c0 - cs + 1) - 1) + cs * k, k = 1..nc
-            const int64_t a = c0 - cs + 1;
-            if (a < 1) return set_err(ctx, BSG_ERR_OOB_INDEX, "bsg_density1b: P1B conjugate start below 1");
-            first = nstart[a - 1] - 1 + cs;   // + isd, 1-based
-            step = cs;
-        } else {
-            // statei = isd + pstart(c0) + pstride * (k - 1)
-            first = pstart[c0 - 1];
-            step = nc > 1 ? pstart[c0 - 1 + cs] - pstart[c0 - 1] : 0;
-        }
-        const int64_t *isd = pro ? dt->p1b_isd : dt->n1b_isd, *fsd = pro ? dt->p1b_fsd : dt->n1b_fsd;
-        const int16_t *cop = pro ? dt->p1b_cop : dt->n1b_cop, *dop = pro ? dt->p1b_dop : dt->n1b_dop;
-        const int8_t *ph = pro ? dt->p1b_phase : dt->n1b_phase;
-        const int nl = pro ? nl_p : nl_n, nq = pro ? nq_p : nq_n;
-        for (int64_t j = j0 - 1; j < j1; ++j) {
-            const int qc = comb(cop[j], nl, nq), qd = comb(dop[j], nl, nq);
-            if (qc < 0 || qd < 0)
-                return set_err(ctx, BSG_ERR_OOB_INDEX, "bsg_density1b: jump " + std::to_string(j + 1) + " label outside nhsps");
-            if (ph[j] != 1 && ph[j] != -1)
-                return set_err(ctx, BSG_ERR_BAD_TABLE, "bsg_density1b: jump " + std::to_string(j + 1) + " phase not +-1");
-            const int64_t ri = isd[j] + first - 1, rf = fsd[j] + first - 1;   // 0-based
-            const int64_t li = ri + step * (nc - 1), lf = rf + step * (nc - 1);
-            if (std::min({ri, rf, li, lf}) < 0 || std::max({ri, rf, li, lf}) >= dim)
-                return set_err(ctx, BSG_ERR_OOB_INDEX, "bsg_density1b: jump " + std::to_string(j + 1) + " reaches a state outside the basis");
-            RawSeg s;
-            const bool bwd = hc == BSG_H_BWD;
-            s.label = (pro ? 0 : nlab_p) + (bwd ? qd * nq + qc : qc * nq + qd);
-            s.row_f = bwd ? ri : rf;
-            s.row_i = bwd ? rf : ri;
-            s.step = step;
-            s.cnt = nc;
-            s.sign = ph[j];
-            raw.push_back(s);
-        }
-    }
+    if ((st = build_segments(ctx, dt, raw))) return st;
     std::stable_sort(raw.begin(), raw.end(), [](const RawSeg &a, const RawSeg &b) { return a.label < b.label; });
     int64_t total = 0;
     for (auto &s : raw) total += s.cnt;
@@ -327,7 +397,7 @@ extern "C" int bsg_density1b(bsg_ctx *ctx, const bsg_density_tables *dt, const d
         return st;
     }
     cudaStream_t s = ctx->stream;
-    e = cudaMemcpyAsync(d_cols.p, vecs, vbytes, cudaMemcpyHostToDevice, s);
+    cudaError_t e = cudaMemcpyAsync(d_cols.p, vecs, vbytes, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_outp.p, 0, d_outp.bytes, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_outn.p, 0, d_outn.bytes, s);
     if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, s);
@@ -364,6 +434,116 @@ extern "C" int bsg_density1b(bsg_ctx *ctx, const bsg_density_tables *dt, const d
         ctx->stats.density_launches = 3;
     }
     st = cuda_check(ctx, e, "bsg_density1b");
+    release();
+    return st;
+}
+
+extern "C" int bsg_apply1b(bsg_ctx *ctx, const bsg_density_tables *dt, const double *ppot, const double *npot,
+                           const double *vin, double *vout, int nvec) {
+    if (!ctx) return BSG_ERR_ARG;
+    if (!dt || !vin || !vout) return set_err(ctx, BSG_ERR_ARG, "bsg_apply1b: null argument");
+    if (nvec < 1 || nvec > 65535) return set_err(ctx, BSG_ERR_ARG, "bsg_apply1b: nvec must be 1..65535");
+    const int64_t dim = ctx->dim;
+    const int nq_p = ctx->t.nhsps_pl + ctx->t.nhsps_pr;
+    const int nlab_p = nq_p * nq_p;
+    const int nq_n = ctx->t.nhsps_nl + ctx->t.nhsps_nr;
+    int st = cuda_check(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+    if (st) return st;
+    std::vector<RawSeg> raw;
+    if ((st = build_segments(ctx, dt, raw))) return st;
+
+    // ---- groups per species: segments with the same output progression
+    std::vector<AGroup> groups[2];
+    std::vector<ASeg> segs;
+    std::vector<int64_t> order(raw.size());
+    std::iota(order.begin(), order.end(), 0);
+    auto species = [&](const RawSeg &r) { return r.label < nlab_p ? 0 : 1; };
+    auto coef_of = [&](const RawSeg &r) {
+        const double *pot = species(r) == 0 ? ppot : npot;
+        const int lab = species(r) == 0 ? r.label : r.label - nlab_p;
+        return pot ? pot[lab] * (double)r.sign : 0.0;
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
+        const RawSeg &x = raw[a], &y = raw[b];
+        const int sx = species(x), sy = species(y);
+        if (sx != sy) return sx < sy;
+        if (x.row_f != y.row_f) return x.row_f < y.row_f;
+        if (x.step != y.step) return x.step < y.step;
+        return x.cnt < y.cnt;
+    });
+    for (size_t k = 0; k < order.size(); ++k) {
+        const RawSeg &r = raw[order[k]];
+        const double w = coef_of(r);
+        if (w == 0.0) continue;
+        if (r.cnt > INT32_MAX) return set_err(ctx, BSG_ERR_UNSUPPORTED, "bsg_apply1b: conjugate range above 2^31");
+        auto &gv = groups[species(r)];
+        if (gv.empty() || gv.back().out0 != r.row_f || gv.back().step != r.step || gv.back().cnt != r.cnt ||
+            gv.back().seg1 != (int32_t)segs.size()) {
+            AGroup g;
+            g.out0 = r.row_f; g.step = r.step; g.cnt = (int32_t)r.cnt;
+            g.seg0 = g.seg1 = (int32_t)segs.size();
+            g.pad = 0;
+            gv.push_back(g);
+        }
+        segs.push_back(ASeg{r.row_i, w});
+        gv.back().seg1 = (int32_t)segs.size();
+    }
+    // one writer per row and species (checked on a bitmap of the basis)
+    std::vector<uint64_t> seen((size_t)(dim + 63) / 64);
+    for (int sp = 0; sp < 2; ++sp) {
+        std::fill(seen.begin(), seen.end(), 0ull);
+        for (const AGroup &g : groups[sp])
+            for (int64_t c = 0; c < g.cnt; ++c) {
+                const int64_t r = g.out0 + c * g.step;
+                uint64_t &w = seen[(size_t)(r >> 6)];
+                const uint64_t bit = 1ull << (r & 63);
+                if (w & bit)
+                    return set_err(ctx, BSG_ERR_UNSUPPORTED, "bsg_apply1b: two jump groups write the same basis state");
+                w |= bit;
+            }
+    }
+    std::vector<AItem> items[2];
+    for (int sp = 0; sp < 2; ++sp)
+        for (size_t gi = 0; gi < groups[sp].size(); ++gi)
+            for (int64_t c0 = 0; c0 < groups[sp][gi].cnt; c0 += kApplyChunk)
+                items[sp].push_back(AItem{(int32_t)gi, (int32_t)c0});
+    (void)nq_n;
+
+    DevBuf d_in, d_out, d_g[2], d_it[2], d_seg;
+    auto release = [&]() {
+        dev_free(d_in); dev_free(d_out); dev_free(d_seg);
+        for (int sp = 0; sp < 2; ++sp) { dev_free(d_g[sp]); dev_free(d_it[sp]); }
+    };
+    const size_t vbytes = sizeof(double) * (size_t)dim * nvec;
+    if ((st = dev_alloc(ctx, d_in, vbytes)) || (st = dev_alloc(ctx, d_out, vbytes)) ||
+        (st = upload(ctx, d_seg, segs.data(), sizeof(ASeg) * segs.size()))) {
+        release();
+        return st;
+    }
+    for (int sp = 0; sp < 2 && !st; ++sp) {
+        st = upload(ctx, d_g[sp], groups[sp].data(), sizeof(AGroup) * groups[sp].size());
+        if (!st) st = upload(ctx, d_it[sp], items[sp].data(), sizeof(AItem) * items[sp].size());
+    }
+    if (st) { release(); return st; }
+    cudaStream_t s = ctx->stream;
+    cudaError_t e = cudaMemcpyAsync(d_in.p, vin, vbytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_out.p, 0, vbytes, s);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, s);
+    // protons, then neutrons: the two passes write the same states
+    for (int sp = 0; sp < 2 && e == cudaSuccess; ++sp) {
+        if (items[sp].empty()) continue;
+        k_apply1b<<<dim3((unsigned)items[sp].size(), (unsigned)nvec), 256, 0, s>>>(
+            (const AGroup *)d_g[sp].p, (const ASeg *)d_seg.p, (const AItem *)d_it[sp].p, (const double *)d_in.p,
+            (double *)d_out.p, dim);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(vout, d_out.p, vbytes, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    float ms = 0.0f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    if (e == cudaSuccess) ctx->stats.apply1b_ms = ms;
+    st = cuda_check(ctx, e, "bsg_apply1b");
     release();
     return st;
 }

@@ -1,4 +1,5 @@
-"""Reduced one-body transition densities of Lanczos eigenstates.
+"""One-body observables of Lanczos eigenstates: reduced transition densities,
+one-body operators read from .opme files, and strength functions.
 
 The m-scheme densities <f| a+_c a_d |i> come from the engine
 (``Hamiltonian.density1b``, C ABI ``bsg_density1b``); this module couples them
@@ -130,3 +131,123 @@ def density1b(H, vecs, J, T=None, isospin=True):
     ``model.build_tables``); J, T e.g. from ``engine.angular_momentum_isospin``.
     The m-scheme densities come from the GPU (bsg_density1b)."""
     return reduced(H.tables, H.density1b(vecs), J, T, isospin)
+
+
+# ---------------------------------------------------------------- operators
+class OneBodyOperator:
+    """A one-body operator as an .opme file gives it (readin1bodyop,
+    src/bdenslib1.f90:1823-2071): reduced matrix elements <a||O||b> between
+    orbits, of angular momentum `jop` and isospin `top` ('iso' files) or
+    separate proton and neutron elements ('pns' / 'xpn' files)."""
+
+    def __init__(self, kind, orbits, jop, top, iso=None, prot=None, neut=None):
+        self.kind, self.orbits, self.jop, self.top = kind, orbits, jop, top
+        self.iso = iso or {}
+        self.prot = prot or {}
+        self.neut = neut or {}
+
+
+def read_opme(text):
+    """Parse the text of an .opme file: first line 'iso', 'pns' or 'xpn'; the
+    number of orbits; one line per orbit (index, n, l, j; xpn also gives the
+    neutron index); 'J T' (iso) or 'J' (pn); then 'a b value' lines (pns:
+    'a b proton neutron'; xpn: neutron orbits offset by the orbit count,
+    charge-changing elements skipped)."""
+    lines = [ln.split("!")[0] for ln in text.splitlines()]
+    lines = [ln for ln in lines if ln.strip()]
+    kind = lines[0].strip()[:3]
+    if kind not in ("iso", "pns", "xpn"):
+        raise ValueError("first line of an .opme file must start with iso, pns or xpn")
+    norb = int(lines[1].split()[0])
+    orbits = []
+    for ln in lines[2:2 + norb]:
+        t = ln.split()
+        if kind == "xpn":
+            t = [t[0]] + t[2:]
+        orbits.append((int(t[1]), int(t[2]), int(round(2 * float(t[3])))))   # n, l, 2j
+    t = lines[2 + norb].split()
+    jop = int(t[0])
+    top = int(t[1]) if kind == "iso" else 2
+    op = OneBodyOperator(kind, orbits, jop, top)
+    for ln in lines[3 + norb:]:
+        t = ln.split()
+        a, b = int(t[0]), int(t[1])
+        if kind == "iso":
+            op.iso[(a, b)] = float(t[2])
+        elif kind == "pns":
+            op.prot[(a, b)] = float(t[2])
+            op.neut[(a, b)] = float(t[3])
+        else:
+            if (a <= norb) != (b <= norb):
+                continue
+            if a <= norb:
+                op.prot[(a, b)] = float(t[2])
+            else:
+                op.neut[(a - norb, b - norb)] = float(t[2])
+    return op
+
+
+def onebody_operator(tables, op):
+    """The M = 0 m-scheme matrix elements of `op` on the combined s.p.
+    indices of `tables`, as decouple1bodyop builds pPOT_h / nPOT_h
+    (src/bdenslib1.f90:2444-2597):
+
+        pPOT(a ma, b mb) = (-1)^(jb-mb) (ja ma, jb -mb | J 0) <a||O||b>
+                           / sqrt(2J+1) [/ sqrt(2T+1) (1/2 1/2, 1/2 -1/2 | T 0)]
+
+    with an extra -1 and (1/2 -1/2, 1/2 1/2 | T 0) for neutrons of an isospin
+    operator.  Returns (ppot, npot), None for a species without particles."""
+    spec = tables.extra["spec"]
+    orbit_j2 = [o[2] for o in spec.orbits]
+    for k, (n, l, j2) in enumerate(op.orbits):
+        o = spec.orbits[k]
+        if (n, l, j2) != (o[0], o[1], o[2]):
+            raise ValueError(f"orbit {k + 1} of the operator ({n} {l} {j2}/2) does not match the model space")
+    if len(op.orbits) != len(spec.orbits):
+        raise ValueError("operator and model space have different orbit counts")
+    J, T = op.jop, op.top
+    out = []
+    for it, (npart, sps) in enumerate(((spec.np_, "p"), (spec.nn, "n"))):
+        ex = tables.extra
+        sp = list(zip(ex["sp_orb_" + sps].tolist(), ex["sp_m2_" + sps].tolist()))
+        if npart == 0:
+            out.append(None)
+            continue
+        pot = np.zeros((len(sp), len(sp)))
+        for qa, (a, ma) in enumerate(sp):
+            ja = orbit_j2[a]
+            for qb, (b, mb) in enumerate(sp):
+                jb = orbit_j2[b]
+                if op.kind == "iso":
+                    x = op.iso.get((a + 1, b + 1), 0.0)
+                else:
+                    x = (op.prot if it == 0 else op.neut).get((a + 1, b + 1), 0.0)
+                if x == 0.0 or ma != mb or 2 * J > ja + jb or 2 * J < abs(ja - jb):
+                    continue
+                ph = -1.0 if ((jb - mb) // 2) % 2 else 1.0
+                w = ph * cleb(ja, ma, jb, -mb, 2 * J, ma - mb) * x / sqrt(2 * J + 1)
+                if op.kind == "iso":
+                    tz = 1 if it == 0 else -1
+                    w *= cleb(1, tz, 1, -tz, 2 * T, 0) / sqrt(2 * T + 1)
+                    if it == 1:
+                        w = -w
+                pot[qa, qb] = w
+        out.append(pot)
+    return out[0], out[1]
+
+
+def strength_function(H, pivot, niter=30):
+    """Strength distribution of the (unnormalized) pivot O|psi>, as the
+    reference's strength option prints it (src/blanczoslib.f90:1109-1142):
+    `niter` Lanczos iterations from the normalized pivot, full
+    reorthogonalization, and for every Ritz pair (E_k, y_k) the strength
+    y_k(1)^2 |pivot|^2.  Returns (energies, strengths, total = |pivot|^2).
+    Ritz vectors come back in the full basis; y_k(1) is their overlap with the
+    normalized pivot."""
+    p = np.asarray(pivot, dtype=np.float64)
+    total = float(p @ p)
+    ph = p / np.sqrt(total)
+    k = min(niter, H.dim)
+    ev, vecs, rep = H.lanczos(nkeep=k, niter=niter, matvec_prec=8, fixed_iter=True, want_vectors=True, pivot=ph)
+    s = (vecs.T @ ph) ** 2 * total
+    return ev, s, total

@@ -9,6 +9,8 @@ Mirrors the reference's operator interface for this path:
                                     (dim,) or (dim, nb) (interleaved layout)
 * ``H.lanczos(...)``             -- lanczos_p / lanczos_block with thick restart
 * ``H.grad(evecs)``              -- adjoint: dE/dhmat for every uncoupled label
+* ``H.density1b(vecs)``          -- master_density1b_bundled for every state pair
+* ``H.apply1b(ppot, npot, v)``   -- master_apply1bop: a one-body operator on vectors
 
 Errors raise ``BsgError`` with the status name and the latched message; there
 is no CPU fallback anywhere on this path.
@@ -188,6 +190,28 @@ class Hamiltonian:
                                     dp.ctypes.data_as(_abi.f64p), dn.ctypes.data_as(_abi.f64p))
         self._check(st, "bsg_density1b")
         return {"p": dp, "n": dn}
+
+    def apply1b(self, ppot, npot, vecs, density_tables=None):
+        """O v for the one-body operator O = sum_cd ppot[c, d] a+_c a_d
+        (protons) + npot[c, d] a+_c a_d (neutrons) on the combined s.p.
+        indices (None: no such part); vecs: dim or dim x k.  Returns the same
+        shape."""
+        v = np.asarray(vecs, dtype=np.float64)
+        one = v.ndim == 1
+        if one:
+            v = v[:, None]
+        if v.shape[0] != self.dim:
+            raise ValueError("vectors do not match the basis")
+        cols = np.ascontiguousarray(v.T)
+        out = np.zeros_like(cols)
+        pp = None if ppot is None else np.ascontiguousarray(ppot, dtype=np.float64)
+        nn = None if npot is None else np.ascontiguousarray(npot, dtype=np.float64)
+        dt = density_tables if density_tables is not None else self.tables.density_ctypes()
+        st = self.lib.bsg_apply1b(self.h, C.byref(dt), pp.ctypes.data_as(_abi.f64p) if pp is not None else None,
+                                  nn.ctypes.data_as(_abi.f64p) if nn is not None else None,
+                                  cols.ctypes.data_as(_abi.f64p), out.ctypes.data_as(_abi.f64p), cols.shape[0])
+        self._check(st, "bsg_apply1b")
+        return out[0] if one else out.T
 
 
 def angular_momentum_isospin(spec, vecs, device=0):

@@ -244,6 +244,17 @@ typedef struct bsg_density_tables {
 int  bsg_density1b(bsg_ctx *ctx, const bsg_density_tables *dt, const double *vecs, int nstates,
                    double *p1bopme, double *n1bopme);
 
+/* ---- one-body operator: replaces master_apply1bop (src/bdenslib1.f90:2612)
+ *      with applyP1Bopbundled_g / applyN1Bopbundled_g (src/bdenslib3.f90:319-584)
+ *      over the same density tables: vout = O vin with
+ *      O = sum_cd ppot[c*nqp + d] a+_c a_d (protons) + npot[...] (neutrons),
+ *      the reference's pPOT_h / nPOT_h on combined s.p. indices (the layout
+ *      of p1bopme).  ppot or npot may be NULL (no such part).  vin, vout:
+ *      host fp64, dim x nvec column-major.  Rows are owned by one writer per
+ *      species and summed in a fixed order: bitwise repeatable. ---- */
+int  bsg_apply1b(bsg_ctx *ctx, const bsg_density_tables *dt, const double *ppot, const double *npot,
+                 const double *vin, double *vout, int nvec);
+
 /* ---- batched systems: many independent Hamiltonians of uneven dimension
  *      (the reference runs one per process).  bsg_batch_applyh applies all of
  *      them in one persistent launch whose CTAs pull (system, row tile) work
@@ -282,6 +293,7 @@ typedef struct bsg_stats {
     int64_t density_rows;
     int32_t density_launches;
     int32_t reserved2;
+    double  apply1b_ms;        /* last bsg_apply1b: device time of its kernels */
 } bsg_stats;
 int  bsg_get_stats(const bsg_ctx *ctx, bsg_stats *st);
 

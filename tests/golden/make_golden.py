@@ -7,6 +7,9 @@ Reads (from the reference checkout given as argv[1], default /root/reference):
   examples/sd/input.mg25altwfn  same nucleus, scaling 0 1 1 1 (xspe = 0)
   examples/sd/output/mg25ref.res, mg25alt.res   10 lowest energies, J, T (5 decimals) and
                                                 every one-body density block (5 decimals)
+  examples/sd/sdspin.opme, output/mg25spinstrength1.res
+                                                the spin operator and the strength function
+                                                of the mg25ref ground state (input.mg25strength)
 and writes the numbers as JSON.  Run once in a checkout that has the reference;
 the JSON is what the tests read (the reference is not needed at test time).
 """
@@ -91,6 +94,30 @@ def read_all_densities(path):
     return blocks
 
 
+def read_strength(path):
+    """Total strength, iteration count and the (energy, strength) table of a
+    strength-function .res file."""
+    lines = open(path).read().splitlines()
+    out = {"total": None, "iterations": None, "table": []}
+    for i, ln in enumerate(lines):
+        m = re.match(r"\s*([0-9.Ee+-]+)\s+= total strength", ln)
+        if m and out["total"] is None:
+            out["total"] = float(m.group(1))
+        m = re.match(r"\s*(\d+)\s+iterations", ln)
+        if m and out["iterations"] is None:
+            out["iterations"] = int(m.group(1))
+        if "Energy" in ln and "Strength" in ln and not out["table"]:
+            for row in lines[i + 2:]:
+                t = row.split()
+                if len(t) != 2:
+                    break
+                try:
+                    out["table"].append([float(t[0]), float(t[1])])
+                except ValueError:
+                    break
+    return out
+
+
 def read_input(path):
     toks = [ln.split("!")[0].split() for ln in open(path)]
     toks = [t for t in toks if t]
@@ -117,6 +144,13 @@ def main():
                     "density_jt0": read_diag_density(os.path.join(ex, "output", name + ".res")),
                     "densities": read_all_densities(os.path.join(ex, "output", name + ".res"))})
         out["runs"][name] = run
+    out["spin_operator"] = {"file": "examples/sd/sdspin.opme",
+                            "text": open(os.path.join(ex, "sdspin.opme")).read()}
+    st = read_strength(os.path.join(ex, "output", "mg25spinstrength1.res"))
+    st.update({"res_file": "examples/sd/output/mg25spinstrength1.res",
+               "pivot": "state 1 of mg25ref with the operator of sdspin.opme applied (input.mg25apply1b, "
+                        "input.mg25strength)", "scaling": [1.0, 18.0, 25.0, 0.3]})
+    out["spin_strength"] = st
     with open(os.path.join(HERE, "mg25.json"), "w") as f:
         json.dump(out, f, separators=(",", ":"))
         f.write("\n")
