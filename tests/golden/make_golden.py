@@ -7,6 +7,9 @@ Reads (from the reference checkout given as argv[1], default /root/reference):
   examples/sd/input.mg25altwfn  same nucleus, scaling 0 1 1 1 (xspe = 0)
   examples/sd/output/mg25ref.res, mg25alt.res   10 lowest energies, J, T (5 decimals) and
                                                 every one-body density block (5 decimals)
+  examples/sd/output/mg25expectH.res, overlap.dat
+                                                <H> of the mg25ref states (6 decimals) and the
+                                                overlaps of mg25ref state 1 with mg25alt's states
   examples/sd/sdspin.opme, output/mg25spinstrength1.res
                                                 the spin operator and the strength function
                                                 of the mg25ref ground state (input.mg25strength)
@@ -118,6 +121,36 @@ def read_strength(path):
     return out
 
 
+def read_expect(path):
+    """<H> table of an expectation-value run: state, E, J, T^2, <H>, norm."""
+    rows = []
+    lines = open(path).read().splitlines()
+    for i, ln in enumerate(lines):
+        if "STATE" in ln and "<H >" in ln:
+            for row in lines[i + 1:]:
+                t = row.split()
+                if len(t) != 6 or not t[0].isdigit():
+                    break
+                rows.append({"n": int(t[0]), "E": float(t[1]), "J": float(t[2]), "T2": float(t[3]),
+                             "H": float(t[4]), "norm": float(t[5])})
+            break
+    return rows
+
+
+def read_overlap(path):
+    """overlap.dat: initial state, then per final state E, J, T, <i|f>, |<i|f>|^2."""
+    lines = open(path).read().splitlines()
+    init = int(lines[0].split("=")[1])
+    rows = []
+    for row in lines[2:]:
+        t = row.split()
+        if len(t) != 6:
+            continue
+        rows.append({"n": int(t[0]), "E": float(t[1]), "J": float(t[2]), "T": float(t[3]),
+                     "overlap": float(t[4]), "overlap2": float(t[5])})
+    return {"initial": init, "finals": rows}
+
+
 def read_input(path):
     toks = [ln.split("!")[0].split() for ln in open(path)]
     toks = [t for t in toks if t]
@@ -144,6 +177,12 @@ def main():
                     "density_jt0": read_diag_density(os.path.join(ex, "output", name + ".res")),
                     "densities": read_all_densities(os.path.join(ex, "output", name + ".res"))})
         out["runs"][name] = run
+    out["expect_h"] = {"res_file": "examples/sd/output/mg25expectH.res",
+                       "of": "the 10 mg25ref states under the mg25ref Hamiltonian (input.mg25expectH)",
+                       "states": read_expect(os.path.join(ex, "output", "mg25expectH.res"))}
+    out["overlap"] = dict(read_overlap(os.path.join(ex, "output", "overlap.dat")),
+                          file="examples/sd/output/overlap.dat",
+                          of="state 1 of mg25ref against the 10 mg25alt states (input.mg25overlap)")
     out["spin_operator"] = {"file": "examples/sd/sdspin.opme",
                             "text": open(os.path.join(ex, "sdspin.opme")).read()}
     st = read_strength(os.path.join(ex, "output", "mg25spinstrength1.res"))

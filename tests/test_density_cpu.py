@@ -102,25 +102,53 @@ def test_reduced_densities_sum_rule_time_reversal_and_jz_independence():
             assert np.abs(blocks[Jt] - sgn * other[Jt]).max() < 5e-5, (i, f, Jt)
 
 
-def test_mg25ref_densities_from_oracle_equal_reference_res():
-    """The oracle chain alone (oracle matvec under ARPACK, oracle density
-    traversal, the coupling) against every density block of
-    examples/sd/output/mg25ref.res: pins the restatement before the GPU."""
+_EIG = {}
+
+
+def _mg25_eig(run, k=10):
+    """Lowest k eigenpairs of a 25Mg run of the golden fixture: the oracle
+    matvec (FP64 vectors, float32 matrix elements) under ARPACK (cached)."""
     import json
     import os
     from scipy.sparse.linalg import LinearOperator, eigsh
-    gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "mg25.json")))
+    if (run, k) not in _EIG:
+        gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "mg25.json")))
+        r = gold["runs"][run]
+        ss, ts = model.ModelSpec.scaling(*r["scaling"])
+        orbits = [tuple(o) for o in gold["orbits"]]
+        spec = model.ModelSpec(orbits, r["np"], r["nn"], r["jz2"], 1, gold["spe"], [tuple(t) for t in gold["tbme"]],
+                               ss, ts)
+        T = model.build_tables(spec)
+        op = LinearOperator((T.dim, T.dim), dtype=np.float64,
+                            matvec=lambda v: oracle.applyh(T, np.ascontiguousarray(v, dtype=np.float64)))
+        w, Z = eigsh(op, k=k, which="SA", tol=1e-13, v0=np.ones(T.dim))
+        o = np.argsort(w)
+        _EIG[(run, k)] = (gold, spec, T, w[o], Z[:, o])
+    return _EIG[(run, k)]
+
+
+def test_mg25_overlaps_from_oracle_equal_reference():
+    """|<mg25ref 1|mg25alt f>|^2 (examples/sd/output/overlap.dat) from the
+    oracle's eigenvectors of both Hamiltonians on the same basis."""
+    gold, _, _, w_ref, z_ref = _mg25_eig("mg25ref")
+    _, _, _, w_alt, z_alt = _mg25_eig("mg25alt")
+    ov = z_alt.T @ z_ref[:, gold["overlap"]["initial"] - 1]
+    for g in gold["overlap"]["finals"]:
+        f = g["n"] - 1
+        assert abs(w_alt[f] - g["E"]) < 1.5e-5
+        assert abs(ov[f] ** 2 - g["overlap2"]) < 2e-5 and abs(abs(ov[f]) - abs(g["overlap"])) < 2e-5
+
+
+def test_mg25ref_densities_from_oracle_equal_reference_res():
+    """The oracle chain alone (oracle matvec under ARPACK, oracle density
+    traversal, the coupling) against every density block of
+    examples/sd/output/mg25ref.res, and the energies against the <H> of
+    mg25expectH.res: pins the restatement before the GPU."""
+    gold, spec, T, w, Z = _mg25_eig("mg25ref")
     r = gold["runs"]["mg25ref"]
-    ss, ts = model.ModelSpec.scaling(*r["scaling"])
-    orbits = [tuple(o) for o in gold["orbits"]]
-    spec = model.ModelSpec(orbits, r["np"], r["nn"], r["jz2"], 1, gold["spe"], [tuple(t) for t in gold["tbme"]], ss, ts)
-    T = model.build_tables(spec)
-    op = LinearOperator((T.dim, T.dim), dtype=np.float64,
-                        matvec=lambda v: oracle.applyh(T, np.ascontiguousarray(v, dtype=np.float64)))
-    w, Z = eigsh(op, k=10, which="SA", tol=1e-12, v0=np.ones(T.dim))
-    o = np.argsort(w)
-    w, Z = w[o], Z[:, o]
     assert np.abs(w - np.array([s["E"] for s in r["states"]])).max() < 1.5e-5
+    # <H> of the same states to the 6 decimals of examples/sd/output/mg25expectH.res
+    assert np.abs(w - np.array([s["H"] for s in gold["expect_h"]["states"]])).max() < 1.5e-6
     Jq = model.build_tables(model.jsq_spec(spec))
     Tq = model.build_tables(model.tsq_spec(spec))
     J = [model.j_from_jsq(float(Z[:, i] @ oracle.applyh(Jq, Z[:, i]))) for i in range(10)]

@@ -1,6 +1,8 @@
 """J and T of Lanczos eigenstates (<J^2>, <T^2> with the operators of
 model.jsq_spec / model.tsq_spec applied by the engine) against the labels the
-reference prints for 25Mg (examples/sd/output/mg25ref.res, mg25alt.res)."""
+reference prints for 25Mg (examples/sd/output/mg25ref.res, mg25alt.res); the
+energies against the 6-decimal <H> of mg25expectH.res; and the overlaps of
+the mg25ref ground state with the mg25alt states (overlap.dat)."""
 import json
 import os
 
@@ -25,6 +27,8 @@ def test_mg25_j_and_t_equal_reference_labels(run):
     H.close()
     gold_e = np.array([s["E"] for s in r["states"]])
     assert np.abs(ev - gold_e).max() < 1.5e-5
+    if run == "mg25ref":
+        assert np.abs(ev - np.array([s["H"] for s in GOLD["expect_h"]["states"]])).max() < 1.5e-6
     J, T = angular_momentum_isospin(spec, vecs)
     gold_j = np.array([s["J"] for s in r["states"]])
     gold_t = np.array([s["T"] for s in r["states"]])
@@ -33,3 +37,33 @@ def test_mg25_j_and_t_equal_reference_labels(run):
     tol = 2e-2 if run == "mg25alt" else 1e-3
     assert np.abs(J - gold_j).max() < tol, (J, gold_j)
     assert np.abs(T - gold_t).max() < 1e-3, (T, gold_t)
+
+
+def _states(run, nkeep):
+    from bigstickpublick_b200.engine import Hamiltonian
+    r = GOLD["runs"][run]
+    ss, ts = model.ModelSpec.scaling(*r["scaling"])
+    orbits = [tuple(o) for o in GOLD["orbits"]]
+    spec = model.ModelSpec(orbits, r["np"], r["nn"], r["jz2"], 1, GOLD["spe"], [tuple(t) for t in GOLD["tbme"]], ss, ts)
+    H = Hamiltonian(model.build_tables(spec))
+    ev, vecs, rep = H.lanczos(nkeep=nkeep, niter=400, matvec_prec=8, want_vectors=True, converge_tol=1e-12)
+    H.close()
+    return ev, vecs
+
+
+def test_mg25_overlap_of_ref_ground_state_with_alt_states():
+    """|<mg25ref 1|mg25alt f>|^2 for the 10 mg25alt states (input.mg25overlap,
+    examples/sd/output/overlap.dat, 5 decimals).  States 7 and 8 of mg25alt
+    lie 0.6 keV apart with different J: the reference's pair is less
+    converged (its J = 7/2 state 7 shows a 1e-5 overlap with a J = 5/2 state)."""
+    e_ref, v_ref = _states("mg25ref", 1)
+    e_alt, v_alt = _states("mg25alt", 10)
+    ov = v_alt.T @ v_ref[:, 0]
+    gold = GOLD["overlap"]
+    assert gold["initial"] == 1
+    for g in gold["finals"]:
+        f = g["n"] - 1
+        assert abs(e_alt[f] - g["E"]) < 1.5e-5
+        tol = 1e-3 if g["n"] in (7, 8) else 5e-5
+        assert abs(ov[f] ** 2 - g["overlap2"]) < tol, (g["n"], ov[f] ** 2, g["overlap2"])
+        assert abs(abs(ov[f]) - abs(g["overlap"])) < max(tol, 5e-5)
