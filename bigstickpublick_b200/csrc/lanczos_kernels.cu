@@ -61,20 +61,17 @@ __global__ void __launch_bounds__(kDotThreads) k_multidot(const double *__restri
             double acc0[NB], acc1[NB];
 #pragma unroll
             for (int b = 0; b < NB; ++b) acc0[b] = acc1[b] = 0.0;
-            // U rows per lane and step, loads first (the sum stays in row
-            // order); eight loads in flight per lane when one vector and at
-            // most two B columns leave the registers for it
-            constexpr int U = (PAIR == 1 && NB <= 2) ? 8 : 4;
+            // four rows per lane and step, loads first (the sum stays in row order)
             int r = lane;
-            for (; r + 32 * (U - 1) < rows; r += 32 * U) {
-                double x0[U], x1[U];
+            for (; r + 96 < rows; r += 128) {
+                double x0[4], x1[4];
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
+                for (int u = 0; u < 4; ++u) {
                     x0[u] = __ldg(col0 + r + 32 * u);
                     x1[u] = PAIR == 2 ? __ldg(col1 + r + 32 * u) : 0.0;
                 }
 #pragma unroll
-                for (int u = 0; u < U; ++u)
+                for (int u = 0; u < 4; ++u)
 #pragma unroll
                     for (int b = 0; b < NB; ++b) {
                         const double y = sB[b * kDotTile + r + 32 * u];
@@ -141,19 +138,13 @@ __global__ void __launch_bounds__(256) k_sub_gemv(const double *__restrict__ H, 
         double acc[NB];
 #pragma unroll
         for (int b = 0; b < NB; ++b) acc[b] = 0.0;
-        // four history vectors per step, loads first; the multiply-adds
-        // stay in j order
         int j = 0;
-        for (; j + 3 < k; j += 4) {
-            double h[4];
+        for (; j + 1 < k; j += 2) {
+            const double h0 = __ldg(H + (int64_t)j * ld + i), h1 = __ldg(H + (int64_t)(j + 1) * ld + i);
 #pragma unroll
-            for (int u = 0; u < 4; ++u) h[u] = __ldg(H + (int64_t)(j + u) * ld + i);
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-#pragma unroll
-                for (int b = 0; b < NB; ++b) acc[b] = fma(h[u], sC[(j + u) * NB + b], acc[b]);
+            for (int b = 0; b < NB; ++b) acc[b] = fma(h1, sC[(j + 1) * NB + b], fma(h0, sC[j * NB + b], acc[b]));
         }
-        for (; j < k; ++j) {
+        if (j < k) {
             const double h0 = __ldg(H + (int64_t)j * ld + i);
 #pragma unroll
             for (int b = 0; b < NB; ++b) acc[b] = fma(h0, sC[j * NB + b], acc[b]);
