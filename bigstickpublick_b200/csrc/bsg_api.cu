@@ -679,8 +679,6 @@ void free_ctx(bsg_ctx *ctx) {
     for (DevBuf *b : bufs) dev_free(*b);
     for (auto &kv : ctx->tiles) dev_free(kv.second.buf);
     ctx->tiles.clear();
-    if (ctx->hgraph.exec) cudaGraphExecDestroy(ctx->hgraph.exec);
-    ctx->hgraph = bsg_ctx::HostGraph{};
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -774,66 +772,6 @@ int bsg_destroy(bsg_ctx *ctx) {
 }
 
 namespace {
-bool pinned(const void *p) {
-    cudaPointerAttributes at;
-    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return at.type == cudaMemoryTypeHost;
-}
-
-// copy in, apply, copy out on stream s (no synchronization)
-int host_sequence(bsg_ctx *ctx, const void *vin, void *vout, size_t bytes, int nb, int prec, int acc,
-                  cudaStream_t s) {
-    int st = cuda_check(ctx, cudaMemcpyAsync(ctx->scratch_in.p, vin, bytes, cudaMemcpyHostToDevice, s), "H2D vin");
-    if (!st && acc) st = cuda_check(ctx, cudaMemcpyAsync(ctx->scratch_out.p, vout, bytes, cudaMemcpyHostToDevice, s), "H2D vout");
-    if (!st) st = launch_applyh(ctx, ctx->scratch_in.p, ctx->scratch_out.p, nb, prec, acc, s);
-    if (!st) st = cuda_check(ctx, cudaMemcpyAsync(vout, ctx->scratch_out.p, bytes, cudaMemcpyDeviceToHost, s), "D2H vout");
-    return st;
-}
-
-// The context's own stream with pinned host buffers: the first call with a
-// key runs the sequence directly (it allocates and sets kernel attributes);
-// a repeat captures it as a graph, later repeats replay the graph.  Any
-// failure to capture falls back to the direct sequence for that key.
-int host_graph_or_direct(bsg_ctx *ctx, const void *vin, void *vout, size_t bytes, int nb, int prec, int acc) {
-    cudaStream_t s = ctx->stream;
-    auto &g = ctx->hgraph;
-    const bool same = g.seen && g.vin == vin && g.vout == vout && g.bytes == bytes && g.nb == nb && g.prec == prec &&
-                      g.acc == acc && g.sin == ctx->scratch_in.p && g.sout == ctx->scratch_out.p;
-    if (!same) {
-        if (g.exec) cudaGraphExecDestroy(g.exec);
-        g = bsg_ctx::HostGraph{};
-        g.vin = vin; g.vout = vout; g.bytes = bytes; g.nb = nb; g.prec = prec; g.acc = acc;
-        g.sin = ctx->scratch_in.p; g.sout = ctx->scratch_out.p;
-        g.seen = true;
-        return host_sequence(ctx, vin, vout, bytes, nb, prec, acc, s);
-    }
-    if (!g.exec && !g.failed) {
-        cudaGraph_t graph = nullptr;
-        int st = cuda_check(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
-        if (!st) {
-            const int st2 = host_sequence(ctx, vin, vout, bytes, nb, prec, acc, s);
-            const cudaError_t e = cudaStreamEndCapture(s, &graph);
-            if (st2 || e != cudaSuccess || !graph ||
-                cudaGraphInstantiate(&g.exec, graph, 0) != cudaSuccess) {
-                g.exec = nullptr;
-                g.failed = true;
-                cudaGetLastError();
-                ctx->last_error.clear();
-            }
-            if (graph) cudaGraphDestroy(graph);
-        } else {
-            g.failed = true;
-            cudaGetLastError();
-            ctx->last_error.clear();
-        }
-    }
-    if (g.exec) return cuda_check(ctx, cudaGraphLaunch(g.exec, s), "graph launch");
-    return host_sequence(ctx, vin, vout, bytes, nb, prec, acc, s);
-}
-
 int applyh_on(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec, int flags, cudaStream_t s) {
     if (!vin || !vout || nb < 1 || nb > 64 || (prec != BSG_PREC_FP32 && prec != BSG_PREC_FP64))
         return set_err(ctx, BSG_ERR_ARG, "bsg_applyh: bad arguments");
@@ -847,10 +785,10 @@ int applyh_on(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec, int f
     if (ctx->scratch_in.bytes < bytes) {
         if ((st = dev_alloc(ctx, ctx->scratch_in, bytes)) || (st = dev_alloc(ctx, ctx->scratch_out, bytes))) return st;
     }
-    if (s == ctx->stream && pinned(vin) && pinned(vout))
-        st = host_graph_or_direct(ctx, vin, vout, bytes, nb, prec, acc);
-    else
-        st = host_sequence(ctx, vin, vout, bytes, nb, prec, acc, s);
+    st = cuda_check(ctx, cudaMemcpyAsync(ctx->scratch_in.p, vin, bytes, cudaMemcpyHostToDevice, s), "H2D vin");
+    if (!st && acc) st = cuda_check(ctx, cudaMemcpyAsync(ctx->scratch_out.p, vout, bytes, cudaMemcpyHostToDevice, s), "H2D vout");
+    if (!st) st = launch_applyh(ctx, ctx->scratch_in.p, ctx->scratch_out.p, nb, prec, acc, s);
+    if (!st) st = cuda_check(ctx, cudaMemcpyAsync(vout, ctx->scratch_out.p, bytes, cudaMemcpyDeviceToHost, s), "D2H vout");
     if (!st) st = cuda_check(ctx, cudaStreamSynchronize(s), "applyh sync");
     return st;
 }

@@ -164,18 +164,6 @@ struct bsg_ctx {
     bsg_stats stats{};
     // scratch vectors for host-pointer applyh
     bsg::DevBuf scratch_in, scratch_out;
-    // host-pointer applyh with pinned buffers: the copy-in / kernel / copy-out
-    // sequence of the last (vin, vout, nb, prec, accumulate) key, captured as
-    // a CUDA graph once the key repeats, and replayed while it stays the same
-    struct HostGraph {
-        const void *vin = nullptr;
-        void *vout = nullptr;
-        const void *sin = nullptr, *sout = nullptr;
-        size_t bytes = 0;
-        int nb = 0, prec = 0, acc = 0;
-        bool seen = false, failed = false;
-        cudaGraphExec_t exec = nullptr;
-    } hgraph;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 

@@ -68,34 +68,3 @@ def test_device_pointer_path_and_determinism(built):
     ref = oracle.applyh(T, x.cpu().numpy().reshape(-1), nb=4).reshape(T.dim, 4)
     err = np.abs(y1.cpu().numpy() - ref).max() / np.abs(ref).max()
     assert err < 2e-5
-
-
-@pytest.mark.parametrize("prec,nb,acc", [(4, 1, False), (8, 1, True), (4, 4, False), (8, 2, True)])
-def test_pinned_host_buffers_replay(built, prec, nb, acc):
-    """Pinned host buffers reused call after call (the drop-in's vec1/vec2):
-    the first call runs directly, the second is captured as a CUDA graph, the
-    rest replay it.  Each call must see the buffer contents of that call."""
-    import torch
-    T, H = built["sd 3p2n jz=1"]
-    dt = torch.float64 if prec == 8 else torch.float32
-    shape = (T.dim,) if nb == 1 else (T.dim, nb)
-    hin = torch.empty(shape, dtype=dt, pin_memory=True)
-    hout = torch.empty(shape, dtype=dt, pin_memory=True)
-    xin, xout = hin.numpy(), hout.numpy()
-    rng = np.random.default_rng(9)
-    tol = 1e-12 if prec == 8 else 2e-5
-    outs = []
-    for step in range(5):
-        xin[...] = rng.standard_normal(shape)
-        base = rng.standard_normal(shape) if acc else np.zeros(shape)
-        xout[...] = base
-        H.applyh(xin, xout, accumulate=acc)
-        ref = base + oracle.applyh(T, xin.reshape(-1).astype(np.float64), nb=nb).reshape(shape)
-        assert np.abs(xout - ref).max() <= tol * (np.abs(ref).max() + 1), step
-        outs.append(xout.copy())
-    # replay is bitwise the direct result: rerun the last input directly from pageable memory
-    last = np.ascontiguousarray(xin.copy())
-    direct = np.zeros(shape, dtype=last.dtype) if not acc else None
-    if not acc:
-        H.applyh(last, direct)
-        assert np.array_equal(direct, outs[-1])
