@@ -112,7 +112,18 @@ struct SpeciesBasis {
     std::vector<uint64_t> sd_bits;     // per SD (0-based index = isd-1)
     std::vector<int> sd_sector;        // 0-based sector of each SD
     std::unordered_map<uint64_t, int64_t> sd_index;  // bits -> 0-based SD index
+    // the same map as a direct table over all occupation patterns when the
+    // species has at most kDenseSps s.p. states (-1: not an SD of the basis);
+    // the jump generators look up every candidate final SD
+    std::vector<int64_t> sd_dense;
+    int64_t find_sd(uint64_t bits) const {
+        if (!sd_dense.empty()) return bits < sd_dense.size() ? sd_dense[bits] : -1;
+        auto f = sd_index.find(bits);
+        return f == sd_index.end() ? -1 : f->second;
+    }
 };
+
+constexpr int kDenseSps = 22;   // 2^22 entries of 8 bytes at most per species
 
 inline int pidx_of(int par) { return par > 0 ? 1 : 2; }
 inline int par_of_idx(int p) { return p == 1 ? 1 : -1; }
@@ -510,6 +521,40 @@ struct Interaction {
     Coupled C;
     // canonical key -> list of (tbme line, sign) contributing to it
     std::map<std::tuple<int, int, int, int, int, int>, std::vector<std::pair<int, int>>> prov;
+    // the same two maps as dense arrays over canonical (a, b, c, d, J, T):
+    // the uncoupling asks for each element many times (once per m-scheme
+    // pair-pair and J), so the lookups must not walk a tree
+    int nj = 0;
+    std::vector<double> dv;
+    std::vector<uint8_t> dhas;
+    std::vector<int32_t> dp0, dp1;                 // provenance range per entry
+    std::vector<std::pair<int, int>> dprov;
+    size_t slot(int a, int b, int c, int d, int J, int T) const {
+        const size_t n = (size_t)C.norb;
+        return (((((size_t)a * n + b) * n + c) * n + d) * (size_t)nj + J) * 2 + T;
+    }
+    void finalize() {
+        int jmax = 0;
+        for (int j : C.j2) jmax = std::max(jmax, j);
+        nj = jmax + 1;
+        const size_t n = (size_t)C.norb, tot = n * n * n * n * (size_t)nj * 2;
+        dv.assign(tot, 0.0);
+        dhas.assign(tot, 0);
+        dp0.assign(tot, 0);
+        dp1.assign(tot, 0);
+        dprov.clear();
+        for (auto &kv : C.v) {
+            const auto &k = kv.first;
+            const size_t q = slot(std::get<0>(k), std::get<1>(k), std::get<2>(k), std::get<3>(k), std::get<4>(k),
+                                  std::get<5>(k));
+            dv[q] = kv.second;
+            dhas[q] = 1;
+            dp0[q] = (int32_t)dprov.size();
+            auto pit = prov.find(k);
+            if (pit != prov.end()) dprov.insert(dprov.end(), pit->second.begin(), pit->second.end());
+            dp1[q] = (int32_t)dprov.size();
+        }
+    }
 };
 
 // V_JT(a,b,c,d) as a linear combination of file lines: returns value, and
@@ -519,15 +564,12 @@ double coupled_with_prov(const Interaction &I, int a, int b, int c, int d, int J
     const Coupled &C = I.C;
     if (!C.pair_ok(a, b, J, T) || !C.pair_ok(c, d, J, T)) return 0.0;
     int sg;
-    auto key = C.canon(a, b, c, d, J, T, sg);
-    auto it = C.v.find(key);
-    if (it == C.v.end()) return 0.0;
-    if (acc) {
-        auto pit = I.prov.find(key);
-        if (pit != I.prov.end())
-            for (auto &pr : pit->second) acc->push_back({pr.first, w * sg * pr.second});
-    }
-    return sg * it->second;
+    const auto key = C.canon(a, b, c, d, J, T, sg);
+    const size_t q = I.slot(std::get<0>(key), std::get<1>(key), std::get<2>(key), std::get<3>(key), J, T);
+    if (!I.dhas[q]) return 0.0;
+    if (acc)
+        for (int32_t p = I.dp0[q]; p < I.dp1[q]; ++p) acc->push_back({I.dprov[p].first, w * sg * I.dprov[p].second});
+    return sg * I.dv[q];
 }
 
 void compress(std::vector<std::pair<int, double>> &v) {
@@ -656,6 +698,7 @@ int build(const bsg_model_spec *s, Built &B) {
         I.C.v[key] += sg * t.v;
         I.prov[key].push_back({i, sg});
     }
+    I.finalize();
     const double vscale = s->tbme_scale;
     const int A = s->np + s->nn;
     const bool call_spe = (A <= 1);
@@ -772,39 +815,72 @@ int build(const bsg_model_spec *s, Built &B) {
     (void)nspsp;
 
     // ---- jumps
+    for (SpeciesBasis *sbp : sbs) {
+        SpeciesBasis &sb = *sbp;
+        const int ns = sb.nl + sb.nr;
+        sb.sd_dense.clear();
+        if (ns <= kDenseSps) {
+            sb.sd_dense.assign((size_t)1 << ns, -1);
+            for (size_t i = 0; i < sb.sd_bits.size(); ++i) sb.sd_dense[sb.sd_bits[i]] = (int64_t)i;
+        }
+    }
     // one-body: proton sector jumps (is >= fs), each with its conjugate
     // neutron sector jump (conj(is) -> conj(fs))
+    // the one-body jumps out of a sector, generated in one pass over its SDs
+    // (SD, then annihilated k, then created i) and bucketed by the final
+    // sector; gen1 appends one bucket, so each (is, fs) keeps that order
+    std::map<std::pair<const SpeciesBasis *, int>, std::vector<Jumps1>> jumps1_from;
     auto gen1 = [&](SpeciesBasis &sb, const std::vector<int64_t> &xstart, int is, int fs, Jumps1 &J) {
-        int64_t cnt = 0;
-        const Sector &S = sb.sectors[is];
-        const int ns = sb.nl + sb.nr;
-        for (int64_t sd = S.xsdstart - 1; sd < S.xsdend; ++sd) {
-            const uint64_t bits = sb.sd_bits[sd];
-            for (int k = 0; k < ns; ++k) {
-                if (!(bits >> k & 1ull)) continue;
-                for (int i = 0; i < ns; ++i) {
-                    if (i != k && (bits >> i & 1ull)) continue;
-                    const uint64_t nb2 = (bits & ~(1ull << k)) | (1ull << i);
-                    auto f = sb.sd_index.find(nb2);
-                    if (f == sb.sd_index.end()) continue;
-                    if (sb.sd_sector[f->second] != fs) continue;
-                    J.isd.push_back(xstart[sd]);
-                    J.fsd.push_back(xstart[f->second]);
-                    J.cop.push_back((int16_t)signed_label(sb, i));
-                    J.dop.push_back((int16_t)signed_label(sb, k));
-                    J.phase.push_back((int8_t)phase1(bits, i, k));
-                    ++cnt;
+        auto key = std::make_pair((const SpeciesBasis *)&sb, is);
+        auto it = jumps1_from.find(key);
+        if (it == jumps1_from.end()) {
+            std::vector<Jumps1> by(sb.sectors.size());
+            const Sector &S = sb.sectors[is];
+            const int ns = sb.nl + sb.nr;
+            for (int64_t sd = S.xsdstart - 1; sd < S.xsdend; ++sd) {
+                const uint64_t bits = sb.sd_bits[sd];
+                for (int k = 0; k < ns; ++k) {
+                    if (!(bits >> k & 1ull)) continue;
+                    for (int i = 0; i < ns; ++i) {
+                        if (i != k && (bits >> i & 1ull)) continue;
+                        const uint64_t nb2 = (bits & ~(1ull << k)) | (1ull << i);
+                        const int64_t f = sb.find_sd(nb2);
+                        if (f < 0) continue;
+                        Jumps1 &B1 = by[sb.sd_sector[f]];
+                        B1.isd.push_back(xstart[sd]);
+                        B1.fsd.push_back(xstart[f]);
+                        B1.cop.push_back((int16_t)signed_label(sb, i));
+                        B1.dop.push_back((int16_t)signed_label(sb, k));
+                        B1.phase.push_back((int8_t)phase1(bits, i, k));
+                    }
                 }
             }
+            it = jumps1_from.emplace(key, std::move(by)).first;
         }
-        return cnt;
+        const Jumps1 &src = it->second[fs];
+        J.isd.insert(J.isd.end(), src.isd.begin(), src.isd.end());
+        J.fsd.insert(J.fsd.end(), src.fsd.begin(), src.fsd.end());
+        J.cop.insert(J.cop.end(), src.cop.begin(), src.cop.end());
+        J.dop.insert(J.dop.end(), src.dop.begin(), src.dop.end());
+        J.phase.insert(J.phase.end(), src.phase.begin(), src.phase.end());
+        return (int64_t)src.isd.size();
     };
-    auto gen2 = [&](SpeciesBasis &sb, const std::vector<int64_t> &xstart, const Pairs &P, int is, int fs, Jumps2 &J) {
+    // pairs (i < j) of each pair section (M, parity), in (i, j) order: the
+    // creation pairs a two-body jump can use for a given annihilated pair
+    auto pairs_by_section = [](const SpeciesBasis &sb, const Pairs &P) {
+        const int ns = sb.nl + sb.nr;
+        std::vector<std::vector<std::pair<int, int>>> by(P.sec_n.size());
+        for (int i = 0; i < ns; ++i)
+            for (int j = i + 1; j < ns; ++j) by[P.pair_sec[P.at(i, j) - 1]].push_back({i, j});
+        return by;
+    };
+    auto gen2 = [&](SpeciesBasis &sb, const std::vector<int64_t> &xstart, const Pairs &P,
+                    const std::vector<std::vector<std::pair<int, int>>> &by_sec, int is, int fs, Jumps2 &J) {
         int64_t cnt = 0;
         const Sector &S = sb.sectors[is];
         const int ns = sb.nl + sb.nr;
         const bool halve = (is == fs);
-        std::vector<int> occ, tgt;
+        std::vector<int> occ;
         for (int64_t sd = S.xsdstart - 1; sd < S.xsdend; ++sd) {
             const uint64_t bits = sb.sd_bits[sd];
             occ.clear();
@@ -814,26 +890,21 @@ int build(const bsg_model_spec *s, Built &B) {
                 for (size_t y = x + 1; y < occ.size(); ++y) {
                     const int k = occ[x], l = occ[y];
                     const uint64_t rest = bits & ~(1ull << k) & ~(1ull << l);
-                    tgt.clear();
-                    for (int q = 0; q < ns; ++q)
-                        if (!(rest >> q & 1ull)) tgt.push_back(q);
                     const int64_t dpair = P.at(k, l);
-                    for (size_t u = 0; u < tgt.size(); ++u)
-                        for (size_t v = u + 1; v < tgt.size(); ++v) {
-                            const int i = tgt[u], j = tgt[v];
-                            const int64_t cpair = P.at(i, j);
-                            if (P.pair_sec[cpair - 1] != P.pair_sec[dpair - 1]) continue;  // M, parity
-                            const uint64_t nb2 = rest | (1ull << i) | (1ull << j);
-                            auto f = sb.sd_index.find(nb2);
-                            if (f == sb.sd_index.end()) continue;
-                            if (sb.sd_sector[f->second] != fs) continue;
-                            if (halve && sd < f->second) continue;  // keep isd >= fsd
-                            J.isd.push_back(xstart[sd]);
-                            J.fsd.push_back(xstart[f->second]);
-                            J.op.push_back((int32_t)xx_label(P, cpair, dpair));
-                            J.phase.push_back((int8_t)phase2(bits, i, j, k, l));
-                            ++cnt;
-                        }
+                    for (const auto &ij : by_sec[P.pair_sec[dpair - 1]]) {   // same M, parity
+                        const int i = ij.first, j = ij.second;
+                        if ((rest >> i & 1ull) || (rest >> j & 1ull)) continue;
+                        const int64_t cpair = P.at(i, j);
+                        const uint64_t nb2 = rest | (1ull << i) | (1ull << j);
+                        const int64_t f = sb.find_sd(nb2);
+                        if (f < 0 || sb.sd_sector[f] != fs) continue;
+                        if (halve && sd < f) continue;  // keep isd >= fsd
+                        J.isd.push_back(xstart[sd]);
+                        J.fsd.push_back(xstart[f]);
+                        J.op.push_back((int32_t)xx_label(P, cpair, dpair));
+                        J.phase.push_back((int8_t)phase2(bits, i, j, k, l));
+                        ++cnt;
+                    }
                 }
         }
         return cnt;
@@ -858,22 +929,26 @@ int build(const bsg_model_spec *s, Built &B) {
             }
             B.p1sj.push_back(sj);
         }
-    if (s->np >= 2)
+    if (s->np >= 2) {
+        const auto by_sec = pairs_by_section(B.pb, B.ppairs);
         for (int is = 0; is < nps; ++is) {
             SectJump sj;
             sj.is = is; sj.fs = is; sj.diag = true;
             sj.nstart = (int64_t)B.p2.isd.size();
-            sj.njumps = gen2(B.pb, B.pstart, B.ppairs, is, is, B.p2);
+            sj.njumps = gen2(B.pb, B.pstart, B.ppairs, by_sec, is, is, B.p2);
             if (sj.njumps > 0) B.p2sj.push_back(sj);
         }
-    if (s->nn >= 2)
+    }
+    if (s->nn >= 2) {
+        const auto by_sec = pairs_by_section(B.nb, B.npairs);
         for (int is = 0; is < nns; ++is) {
             SectJump sj;
             sj.is = is; sj.fs = is; sj.diag = true;
             sj.nstart = (int64_t)B.n2.isd.size();
-            sj.njumps = gen2(B.nb, B.nstart, B.npairs, is, is, B.n2);
+            sj.njumps = gen2(B.nb, B.nstart, B.npairs, by_sec, is, is, B.n2);
             if (sj.njumps > 0) B.n2sj.push_back(sj);
         }
+    }
 
     // ---- one-body density jumps (set1bsectorjumps + master1bodyjumps for
     // densities, src/bdenslib1.f90:190-213): every sector jump is -> fs
