@@ -278,7 +278,7 @@ def batch_leg(args):
     from bigstickpublick_b200 import model
     from bigstickpublick_b200.engine import Batch
     t0 = time.perf_counter()
-    tabs = [model.build_tables(model.batch_member(s)) for s in range(1000, 1000 + args.batch_n)]
+    tabs = model.build_tables_many([model.batch_member(s) for s in range(1000, 1000 + args.batch_n)])
     t_build = time.perf_counter() - t0
     t0 = time.perf_counter()
     cache = os.path.join(ROOT, ".tune_cache", "batch_tuning.json") if args.tune_cache else None

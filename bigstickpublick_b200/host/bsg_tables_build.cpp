@@ -52,14 +52,18 @@ struct SPS {
 };
 
 // ---------------------------------------------------------------- CG -------
-double g_lfact[256];
-bool g_lfact_ready = false;
-void init_lfact() {
-    if (g_lfact_ready) return;
-    g_lfact[0] = 0.0;
-    for (int i = 1; i < 256; ++i) g_lfact[i] = g_lfact[i - 1] + std::log((double)i);
-    g_lfact_ready = true;
-}
+// log n! for n < 256, filled when the library loads and read-only after, so
+// several threads may build tables at the same time
+struct LogFact {
+    double v[256];
+    LogFact() {
+        v[0] = 0.0;
+        for (int i = 1; i < 256; ++i) v[i] = v[i - 1] + std::log((double)i);
+    }
+};
+const LogFact g_lfact_table;
+const double *const g_lfact = g_lfact_table.v;
+void init_lfact() {}
 // <j1/2 m1/2 j2/2 m2/2 | J/2 M/2>, all arguments doubled (Racah's formula).
 double cg2(int j1, int m1, int j2, int m2, int J, int M) {
     if (m1 + m2 != M) return 0.0;

@@ -15,6 +15,7 @@ real ones: every canonical J-T coupled matrix element drawn N(0, 1 MeV) from a
 SplitMix64 stream through Box-Muller.
 """
 import ctypes as C
+import os
 import math
 from dataclasses import dataclass, field
 
@@ -311,6 +312,16 @@ def build_tables(spec: ModelSpec) -> Tables:
     finally:
         lib.bsg_host_free(hp)
     return Tables(arrs, scal, extra)
+
+
+def build_tables_many(specs, threads=None):
+    """build_tables for many specs on host threads (the builder runs outside
+    the GIL); results in the order of `specs`."""
+    from concurrent.futures import ThreadPoolExecutor
+    specs = list(specs)
+    n = threads or min(len(specs), os.cpu_count() or 1) or 1
+    with ThreadPoolExecutor(max_workers=n) as ex:
+        return list(ex.map(build_tables, specs))
 
 
 # ------------------------------------------------------------ presets
