@@ -102,3 +102,23 @@ def test_mg25_spin_strength_oracle_chain():
     ev, vecs, rep = ol.lanczos(T, nkeep=30, niter=30, fixed_iter=True, want_vectors=True, pivot=piv, matvec=mv)
     S = (vecs.T @ (piv / np.sqrt(total))) ** 2 * total
     strength_checks(ev, S, total, GOLD["spin_strength"])
+
+
+def test_backward_bundles_equal_forward_in_oracle():
+    """The oracle's 'b' branches (densities and operator application) on
+    tables where half the jumps come through 'b' bundles equal the all-'f'
+    tables: the split is the one the GPU tests use."""
+    from test_density_gpu import _split_with_backward
+    T = model.build_tables(model.sd_model(3, 2, seed=4, jz2=1))
+    d = _split_with_backward(T)
+    assert (d["hchar"] == ord("b")).any()
+    alt = model.Tables(T.a, T.s, dict(T.extra, density=d))
+    rng = np.random.default_rng(2)
+    X = rng.standard_normal((T.dim, 3))
+    nqp = T.s["nhsps_pl"] + T.s["nhsps_pr"]
+    nqn = T.s["nhsps_nl"] + T.s["nhsps_nr"]
+    P, N = rng.standard_normal((nqp, nqp)), rng.standard_normal((nqn, nqn))
+    for a, b in zip(od.bundled(alt, X), od.bundled(T, X)):
+        assert np.abs(a - b).max() < 1e-12 * max(1.0, np.abs(b).max())
+    Y, Yref = od.apply1b_bundled(alt, P, N, X), od.apply1b_bundled(T, P, N, X)
+    assert np.abs(Y - Yref).max() < 1e-12 * max(1.0, np.abs(Yref).max())

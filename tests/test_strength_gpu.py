@@ -58,3 +58,20 @@ def test_mg25_spin_strength_function():
     H.close()
     assert len(E) == 30
     strength_checks(E, S, total, GOLD["spin_strength"])
+
+
+def test_apply1b_backward_bundles_equal_forward():
+    from test_density_gpu import _split_with_backward, _with_density
+    T = model.build_tables(model.sd_model(4, 3, seed=4, jz2=1))
+    rng = np.random.default_rng(8)
+    nqp = T.s["nhsps_pl"] + T.s["nhsps_pr"]
+    nqn = T.s["nhsps_nl"] + T.s["nhsps_nr"]
+    P, N = rng.standard_normal((nqp, nqp)), rng.standard_normal((nqn, nqn))
+    X = rng.standard_normal((T.dim, 2))
+    H = _H(T)
+    ref = H.apply1b(P, N, X)
+    dt, keep = _with_density(T, _split_with_backward(T))
+    got = H.apply1b(P, N, X, density_tables=dt)
+    assert np.abs(got - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max())
+    assert np.abs(got - od.apply1b_bundled(keep, P, N, X)).max() <= 1e-12 * max(1.0, np.abs(ref).max())
+    H.close()
