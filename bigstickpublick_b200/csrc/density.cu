@@ -308,6 +308,41 @@ __global__ void __launch_bounds__(256) k_apply1b(const AGroup *__restrict__ grou
         if (ok[u]) y[g.out0 + c[u] * g.step] += acc[u];
 }
 
+// Neutron groups: the rows of a group step by the neutron-sector size, so the
+// row-parallel kernel above reads one word per 32-byte sector.  Here thread t
+// takes group g0 + t (consecutive groups of a bundle write consecutive
+// states: one final neutron SD each) and kApplyCols of its rows; the gathers
+// of one proton SD's neutron slice stay in L1.  The sum per row runs over the
+// group's segments in the same order as in k_apply1b.
+constexpr int kApplyCols = 8;
+struct ATItem {
+    int32_t g0, ng, c0, pad;
+};
+
+__global__ void __launch_bounds__(256) k_apply1b_t(const AGroup *__restrict__ groups, const ASeg *__restrict__ segs,
+                                                 const ATItem *__restrict__ items, const double *__restrict__ vin,
+                                                 double *__restrict__ vout, int64_t dim) {
+    const ATItem it = items[blockIdx.x];
+    if ((int)threadIdx.x >= it.ng) return;
+    const AGroup g = groups[it.g0 + threadIdx.x];
+    const int nc = min(kApplyCols, g.cnt - it.c0);
+    if (nc <= 0) return;
+    const double *__restrict__ x = vin + (int64_t)blockIdx.y * dim + (int64_t)it.c0 * g.step;
+    double *__restrict__ y = vout + (int64_t)blockIdx.y * dim + g.out0 + (int64_t)it.c0 * g.step;
+    double acc[kApplyCols];
+#pragma unroll
+    for (int u = 0; u < kApplyCols; ++u) acc[u] = 0.0;
+    for (int q = g.seg0; q < g.seg1; ++q) {
+        const ASeg sg = segs[q];
+#pragma unroll
+        for (int u = 0; u < kApplyCols; ++u)
+            if (u < nc) acc[u] = fma(sg.coef, x[sg.in0 + (int64_t)u * g.step], acc[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < kApplyCols; ++u)
+        if (u < nc) y[(int64_t)u * g.step] += acc[u];
+}
+
 }  // namespace
 
 }  // namespace bsg
@@ -502,11 +537,19 @@ extern "C" int bsg_apply1b(bsg_ctx *ctx, const bsg_density_tables *dt, const dou
                 w |= bit;
             }
     }
+    // protons: row chunks of one group per CTA; neutrons: 256 consecutive
+    // groups per CTA, kApplyCols rows each
     std::vector<AItem> items[2];
-    for (int sp = 0; sp < 2; ++sp)
-        for (size_t gi = 0; gi < groups[sp].size(); ++gi)
-            for (int64_t c0 = 0; c0 < groups[sp][gi].cnt; c0 += kApplyChunk)
-                items[sp].push_back(AItem{(int32_t)gi, (int32_t)c0});
+    for (size_t gi = 0; gi < groups[0].size(); ++gi)
+        for (int64_t c0 = 0; c0 < groups[0][gi].cnt; c0 += kApplyChunk)
+            items[0].push_back(AItem{(int32_t)gi, (int32_t)c0});
+    std::vector<ATItem> titems;
+    for (size_t g0 = 0; g0 < groups[1].size(); g0 += 256) {
+        const int ng = (int)std::min<size_t>(256, groups[1].size() - g0);
+        int32_t cmax = 0;
+        for (int t = 0; t < ng; ++t) cmax = std::max(cmax, groups[1][g0 + t].cnt);
+        for (int32_t c0 = 0; c0 < cmax; c0 += kApplyCols) titems.push_back(ATItem{(int32_t)g0, ng, c0, 0});
+    }
     (void)nq_n;
 
     DevBuf d_in, d_out, d_g[2], d_it[2], d_seg;
@@ -520,20 +563,25 @@ extern "C" int bsg_apply1b(bsg_ctx *ctx, const bsg_density_tables *dt, const dou
         release();
         return st;
     }
-    for (int sp = 0; sp < 2 && !st; ++sp) {
+    for (int sp = 0; sp < 2 && !st; ++sp)
         st = upload(ctx, d_g[sp], groups[sp].data(), sizeof(AGroup) * groups[sp].size());
-        if (!st) st = upload(ctx, d_it[sp], items[sp].data(), sizeof(AItem) * items[sp].size());
-    }
+    if (!st) st = upload(ctx, d_it[0], items[0].data(), sizeof(AItem) * items[0].size());
+    if (!st) st = upload(ctx, d_it[1], titems.data(), sizeof(ATItem) * titems.size());
     if (st) { release(); return st; }
     cudaStream_t s = ctx->stream;
     cudaError_t e = cudaMemcpyAsync(d_in.p, vin, vbytes, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_out.p, 0, vbytes, s);
     if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, s);
     // protons, then neutrons: the two passes write the same states
-    for (int sp = 0; sp < 2 && e == cudaSuccess; ++sp) {
-        if (items[sp].empty()) continue;
-        k_apply1b<<<dim3((unsigned)items[sp].size(), (unsigned)nvec), 256, 0, s>>>(
-            (const AGroup *)d_g[sp].p, (const ASeg *)d_seg.p, (const AItem *)d_it[sp].p, (const double *)d_in.p,
+    if (e == cudaSuccess && !items[0].empty()) {
+        k_apply1b<<<dim3((unsigned)items[0].size(), (unsigned)nvec), 256, 0, s>>>(
+            (const AGroup *)d_g[0].p, (const ASeg *)d_seg.p, (const AItem *)d_it[0].p, (const double *)d_in.p,
+            (double *)d_out.p, dim);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && !titems.empty()) {
+        k_apply1b_t<<<dim3((unsigned)titems.size(), (unsigned)nvec), 256, 0, s>>>(
+            (const AGroup *)d_g[1].p, (const ASeg *)d_seg.p, (const ATItem *)d_it[1].p, (const double *)d_in.p,
             (double *)d_out.p, dim);
         e = cudaGetLastError();
     }
