@@ -783,21 +783,30 @@ int build(const bsg_model_spec *s, Built &B) {
                 B.dpn[idx] = pos + nme;
             }
             if (!have_pn) continue;
+            // (ja ma, jb mb | J M) of every pair of the section, J = 0..20:
+            // each appears in n matrix elements as the bra and n as the ket
+            constexpr int kJ = 21;
+            std::vector<double> cgt((size_t)n * kJ);
+            for (int64_t pos = 1; pos <= n; ++pos) {
+                const int qp = P.list[first + pos - 2].first, qn = P.list[first + pos - 2].second;
+                const int jp = I.C.j2[B.pb.q_orb[qp]], jn = I.C.j2[B.nb.q_orb[qn]];
+                const int m2 = B.pb.q_m2[qp] + B.nb.q_m2[qn];
+                for (int J = 0; J < kJ; ++J)
+                    cgt[(size_t)(pos - 1) * kJ + J] = cg2(jp, B.pb.q_m2[qp], jn, B.nb.q_m2[qn], 2 * J, m2);
+            }
             for (int64_t cpos = 1; cpos <= n; ++cpos)
                 for (int64_t dpos = 1; dpos <= n; ++dpos) {
                     const int64_t lab = nme + (cpos - 1) * n + dpos;
                     const int qa = P.list[first + cpos - 2].first, qb = P.list[first + cpos - 2].second;
                     const int qc = P.list[first + dpos - 2].first, qd = P.list[first + dpos - 2].second;
                     const int a = B.pb.q_orb[qa], b = B.nb.q_orb[qb], c = B.pb.q_orb[qc], d = B.nb.q_orb[qd];
-                    const int ja = I.C.j2[a], jb = I.C.j2[b], jc = I.C.j2[c], jd = I.C.j2[d];
-                    const int M2 = B.pb.q_m2[qa] + B.nb.q_m2[qb];
                     const double zab = (a == b) ? std::sqrt(2.0) : 1.0, zcd = (c == d) ? std::sqrt(2.0) : 1.0;
                     double v = 0.0;
                     std::vector<std::pair<int, double>> pv;
-                    for (int J = 0; J <= 20; ++J) {
-                        const double cgab = cg2(ja, B.pb.q_m2[qa], jb, B.nb.q_m2[qb], 2 * J, M2);
+                    for (int J = 0; J < kJ; ++J) {
+                        const double cgab = cgt[(size_t)(cpos - 1) * kJ + J];
                         if (cgab == 0.0) continue;
-                        const double cgcd = cg2(jc, B.pb.q_m2[qc], jd, B.nb.q_m2[qd], 2 * J, M2);
+                        const double cgcd = cgt[(size_t)(dpos - 1) * kJ + J];
                         if (cgcd == 0.0) continue;
                         const double w = 0.5 * zab * zcd * cgab * cgcd * vscale;
                         for (int T = 0; T <= 1; ++T) v += w * coupled_with_prov(I, a, b, c, d, J, T, w, &pv);
