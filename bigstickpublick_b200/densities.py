@@ -96,6 +96,29 @@ def coupled_densities(orbit_j2, sp_p, sp_n, mp, mn, Jt, Ji, Ti, Jf, Tf, jz2, tz2
     return False, den / cg
 
 
+def tiled_pairs(k, call, block=16):
+    """All k x k m-scheme density pairs from a routine that handles at most
+    2*block states per call.  call(idx) returns {'p': D, 'n': D} for the
+    states idx (D[f, i, c, d] over positions in idx); blocks of `block`
+    states are taken two at a time, so every (f, i) pair is covered once."""
+    if k <= 2 * block:
+        return call(list(range(k)))
+    nblk = (k + block - 1) // block
+    out = None
+    for bi in range(nblk):
+        for bj in range(bi, nblk):
+            idx = list(range(bi * block, min(k, (bi + 1) * block)))
+            if bj != bi:
+                idx += list(range(bj * block, min(k, (bj + 1) * block)))
+            md = call(idx)
+            if out is None:
+                out = {sp: np.zeros((k, k) + md[sp].shape[2:]) for sp in md}
+            for sp in md:
+                ix = np.array(idx)
+                out[sp][np.ix_(ix, ix)] = md[sp]
+    return out
+
+
 def reduced(tables, md, J, T=None, isospin=True):
     """Reduced densities of every (initial, final) pair from the m-scheme
     densities `md` ({'p': D_p, 'n': D_n}, D[f, i, c, d] as

@@ -168,7 +168,9 @@ class Hamiltonian:
 
     def density1b(self, vecs, density_tables=None):
         """m-scheme one-body transition densities of every pair of the states
-        `vecs` (dim x k, k <= 32): {'p': D_p, 'n': D_n} with
+        `vecs` (dim x k; above 32 states the pairs are computed in tiles of
+        two 16-state blocks, bsg_density1b taking 32 at most): {'p': D_p,
+        'n': D_n} with
         D[f, i, c, d] = <f| a+_c a_d |i>, c and d the combined s.p. indices of
         the builder (``extra['sp_orb_p']`` etc.).  `density_tables`: a
         ``bsg_density_tables`` (default: the builder's own, from these
@@ -178,6 +180,9 @@ class Hamiltonian:
             v = v[:, None]
         if v.shape[0] != self.dim:
             raise ValueError("vectors do not match the basis")
+        if v.shape[1] > 32:
+            from .densities import tiled_pairs
+            return tiled_pairs(v.shape[1], lambda idx: self.density1b(v[:, idx], density_tables))
         cols = np.ascontiguousarray(v.T)  # (k, dim): dim x k column-major
         ns = cols.shape[0]
         s = self.tables.s

@@ -168,3 +168,21 @@ def test_mg25ref_densities_from_oracle_equal_reference_res():
         ours = red[(b["i"], b["f"])][b["Jt"]] * sign[(min(b["i"], b["f"]), max(b["i"], b["f"]))]
         for a, c, t0, t1 in b["rho"]:
             assert abs(ours[a - 1, c - 1, 0] - t0) < 5e-5 and abs(ours[a - 1, c - 1, 1] - t1) < 5e-5
+
+
+@pytest.mark.parametrize("k", [5, 32, 33, 47])
+def test_tiled_pairs_cover_every_pair(k):
+    """More states than one bsg_density1b call takes: the tiles of two
+    16-state blocks give every (f, i) pair, checked with the oracle as the
+    per-call routine (limited to 32 states like the C ABI)."""
+    T = model.build_tables(model.sd_model(2, 1, seed=4, jz2=1))
+    X = np.random.default_rng(k).standard_normal((T.dim, k))
+
+    def call(idx):
+        assert len(idx) <= 32
+        Dp, Dn = od.bundled(T, X[:, idx])
+        return {"p": Dp, "n": Dn}
+
+    got = D.tiled_pairs(k, call)
+    Dp, Dn = od.bundled(T, X)
+    assert np.abs(got["p"] - Dp).max() < 1e-12 and np.abs(got["n"] - Dn).max() < 1e-12
