@@ -481,7 +481,6 @@ extern "C" int bsg_apply1b(bsg_ctx *ctx, const bsg_density_tables *dt, const dou
     const int64_t dim = ctx->dim;
     const int nq_p = ctx->t.nhsps_pl + ctx->t.nhsps_pr;
     const int nlab_p = nq_p * nq_p;
-    const int nq_n = ctx->t.nhsps_nl + ctx->t.nhsps_nr;
     int st = cuda_check(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
     if (st) return st;
     std::vector<RawSeg> raw;
@@ -550,7 +549,6 @@ extern "C" int bsg_apply1b(bsg_ctx *ctx, const bsg_density_tables *dt, const dou
         for (int t = 0; t < ng; ++t) cmax = std::max(cmax, groups[1][g0 + t].cnt);
         for (int32_t c0 = 0; c0 < cmax; c0 += kApplyCols) titems.push_back(ATItem{(int32_t)g0, ng, c0, 0});
     }
-    (void)nq_n;
 
     DevBuf d_in, d_out, d_g[2], d_it[2], d_seg;
     auto release = [&]() {
