@@ -122,3 +122,27 @@ def test_backward_bundles_equal_forward_in_oracle():
         assert np.abs(a - b).max() < 1e-12 * max(1.0, np.abs(b).max())
     Y, Yref = od.apply1b_bundled(alt, P, N, X), od.apply1b_bundled(T, P, N, X)
     assert np.abs(Y - Yref).max() < 1e-12 * max(1.0, np.abs(Yref).max())
+
+
+def test_pn_operator_elements_follow_their_species():
+    """A 'pns' operator: the proton table comes from the proton column, the
+    neutron table from the neutron one, with 1/sqrt(2J+1) and no isospin
+    factors (decouple1bodyop's pnoperators branch)."""
+    T = model.build_tables(model.sd_model(2, 2, seed=4, jz2=0))
+    text = "pns\n 3\n 1 0 2 1.5\n 2 0 2 2.5\n 3 1 0 0.5\n 0\n 2 2 1.0 0.0\n 3 3 0.0 2.0\n"
+    P, N = D.onebody_operator(T, D.read_opme(text))
+    orb_p, orb_n = T.extra["sp_orb_p"], T.extra["sp_orb_n"]
+    # J = 0: diagonal in (orbit, m), (-1)^(j-m) (j m, j -m | 0 0) = 1/sqrt(2j+1)
+    for q in range(len(orb_p)):
+        if orb_p[q] == 1:
+            assert abs(P[q, q] - 1.0 / np.sqrt(6.0)) < 1e-14
+        else:
+            assert P[q, q] == 0.0
+        if orb_n[q] == 2:
+            assert abs(N[q, q] - 2.0 / np.sqrt(2.0)) < 1e-14
+    assert np.count_nonzero(P - np.diag(np.diag(P))) == 0
+
+
+def test_read_opme_rejects_unknown_format():
+    with pytest.raises(ValueError):
+        D.read_opme("foo\n 3\n")
