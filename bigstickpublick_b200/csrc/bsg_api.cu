@@ -524,17 +524,21 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
             }
         }
     }
+    // CSR over (row, warp) slots; inside a slot the contributions keep their
+    // order (a counting sort by slot, stable in the input order)
     auto by_slot = [&](auto &v, const std::vector<uint8_t> &wv, std::vector<int32_t> &ptr, auto &flat,
                        std::vector<int32_t> *perm) {
         const int64_t nslot = nrows * W;
         std::vector<int64_t> key(v.size());
         for (size_t i = 0; i < v.size(); ++i) key[i] = (int64_t)v[i].first * W + wv[i];
-        std::vector<size_t> idx(v.size());
-        std::iota(idx.begin(), idx.end(), 0);
-        std::stable_sort(idx.begin(), idx.end(), [&](size_t x, size_t y) { return key[x] < key[y]; });
         ptr.assign(nslot + 1, 0);
         for (int64_t k : key) ptr[k + 1]++;
         for (int64_t r = 0; r < nslot; ++r) ptr[r + 1] += ptr[r];
+        std::vector<size_t> idx(v.size());
+        {
+            std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
+            for (size_t i = 0; i < v.size(); ++i) idx[fill[key[i]]++] = i;
+        }
         flat.resize(v.size());
         if (perm) perm->resize(v.size());
         for (size_t k = 0; k < idx.size(); ++k) {
