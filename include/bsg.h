@@ -4,7 +4,7 @@
  * The engine replaces BIGSTICK's on-the-fly factorized matvec and the Lanczos
  * loop around it.  The Fortran host keeps building the basis, sectors, jumps,
  * opbundles and uncoupled matrix elements; it passes plain pointers to those
- * module arrays through this ABI (ISO_C_BINDING).  The
+ * module arrays through this ABI (an ISO_C_BINDING interface block).  The
  * arrays are uploaded to the device unchanged; every derived index the GPU
  * kernels need lives in separate device buffers.
  *
