@@ -7,6 +7,7 @@ Reads (from the reference checkout given as argv[1], default /root/reference):
   examples/sd/input.mg25altwfn  same nucleus, scaling 0 1 1 1 (xspe = 0)
   examples/sd/output/mg25ref.res, mg25alt.res   10 lowest energies, J, T (5 decimals) and
                                                 every one-body density block (5 decimals)
+  examples/sd/output/mg25dx_dres.m              the same density blocks to 8 decimals
   examples/sd/output/mg25expectH.res, overlap.dat
                                                 <H> of the mg25ref states (6 decimals) and the
                                                 overlaps of mg25ref state 1 with mg25alt's states
@@ -151,6 +152,22 @@ def read_overlap(path):
     return {"initial": init, "finals": rows}
 
 
+def read_dres_m(path):
+    """The Mathematica-form density file of a density-from-wavefunction run:
+    state energies (8 decimals) and every (initial, final, Jt) block with
+    rows [a, b, rho_Tt=0, rho_Tt=1] (8 decimals)."""
+    txt = open(path).read()
+    states = re.search(r"densSetStates\[\{(.*?)\}\];", txt, re.S).group(1)
+    energies = [float(r.split(",")[1]) for r in re.findall(r"\{([^{}]*)\}", states) if r.strip()[:1].isdigit()]
+    blocks = []
+    for m in re.finditer(r"densMatElem\[\s*(\d+),\s*(\d+),\s*(\d+),\s*\{(.*?)\}\];", txt, re.S):
+        rows = [[float(x) for x in r.split(",")] for r in re.findall(r"\{([^{}]*)\}", m.group(4))]
+        if rows:
+            blocks.append({"i": int(m.group(1)), "f": int(m.group(2)), "Jt": int(m.group(3)),
+                           "rho": [[int(r[0]), int(r[1]), r[2], r[3]] for r in rows]})
+    return {"energies": energies, "blocks": blocks}
+
+
 def read_input(path):
     toks = [ln.split("!")[0].split() for ln in open(path)]
     toks = [t for t in toks if t]
@@ -183,6 +200,10 @@ def main():
     out["overlap"] = dict(read_overlap(os.path.join(ex, "output", "overlap.dat")),
                           file="examples/sd/output/overlap.dat",
                           of="state 1 of mg25ref against the 10 mg25alt states (input.mg25overlap)")
+    out["density_8dec"] = dict(read_dres_m(os.path.join(ex, "output", "mg25dx_dres.m")),
+                               file="examples/sd/output/mg25dx_dres.m",
+                               of="one-body densities of the 10 mg25ref states from their wavefunction file "
+                                  "(input.mg25denfromwfn), 8 decimals")
     out["spin_operator"] = {"file": "examples/sd/sdspin.opme",
                             "text": open(os.path.join(ex, "sdspin.opme")).read()}
     st = read_strength(os.path.join(ex, "output", "mg25spinstrength1.res"))
