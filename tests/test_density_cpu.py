@@ -153,6 +153,9 @@ def test_mg25ref_densities_from_oracle_equal_reference_res():
     Tq = model.build_tables(model.tsq_spec(spec))
     J = [model.j_from_jsq(float(Z[:, i] @ oracle.applyh(Jq, Z[:, i]))) for i in range(10)]
     Tv = [model.j_from_jsq(float(Z[:, i] @ oracle.applyh(Tq, Z[:, i]))) for i in range(10)]
+    # the J and T labels of the .res file
+    assert np.abs(np.array(J) - np.array([s["J"] for s in r["states"]])).max() < 1e-3
+    assert np.abs(np.array(Tv) - np.array([s["T"] for s in r["states"]])).max() < 1e-3
     Dp, Dn = od.bundled(T, Z)
     red = D.reduced(T, {"p": Dp, "n": Dn}, J, Tv)
     sign, big = {}, {}
