@@ -576,12 +576,19 @@ double coupled_with_prov(const Interaction &I, int a, int b, int c, int d, int J
     return sg * I.dv[q];
 }
 
+// sum the coefficients of each file line (in their order of appearance),
+// ascending lines, zeros dropped
 void compress(std::vector<std::pair<int, double>> &v) {
-    std::map<int, double> m;
-    for (auto &p : v) m[p.first] += p.second;
-    v.clear();
-    for (auto &p : m)
-        if (p.second != 0.0) v.push_back(p);
+    std::stable_sort(v.begin(), v.end(),
+                     [](const std::pair<int, double> &x, const std::pair<int, double> &y) { return x.first < y.first; });
+    size_t out = 0;
+    for (size_t i = 0; i < v.size();) {
+        const int line = v[i].first;
+        double sum = 0.0;
+        for (; i < v.size() && v[i].first == line; ++i) sum += v[i].second;
+        if (sum != 0.0) v[out++] = {line, sum};
+    }
+    v.resize(out);
 }
 
 int build(const bsg_model_spec *s, Built &B) {
