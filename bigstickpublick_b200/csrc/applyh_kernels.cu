@@ -71,8 +71,10 @@ constexpr auto rows_kernel() {
 template <typename T, int NB, int ITEMS>
 static int launch_one(bsg_ctx *ctx, const T *vin, T *vout, int ld, int v0, int accumulate,
                       cudaStream_t s, TileLookup lookup, double *cols) {
+    ctx->last_status = BSG_OK;
     const TileSet *ts = lookup ? lookup(ctx, 32 * ITEMS) : get_tiles(ctx, 32 * ITEMS);
-    if (!ts) return ctx->last_error.empty() ? BSG_ERR_NOMEM : BSG_ERR_CUDA;
+    // the status the failing lookup recorded (a refused size is BSG_ERR_ARG)
+    if (!ts) return ctx->last_status ? ctx->last_status : BSG_ERR_NOMEM;
     if (ts->ntiles == 0) return BSG_OK;
     RowArgs a = ctx->args;
     a.tiles = (const Tile *)ts->buf.p;

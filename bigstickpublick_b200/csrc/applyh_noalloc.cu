@@ -1,9 +1,9 @@
 // bsg_applyh_noalloc: applyH on host vectors without any device allocation.
 //
 // Some callers of this library cannot allocate device memory at the point
-// where they need a matvec: code running while a CUDA stream is being
-// captured into a graph (cudaMalloc is not allowed there), hosts whose device
-// memory is handed out by a fixed-budget pool owned by another component, and
+// where they need a matvec: hosts whose device memory is handed out by a
+// fixed-budget pool owned by another component (the pool takes the free
+// memory at start-up, so a later cudaMalloc fails or steals from it), and
 // Fortran/C drivers that must not grow the device footprint after set-up.
 // bsg_applyh with host pointers stages vin/vout in device buffers that it
 // allocates on first use; this entry point stages them instead in one
@@ -14,11 +14,19 @@
 //  * each staged vector (dim * nb * element size) must fit in
 //    BSG_NOALLOC_MAX_VECTOR_BYTES; larger calls are rejected with
 //    BSG_ERR_ARG before anything is copied;
+//  * the call is synchronous: it copies vin in, runs the matvec and copies
+//    vout back on the context's stream, then waits for that stream.  It must
+//    not be made while that stream is being captured into a CUDA graph (a
+//    synchronizing call would invalidate the capture); it checks, and returns
+//    BSG_ERR_ARG instead;
 //  * the first call on a device looks up the array's device address with
-//    cudaGetSymbolAddress (once per device, with that device current); make
-//    that first call before any stream capture;
-//  * the row tiles of the context are used when bsg_applyh already built
-//    them; otherwise the tile list is written into the same static array;
+//    cudaGetSymbolAddress (once per device, with that device current);
+//  * the row tiles of the context are used when an earlier bsg_applyh or
+//    bsg_lanczos call on the context built them; otherwise the tile list is
+//    written into the same static array, which holds at most
+//    kTileBytes / sizeof(Tile) = 65536 row tiles (a context with more gets
+//    BSG_ERR_ARG; an applyH made on it during set-up, when allocation is
+//    still allowed, caches its tiles and lifts the limit);
 //  * every call on every context of the process shares the array and leaves
 //    its contents behind; the kernel writes every output element, so nothing
 //    needs clearing, but two calls that overlap on the GPU (other host threads
@@ -70,8 +78,10 @@ const bsg::TileSet *static_tiles(bsg_ctx *ctx, int tp) {
     bsg::build_tile_list(ctx, tp, tiles);
     const size_t bytes = tiles.size() * sizeof(bsg::Tile);
     if (bytes > kTileBytes) {
-        bsg::set_err(ctx, BSG_ERR_ARG, "bsg_applyh_noalloc: more row tiles than the static array holds; "
-                                       "call bsg_applyh once on this context first");
+        bsg::set_err(ctx, BSG_ERR_ARG,
+                     "bsg_applyh_noalloc: " + std::to_string(tiles.size()) + " row tiles exceed the static array's " +
+                         std::to_string(kTileBytes / sizeof(bsg::Tile)) +
+                         "; an applyH on this context during set-up caches its tiles and lifts the limit");
         return nullptr;
     }
     cudaError_t e = cudaMemcpyAsync(t_tile_region, tiles.data(), bytes, cudaMemcpyHostToDevice, t_stream);
@@ -101,6 +111,11 @@ extern "C" int bsg_applyh_noalloc(bsg_ctx *ctx, const void *vin, void *vout, int
                                 " bytes exceeds the static staging limit of " + std::to_string(kVecBytes) + " bytes");
     int st = bsg::cuda_check(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
     if (st) return st;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if ((st = bsg::cuda_check(ctx, cudaStreamIsCapturing(ctx->stream, &cap), "cudaStreamIsCapturing"))) return st;
+    if (cap != cudaStreamCaptureStatusNone)
+        return bsg::set_err(ctx, BSG_ERR_ARG,
+                            "bsg_applyh_noalloc synchronizes its stream and cannot run while the stream is captured");
     void *base = nullptr;
     if ((st = scratch_address(ctx, &base))) return st;
     unsigned char *in = (unsigned char *)base, *out = in + kVecBytes;

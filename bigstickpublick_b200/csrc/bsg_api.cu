@@ -23,7 +23,10 @@
 namespace bsg {
 
 int set_err(bsg_ctx *ctx, int code, const std::string &msg) {
-    if (ctx) ctx->last_error = msg;
+    if (ctx) {
+        ctx->last_error = msg;
+        ctx->last_status = code;
+    }
     return code;
 }
 

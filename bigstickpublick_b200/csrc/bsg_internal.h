@@ -131,6 +131,7 @@ struct bsg_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::string last_error;
+    int last_status = 0;      // status of the last set_err
     bsg_tables t{};           // sizes only (pointers are host-owned by caller)
     int64_t dim = 0, nrows = 0;
     int32_t max_rowlen = 0;

@@ -144,8 +144,9 @@ extern "C" int bsg_grad(bsg_ctx *ctx, const double *evecs, int nstates, double *
     const size_t nsp = (size_t)ctx->t.nsd_p, nsn = (size_t)ctx->t.nsd_n;
     DevBuf psi, gpp, gnn, gpn, gsp, gsn;
     constexpr int ITEMS = 4;
+    ctx->last_status = BSG_OK;
     const TileSet *ts = get_tiles(ctx, 32 * ITEMS);
-    if (!ts) return ctx->last_error.empty() ? BSG_ERR_NOMEM : BSG_ERR_CUDA;
+    if (!ts) return ctx->last_status ? ctx->last_status : BSG_ERR_NOMEM;
     if ((st = dev_alloc(ctx, psi, sizeof(double) * n)) || (st = dev_alloc(ctx, gpp, sizeof(double) * npp)) ||
         (st = dev_alloc(ctx, gnn, sizeof(double) * nnn)) || (st = dev_alloc(ctx, gpn, sizeof(double) * npn)) ||
         (st = dev_alloc(ctx, gsp, sizeof(double) * nsp)) || (st = dev_alloc(ctx, gsn, sizeof(double) * nsn))) {

@@ -174,14 +174,17 @@ int  bsg_applyh_stream(bsg_ctx *ctx, const void *vin, void *vout, int nb, int pr
 
 /* ---- applyH on host vectors with no device allocation.  No counterpart in
  *      the reference.  For callers that cannot allocate device memory when
- *      they need a matvec (code running under CUDA stream capture, where
- *      cudaMalloc is not allowed; hosts whose device memory is a fixed pool
- *      owned by another component): vin/vout are staged through one static
+ *      they need a matvec: hosts whose device memory is a fixed pool owned by
+ *      another component, and drivers that must not grow the device
+ *      footprint after set-up.  vin/vout are staged through one static
  *      __device__ array instead of buffers allocated on first use.  Each
  *      vector (dim*nb*element size) must fit in BSG_NOALLOC_MAX_VECTOR_BYTES,
- *      else BSG_ERR_ARG.  The first call on a device looks up the array's
- *      address; make it before any stream capture.  All calls in the process
- *      share the array: calls that overlap on the GPU race.  Same semantics as
+ *      else BSG_ERR_ARG.  The call is synchronous on the context's stream and
+ *      returns BSG_ERR_ARG if that stream is being captured.  The first call
+ *      on a device looks up the array's address.  Row tiles: the context's
+ *      own when an earlier applyH built them, else at most 65536 tiles in the
+ *      static array (more: BSG_ERR_ARG).  All calls in the process share the
+ *      array: calls that overlap on the GPU race.  Same semantics as
  *      bsg_applyh otherwise (host pointers only, BSG_ACCUMULATE honoured). ---- */
 #define BSG_NOALLOC_MAX_VECTOR_BYTES (8u << 20)
 int  bsg_applyh_noalloc(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec, int flags);

@@ -1,6 +1,6 @@
 """Regenerate tests/golden/mg25.json from the reference's own example files.
 
-Reads (from the reference checkout given as argv[1], default /root/reference):
+Reads (from the reference checkout given as argv[1], a required argument):
   examples/sd/sd.sps            orbits (isospin format)
   examples/sd/usdb.int          USDB interaction (63 TBMEs + 3 SPEs)
   examples/sd/input.mg25ref     4 protons, 5 neutrons, 2Jz = 1, scaling 1 18 25 0.3
@@ -180,7 +180,9 @@ def read_input(path):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_golden.py <reference checkout> (the BIGSTICK source tree holding examples/sd)")
+    ref = sys.argv[1]
     ex = os.path.join(ref, "examples", "sd")
     orbits = model.read_sps(os.path.join(ex, "sd.sps"))
     spe, tbme = model.read_int(os.path.join(ex, "usdb.int"), len(orbits))

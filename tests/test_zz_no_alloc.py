@@ -1,9 +1,9 @@
 """bsg_applyh_noalloc: the host-vector applyH that allocates no device memory.
 
 It exists for callers that cannot allocate device memory at the time of the
-matvec (for example code running while a CUDA stream is captured into a
-graph, or a host whose device memory is a fixed pool owned by someone else).
-It stages vectors through a fixed static device array, so its results must be
+matvec (a host whose device memory is a fixed pool owned by another
+component, or a driver whose device footprint is fixed after set-up).  It
+stages vectors through a fixed static device array, so its results must be
 those of the ordinary bsg_applyh entry point.  This file is collected last so
 that a stop-at-first-failure run has already run every other test.
 """
@@ -28,7 +28,7 @@ def _noalloc(H, vin, vout, nb, prec, flags=0):
 
 @pytest.mark.parametrize("builder", [lambda: model.sd_model(2, 2, seed=1),
                                      lambda: model.pf_model(2, 2, seed=5)])
-@pytest.mark.parametrize("prec,nb", [(8, 1), (4, 1), (8, 4), (4, 8)])
+@pytest.mark.parametrize("prec,nb", [(8, 1), (4, 1), (8, 3), (8, 4), (4, 8)])
 def test_noalloc_matches_applyh_twice(builder, prec, nb):
     from bigstickpublick_b200.engine import Hamiltonian
     T = model.build_tables(builder())
@@ -69,4 +69,46 @@ def test_noalloc_rejects_oversize_vectors():
     H.lib.bsg_last_error(H.h, buf, 256)
     assert b"static staging limit" in buf.value
     assert not out.any()
+    H.close()
+
+
+def _spe_rows(nrows, seed=3):
+    """An SPE-only Hamiltonian of nrows proton SDs with one neutron SD each
+    (rows of one state, so one 32-position row tile per row): H is the
+    diagonal pspe + nspe (the SPE case of src/bapplyhlibOMP.f90:988-1011)."""
+    rng = np.random.default_rng(seed)
+    i8 = lambda *x: np.array(x, dtype=np.int64)
+    a = {k: np.zeros(0, dtype=v.dtype) for k, v in model.build_tables(model.sd_model(1, 0, seed=12, jz2=1)).a.items()}
+    a.update(pstart=np.arange(nrows, dtype=np.int64), nstart=i8(1),
+             hmatpp=np.zeros(1, np.float32), hmatnn=np.zeros(1, np.float32), hmatpn=np.zeros(1, np.float32),
+             cpnpair=i8(0), dpnpair=i8(0), pspe_h=rng.standard_normal(nrows).astype(np.float32),
+             nspe_h=np.array([0.25], np.float32), optype=np.array([1], np.int32), hchar=np.array([ord("f")], np.int32),
+             pxstart=i8(1), pxend=i8(nrows), nxstart=i8(1), nxend=i8(1), cstride=i8(1))
+    s = dict(dimbasis=nrows, nsd_p=nrows, nsd_n=1, np1b=0, nn1b=0, np2b=0, nn2b=0, nmatpp=1, nmatnn=1, nmatpn=1,
+             nhsps_pl=0, nhsps_pr=0, nhsps_nl=0, nhsps_nr=0, call_spe=1, nbundles=1)
+    return model.Tables(a, s, {})
+
+
+def test_noalloc_tile_limit_status_and_cached_tiles():
+    """A fresh context with more row tiles than the static array holds is
+    refused with BSG_ERR_ARG and a message; once an applyH on the context (at
+    set-up, where allocation is allowed) has cached its tiles, the same call
+    works and matches bsg_applyh, twice in a row."""
+    from bigstickpublick_b200.engine import Hamiltonian
+    T = _spe_rows(70000)
+    H = Hamiltonian(T)
+    vin = np.random.default_rng(1).standard_normal(T.dim)
+    out = np.zeros_like(vin)
+    assert _noalloc(H, vin, out, 1, 8) == 7  # BSG_ERR_ARG
+    buf = C.create_string_buffer(256)
+    H.lib.bsg_last_error(H.h, buf, 256)
+    assert b"row tiles exceed" in buf.value
+    assert not out.any()
+    ref = H.applyh(vin)
+    diag = T.a["pspe_h"].astype(np.float32) + np.float32(0.25)
+    assert np.abs(ref - diag.astype(np.float64) * vin).max() < 1e-12
+    for _ in range(2):
+        got = np.full_like(vin, np.nan)
+        assert _noalloc(H, vin, got, 1, 8) == 0
+        assert np.array_equal(got, ref)
     H.close()
