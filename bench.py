@@ -1,22 +1,33 @@
 #!/usr/bin/env python
 """Benchmark: BIGSTICK M-scheme applyH on B200.
 
-Default workload: sd shell, 6 protons + 6 neutrons, 2Jz = 0 (M-scheme dim
-93,710), seeded synthetic isospin interaction (63 TBMEs ~ N(0,1) MeV, seed 2,
-SPEs -3.9/-3.2/+2.1 MeV), FP32 applyH (fp32 matrix elements, fp32 vectors,
-fp32 accumulation).  One step = one applyH over one vector.
+Default workload (the largest single-GPU configuration): pf shell
+(0f7/2, 1p3/2, 0f5/2, 1p1/2), 6 protons + 6 neutrons, 2Jz = 0 (M-scheme dim
+109,954,620), seeded synthetic isospin interaction (195 TBMEs ~ N(0,1) MeV
+and 4 SPEs, seed 5), FP32 applyH (fp32 matrix elements, fp32 vectors, fp32
+accumulation).  One step = one applyH over one vector (152,771,809,712
+inner-loop updates).
 
-Timing: W warm-up matvecs, then exactly K timed matvecs; before every timed
-matvec the L2 is flushed by writing a 256 MiB buffer, and the matvec kernel
-itself is timed with CUDA events on its stream; barrier + synchronize on both
-sides; max over ranks.  `e2e` calls the C ABI with pinned host buffers, so
-the host->device copy of the input and the device->host copy of the output
-are inside each timed step.
+Timing: W warm-up matvecs, then exactly K timed matvecs; the vectors (0.44 GB
+each) are larger than the 126 MB L2 and a 256 MiB buffer is also written
+before every timed matvec; the matvec kernel is timed with CUDA events on its
+stream; barrier + synchronize on both sides; max over ranks.  `e2e` calls the
+C ABI with pinned host buffers, so the host->device copy of the input and the
+device->host copy of the output are inside each timed step.
+
+Legs beside the headline (rank 0): Lanczos on sd 6p6n (FP64 against mixed),
+time to a 1e-6 solution on pf 4p4n (FP64 scalar against mixed scalar and
+mixed block nb = 8), the 256-system batch with its gradients, the pf 6p6n
+thick-restart solve (mixed against FP64 on the same schedule) with the
+ground-state gradient, one-body densities; each reports its eigenvalue and
+wavefunction-overlap error against FP64.
 
 `--impl reference` times the reference's CPU algorithm for this path on the
 host cores: the reference is Fortran and no Fortran compiler exists in this
-image, so it runs the oracle's C restatement of applyHbundled_g with its
-OpenMP partition (kind "port").
+image, so it runs the oracle's C restatement of applyHbundled_omp with its
+owner-computes OpenMP partition (kind "port"), each step a bounded sample of
+the same matvec (a slice of every thread's output rows), scaled to matvec/s
+by the exact share of the inner-loop updates it covered.
 
 Multi-GPU: the matvec does not shard across GPUs in this build; --gpus N runs
 N independent replicas (one per rank) and reports the aggregate rate.
@@ -38,10 +49,14 @@ METRIC = "applyH matvec/s & HBM-roofline %, mixed vs FP64 GPU at ≤1e-6 rel eig
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 WORKLOADS = {
     # name: (shell, np, nn, jz2, seed)
-    "sd6p6n": ("sd", 6, 6, 0, 2),
     "sd2p2n": ("sd", 2, 2, 0, 1),
+    "sd6p6n": ("sd", 6, 6, 0, 2),
     "pf4p4n": ("pf", 4, 4, 0, 3),
+    "pf5p5n": ("pf", 5, 5, 0, 5),
+    "pf6p5n": ("pf", 6, 5, 1, 5),
+    "pf6p6n": ("pf", 6, 6, 0, 5),
 }
+DEFAULT_WORKLOAD = "pf6p6n"
 
 
 def load_peaks():
@@ -147,23 +162,81 @@ def table_checksum(tables):
     return h.hexdigest()
 
 
+class CpuSampler:
+    """The reference arm's matvec on the host cores, in bounded samples.
+
+    applyHbundled_omp gives every OpenMP thread the output rows getLoadDist
+    assigns it (src/bapplyhlibOMP.f90:34-868); the oracle restates that
+    owner-computes matvec.  A sample runs a slice of every owner range (the
+    rows holding the fraction `frac` of that range's inner-loop updates,
+    starting at fraction `offset`), so it touches the whole basis the way the
+    full matvec does, and the rate is scaled by the exact share of updates it
+    covered."""
+
+    def __init__(self, tables, nb=1, prec=4, nthreads=None, seed=0):
+        import oracle
+        self.oracle = oracle
+        self.T = tables
+        self.nb, self.prec = nb, prec
+        self.nthreads = nthreads or os.cpu_count()
+        self.rs, self.ops = oracle.row_ops(tables)
+        self.csum = np.cumsum(self.ops)
+        self.total = int(self.csum[-1])
+        self.ends = np.append(self.rs[1:], tables.dim)
+        # one owner range per thread, as getLoadDist assigns them
+        self.owners = oracle.owner_ranges(self.rs, self.ops, tables.dim, self.nthreads)
+        dt = np.float32 if prec == 4 else np.float64
+        self.vin = np.random.default_rng(seed).standard_normal(tables.dim * nb).astype(dt)
+        self.out = np.zeros_like(self.vin)
+
+    def ranges(self, frac, offset=0.0):
+        """Row ranges of one sample and the updates they hold."""
+        out, n = [], 0
+        for lo, hi in self.owners:
+            i0, i1 = int(np.searchsorted(self.rs, lo)), int(np.searchsorted(self.rs, hi))
+            if i1 <= i0:
+                continue
+            base = int(self.csum[i0 - 1]) if i0 > 0 else 0
+            w = int(self.csum[i1 - 1]) - base
+            off = (offset % 1.0) * w
+            a = min(i1 - 1, int(np.searchsorted(self.csum, base + off, side="right")))
+            b = min(i1, max(a + 1, int(np.searchsorted(self.csum, base + off + frac * w, side="left")) + 1))
+            out.append((int(self.rs[a]), int(self.ends[b - 1])))
+            n += int(self.csum[b - 1]) - (int(self.csum[a - 1]) if a > 0 else 0)
+        return np.array(out, dtype=np.int64).reshape(-1, 2), n
+
+    def run(self, frac, offset=0.0):
+        """(share of one matvec covered, seconds)."""
+        rg, n = self.ranges(frac, offset)
+        t0 = time.perf_counter()
+        self.oracle.applyh_owner(self.T, self.vin, rg, nb=self.nb, nthreads=self.nthreads, out=self.out)
+        return n / self.total, time.perf_counter() - t0
+
+    def calibrate(self, budget_s):
+        """The sample fraction that takes about budget_s seconds: the fixed
+        cost of a sample (every owner scans its bundles' jump lists, as the
+        reference's 'b' bundles do) measured apart from the cost per share."""
+        _, t0 = self.run(1e-6)
+        f = 1e-3
+        share, el = self.run(f)
+        while el - t0 < 0.2 and f < 1.0:
+            f = min(1.0, f * 8)
+            share, el = self.run(f)
+        per = max(el - t0, 1e-6) / max(share, 1e-12)
+        return float(min(1.0, max(1e-4, (budget_s - t0) / per)))
+
+
 def cpu_baseline(tables, nb, prec, budget_s=10.0, nthreads=None):
-    import oracle
-    dt = np.float32 if prec == 4 else np.float64
-    rng = np.random.default_rng(0)
-    vin = rng.standard_normal(tables.dim * nb).astype(dt)
-    out = np.zeros_like(vin)
-    nthreads = nthreads or os.cpu_count()
-    oracle.applyh_omp(tables, vin, nb=nb, nthreads=nthreads, out=out)  # warm-up
-    n, t0 = 0, time.perf_counter()
-    while True:
-        out[:] = 0
-        oracle.applyh_omp(tables, vin, nb=nb, nthreads=nthreads, out=out)
-        n += 1
-        el = time.perf_counter() - t0
-        if el > budget_s or n >= 2000:
-            break
-    return n / el, nthreads, n, el
+    """matvec/s of the oracle's owner-computes OpenMP matvec on all host
+    cores, timed on bounded samples of about budget_s seconds in total."""
+    cs = CpuSampler(tables, nb, prec, nthreads)
+    frac = cs.calibrate(budget_s / 3)
+    shares, secs = 0.0, 0.0
+    for k in range(3):
+        sh, el = cs.run(frac, offset=0.37 * (k + 1))
+        shares += sh
+        secs += el
+    return shares / secs, cs.nthreads, shares, secs
 
 
 def traffic_from_profile(workload, nb, prec):
@@ -177,60 +250,112 @@ def traffic_from_profile(workload, nb, prec):
         return None
 
 
-def lanczos_leg(H, tables, args):
-    """The eigenvalue side of the metric: FP64 vs mixed (FP32 applyH, FP64
-    Lanczos) on the same workload and pivot, lowest 10 states, fixed
-    iteration count; relative eigenvalue error of mixed vs FP64 and the
-    iterations per second of each.  For the pf 4p4n workload also the block
-    (nb = 8) mixed run with thick restart keeping 20 vectors."""
-    import torch
-    rng = np.random.default_rng(11)
-    piv = rng.standard_normal(tables.dim)
-    out = {}
-    niter = args.lanczos_iters
-    runs = {}
-    # untimed warm-up solves: the first use of a kernel loads its code
-    for prec in (8, 4):
-        H.lanczos(nkeep=2, niter=6, matvec_prec=prec, fixed_iter=True, pivot=piv)
-    for name, prec in (("fp64", 8), ("mixed", 4)):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        ev, _, rep = H.lanczos(nkeep=10, niter=niter, matvec_prec=prec, fixed_iter=True, pivot=piv)
-        torch.cuda.synchronize()
-        el = time.perf_counter() - t0
-        runs[name] = (ev, rep, el)
-        # rates on the solver's own device clock (CUDA events around the whole
-        # solve, host-driven steps included); the Python wall time beside it
-        tot = rep["t_total_ms"] / 1e3
-        out[name] = {"iterations": rep["total_iterations"], "its_per_s": rep["total_iterations"] / tot,
-                     "solve_s": tot, "wall_s": el, "t_matvec_ms": rep["t_matvec_ms"], "t_reorth_ms": rep["t_reorth_ms"],
-                     "t_eig_ms": rep["t_eig_ms"], "lowest": [float(x) for x in ev[:3]]}
-    e64, e32 = runs["fp64"][0], runs["mixed"][0]
-    out["mixed_vs_fp64_max_rel_eig_err"] = float(np.max(np.abs(e32 - e64) / np.abs(e64)))
-    out["speedup_its_per_s"] = out["mixed"]["its_per_s"] / out["fp64"]["its_per_s"]
-    out["config"] = f"{niter} iterations, lowest 10, fixed iteration count, seeded generic pivot"
-    if args.block_leg:
-        nb = 8
-        pivb = rng.standard_normal(tables.dim * nb)
-        H.lanczos(nkeep=2, niter=3, nb=nb, matvec_prec=4, fixed_iter=True, pivot=pivb)  # untimed warm-up
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        evb, _, repb = H.lanczos(nkeep=10, niter=args.block_iters, nb=nb, nthick_add=10, max_restarts=args.block_restarts,
-                                 matvec_prec=4, converge_tol=1e-9, pivot=pivb)
-        torch.cuda.synchronize()
-        elb = time.perf_counter() - t0
-        totb = repb["t_total_ms"] / 1e3
-        out["block_mixed"] = {"nb": nb, "keep": 20, "iterations": repb["total_iterations"], "restarts": repb["restarts"],
-                              "vector_matvecs_per_s": repb["total_iterations"] * nb / totb, "solve_s": totb, "wall_s": elb,
-                              "max_rel_eig_err_vs_fp64": float(np.max(np.abs(evb - e64) / np.abs(e64))),
-                              "converged": repb["converged"], "t_matvec_ms": repb["t_matvec_ms"],
-                              "t_reorth_ms": repb["t_reorth_ms"], "t_eig_ms": repb["t_eig_ms"]}
-        out["block_vs_fp64_vector_matvec_rate"] = out["block_mixed"]["vector_matvecs_per_s"] / out["fp64"]["its_per_s"]
-        out["fp64"]["vector_matvecs_per_s"] = out["fp64"]["its_per_s"]
+def compare_states(ev, vecs, ev_ref, vecs_ref):
+    """max relative eigenvalue error and the smallest |<psi|psi_ref>| over the
+    states (vectors dim x k, normalized)."""
+    ev, ev_ref = np.asarray(ev), np.asarray(ev_ref)
+    k = min(len(ev), len(ev_ref))
+    out = {"max_rel_eig_err": float(np.max(np.abs(ev[:k] - ev_ref[:k]) / np.abs(ev_ref[:k])))}
+    if vecs is not None and vecs_ref is not None:
+        ov = [abs(float(vecs[:, j] @ vecs_ref[:, j])) for j in range(k)]
+        out["min_overlap"] = float(min(ov))
+        out["overlaps"] = [float(x) for x in ov]
     return out
 
 
-def density_leg(H, tables, args, k=10, reps=5):
+def _solve(H, **kw):
+    import torch
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ev, vecs, rep = H.lanczos(**kw)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    tot = rep["t_total_ms"] / 1e3
+    nb = kw.get("nb", 1)
+    info = {"iterations": rep["total_iterations"], "restarts": rep["restarts"], "converged": rep["converged"],
+            "vector_matvecs": rep["matvecs"] * nb, "solve_s": tot, "wall_s": wall,
+            "its_per_s": rep["total_iterations"] / tot, "vector_matvecs_per_s": rep["matvecs"] * nb / tot,
+            "t_matvec_ms": rep["t_matvec_ms"], "t_reorth_ms": rep["t_reorth_ms"], "t_eig_ms": rep["t_eig_ms"]}
+    return ev, vecs, info
+
+
+def lanczos_sd6p6n_leg(args):
+    """sd 6p6n, lowest 10 states, 300 iterations (fixed) from one seeded
+    pivot: FP64 applyH against mixed (FP32 applyH, FP64 Lanczos); the mixed
+    run's eigenvalue and wavefunction-overlap error against FP64, and the
+    iterations per second of each."""
+    from bigstickpublick_b200.engine import Hamiltonian
+    T = make_tables("sd6p6n")
+    H = Hamiltonian(T)
+    try:
+        piv = np.random.default_rng(11).standard_normal(T.dim)
+        for prec in (8, 4):  # untimed: the first use of a kernel loads its code
+            H.lanczos(nkeep=2, niter=6, matvec_prec=prec, fixed_iter=True, pivot=piv)
+        out = {}
+        res = {}
+        for name, prec in (("fp64", 8), ("mixed", 4)):
+            ev, vecs, info = _solve(H, nkeep=10, niter=args.lanczos_iters, matvec_prec=prec, fixed_iter=True,
+                                    pivot=piv, want_vectors=True)
+            res[name] = (ev, vecs)
+            info["lowest"] = [float(x) for x in ev[:3]]
+            out[name] = info
+        out["mixed"].update(compare_states(*res["mixed"], *res["fp64"]))
+        out["speedup_its_per_s"] = out["mixed"]["its_per_s"] / out["fp64"]["its_per_s"]
+        out["config"] = (f"sd 6p6n, {args.lanczos_iters} iterations (fixed), lowest 10, seeded generic pivot; "
+                         "errors of mixed against FP64 from the same pivot")
+        return out
+    finally:
+        H.close()
+
+
+def time_to_solution_leg(args):
+    """pf 4p4n, lowest 10 states to a relative eigenvalue error of 1e-6:
+    FP64 scalar Lanczos (the plain FP64 GPU path), mixed scalar and mixed
+    block (nb = 8), each with thick restart and the reference's convergence
+    test at the same tolerance, timed on the solver's device clock.  Errors
+    are against a tightly converged FP64 solve from the same pivot.  Also the
+    one-body density leg on the same Hamiltonian."""
+    from bigstickpublick_b200.engine import Hamiltonian
+    T = make_tables("pf4p4n")
+    H = Hamiltonian(T)
+    try:
+        rng = np.random.default_rng(11)
+        piv = rng.standard_normal(T.dim)
+        pivb = rng.standard_normal((T.dim, 8))
+        pivb[:, 0] = piv
+        pivb = pivb.reshape(-1)
+        for prec in (8, 4):
+            H.lanczos(nkeep=2, niter=6, matvec_prec=prec, fixed_iter=True, pivot=piv)
+        H.lanczos(nkeep=2, niter=3, nb=8, matvec_prec=4, fixed_iter=True, pivot=pivb)
+        scal = dict(nkeep=10, niter=args.tts_niter, nthick_add=10, max_restarts=200)
+        ev_ref, v_ref, info_ref = _solve(H, matvec_prec=8, converge_tol=1e-9, pivot=piv, want_vectors=True, **scal)
+        out = {"reference": dict(info_ref, converge_tol=1e-9, lowest=[float(x) for x in ev_ref[:3]])}
+        runs = [("fp64", dict(matvec_prec=8, pivot=piv, **scal)),
+                ("mixed", dict(matvec_prec=4, pivot=piv, **scal)),
+                ("block8_mixed", dict(nkeep=10, niter=args.tts_block_niter, nb=8, nthick_add=10, max_restarts=200,
+                                      matvec_prec=4, pivot=pivb))]
+        for name, kw in runs:
+            ev, vecs, info = _solve(H, converge_tol=args.tts_tol, want_vectors=True, **kw)
+            info.update(compare_states(ev, vecs, ev_ref, v_ref))
+            info["meets_1e-6"] = info["max_rel_eig_err"] <= 1e-6
+            out[name] = info
+        for name in ("mixed", "block8_mixed"):
+            out[name]["speedup_time_to_solution_vs_fp64"] = out["fp64"]["solve_s"] / out[name]["solve_s"]
+            out[name]["its_per_s_vs_fp64"] = out[name]["its_per_s"] / out["fp64"]["its_per_s"]
+        out["config"] = (f"pf 4p4n, lowest 10, keep 20 on thick restart, convergence test option 0 at tol "
+                         f"{args.tts_tol} MeV; scalar {args.tts_niter} iterations per cycle, block nb=8 "
+                         f"{args.tts_block_niter} block iterations per cycle; errors against FP64 converged to 1e-9")
+        if not args.no_density:
+            try:
+                out["density"] = density_leg(H, T)
+            except Exception as e:  # a failing leg must not cost the headline line
+                out["density"] = {"error": repr(e)[:300]}
+        return out
+    finally:
+        H.close()
+
+
+def density_leg(H, tables, k=10, reps=5):
     """One-body transition densities of every pair of k states (bsg_density1b):
     device time of its kernels (CUDA events inside the call) and the call's
     wall time with host vectors in and host densities out; and a one-body
@@ -260,8 +385,8 @@ def density_leg(H, tables, args, k=10, reps=5):
     for _ in range(reps):
         H.apply1b(P, N, X)
         ams.append(H.stats()["apply1b_ms"])
-    return {"states": k, "pairs": k * k, "rows": rows, "kernel_ms": kms, "e2e_ms": float(np.median(wall)) * 1e3,
-            "launches": st["density_launches"],
+    return {"workload": "pf4p4n", "states": k, "pairs": k * k, "rows": rows, "kernel_ms": kms,
+            "e2e_ms": float(np.median(wall)) * 1e3, "launches": st["density_launches"],
             "fp64_gflop_per_s": 2.0 * rows * k * k / (kms * 1e-3) / 1e9,
             "gathered_gb_per_s": rows * 2 * k * 8 / (kms * 1e-3) / 1e9,
             "h2d_bytes": tables.dim * k * 8,
@@ -271,9 +396,10 @@ def density_leg(H, tables, args, k=10, reps=5):
 def batch_leg(args):
     """Config 4: 256 sd-shell Hamiltonians (seeds 1000..1255, valence Z and N
     uniform in 2..8), one persistent launch per batched matvec, lock-step
-    Lanczos with one captured graph per iteration, then the adjoint gradient
-    of the lowest 5 eigenvalues of every system with respect to its 63 TBMEs
-    and 3 SPEs."""
+    Lanczos with one captured graph per iteration (FP64 applyH, and mixed:
+    FP32 applyH, with its eigenvalue and overlap error against FP64 over all
+    systems), then the adjoint gradient of the lowest 5 eigenvalues of every
+    system with respect to its 63 TBMEs and 3 SPEs."""
     import torch
     from bigstickpublick_b200 import model
     from bigstickpublick_b200.engine import Batch
@@ -283,96 +409,99 @@ def batch_leg(args):
     t0 = time.perf_counter()
     cache = os.path.join(ROOT, ".tune_cache", "batch_tuning.json") if args.tune_cache else None
     b = Batch(tabs, autotune=True, tune_cache=cache)
-    t_create = time.perf_counter() - t0
-    dims = [t.dim for t in tabs]
-    vin = [torch.randn(d, dtype=torch.float32, device="cuda") for d in dims]
-    vout = [torch.empty_like(v) for v in vin]
-    for _ in range(3):
-        b.applyh(vin, vout)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(20):
-        b.applyh(vin, vout)
-    e1.record()
-    torch.cuda.synchronize()
-    mv_ms = e0.elapsed_time(e1) / 20
-    ev, vecs, rep = b.lanczos(nkeep=5, niter=args.batch_iters, matvec_prec=8, want_vectors=True)
-    t0 = time.perf_counter()
-    grads = []
-    for s, t in enumerate(tabs):
-        g = b.system(s).grad(vecs[s])
-        grads.append([model.chain_rule(t, {k: v[i] for k, v in g.items()}) for i in range(5)])
-    t_grad = time.perf_counter() - t0
-    b.close()
-    return {"systems": len(tabs), "dims_min": min(dims), "dims_max": max(dims), "dims_sum": int(sum(dims)),
-            "tuning": b.tuning, "build_s": t_build, "create_s": t_create,
-            "batched_matvec_ms": mv_ms, "system_matvecs_per_s": len(tabs) / (mv_ms / 1e3),
-            "lanczos_iters": args.batch_iters, "lanczos_graph_ms": rep["t_matvec_ms"],
-            "lanczos_eig_ms": rep["t_eig_ms"], "grad_s_all_systems_5_states": t_grad,
-            "ground_states_first4": [float(x) for x in ev[:4, 0]]}
+    try:
+        t_create = time.perf_counter() - t0
+        dims = [t.dim for t in tabs]
+        vin = [torch.randn(d, dtype=torch.float32, device="cuda") for d in dims]
+        vout = [torch.empty_like(v) for v in vin]
+        for _ in range(3):
+            b.applyh(vin, vout)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(20):
+            b.applyh(vin, vout)
+        e1.record()
+        torch.cuda.synchronize()
+        mv_ms = e0.elapsed_time(e1) / 20
+        res = {}
+        for name, prec in (("fp64", 8), ("mixed", 4)):
+            t0 = time.perf_counter()
+            ev, vecs, rep = b.lanczos(nkeep=5, niter=args.batch_iters, matvec_prec=prec, want_vectors=True)
+            res[name] = (ev, vecs, rep, time.perf_counter() - t0)
+        ev64, v64 = res["fp64"][0], res["fp64"][1]
+        evm, vm = res["mixed"][0], res["mixed"][1]
+        rel = np.abs(evm - ev64) / np.abs(ev64)
+        ovl = np.array([[abs(float(vm[s][:, j] @ v64[s][:, j])) for j in range(5)] for s in range(len(tabs))])
+        t0 = time.perf_counter()
+        for s, t in enumerate(tabs):
+            g = b.system(s).grad(v64[s])
+            [model.chain_rule(t, {k: v[i] for k, v in g.items()}) for i in range(5)]
+        t_grad = time.perf_counter() - t0
+        return {"systems": len(tabs), "dims_min": min(dims), "dims_max": max(dims), "dims_sum": int(sum(dims)),
+                "tuning": b.tuning, "build_s": t_build, "create_s": t_create,
+                "batched_matvec_ms": mv_ms, "system_matvecs_per_s": len(tabs) / (mv_ms / 1e3),
+                "lanczos_iters": args.batch_iters,
+                "fp64": {"graph_ms": res["fp64"][2]["t_matvec_ms"], "eig_ms": res["fp64"][2]["t_eig_ms"],
+                         "wall_s": res["fp64"][3]},
+                "mixed": {"graph_ms": res["mixed"][2]["t_matvec_ms"], "eig_ms": res["mixed"][2]["t_eig_ms"],
+                          "wall_s": res["mixed"][3], "max_rel_eig_err": float(rel.max()),
+                          "min_overlap": float(ovl.min())},
+                "grad_s_all_systems_5_states": t_grad,
+                "ground_states_first4": [float(x) for x in ev64[:4, 0]]}
+    finally:
+        b.close()
 
 
-def large_leg(args):
-    """Config 5: pf shell 6p6n, 2Jz = 0 (M-scheme dim 109,954,620), seeded
-    synthetic pf interaction; FP32 applyH rate, thick-restart mixed-precision
-    Lanczos for the lowest 5 states (FP64 history and reorthogonalization),
-    adjoint gradient of the ground state w.r.t. all 195 TBMEs and 4 SPEs,
-    everything resident in device memory."""
+def large_leg(H, T, args):
+    """Config 5 (the headline workload): thick-restart Lanczos for the lowest
+    5 states, keep 20, mixed (FP32 applyH, FP64 history and
+    reorthogonalization) and FP64 on the same fixed schedule from the same
+    seeded pivot, so that their difference is the precision alone; each
+    state's FP64 residual |H psi - E psi| / |E|; the adjoint gradient of the
+    ground state w.r.t. all 195 TBMEs and 4 SPEs with the Euler identity
+    E = sum V dE/dV + sum e dE/de; everything resident in device memory."""
     import torch
     from bigstickpublick_b200 import model
-    from bigstickpublick_b200.engine import Hamiltonian
+    piv = np.random.default_rng(11).standard_normal(T.dim)
+    kw = dict(nkeep=5, niter=args.large_iters, nthick_add=15, max_restarts=args.large_restarts, fixed_iter=True,
+              pivot=piv, want_vectors=True)
+    res, out = {}, {}
+    for name, prec in (("mixed", 4), ("fp64", 8)):
+        ev, vecs, info = _solve(H, matvec_prec=prec, **kw)
+        # FP64 residuals of the returned Ritz pairs
+        r = []
+        for j in range(len(ev)):
+            x = torch.from_numpy(np.ascontiguousarray(vecs[:, j])).cuda()
+            y = H.applyh(x)
+            r.append(float(torch.linalg.vector_norm(y - ev[j] * x).item() / abs(ev[j])))
+            del x, y
+        info["evals"] = [float(v) for v in ev]
+        info["rel_residuals"] = r
+        res[name] = (ev, vecs)
+        out[name] = info
+    out["mixed"].update(compare_states(*res["mixed"], *res["fp64"]))
     t0 = time.perf_counter()
-    T = model.build_tables(model.pf_model(6, 6, seed=5))
-    t_build = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    H = Hamiltonian(T)
-    t_create = time.perf_counter() - t0
-    st = H.stats()
-    x = torch.randn(T.dim, dtype=torch.float32, device="cuda")
-    y = torch.empty_like(x)
-    H.applyh(x, y)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(3):
-        H.applyh(x, y)
-    e1.record()
-    torch.cuda.synchronize()
-    mv_s = e0.elapsed_time(e1) / 3 / 1e3
-    balg, nops = alg_bytes(st, T, 1, 4)
-    peaks, _ = load_peaks()
-    del x, y
-    t0 = time.perf_counter()
-    ev, vecs, rep = H.lanczos(nkeep=5, niter=args.large_iters, nthick_add=15, max_restarts=args.large_restarts,
-                              matvec_prec=4, converge_tol=args.large_tol, want_vectors=True)
-    t_lz = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    g = H.grad(vecs[:, :1])
+    g = H.grad(res["fp64"][1][:, :1])
     gtb, gspe = model.chain_rule(T, {k: v[0] for k, v in g.items()})
     t_grad = time.perf_counter() - t0
     spec = T.extra["spec"]
+    e0 = res["fp64"][0][0]
     euler = float(np.array([t[6] for t in spec.tbme]) @ gtb + np.array(spec.spe) @ gspe)
     free, total = torch.cuda.mem_get_info()
-    H.close()
-    return {"dim": T.dim, "ops_per_matvec": nops, "build_s": t_build, "create_s": t_create,
-            "matvec_fp32_s": mv_s, "matvec_alg_GBps": balg / mv_s / 1e9,
-            "matvec_roofline_frac": balg / mv_s / 1e9 / peaks["hbm_gbs"],
-            "lanczos": {"evals": [float(v) for v in ev], "restarts": rep["restarts"],
-                        "total_iterations": rep["total_iterations"], "converged": rep["converged"],
-                        "wall_s": t_lz, "t_matvec_ms": rep["t_matvec_ms"], "t_reorth_ms": rep["t_reorth_ms"],
-                        "t_eig_ms": rep["t_eig_ms"], "converge_tol": args.large_tol,
-                        "basis": f"{args.large_iters} vectors, thick restart keeping 20"},
-            "grad_ground_state_s": t_grad, "euler_identity_rel_err": abs(euler - ev[0]) / abs(ev[0]),
-            "grad_tbme_norm": float(np.linalg.norm(gtb)), "grad_spe": [float(v) for v in gspe],
-            "device_mem_total_GB": total / 1e9}
+    out.update({"config": f"pf 6p6n, lowest 5, {args.large_iters}-vector basis, keep 20, {args.large_restarts} "
+                          "restarts (fixed schedule), seeded generic pivot",
+                "grad_ground_state_s": t_grad, "euler_identity_rel_err": abs(euler - e0) / abs(e0),
+                "grad_tbme_norm": float(np.linalg.norm(gtb)), "grad_spe": [float(v) for v in gspe],
+                "device_mem_total_GB": total / 1e9})
+    return out
 
 
 def workload_config(args, tables, world):
     """The `config` object of both arms' JSON lines."""
     return {"workload": args.workload, "dim": tables.dim, "nb": args.nb,
             "interaction": "seeded synthetic isospin TBMEs N(0,1) MeV",
-            "l2": "flushed (256 MiB write) before every timed matvec; kernel timed alone",
+            "l2": "vectors larger than L2, and a 256 MiB write before every timed matvec; kernel timed alone",
             "parallelism": f"replicas x{world}"}
 
 
@@ -381,61 +510,74 @@ def run_reference(args):
     if rank != 0:
         return 0
     tables = make_tables(args.workload)
-    per_step = []
-    n_total = 0
-    t_total = 0.0
-    nthreads = os.cpu_count()
-    for _ in range(args.warmup):
-        cpu_baseline(tables, args.nb, args.prec, budget_s=0.0, nthreads=nthreads)
-    for _ in range(args.steps):
-        rate, cores, n, el = cpu_baseline(tables, args.nb, args.prec, budget_s=args.ref_budget, nthreads=nthreads)
-        per_step.append(rate)
-        n_total += n
-        t_total += el
-    value = n_total / t_total
+    cs = CpuSampler(tables, args.nb, args.prec)
+    frac = cs.calibrate(args.ref_budget)
+    for k in range(args.warmup):
+        cs.run(min(frac, 1e-3), offset=0.11 * k)
+    shares, secs, per = 0.0, 0.0, []
+    for k in range(args.steps):
+        sh, el = cs.run(frac, offset=(0.618 * k) % 1.0)
+        shares += sh
+        secs += el
+        per.append(el)
+    value = shares / secs
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "matvec/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_total / max(1, n_total),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / max(1, args.steps),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if args.prec == 4 else "f64", "data": "synthetic",
         "config": workload_config(args, tables, int(os.environ.get("WORLD_SIZE", "1"))),
-        "cpu_baseline": {"value": value, "unit": "matvec/s", "cores": nthreads, "kind": "port",
-                         "sample": f"{n_total} matvecs over {t_total:.1f} s (reference is Fortran; "
-                                   "no Fortran compiler in the image)"},
+        "matvec_share_per_step": shares / max(1, args.steps),
+        "cpu_baseline": {"value": value, "unit": "matvec/s", "cores": cs.nthreads, "kind": "port",
+                         "sample": f"{args.steps} steps, each {100 * shares / max(1, args.steps):.2f}% of one "
+                                   f"matvec (a slice of every owner's rows), {secs:.1f} s in all; oracle C "
+                                   "restatement of applyHbundled_omp's owner-computes OpenMP partition (the "
+                                   "reference is Fortran; no Fortran compiler in the image)"},
         "e2e": {"value": value, "unit": "matvec/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
     return 0
 
 
+def _leg(line, key, fn, *a):
+    """Run one leg; a failing leg is recorded and does not cost the line."""
+    try:
+        line[key] = fn(*a)
+    except Exception as e:
+        line[key] = {"error": repr(e)[:500]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="sd6p6n", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--nb", type=int, default=1)
     ap.add_argument("--prec", type=int, default=4, choices=[4, 8])
-    ap.add_argument("--ref-budget", type=float, default=3.0)
-    ap.add_argument("--cpu-budget", type=float, default=10.0)
+    ap.add_argument("--ref-budget", type=float, default=4.0, help="seconds of CPU work per reference step")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--quick", action="store_true", help="headline line only (no legs)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-lanczos", action="store_true")
     ap.add_argument("--no-density", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-large", action="store_true")
+    ap.add_argument("--no-tts", action="store_true")
     ap.add_argument("--lanczos-iters", type=int, default=300)
-    ap.add_argument("--block-leg", action="store_true")
-    ap.add_argument("--block-iters", type=int, default=20)
-    ap.add_argument("--block-restarts", type=int, default=30)
-    ap.add_argument("--batch-leg", action="store_true")
+    ap.add_argument("--tts-tol", type=float, default=1e-5)
+    ap.add_argument("--tts-niter", type=int, default=150)
+    ap.add_argument("--tts-block-niter", type=int, default=20)
     ap.add_argument("--batch-n", type=int, default=256)
     ap.add_argument("--batch-iters", type=int, default=150)
     ap.add_argument("--tune-cache", action="store_true")
-    ap.add_argument("--large-leg", action="store_true")
-    ap.add_argument("--large-iters", type=int, default=60)
-    ap.add_argument("--large-restarts", type=int, default=20)
-    ap.add_argument("--large-tol", type=float, default=1e-4)
+    ap.add_argument("--large-iters", type=int, default=50)
+    ap.add_argument("--large-restarts", type=int, default=3)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.quick:
+        args.no_cpu = args.no_lanczos = args.no_density = args.no_batch = args.no_large = args.no_tts = True
 
     if args.impl == "reference":
         return run_reference(args)
@@ -458,8 +600,12 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
+    t0 = time.perf_counter()
     tables = make_tables(args.workload)
+    t_build = time.perf_counter() - t0
+    t0 = time.perf_counter()
     H = Hamiltonian(tables, device=local)
+    t_create = time.perf_counter() - t0
     st = H.stats()
     nb, prec = args.nb, args.prec
     dt = torch.float32 if prec == 4 else torch.float64
@@ -487,14 +633,6 @@ def main():
         evs[k][1].record(stream)
     barrier()
     kern_ms = [a.elapsed_time(b) for a, b in evs]
-    # warm-L2 rate (vectors resident in L2, the steady state inside Lanczos)
-    w0, w1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    w0.record(stream)
-    for _ in range(args.steps):
-        H.applyh(vin, vout)
-    w1.record(stream)
-    barrier()
-    warm_ms = w0.elapsed_time(w1) / args.steps
     clocks = sampler.stop()
 
     total_ms = reduce_max(float(sum(kern_ms)), dist, device="cuda")
@@ -505,6 +643,7 @@ def main():
     hin.copy_(vin.cpu())
     hout = torch.empty(shape, dtype=dt, pin_memory=True)
     hin_np, hout_np = hin.numpy(), hout.numpy()
+    del vin, vout, flush
     for _ in range(2):
         H.applyh(hin_np, hout_np)
     barrier()
@@ -514,11 +653,13 @@ def main():
     e2e_s = reduce_max(time.perf_counter() - t0, dist, device="cuda")
     e2e = replica_rate(args.steps, world, e2e_s)
     vbytes = tables.dim * nb * s_bytes
+    del hin, hout, hin_np, hout_np
 
     peaks, peak_kind = load_peaks()
     balg, nops = alg_bytes(st, tables, nb, s_bytes)
     mean_s = total_ms / 1e3 / args.steps
     achieved = balg / mean_s / 1e9
+    traffic = traffic_from_profile(args.workload, nb, prec)
     line = {
         "metric": METRIC, "value": value, "unit": "matvec/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -527,27 +668,31 @@ def main():
         "e2e": {"value": e2e, "unit": "matvec/s", "h2d_bytes_per_step": vbytes, "d2h_bytes_per_step": vbytes},
         "gpu_launches": args.steps * st["kernel_launches_per_matvec"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"], "traffic": traffic_from_profile(args.workload, nb, prec),
-                     "peak_kind": peak_kind, "alg_bytes_per_launch": balg, "ops_per_matvec": nops},
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                     "peak_kind": peak_kind, "alg_bytes_per_launch": balg, "ops_per_matvec": nops,
+                     "dram_GBps": (traffic / mean_s / 1e9) if traffic else None,
+                     "dram_frac": (traffic / mean_s / 1e9 / peaks["hbm_gbs"]) if traffic else None},
         "clocks": clocks,
-        "warm_l2_matvec_per_s": world / (warm_ms / 1e3),
+        "setup_s": {"tables": t_build, "bsg_create": t_create},
     }
+    if rank == 0 and not args.no_large and args.workload == "pf6p6n":
+        _leg(line, "large", large_leg, H, tables, args)
+    H.close()
+    del H
     if rank == 0 and not args.no_lanczos:
-        line["lanczos"] = lanczos_leg(H, tables, args)
-    if rank == 0 and not args.no_density:
-        line["density"] = density_leg(H, tables, args)
-    if rank == 0 and args.batch_leg:
-        line["batch"] = batch_leg(args)
-    if rank == 0 and args.large_leg:
-        line["large"] = large_leg(args)
+        _leg(line, "lanczos", lanczos_sd6p6n_leg, args)
+    if rank == 0 and not args.no_tts:
+        _leg(line, "time_to_solution", time_to_solution_leg, args)
+    if rank == 0 and not args.no_batch:
+        _leg(line, "batch", batch_leg, args)
     if rank == 0 and world == 1 and not args.no_cpu:
-        rate, cores, n, el = cpu_baseline(tables, nb, prec, budget_s=args.cpu_budget)
+        rate, cores, shares, secs = cpu_baseline(tables, nb, prec, budget_s=args.cpu_budget)
         line["cpu_baseline"] = {"value": rate, "unit": "matvec/s", "cores": cores, "kind": "port",
-                                "sample": f"{n} full matvecs of the same workload in {el:.1f} s, "
-                                          "oracle C restatement of applyHbundled_g with OpenMP"}
+                                "sample": f"{100 * shares:.2f}% of one matvec of the same workload (slices of "
+                                          f"every owner's rows) in {secs:.1f} s, oracle C restatement of "
+                                          "applyHbundled_omp's owner-computes OpenMP partition"}
     if rank == 0:
         print(json.dumps(line))
-    del H
     if dist is not None:
         dist.destroy_process_group()
     return 0

@@ -5,8 +5,10 @@ this package, as the checker.  The product (bigstickpublick_b200) never
 imports, links or calls it.
 
 * liboracle.so (oracle_applyh.c): plain-C restatement of BIGSTICK's
-  applyHbundled_omp / applyHbundled_block_omp loops, plus the OpenMP
-  serial-path split routines used as the timed CPU baseline.
+  applyHbundled_omp / applyHbundled_block_omp loops; its owner-computes
+  OpenMP partition (each thread the output rows getLoadDist gives it), used
+  as the timed CPU baseline and, restricted to a few rows, as the checker of
+  large systems; and the serial-path split routines of applyHbundled_g.
 * dense_h.py: independent dense Hamiltonian from second quantization.
 * lanczos.py: numpy restatement of lanczos_p / lanczos_block with full
   reorthogonalization, convergence test and thick restart.
@@ -44,6 +46,13 @@ def lib():
         L.oracle_count_ops.restype = None
         L.oracle_density.argtypes = [C.c_void_p] + [C.c_void_p] * 6
         L.oracle_density.restype = C.c_int
+        L.oracle_row_ops.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oracle_row_ops.restype = C.c_int64
+        L.oracle_applyh_rows.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int64, C.c_int64]
+        L.oracle_applyh_rows.restype = C.c_int
+        L.oracle_applyh_owner.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                          C.c_void_p, C.c_int]
+        L.oracle_applyh_owner.restype = C.c_int
         _LIB = L
     return _LIB
 
@@ -77,6 +86,68 @@ def applyh_omp(tables, vin, nb=1, nthreads=None, out=None):
                                  nthreads or os.cpu_count())
     if st != 0:
         raise RuntimeError(f"oracle_applyh_omp status {st}")
+    return out
+
+
+def row_ops(tables):
+    """The output rows and their work, as getLoadDist buckets it
+    (src/bapplyhlibOMP.f90:213-327): (row_start, ops), row_start the distinct
+    pstart values in ascending order, ops the inner-loop updates landing in
+    each row.  Row r holds the basis states row_start[r]+1 .. row_start[r+1]
+    (1-based; the last row ends at dim)."""
+    n = int(tables.s["nsd_p"])
+    rs = np.zeros(n, dtype=np.int64)
+    ops = np.zeros(n, dtype=np.int64)
+    p, keep = _tp(tables)
+    m = lib().oracle_row_ops(p, rs.ctypes.data, ops.ctypes.data)
+    return rs[:m].copy(), ops[:m].copy()
+
+
+def owner_ranges(row_start, ops, dim, nparts):
+    """Cut the rows into nparts contiguous runs of about equal work (the
+    equal-weight bucket runs of getLoadDist, src/bapplyhlibOMP.f90:330-420):
+    int64 array (nparts, 2) of [lo, hi) row-start bounds."""
+    csum = np.cumsum(ops)
+    total = int(csum[-1]) if len(csum) else 0
+    cuts = [0]
+    for k in range(1, nparts):
+        cuts.append(max(cuts[-1], int(np.searchsorted(csum, total * k / nparts, side="left")) + 1))
+    cuts.append(len(row_start))
+    lo = [int(row_start[c]) if c < len(row_start) else dim for c in cuts[:-1]]
+    hi = lo[1:] + [dim]
+    return np.array([[a, b] for a, b in zip(lo, hi) if b > a], dtype=np.int64).reshape(-1, 2)
+
+
+def applyh_rows(tables, vin, lo, hi, nb=1, out=None):
+    """out += (H vin) on the rows with pstart value in [lo, hi) only (one
+    owner's share of applyHbundled_omp, one thread); other entries of out are
+    left as they are."""
+    vin = np.ascontiguousarray(vin)
+    prec = 4 if vin.dtype == np.float32 else 8
+    if out is None:
+        out = np.zeros_like(vin)
+    p, keep = _tp(tables)
+    st = lib().oracle_applyh_rows(p, vin.ctypes.data, out.ctypes.data, nb, prec, int(lo), int(hi))
+    if st != 0:
+        raise RuntimeError(f"oracle_applyh_rows status {st}")
+    return out
+
+
+def applyh_owner(tables, vin, ranges, nb=1, nthreads=None, out=None):
+    """out += (H vin) on the row ranges `ranges` ((n, 2) [lo, hi) bounds),
+    the ranges spread over nthreads OpenMP threads: applyHbundled_omp's
+    owner-computes partition when the ranges are owner_ranges(...) of all
+    rows."""
+    vin = np.ascontiguousarray(vin)
+    prec = 4 if vin.dtype == np.float32 else 8
+    if out is None:
+        out = np.zeros_like(vin)
+    b = np.ascontiguousarray(ranges, dtype=np.int64).reshape(-1, 2)
+    p, keep = _tp(tables)
+    st = lib().oracle_applyh_owner(p, vin.ctypes.data, out.ctypes.data, nb, prec, len(b), b.ctypes.data,
+                                   nthreads or os.cpu_count())
+    if st != 0:
+        raise RuntimeError(f"oracle_applyh_owner status {st}")
     return out
 
 

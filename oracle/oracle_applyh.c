@@ -10,6 +10,12 @@
  *                        NN :1012-1066, PP :1068-1241, PN :1242-1442) and its
  *                        block form applyHbundled_block_omp
  *                        (src/bapplyhlibOMP_block.f90:43-886) for nb > 1.
+ *   oracle_applyh_rows() / oracle_applyh_owner()
+ *                        applyHbundled_omp's owner-computes OpenMP
+ *                        partition: every thread computes the output rows
+ *                        getLoadDist gives it (src/bapplyhlibOMP.f90:34-868,
+ *                        :954-1442).  The timed CPU baseline, and the checker
+ *                        of systems too large for one thread (a few rows).
  *   oracle_applyh_omp()  the OpenMP serial-path split routines
  *                        applyhPPbundled_g / applyhNNbundled_g /
  *                        applyhPNbundled_g (src/bapplyhlib1.f90:325-818):
@@ -17,8 +23,7 @@
  *                        chunks, PN forward over proton-jump chunks cut at
  *                        p1b_fsd changes, PN backward over neutron-jump chunks
  *                        cut at n1b_isd changes (jumps are sorted that way,
- *                        src/bsortjumpslib.f90:57-95).  Used as the timed CPU
- *                        baseline.
+ *                        src/bsortjumpslib.f90:57-95).
  *
  * Arithmetic follows the reference: xme is real(4) (hmat * phase), the update
  * is vout = vout + xme*vin in the vector precision (float for lanc_prec=4,
@@ -266,6 +271,175 @@ int oracle_applyh_omp(const bsg_tables *t, const void *vin, void *vout, int nb, 
         omp_f64(t, (const double *)vin, (double *)vout, nb, nthreads, cuts);
     free(cuts);
     return BSG_OK;
+}
+
+/* ------------------------------------------ owner-computes partition ---- */
+/* applyHbundled_omp gives each OpenMP thread the output rows whose pstart
+ * value lies in [mybasisstart-1, mybasisstop) (getLoadDist buckets the work
+ * of every jump by the pstart value of its output row and cuts the buckets
+ * into equal-work runs, src/bapplyhlibOMP.f90:34-868); per bundle the thread
+ * visits the jumps whose output row is its own (threadStart/threadStop, and
+ * the rescans of the 'b' bundles that keep psdi in range, :1340-1356).
+ * oracle_applyh_rows() is one owner's share: the outputs of the rows whose
+ * pstart value r satisfies lo <= r < hi, in bundle order, every other output
+ * untouched.  Output row of a jump: PP psdf (psdi for 'b'), NN and SPE
+ * pstart(ip), PN p1b_fsd ('b': p1b_isd).  Rows are contiguous runs of basis
+ * states (a proton SD and its neutron partners), so disjoint [lo, hi) ranges
+ * write disjoint outputs. */
+#define DEFINE_ROWS(T, NAME)                                                             \
+static void NAME(const bsg_tables *t, const T *vin, T *vout, int nb, int64_t lo, int64_t hi) { \
+    for (int64_t ib = 0; ib < t->nbundles; ++ib) {                                       \
+        const int op = t->optype[ib];                                                    \
+        const int hc = t->hchar[ib];                                                     \
+        const int64_t px0 = t->pxstart[ib], px1 = t->pxend[ib];                          \
+        const int64_t nx0 = t->nxstart[ib], nx1 = t->nxend[ib];                          \
+        const int64_t cs = t->cstride[ib] > 0 ? t->cstride[ib] : 1;                      \
+        if (op == BSG_OP_SPE) {                                                          \
+            for (int64_t ip = px0; ip <= px1; ++ip) {                                    \
+                const int64_t row = t->pstart[ip - 1];                                   \
+                if (row < lo || row >= hi) continue;                                     \
+                const float pspe = t->pspe_h[ip - 1];                                    \
+                int64_t statef = row + t->nstart[nx0 - 1];                               \
+                for (int64_t in = nx0; in <= nx1; ++in) {                                \
+                    const float e = pspe + t->nspe_h[in - 1];                            \
+                    for (int v = 0; v < nb; ++v)                                         \
+                        vout[(statef - 1) * nb + v] += vin[(statef - 1) * nb + v] * (T)e; \
+                    ++statef;                                                            \
+                }                                                                        \
+            }                                                                            \
+        } else if (op == BSG_OP_NN) {                                                    \
+            const int64_t *s1 = hc == 'b' ? t->n2b_fsd : t->n2b_isd;                     \
+            const int64_t *s2 = hc == 'b' ? t->n2b_isd : t->n2b_fsd;                     \
+            for (int64_t csd = px0; csd <= px1; csd += cs) {                             \
+                const int64_t psd = t->pstart[csd - 1];                                  \
+                if (psd < lo || psd >= hi) continue;                                     \
+                for (int64_t x = nx0; x <= nx1; ++x) {                                   \
+                    float xme = t->hmatnn[t->n2b_op[x - 1] - 1];                         \
+                    xme = xme * (float)t->n2b_phase[x - 1];                              \
+                    const int64_t si = s1[x - 1] + psd, sf = s2[x - 1] + psd;            \
+                    for (int v = 0; v < nb; ++v)                                         \
+                        vout[(sf - 1) * nb + v] += (T)xme * vin[(si - 1) * nb + v];      \
+                }                                                                        \
+            }                                                                            \
+        } else if (op == BSG_OP_PP) {                                                    \
+            const int64_t *s1 = hc == 'b' ? t->p2b_fsd : t->p2b_isd;                     \
+            const int64_t *s2 = hc == 'b' ? t->p2b_isd : t->p2b_fsd;                     \
+            for (int64_t x = px0; x <= px1; ++x) {                                       \
+                const int64_t psdi = s1[x - 1], psdf = s2[x - 1];                        \
+                if (psdf < lo || psdf >= hi) continue;                                   \
+                float xme = t->hmatpp[t->p2b_op[x - 1] - 1];                             \
+                xme = xme * (float)t->p2b_phase[x - 1];                                  \
+                for (int64_t csd = nx0; csd <= nx1; csd += cs) {                         \
+                    const int64_t nsd = t->nstart[csd - 1];                              \
+                    const int64_t sf = psdf + nsd, si = psdi + nsd;                      \
+                    for (int v = 0; v < nb; ++v)                                         \
+                        vout[(sf - 1) * nb + v] += (T)xme * vin[(si - 1) * nb + v];      \
+                }                                                                        \
+            }                                                                            \
+        } else if (op == BSG_OP_PN) {                                                    \
+            const int bwd = hc == 'b';                                                   \
+            for (int64_t pj = px0; pj <= px1; ++pj) {                                    \
+                const int64_t psdi = t->p1b_isd[pj - 1], psdf = t->p1b_fsd[pj - 1];      \
+                const int64_t own = bwd ? psdi : psdf;                                   \
+                if (own < lo || own >= hi) continue;                                     \
+                const int phasep = t->p1b_phase[pj - 1];                                 \
+                const int a = t->p1b_cop[pj - 1], c = t->p1b_dop[pj - 1];                \
+                for (int64_t nj = nx0; nj <= nx1; ++nj) {                                \
+                    const int b = t->n1b_cop[nj - 1], d = t->n1b_dop[nj - 1];            \
+                    float xme = t->hmatpn[CPN(t, b, a) + DPN(t, d, c) - 1];              \
+                    xme = xme * (float)phasep * (float)t->n1b_phase[nj - 1];             \
+                    const int64_t sf = t->n1b_fsd[nj - 1] + psdf;                        \
+                    const int64_t si = t->n1b_isd[nj - 1] + psdi;                        \
+                    if (!bwd) {                                                          \
+                        for (int v = 0; v < nb; ++v)                                     \
+                            vout[(sf - 1) * nb + v] += (T)xme * vin[(si - 1) * nb + v];  \
+                    } else {                                                             \
+                        for (int v = 0; v < nb; ++v)                                     \
+                            vout[(si - 1) * nb + v] += (T)xme * vin[(sf - 1) * nb + v];  \
+                    }                                                                    \
+                }                                                                        \
+            }                                                                            \
+        }                                                                                \
+    }                                                                                    \
+}
+
+DEFINE_ROWS(float, rows_f32)
+DEFINE_ROWS(double, rows_f64)
+
+static int cmp_i64(const void *x, const void *y) {
+    const int64_t a = *(const int64_t *)x, b = *(const int64_t *)y;
+    return a < b ? -1 : (a > b ? 1 : 0);
+}
+
+/* index of the row whose start value is r in the ascending list rs[n] */
+static int64_t row_index(const int64_t *rs, int64_t n, int64_t r) {
+    int64_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi + 1) / 2;
+        if (rs[mid] <= r) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+/* The work getLoadDist buckets, per output row: row_start[] receives the
+ * distinct pstart values in ascending order (the rows), ops[] the inner-loop
+ * updates landing in each row (the bucket counts of src/bapplyhlibOMP.f90
+ * :213-327 at row granularity).  Both arrays need nsd_p entries; returns the
+ * number of rows. */
+int64_t oracle_row_ops(const bsg_tables *t, int64_t *row_start, int64_t *ops) {
+    int64_t n = t->nsd_p;
+    memcpy(row_start, t->pstart, sizeof(int64_t) * (size_t)n);
+    qsort(row_start, (size_t)n, sizeof(int64_t), cmp_i64);
+    int64_t m = 0;
+    for (int64_t i = 0; i < n; ++i)
+        if (m == 0 || row_start[i] != row_start[m - 1]) row_start[m++] = row_start[i];
+    memset(ops, 0, sizeof(int64_t) * (size_t)m);
+    for (int64_t ib = 0; ib < t->nbundles; ++ib) {
+        const int op = t->optype[ib], hc = t->hchar[ib];
+        const int64_t px0 = t->pxstart[ib], px1 = t->pxend[ib];
+        const int64_t nx0 = t->nxstart[ib], nx1 = t->nxend[ib];
+        const int64_t cs = t->cstride[ib] > 0 ? t->cstride[ib] : 1;
+        if (op == BSG_OP_SPE) {
+            for (int64_t ip = px0; ip <= px1; ++ip) ops[row_index(row_start, m, t->pstart[ip - 1])] += nx1 - nx0 + 1;
+        } else if (op == BSG_OP_NN) {
+            for (int64_t csd = px0; csd <= px1; csd += cs) ops[row_index(row_start, m, t->pstart[csd - 1])] += nx1 - nx0 + 1;
+        } else if (op == BSG_OP_PP) {
+            const int64_t *s2 = hc == 'b' ? t->p2b_isd : t->p2b_fsd;
+            const int64_t nc = (nx1 + cs - nx0) / cs;
+            for (int64_t x = px0; x <= px1; ++x) ops[row_index(row_start, m, s2[x - 1])] += nc;
+        } else if (op == BSG_OP_PN) {
+            const int64_t *own = hc == 'b' ? t->p1b_isd : t->p1b_fsd;
+            for (int64_t pj = px0; pj <= px1; ++pj) ops[row_index(row_start, m, own[pj - 1])] += nx1 - nx0 + 1;
+        }
+    }
+    return m;
+}
+
+/* vout += H vin restricted to the rows with pstart value in [lo, hi) */
+int oracle_applyh_rows(const bsg_tables *t, const void *vin, void *vout, int nb, int prec, int64_t lo, int64_t hi) {
+    if (!t || !vin || !vout || nb < 1) return BSG_ERR_ARG;
+    if (prec == BSG_PREC_FP32)
+        rows_f32(t, (const float *)vin, (float *)vout, nb, lo, hi);
+    else
+        rows_f64(t, (const double *)vin, (double *)vout, nb, lo, hi);
+    return BSG_OK;
+}
+
+/* The owner-computes matvec: range i is [bounds[2i], bounds[2i+1]) of row
+ * start values, one range per OpenMP work item (dynamic schedule).  With
+ * equal-work ranges that cover every row this is applyHbundled_omp's
+ * partition; ranges that cover part of the rows compute those rows only. */
+int oracle_applyh_owner(const bsg_tables *t, const void *vin, void *vout, int nb, int prec,
+                        int nranges, const int64_t *bounds, int nthreads) {
+    if (!t || !vin || !vout || nb < 1 || nranges < 0 || !bounds) return BSG_ERR_ARG;
+    if (nthreads < 1) nthreads = 1;
+    int st = BSG_OK;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+    for (int i = 0; i < nranges; ++i) {
+        const int r = oracle_applyh_rows(t, vin, vout, nb, prec, bounds[2 * i], bounds[2 * i + 1]);
+        if (r) st = r;
+    }
+    return st;
 }
 
 /* number of inner-loop updates one applyH executes (the N_ops of the
