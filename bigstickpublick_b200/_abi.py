@@ -62,6 +62,15 @@ class BsgLanczosParams(C.Structure):
         ("max_restarts", C.c_int32), ("nb", C.c_int32), ("matvec_prec", C.c_int32),
         ("fixed_iter", C.c_int32), ("ncheck", C.c_int32), ("converge_tol", C.c_double),
         ("want_vectors", C.c_int32), ("pivot", C.c_int32), ("seed", C.c_uint64),
+        ("lanc_prec", C.c_int32), ("reserved", C.c_int32),
+    ]
+
+
+class BsgSpecies(C.Structure):
+    _fields_ = [
+        ("nsps", C.c_int32), ("nl", C.c_int32), ("m2", C.POINTER(C.c_int32)), ("par", C.POINTER(C.c_int32)),
+        ("nsd", C.c_int64), ("sd_bits", C.POINTER(C.c_uint64)), ("xstart", C.POINTER(C.c_int64)),
+        ("nsectors", C.c_int32), ("sector_start", C.POINTER(C.c_int64)), ("sector_end", C.POINTER(C.c_int64)),
     ]
 
 
@@ -83,7 +92,7 @@ class BsgStats(C.Structure):
         ("kernel_launches_per_matvec", C.c_int32), ("reserved", C.c_int32),
         ("density_ms", C.c_double), ("density_rows", C.c_int64),
         ("density_launches", C.c_int32), ("reserved2", C.c_int32),
-        ("apply1b_ms", C.c_double),
+        ("apply1b_ms", C.c_double), ("grad_ms", C.c_double),
     ]
 
 
@@ -218,5 +227,21 @@ def gpu_lib():
         lib.bsg_batch_set_tuning.restype = C.c_int
         lib.bsg_batch_lanczos.argtypes = [vp, C.POINTER(BsgLanczosParams), f64p, C.POINTER(f64p), C.POINTER(BsgReport)]
         lib.bsg_batch_lanczos.restype = C.c_int
+        lib.bsg_batch_grad.argtypes = [vp, C.POINTER(f64p), C.c_int, C.POINTER(f64p), C.POINTER(f64p),
+                                       C.POINTER(f64p), C.POINTER(f64p), C.POINTER(f64p), C.POINTER(C.c_double)]
+        lib.bsg_batch_grad.restype = C.c_int
+        lib.bsg_jumpgen_create.argtypes = [C.c_int, C.POINTER(BsgSpecies), C.POINTER(vp)]
+        lib.bsg_jumpgen_create.restype = C.c_int
+        lib.bsg_jumpgen_destroy.argtypes = [vp]
+        lib.bsg_jumpgen_destroy.restype = C.c_int
+        lib.bsg_jumpgen_last_error.argtypes = [vp, C.c_char_p, C.c_size_t]
+        lib.bsg_jumpgen_last_error.restype = C.c_int
+        lib.bsg_jumpgen_one.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, C.POINTER(C.c_double)]
+        lib.bsg_jumpgen_one.restype = C.c_int
+        lib.bsg_jumpgen_two.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp, C.POINTER(C.c_double)]
+        lib.bsg_jumpgen_two.restype = C.c_int
+        lib.bsg_jumpgen_sort1.argtypes = [vp, C.c_int, vp, vp, C.c_int, C.c_int64, vp, vp, vp, vp, vp,
+                                          C.POINTER(C.c_double)]
+        lib.bsg_jumpgen_sort1.restype = C.c_int
         _gpu = lib
     return _gpu

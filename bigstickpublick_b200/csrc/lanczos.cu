@@ -1,6 +1,8 @@
 // bsg_lanczos: scalar and block Lanczos with full reorthogonalization and
-// thick restart, everything on the device in FP64 except the applyH call
-// (FP32 or FP64 as requested).
+// thick restart, everything on the device: the applyH call in FP32 or FP64,
+// the Lanczos vectors stored in FP64 or FP32 (lanc_prec, as the reference's
+// shipped lanc_prec = 4 stores them), every dot product, update, alpha,
+// beta and the projected eigenproblem in FP64.
 //
 // Restates lanczos_p (src/blanczosmain.f90:1413-1793) and lanczos_block
 // (:1804-2153):
@@ -26,11 +28,15 @@
 //   * convergence_test option 0 (src/blanczoslib.f90:2660-2800): mean energy
 //     change over ncheck states, scaled by (1+restarts)/sqrt(ncheck+1),
 //     below converge_tol;
-//   * thick restart when the next step would be the niter-th
+//   * thick restart when the next step would be the niter-th.  Scalar
 //     (thick_restart_sub_p, src/blanczoslib.f90:1656-1894): Ritz pairs of the
-//     projected matrix without its last block, alpha_i = theta_i,
-//     coupling beta_prev * y_last,i, basis V <- V Y (br_transform_basis), the
-//     last Lanczos block continues the recursion.
+//     projected matrix without its last column, alpha_i = theta_i, coupling
+//     beta_prev * y_last,i, basis V <- V Y (br_transform_basis), the last
+//     Lanczos vector continues the recursion.  Block
+//     (block_thick_restart_sub_p, :1923-2170): Ritz pairs of the whole
+//     projected matrix, floor(nthick/nb)*nb of them kept, coupling
+//     beta_last * Y[last block rows, kept], and the block made for the next
+//     step continues.
 
 #include <algorithm>
 #include <cmath>
@@ -53,6 +59,7 @@ struct Lz {
     cudaStream_t s;
     int64_t n;
     int nb, prec;
+    int hprec = 8;   // history storage: 8 FP64, 4 FP32 (lanc_prec)
     int maxcol;      // history columns
     DevBuf hist, W, X, tmp, partial, coef, sqp, sq, Adev, Vtmp, Zdev, wdev, al, bt, ev, M, tau, ework;
     DevBuf Ydev;     // Ritz coefficients of a thick restart (maxcol x 128)
@@ -73,8 +80,8 @@ struct Lz {
     double *pin_al() { return hpin + kPinW + maxcol; }
     double *pin_bt() { return hpin + kPinW + 2 * (size_t)maxcol; }
     size_t pin_doubles() const { return kPinW + 3 * (size_t)maxcol; }
-    // side stream for the convergence test of the scalar recursion, which
-    // then overlaps the next step's applyH
+    // side stream (highest priority) for the convergence test, which then
+    // overlaps the next step's applyH
     cudaStream_t s2 = nullptr;
     cudaEvent_t econv = nullptr;
     DevBuf al2, bt2, w2;
@@ -82,7 +89,8 @@ struct Lz {
     double *pinA = nullptr;
     DevBuf Adev2, Vtmp2, tau2, ework2;
 
-    double *col(int j) { return (double *)hist.p + (int64_t)j * n; }
+    // history column j (FP32 or FP64 storage, hprec)
+    void *col(int j) { return (char *)hist.p + (size_t)j * (size_t)n * (size_t)hprec; }
     double &Tm(int i, int j) { return T[(size_t)i * maxcol + j]; }
 };
 
@@ -208,8 +216,9 @@ int eig_collect(Lz &L, int want, std::vector<double> &w) {
 int cgs(Lz &L, int k, std::vector<double> *sq, bool sq_on_device = false) {
     double *C = (double *)L.coef.p;
     const bool want_sq = sq || sq_on_device;
-    if (k > 0) CK(multidot(L.col(0), k, (const double *)L.W.p, L.nb, L.n, L.n, (double *)L.partial.p, C, L.s));
-    CK(sub_gemv(L.col(0), k, C, (double *)L.W.p, L.nb, L.n, L.n, want_sq ? (double *)L.sqp.p : nullptr,
+    if (k > 0)
+        CK(multidot(L.col(0), L.hprec, k, (const double *)L.W.p, L.nb, L.n, L.n, (double *)L.partial.p, C, L.s));
+    CK(sub_gemv(L.col(0), L.hprec, k, C, (double *)L.W.p, L.nb, L.n, L.n, want_sq ? (double *)L.sqp.p : nullptr,
                 want_sq ? (double *)L.sq.p : nullptr, L.s));
     if (sq) {
         sq->resize(L.nb);
@@ -293,7 +302,7 @@ int block_finish(Lz &L, int dst, const double *Shost, std::vector<double> &beta,
         }
     }
     CK(cudaMemcpyAsync(L.M.p, Mh, sizeof(double) * nb * nb, cudaMemcpyHostToDevice, L.s));
-    CK(transform((const double *)L.W.p, nb, (const double *)L.M.p, nb, nb, L.col(dst), L.n, L.n, L.n, L.s, L.X.p,
+    CK(transform(L.W.p, 8, nb, (const double *)L.M.p, nb, nb, L.col(dst), L.hprec, L.n, L.n, L.n, L.s, L.X.p,
                  L.prec));
     L.x_ready = true;
     return BSG_OK;
@@ -312,7 +321,7 @@ int next_block(Lz &L, int dst, const std::vector<double> &sq, std::vector<double
         if (b == 0.0) return BSG_OK;
         const double inv = 1.0 / b;
         CK(cudaMemcpyAsync(L.M.p, &inv, sizeof(double), cudaMemcpyHostToDevice, L.s));
-        CK(scale_cols((const double *)L.W.p, L.col(dst), (const double *)L.M.p, 1, L.n, L.n, L.s));
+        CK(scale_cols((const double *)L.W.p, L.col(dst), L.hprec, (const double *)L.M.p, 1, L.n, L.n, L.s));
         return BSG_OK;
     }
     // S = W^T W, then the decomposition on the host
@@ -370,7 +379,7 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
         ++iter;
         ++total;
         // ---- W = H V
-        if (!L.x_ready) CK(pack(L.col(cur), nb, n, n, L.X.p, L.prec, L.s));
+        if (!L.x_ready) CK(pack(L.col(cur), L.hprec, nb, n, n, L.X.p, L.prec, L.s));
         L.x_ready = false;
         CK(cudaEventRecord(L.e0, L.s));
         ST(launch_applyh_cols(ctx, L.X.p, (double *)L.W.p, nb, L.prec, L.s));  // W columns directly
@@ -380,13 +389,16 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
         // without a host round trip; the scalar recursion also normalizes
         // the residual on the device (V_{i+1} = W / |W|), which the
         // safeguards below redo in the rare steps where they trigger
-        CK(multidot(L.col(cur), nb, (const double *)L.W.p, nb, n, n, (double *)L.partial.p, (double *)L.coef.p, L.s));
+        CK(multidot(L.col(cur), L.hprec, nb, (const double *)L.W.p, nb, n, n, (double *)L.partial.p,
+                    (double *)L.coef.p, L.s));
         CK(cudaMemcpyAsync(L.hpin + Lz::kPinAlpha, L.coef.p, sizeof(double) * nb * nb, cudaMemcpyDeviceToHost, L.s));
-        CK(sub_gemv(L.col(cur), nb, (const double *)L.coef.p, (double *)L.W.p, nb, n, n, nullptr, nullptr, L.s));
+        CK(sub_gemv(L.col(cur), L.hprec, nb, (const double *)L.coef.p, (double *)L.W.p, nb, n, n, nullptr, nullptr,
+                    L.s));
         ST(cgs(L, cur, nullptr, true));
         CK(cudaMemcpyAsync(L.hpin + Lz::kPinSq, L.sq.p, sizeof(double) * nb, cudaMemcpyDeviceToHost, L.s));
         if (nb == 1) {
-            CK(normalize_col((const double *)L.W.p, L.col(cur + 1), (const double *)L.sq.p, n, L.s, L.X.p, L.prec));
+            CK(normalize_col((const double *)L.W.p, L.col(cur + 1), L.hprec, (const double *)L.sq.p, n, L.s, L.X.p,
+                             L.prec));
         } else {
             // W^T W for the block step, read back with alpha and the norms
             CK(multidot((const double *)L.W.p, nb, (const double *)L.W.p, nb, n, n, (double *)L.partial.p,
@@ -521,8 +533,13 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
                 finished = true;
                 break;
             }
-            const int m = mT - nb;           // projected matrix without its last block
-            const int k = std::min(nthick, m - 1);
+            // scalar (thick_restart_sub_p): Ritz pairs of the projected matrix
+            // without its last column, whose vector continues the recursion.
+            // block (block_thick_restart_sub_p): Ritz pairs of the whole
+            // projected matrix, whole blocks kept, and the block already made
+            // for the next step (column mT) continues
+            const int m = (nb == 1) ? mT - nb : mT;
+            const int k = (nb == 1) ? std::min(nthick, m - 1) : (std::min(nthick, m - 1) / nb) * nb;
             std::vector<double> w, Z;          // Z column-major m x k
             ST(eig_lowest(L, m, karrow, k, w, &Z));
             // coupling rows: beta_prev block between block [m-nb, m) and [m, m+nb)
@@ -537,9 +554,9 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
             // Y (m x k <= maxcol x 128) through the solve's own buffer: no
             // allocation per restart
             CK(cudaMemcpyAsync(L.Ydev.p, Yk.data(), sizeof(double) * Yk.size(), cudaMemcpyHostToDevice, L.s));
-            CK(transform(L.col(0), m, (const double *)L.Ydev.p, k, k, (double *)L.tmp.p, n, n, n, L.s));
-            CK(cudaMemcpyAsync(L.col(0), L.tmp.p, sizeof(double) * n * k, cudaMemcpyDeviceToDevice, L.s));
-            CK(cudaMemcpyAsync(L.col(k), L.col(m), sizeof(double) * n * nb, cudaMemcpyDeviceToDevice, L.s));
+            CK(transform(L.col(0), L.hprec, m, (const double *)L.Ydev.p, k, k, L.tmp.p, L.hprec, n, n, n, L.s));
+            CK(cudaMemcpyAsync(L.col(0), L.tmp.p, (size_t)L.hprec * n * k, cudaMemcpyDeviceToDevice, L.s));
+            CK(cudaMemcpyAsync(L.col(k), L.col(m), (size_t)L.hprec * n * nb, cudaMemcpyDeviceToDevice, L.s));
             cudaEventRecord(L.e1, L.s);
             L.t_ort += elapsed(L);
             std::fill(L.T.begin(), L.T.end(), 0.0);
@@ -555,7 +572,10 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
             mT = k;
             karrow = k;
             ++restarts;
-            L.x_ready = false;  // the continuation block was moved
+            // scalar: the continuation vector moved and its applyH input must
+            // be packed again; block: the continuation is the block whose
+            // packed input the last spectral step already wrote
+            if (nb == 1) L.x_ready = false;
             iter = k / nb;
             beta_prev = -1.0;
         }
@@ -580,7 +600,7 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
         ST(upload(ctx, Yd, Yk.data(), sizeof(double) * Yk.size()));
         int st2 = dev_alloc(ctx, out, sizeof(double) * (size_t)n * nk);
         if (st2) { dev_free(Yd); return st2; }
-        cudaError_t te = transform(L.col(0), mT, (const double *)Yd.p, nk, nk, (double *)out.p, n, n, n, L.s);
+        cudaError_t te = transform(L.col(0), L.hprec, mT, (const double *)Yd.p, nk, nk, out.p, 8, n, n, n, L.s);
         if (te == cudaSuccess)
             te = cudaMemcpyAsync(evecs, out.p, sizeof(double) * (size_t)n * nk, cudaMemcpyDeviceToHost, L.s);
         if (te == cudaSuccess) te = cudaStreamSynchronize(L.s);
@@ -611,7 +631,8 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
     if (!p || !evals) return set_err(ctx, BSG_ERR_ARG, "bsg_lanczos: null argument");
     if ((p->nb != 1 && p->nb != 2 && p->nb != 4 && p->nb != 8 && p->nb != 16) || p->nkeep < 1 || p->niter < 2 ||
         p->nkeep + std::max(p->nthick_add, 0) > 128 ||
-        (p->matvec_prec != BSG_PREC_FP32 && p->matvec_prec != BSG_PREC_FP64))
+        (p->matvec_prec != BSG_PREC_FP32 && p->matvec_prec != BSG_PREC_FP64) ||
+        (p->lanc_prec != 0 && p->lanc_prec != BSG_PREC_FP32 && p->lanc_prec != BSG_PREC_FP64))
         return set_err(ctx, BSG_ERR_ARG, "bsg_lanczos: bad parameters");
     if ((int64_t)p->niter * p->nb + p->nb > 2048)
         return set_err(ctx, BSG_ERR_UNSUPPORTED, "bsg_lanczos: niter*nb above 2048 (projected matrix too large)");
@@ -624,20 +645,22 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
     L.n = ctx->dim;
     L.nb = p->nb;
     L.prec = p->matvec_prec;
+    L.hprec = (p->lanc_prec == BSG_PREC_FP32) ? 4 : 8;
     const int niter_eff = (int)std::min<int64_t>(p->niter, (ctx->dim + p->nb - 1) / p->nb + 1);
     bsg_lanczos_params pp = *p;
     pp.niter = std::max(2, niter_eff);
     const int maxcol = pp.niter * L.nb + L.nb;
     const int N = maxcol;
     const size_t vb = sizeof(double) * (size_t)L.n;
-    size_t need = vb * ((size_t)maxcol + 2 * L.nb + (size_t)std::max(L.nb, pp.nkeep + pp.nthick_add + 1)) +
+    const size_t hb = (size_t)L.hprec * (size_t)L.n;  // one history column
+    size_t need = hb * (size_t)maxcol + vb * (2 * L.nb + (size_t)std::max(L.nb, pp.nkeep + pp.nthick_add + 1)) +
                   (size_t)L.n * L.nb * (L.prec == 4 ? 4 : 8);
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
     if (need > fr) return set_err(ctx, BSG_ERR_NOMEM, "bsg_lanczos: history does not fit in device memory");
     const int G = dot_grid(L.n);
     const int ktmp = std::max(L.nb, pp.nkeep + std::max(pp.nthick_add, 0) + 1);
-    if ((st = dev_alloc(ctx, L.hist, vb * maxcol)) || (st = dev_alloc(ctx, L.W, vb * L.nb)) ||
+    if ((st = dev_alloc(ctx, L.hist, hb * maxcol)) || (st = dev_alloc(ctx, L.W, vb * L.nb)) ||
         (st = dev_alloc(ctx, L.tmp, vb * ktmp)) ||
         (st = dev_alloc(ctx, L.X, (size_t)L.n * L.nb * (L.prec == 4 ? 4 : 8))) ||
         (st = dev_alloc(ctx, L.partial, sizeof(double) * (size_t)4096 * G)) ||
@@ -669,7 +692,15 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
                         "cudaHostAlloc (Lanczos projected matrix)");
     if (!st) st = cuda_check(ctx, cudaHostAlloc((void **)&L.hpin, sizeof(double) * L.pin_doubles(), cudaHostAllocDefault),
                              "cudaHostAlloc (Lanczos staging)");
-    if (!st) st = cuda_check(ctx, cudaStreamCreateWithFlags(&L.s2, cudaStreamNonBlocking), "cudaStreamCreate");
+    // the side stream runs the convergence test's small eigen-solve beside the
+    // next step's applyH; at the highest priority its few CTAs are scheduled
+    // as soon as any SM has room, instead of after the applyH grid's
+    // remaining CTAs
+    if (!st) {
+        int prio_lo = 0, prio_hi = 0;
+        cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+        st = cuda_check(ctx, cudaStreamCreateWithPriority(&L.s2, cudaStreamNonBlocking, prio_hi), "cudaStreamCreate");
+    }
     if (!st) {
         cudaEventCreate(&L.e0);
         cudaEventCreate(&L.e1);

@@ -13,6 +13,12 @@
 //
 // All reductions are two-pass with a fixed grid and fixed summation order, so
 // every coefficient is bitwise repeatable.
+//
+// History columns are stored in FP64 or, as with the reference's shipped
+// lanc_prec = 4 (src/bmodules_main.f90:171), in FP32; every dot product and
+// update accumulates in FP64 either way (dot_product8 and the REAL(...,8)
+// sums of src/breorthog.f90:658-673, :1055-1116), and the working block W is
+// always FP64.
 
 #include <cuda_runtime.h>
 #include <algorithm>
@@ -35,8 +41,8 @@ constexpr int kDotTile = 512;      // rows per tile
 // vector, and a warp reduction adds them into the CTA's shared accumulator
 // (each (a,b) owned by one warp, added in chunk order).  The CTA writes
 // partial[p * gridDim.x + x] for its vectors.
-template <int NB, int PAIR>
-__global__ void __launch_bounds__(kDotThreads) k_multidot(const double *__restrict__ A, int nA,
+template <typename TA, int NB, int PAIR>
+__global__ void __launch_bounds__(kDotThreads) k_multidot(const TA *__restrict__ A, int nA,
                                                          const double *__restrict__ B, int64_t n, int64_t ld,
                                                          double *__restrict__ partial) {
     extern __shared__ double sm[];
@@ -56,8 +62,8 @@ __global__ void __launch_bounds__(kDotThreads) k_multidot(const double *__restri
         __syncthreads();
         for (int a = a_lo + warp * PAIR; a < a_hi; a += nw * PAIR) {
             const bool two = PAIR == 2 && a + 1 < a_hi;
-            const double *__restrict__ col0 = A + (int64_t)a * ld + t0;
-            const double *__restrict__ col1 = two ? col0 + ld : col0;
+            const TA *__restrict__ col0 = A + (int64_t)a * ld + t0;
+            const TA *__restrict__ col1 = two ? col0 + ld : col0;
             double acc0[NB], acc1[NB];
 #pragma unroll
             for (int b = 0; b < NB; ++b) acc0[b] = acc1[b] = 0.0;
@@ -67,8 +73,8 @@ __global__ void __launch_bounds__(kDotThreads) k_multidot(const double *__restri
                 double x0[4], x1[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
-                    x0[u] = __ldg(col0 + r + 32 * u);
-                    x1[u] = PAIR == 2 ? __ldg(col1 + r + 32 * u) : 0.0;
+                    x0[u] = (double)__ldg(col0 + r + 32 * u);
+                    x1[u] = PAIR == 2 ? (double)__ldg(col1 + r + 32 * u) : 0.0;
                 }
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
@@ -80,8 +86,8 @@ __global__ void __launch_bounds__(kDotThreads) k_multidot(const double *__restri
                     }
             }
             for (; r < rows; r += 32) {
-                const double x0 = __ldg(col0 + r);
-                const double x1 = PAIR == 2 ? __ldg(col1 + r) : 0.0;
+                const double x0 = (double)__ldg(col0 + r);
+                const double x1 = PAIR == 2 ? (double)__ldg(col1 + r) : 0.0;
 #pragma unroll
                 for (int b = 0; b < NB; ++b) {
                     const double y = sB[b * kDotTile + r];
@@ -124,8 +130,8 @@ __global__ void k_reduce_partials(const double *__restrict__ partial, int npairs
 
 // W[b] -= sum_j H[j] * C[j*nB + b]   (j < k), fused sum of squares of the
 // result per column when sq != nullptr (partials per block, NB entries)
-template <int NB>
-__global__ void __launch_bounds__(256) k_sub_gemv(const double *__restrict__ H, int k, const double *__restrict__ C,
+template <typename TH, int NB>
+__global__ void __launch_bounds__(256) k_sub_gemv(const TH *__restrict__ H, int k, const double *__restrict__ C,
                                                   double *__restrict__ W, int64_t n, int64_t ld,
                                                   double *__restrict__ sq) {
     extern __shared__ double sC[];  // [k*NB] then [8][NB] warp sums
@@ -140,12 +146,12 @@ __global__ void __launch_bounds__(256) k_sub_gemv(const double *__restrict__ H, 
         for (int b = 0; b < NB; ++b) acc[b] = 0.0;
         int j = 0;
         for (; j + 1 < k; j += 2) {
-            const double h0 = __ldg(H + (int64_t)j * ld + i), h1 = __ldg(H + (int64_t)(j + 1) * ld + i);
+            const double h0 = (double)__ldg(H + (int64_t)j * ld + i), h1 = (double)__ldg(H + (int64_t)(j + 1) * ld + i);
 #pragma unroll
             for (int b = 0; b < NB; ++b) acc[b] = fma(h1, sC[(j + 1) * NB + b], fma(h0, sC[j * NB + b], acc[b]));
         }
         if (j < k) {
-            const double h0 = __ldg(H + (int64_t)j * ld + i);
+            const double h0 = (double)__ldg(H + (int64_t)j * ld + i);
 #pragma unroll
             for (int b = 0; b < NB; ++b) acc[b] = fma(h0, sC[j * NB + b], acc[b]);
         }
@@ -178,9 +184,9 @@ __global__ void __launch_bounds__(256) k_sub_gemv(const double *__restrict__ H, 
 // K is a template parameter so that the K accumulators live in registers
 // xpack (optional): the result also as the interleaved applyH input of the
 // next step (x[i*K + l], FP32 for xprec 4, FP64 for 8), as k_pack would make it
-template <int K>
-__global__ void __launch_bounds__(256) k_transform(const double *__restrict__ V, int m, const double *__restrict__ Y,
-                                                   int ldy, double *__restrict__ out, int64_t n, int64_t ld,
+template <int K, typename TV, typename TO>
+__global__ void __launch_bounds__(256) k_transform(const TV *__restrict__ V, int m, const double *__restrict__ Y,
+                                                   int ldy, TO *__restrict__ out, int64_t n, int64_t ld,
                                                    int64_t ldo, void *__restrict__ xpack, int xprec) {
     extern __shared__ double sY[];  // [m][K]
     for (int e = threadIdx.x; e < m * K; e += blockDim.x) {
@@ -194,17 +200,17 @@ __global__ void __launch_bounds__(256) k_transform(const double *__restrict__ V,
         for (int l = 0; l < K; ++l) acc[l] = 0.0;
         int j = 0;
         for (; j + 1 < m; j += 2) {
-            const double v0 = __ldg(V + (int64_t)j * ld + i), v1 = __ldg(V + (int64_t)(j + 1) * ld + i);
+            const double v0 = (double)__ldg(V + (int64_t)j * ld + i), v1 = (double)__ldg(V + (int64_t)(j + 1) * ld + i);
 #pragma unroll
             for (int l = 0; l < K; ++l) acc[l] = fma(v1, sY[(j + 1) * K + l], fma(v0, sY[j * K + l], acc[l]));
         }
         if (j < m) {
-            const double v0 = __ldg(V + (int64_t)j * ld + i);
+            const double v0 = (double)__ldg(V + (int64_t)j * ld + i);
 #pragma unroll
             for (int l = 0; l < K; ++l) acc[l] = fma(v0, sY[j * K + l], acc[l]);
         }
 #pragma unroll
-        for (int l = 0; l < K; ++l) out[(int64_t)l * ldo + i] = acc[l];
+        for (int l = 0; l < K; ++l) out[(int64_t)l * ldo + i] = (TO)acc[l];
         if (xpack) {
             if (xprec == 4) {
 #pragma unroll
@@ -218,23 +224,24 @@ __global__ void __launch_bounds__(256) k_transform(const double *__restrict__ V,
 }
 
 // y[b] = s[b] * x[b] (scale columns), x and y may alias
-__global__ void k_scale_cols(const double *__restrict__ x, double *y, const double *__restrict__ s, int nB,
-                             int64_t n, int64_t ld) {
+template <typename TO>
+__global__ void k_scale_cols(const double *x, TO *y, const double *__restrict__ s, int nB, int64_t n, int64_t ld) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        for (int b = 0; b < nB; ++b) y[(int64_t)b * ld + i] = x[(int64_t)b * ld + i] * s[b];
+        for (int b = 0; b < nB; ++b) y[(int64_t)b * ld + i] = (TO)(x[(int64_t)b * ld + i] * s[b]);
 }
 
 // y = x / sqrt(sq[0]) when sq[0] > 0 (nothing written otherwise): the
 // scalar normalization of the residual, with the norm left on the device
 // (xpack as for k_transform)
-__global__ void k_normalize_col(const double *__restrict__ x, double *__restrict__ y, const double *__restrict__ sq,
+template <typename TO>
+__global__ void k_normalize_col(const double *__restrict__ x, TO *__restrict__ y, const double *__restrict__ sq,
                                 int64_t n, void *__restrict__ xpack, int xprec) {
     const double q = sq[0];
     if (!(q > 0.0)) return;
     const double inv = 1.0 / sqrt(q);
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const double v = x[i] * inv;
-        y[i] = v;
+        y[i] = (TO)v;
         if (xpack) {
             if (xprec == 4)
                 static_cast<float *>(xpack)[i] = (float)v;
@@ -244,9 +251,9 @@ __global__ void k_normalize_col(const double *__restrict__ x, double *__restrict
     }
 }
 
-// interleaved applyH vector from nB history columns (fp64 -> T)
-template <typename T>
-__global__ void k_pack(const double *__restrict__ V, int nB, int64_t n, int64_t ld, T *__restrict__ x) {
+// interleaved applyH vector from nB history columns (TV -> T)
+template <typename TV, typename T>
+__global__ void k_pack(const TV *__restrict__ V, int nB, int64_t n, int64_t ld, T *__restrict__ x) {
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n * nB; e += (int64_t)gridDim.x * blockDim.x) {
         const int64_t s = e / nB;
         const int b = (int)(e - s * nB);
@@ -612,8 +619,8 @@ static int stream_grid(int64_t n) {
     return (NB == 1 && n >= (int64_t)592 * kDotTile) ? kMaxDotGrid : 592;
 }
 
-template <int NB>
-static cudaError_t multidot_nb(const double *A, int nA, const double *B, int64_t n, int64_t ld, double *partial,
+template <typename TA, int NB>
+static cudaError_t multidot_nb(const TA *A, int nA, const double *B, int64_t n, int64_t ld, double *partial,
                                double *out, cudaStream_t s) {
     const int64_t tiles = (n + kDotTile - 1) / kDotTile;
     const int G = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, stream_grid<NB>(n)));
@@ -627,11 +634,11 @@ static cudaError_t multidot_nb(const double *A, int nA, const double *B, int64_t
         // two A vectors per warp pass halve the shared loads per multiply-add
         // for NB >= 4, once there are enough vectors to keep all 8 warps busy
         if (NB >= 4 && na >= 16) {
-            cudaFuncSetAttribute(k_multidot<NB, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            k_multidot<NB, 2><<<dim3(G, gy), kDotThreads, smem, s>>>(A + (int64_t)a0 * ld, na, B, n, ld, partial);
+            cudaFuncSetAttribute(k_multidot<TA, NB, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            k_multidot<TA, NB, 2><<<dim3(G, gy), kDotThreads, smem, s>>>(A + (int64_t)a0 * ld, na, B, n, ld, partial);
         } else {
-            cudaFuncSetAttribute(k_multidot<NB, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            k_multidot<NB, 1><<<dim3(G, gy), kDotThreads, smem, s>>>(A + (int64_t)a0 * ld, na, B, n, ld, partial);
+            cudaFuncSetAttribute(k_multidot<TA, NB, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            k_multidot<TA, NB, 1><<<dim3(G, gy), kDotThreads, smem, s>>>(A + (int64_t)a0 * ld, na, B, n, ld, partial);
         }
         k_reduce_partials<<<(na * NB * 32 + 255) / 256, 256, 0, s>>>(partial, na * NB, G, out + (int64_t)a0 * NB);
         a0 += na;
@@ -639,22 +646,34 @@ static cudaError_t multidot_nb(const double *A, int nA, const double *B, int64_t
     return cudaGetLastError();
 }
 
-cudaError_t multidot(const double *A, int nA, const double *B, int nB, int64_t n, int64_t ld, double *partial,
-                     double *out, cudaStream_t s) {
+template <typename TA>
+static cudaError_t multidot_t(const TA *A, int nA, const double *B, int nB, int64_t n, int64_t ld, double *partial,
+                              double *out, cudaStream_t s) {
     if (nA <= 0 || nB <= 0) return cudaSuccess;
     switch (nB) {
-    case 1: return multidot_nb<1>(A, nA, B, n, ld, partial, out, s);
-    case 2: return multidot_nb<2>(A, nA, B, n, ld, partial, out, s);
-    case 4: return multidot_nb<4>(A, nA, B, n, ld, partial, out, s);
-    case 8: return multidot_nb<8>(A, nA, B, n, ld, partial, out, s);
-    case 16: return multidot_nb<16>(A, nA, B, n, ld, partial, out, s);
+    case 1: return multidot_nb<TA, 1>(A, nA, B, n, ld, partial, out, s);
+    case 2: return multidot_nb<TA, 2>(A, nA, B, n, ld, partial, out, s);
+    case 4: return multidot_nb<TA, 4>(A, nA, B, n, ld, partial, out, s);
+    case 8: return multidot_nb<TA, 8>(A, nA, B, n, ld, partial, out, s);
+    case 16: return multidot_nb<TA, 16>(A, nA, B, n, ld, partial, out, s);
     default:
         return cudaErrorInvalidValue;
     }
 }
 
-template <int NB>
-static cudaError_t sub_gemv_nb(const double *H, int k, const double *C, double *W, int64_t n, int64_t ld,
+cudaError_t multidot(const void *A, int aprec, int nA, const double *B, int nB, int64_t n, int64_t ld,
+                     double *partial, double *out, cudaStream_t s) {
+    if (aprec == 4) return multidot_t<float>((const float *)A, nA, B, nB, n, ld, partial, out, s);
+    return multidot_t<double>((const double *)A, nA, B, nB, n, ld, partial, out, s);
+}
+
+cudaError_t multidot(const double *A, int nA, const double *B, int nB, int64_t n, int64_t ld, double *partial,
+                     double *out, cudaStream_t s) {
+    return multidot_t<double>(A, nA, B, nB, n, ld, partial, out, s);
+}
+
+template <typename TH, int NB>
+static cudaError_t sub_gemv_nb(const TH *H, int k, const double *C, double *W, int64_t n, int64_t ld,
                                double *sq_partial, double *sq_out, cudaStream_t s) {
     const int G = stream_grid<NB>(n);
     int j0 = 0;
@@ -662,29 +681,42 @@ static cudaError_t sub_gemv_nb(const double *H, int k, const double *C, double *
         const int kk = (k - j0) < 512 ? (k - j0) : 512;
         const bool last = (j0 + kk >= k);
         const size_t smem = sizeof(double) * ((size_t)kk * NB + 8 * NB);
-        cudaFuncSetAttribute(k_sub_gemv<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(smem + 256));
-        k_sub_gemv<NB><<<G, 256, smem, s>>>(H + (int64_t)j0 * ld, kk, C + (int64_t)j0 * NB, W, n, ld,
-                                             last ? sq_partial : nullptr);
+        cudaFuncSetAttribute(k_sub_gemv<TH, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(smem + 256));
+        k_sub_gemv<TH, NB><<<G, 256, smem, s>>>(H + (int64_t)j0 * ld, kk, C + (int64_t)j0 * NB, W, n, ld,
+                                                 last ? sq_partial : nullptr);
         j0 += kk;
     } while (j0 < k);
     if (sq_partial && sq_out) k_reduce_partials<<<(NB * 32 + 255) / 256, 256, 0, s>>>(sq_partial, NB, G, sq_out);
     return cudaGetLastError();
 }
 
-cudaError_t sub_gemv(const double *H, int k, const double *C, double *W, int nB, int64_t n, int64_t ld,
-                     double *sq_partial, double *sq_out, cudaStream_t s) {
+template <typename TH>
+static cudaError_t sub_gemv_t(const TH *H, int k, const double *C, double *W, int nB, int64_t n, int64_t ld,
+                              double *sq_partial, double *sq_out, cudaStream_t s) {
     switch (nB) {
-    case 1: return sub_gemv_nb<1>(H, k, C, W, n, ld, sq_partial, sq_out, s);
-    case 2: return sub_gemv_nb<2>(H, k, C, W, n, ld, sq_partial, sq_out, s);
-    case 4: return sub_gemv_nb<4>(H, k, C, W, n, ld, sq_partial, sq_out, s);
-    case 8: return sub_gemv_nb<8>(H, k, C, W, n, ld, sq_partial, sq_out, s);
-    case 16: return sub_gemv_nb<16>(H, k, C, W, n, ld, sq_partial, sq_out, s);
+    case 1: return sub_gemv_nb<TH, 1>(H, k, C, W, n, ld, sq_partial, sq_out, s);
+    case 2: return sub_gemv_nb<TH, 2>(H, k, C, W, n, ld, sq_partial, sq_out, s);
+    case 4: return sub_gemv_nb<TH, 4>(H, k, C, W, n, ld, sq_partial, sq_out, s);
+    case 8: return sub_gemv_nb<TH, 8>(H, k, C, W, n, ld, sq_partial, sq_out, s);
+    case 16: return sub_gemv_nb<TH, 16>(H, k, C, W, n, ld, sq_partial, sq_out, s);
     default: return cudaErrorInvalidValue;
     }
 }
 
-cudaError_t transform(const double *V, int m, const double *Y, int ldy, int K, double *out, int64_t n, int64_t ld,
-                      int64_t ldo, cudaStream_t s, void *xpack, int xprec) {
+cudaError_t sub_gemv(const void *H, int hprec, int k, const double *C, double *W, int nB, int64_t n, int64_t ld,
+                     double *sq_partial, double *sq_out, cudaStream_t s) {
+    if (hprec == 4) return sub_gemv_t<float>((const float *)H, k, C, W, nB, n, ld, sq_partial, sq_out, s);
+    return sub_gemv_t<double>((const double *)H, k, C, W, nB, n, ld, sq_partial, sq_out, s);
+}
+
+cudaError_t sub_gemv(const double *H, int k, const double *C, double *W, int nB, int64_t n, int64_t ld,
+                     double *sq_partial, double *sq_out, cudaStream_t s) {
+    return sub_gemv_t<double>(H, k, C, W, nB, n, ld, sq_partial, sq_out, s);
+}
+
+template <typename TV, typename TO>
+static cudaError_t transform_t(const TV *V, int m, const double *Y, int ldy, int K, TO *out, int64_t n, int64_t ld,
+                               int64_t ldo, cudaStream_t s, void *xpack, int xprec) {
     if (xpack && K > 16) return cudaErrorInvalidValue;  // the packed copy needs one pass
     for (int l0 = 0; l0 < K; l0 += 16) {
         const int kk = (K - l0) < 16 ? (K - l0) : 16;
@@ -695,10 +727,11 @@ cudaError_t transform(const double *V, int m, const double *Y, int ldy, int K, d
         switch (kk) {
 #define BSG_TRANSFORM_CASE(KT)                                                                              \
     case KT:                                                                                                \
-        e = cudaFuncSetAttribute(k_transform<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024); \
+        e = cudaFuncSetAttribute(k_transform<KT, TV, TO>, cudaFuncAttributeMaxDynamicSharedMemorySize,      \
+                                 160 * 1024);                                                               \
         if (e == cudaSuccess)                                                                               \
-            k_transform<KT><<<592, 256, smem, s>>>(V, m, Y + l0, ldy, out + (int64_t)l0 * ldo, n, ld, ldo, \
-                                                    xpack, xprec);                                       \
+            k_transform<KT, TV, TO><<<592, 256, smem, s>>>(V, m, Y + l0, ldy, out + (int64_t)l0 * ldo, n, ld, \
+                                                            ldo, xpack, xprec);                             \
         break;
             BSG_TRANSFORM_CASE(1) BSG_TRANSFORM_CASE(2) BSG_TRANSFORM_CASE(3) BSG_TRANSFORM_CASE(4)
             BSG_TRANSFORM_CASE(5) BSG_TRANSFORM_CASE(6) BSG_TRANSFORM_CASE(7) BSG_TRANSFORM_CASE(8)
@@ -711,22 +744,56 @@ cudaError_t transform(const double *V, int m, const double *Y, int ldy, int K, d
     return cudaGetLastError();
 }
 
-cudaError_t scale_cols(const double *x, double *y, const double *sc, int nB, int64_t n, int64_t ld, cudaStream_t s) {
-    k_scale_cols<<<592, 256, 0, s>>>(x, y, sc, nB, n, ld);
-    return cudaGetLastError();
+cudaError_t transform(const void *V, int vprec, int m, const double *Y, int ldy, int K, void *out, int oprec,
+                      int64_t n, int64_t ld, int64_t ldo, cudaStream_t s, void *xpack, int xprec) {
+    if (vprec == 4 && oprec == 4)
+        return transform_t<float, float>((const float *)V, m, Y, ldy, K, (float *)out, n, ld, ldo, s, xpack, xprec);
+    if (vprec == 4)
+        return transform_t<float, double>((const float *)V, m, Y, ldy, K, (double *)out, n, ld, ldo, s, xpack, xprec);
+    if (oprec == 4)
+        return transform_t<double, float>((const double *)V, m, Y, ldy, K, (float *)out, n, ld, ldo, s, xpack, xprec);
+    return transform_t<double, double>((const double *)V, m, Y, ldy, K, (double *)out, n, ld, ldo, s, xpack, xprec);
 }
 
-cudaError_t normalize_col(const double *x, double *y, const double *sq, int64_t n, cudaStream_t s, void *xpack,
-                          int xprec) {
-    k_normalize_col<<<592, 256, 0, s>>>(x, y, sq, n, xpack, xprec);
-    return cudaGetLastError();
+cudaError_t transform(const double *V, int m, const double *Y, int ldy, int K, double *out, int64_t n, int64_t ld,
+                      int64_t ldo, cudaStream_t s, void *xpack, int xprec) {
+    return transform_t<double, double>(V, m, Y, ldy, K, out, n, ld, ldo, s, xpack, xprec);
 }
 
-cudaError_t pack(const double *V, int nB, int64_t n, int64_t ld, void *x, int prec, cudaStream_t s) {
-    if (prec == 4)
-        k_pack<float><<<1184, 256, 0, s>>>(V, nB, n, ld, (float *)x);
+cudaError_t scale_cols(const double *x, void *y, int yprec, const double *sc, int nB, int64_t n, int64_t ld,
+                       cudaStream_t s) {
+    if (yprec == 4)
+        k_scale_cols<float><<<592, 256, 0, s>>>(x, (float *)y, sc, nB, n, ld);
     else
-        k_pack<double><<<1184, 256, 0, s>>>(V, nB, n, ld, (double *)x);
+        k_scale_cols<double><<<592, 256, 0, s>>>(x, (double *)y, sc, nB, n, ld);
+    return cudaGetLastError();
+}
+
+cudaError_t scale_cols(const double *x, double *y, const double *sc, int nB, int64_t n, int64_t ld, cudaStream_t s) {
+    return scale_cols(x, y, 8, sc, nB, n, ld, s);
+}
+
+cudaError_t normalize_col(const double *x, void *y, int yprec, const double *sq, int64_t n, cudaStream_t s,
+                          void *xpack, int xprec) {
+    if (yprec == 4)
+        k_normalize_col<float><<<592, 256, 0, s>>>(x, (float *)y, sq, n, xpack, xprec);
+    else
+        k_normalize_col<double><<<592, 256, 0, s>>>(x, (double *)y, sq, n, xpack, xprec);
+    return cudaGetLastError();
+}
+
+cudaError_t pack(const void *V, int vprec, int nB, int64_t n, int64_t ld, void *x, int prec, cudaStream_t s) {
+    if (vprec == 4) {
+        if (prec == 4)
+            k_pack<float, float><<<1184, 256, 0, s>>>((const float *)V, nB, n, ld, (float *)x);
+        else
+            k_pack<float, double><<<1184, 256, 0, s>>>((const float *)V, nB, n, ld, (double *)x);
+    } else {
+        if (prec == 4)
+            k_pack<double, float><<<1184, 256, 0, s>>>((const double *)V, nB, n, ld, (float *)x);
+        else
+            k_pack<double, double><<<1184, 256, 0, s>>>((const double *)V, nB, n, ld, (double *)x);
+    }
     return cudaGetLastError();
 }
 

@@ -113,7 +113,12 @@ class Hamiltonian:
     # ----------------------------------------------------------- Lanczos
     def lanczos(self, nkeep=10, niter=300, nthick_add=0, max_restarts=0, nb=1, matvec_prec=8,
                 fixed_iter=False, ncheck=None, converge_tol=1e-3, want_vectors=False, pivot=None,
-                seed=12345):
+                seed=12345, lanc_prec=8):
+        """lanczos_p (nb = 1) / lanczos_block (nb > 1) with thick restart.
+        matvec_prec: applyH precision (4 or 8); lanc_prec: storage of the
+        Lanczos vectors (4 or 8, the reference's lanc_prec), dots and updates
+        accumulating in FP64 either way.  Returns (eigenvalues, eigenvectors
+        dim x nkeep or None, report dict)."""
         p = _abi.BsgLanczosParams()
         p.nkeep = nkeep
         p.niter = niter
@@ -127,6 +132,7 @@ class Hamiltonian:
         p.want_vectors = 1 if want_vectors else 0
         p.pivot = 0
         p.seed = seed
+        p.lanc_prec = lanc_prec
         ev = np.zeros(nkeep, dtype=np.float64)
         vecs = np.zeros((nkeep, self.dim), dtype=np.float64) if want_vectors else None
         pv = None
@@ -336,9 +342,47 @@ class Batch:
         s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
         self._check(self.lib.bsg_batch_applyh(self.h, vi, vo, prec, C.c_void_p(s)), "bsg_batch_applyh")
 
-    def lanczos(self, nkeep=5, niter=150, matvec_prec=8, want_vectors=False):
+    def grad(self, vecs):
+        """Adjoint gradients of every system in one launch (bsg_batch_grad):
+        vecs[s] dim_s x k eigenvectors of system s; returns a list of dicts
+        of (k, nmat) arrays 'pp', 'nn', 'pn' (and 'spe_p', 'spe_n' for
+        members with SPE bundles), bitwise equal to each member's own
+        Hamiltonian.grad, and sets self.grad_ms to the launch's device time."""
+        n = len(self.tables)
+        if len(vecs) != n:
+            raise ValueError("one eigenvector block per system")
+        k = np.asarray(vecs[0]).shape[1] if np.asarray(vecs[0]).ndim == 2 else 1
+        cols, outs = [], []
+        for t, v in zip(self.tables, vecs):
+            v = np.asarray(v, dtype=np.float64).reshape(t.dim, -1)
+            if v.shape[1] != k:
+                raise ValueError("every system needs the same number of states")
+            cols.append(np.ascontiguousarray(v.T))
+            s = t.s
+            o = {"pp": np.zeros((k, s["nmatpp"])), "nn": np.zeros((k, s["nmatnn"])), "pn": np.zeros((k, s["nmatpn"]))}
+            if s["call_spe"]:
+                o["spe_p"] = np.zeros((k, s["nsd_p"]))
+                o["spe_n"] = np.zeros((k, s["nsd_n"]))
+            outs.append(o)
+        arr = lambda xs: (_abi.f64p * n)(*[x.ctypes.data_as(_abi.f64p) if x is not None else None for x in xs])
+        ms = C.c_double()
+        st = self.lib.bsg_batch_grad(self.h, arr(cols), k, arr([o["pp"] for o in outs]), arr([o["nn"] for o in outs]),
+                                     arr([o["pn"] for o in outs]), arr([o.get("spe_p") for o in outs]),
+                                     arr([o.get("spe_n") for o in outs]), C.byref(ms))
+        self._check(st, "bsg_batch_grad")
+        self.grad_ms = ms.value
+        return outs
+
+    def lanczos(self, nkeep=5, niter=150, matvec_prec=8, want_vectors=False, pivot="uniform", seed=12345):
+        """Lock-step Lanczos over all systems, exactly niter iterations.
+        pivot: "uniform" (the reference's option 0) or "random" (a seeded
+        random normalized pivot per system)."""
         p = _abi.BsgLanczosParams()
         p.nkeep, p.niter, p.nb, p.matvec_prec, p.fixed_iter = nkeep, niter, 1, matvec_prec, 1
+        if pivot not in ("uniform", "random"):
+            raise ValueError("pivot must be 'uniform' or 'random'")
+        p.pivot = 1 if pivot == "random" else 0
+        p.seed = seed
         ev = np.zeros(len(self.tables) * nkeep)
         vecs = [np.zeros((nkeep, d)) for d in self.dims] if want_vectors else None
         vp = (_abi.f64p * len(self.tables))(*[v.ctypes.data_as(_abi.f64p) for v in vecs]) if vecs else None

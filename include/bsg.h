@@ -132,8 +132,14 @@ typedef struct bsg_lanczos_params {
     int32_t ncheck;        /* states in the convergence test (nkeep+ncheck_ex) */
     double  converge_tol;  /* converge_tol0_def = 1e-3 (blanczoslib.f90:2642)  */
     int32_t want_vectors;  /* 1: return nkeep eigenvectors (fp64, dim x nkeep) */
-    int32_t pivot;         /* 0: uniform 1/sqrt(dim) (blanczoslib.f90:825-831) */
+    int32_t pivot;         /* 0: uniform 1/sqrt(dim) (blanczoslib.f90:825-831);
+                              bsg_batch_lanczos also takes 1: a seeded random
+                              normalized pivot per system (seed, system)   */
     uint64_t seed;         /* random restart / block pivot seed                */
+    int32_t lanc_prec;     /* Lanczos vector storage (src/bmodules_main.f90:171):
+                              BSG_PREC_FP32 or BSG_PREC_FP64 (0 = FP64); dots,
+                              updates and alpha/beta accumulate in FP64 */
+    int32_t reserved;
 } bsg_lanczos_params;
 
 typedef struct bsg_report {
@@ -204,6 +210,9 @@ int  bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const double *pivot_
  *      dspe_n[nstates*nsd_n] (the last two only when call_spe; may be NULL). ---- */
 int  bsg_grad(bsg_ctx *ctx, const double *evecs, int nstates,
               double *dpp, double *dnn, double *dpn, double *dspe_p, double *dspe_n);
+/*      All states in one launch; every label's sum is accumulated exactly (to
+ *      2^-64) in 128-bit fixed point with integer atomics, so the result is
+ *      bitwise repeatable and independent of how the work is split. */
 
 /* ---- one-body densities: replaces master_density1b_bundled
  *      (src/bdenslib1.f90:1506-1607), i.e. applyP1Bdenbundled_g and
@@ -280,6 +289,56 @@ int  bsg_batch_autotune(bsg_batch *b, int *items, int *ctas_per_sm, double *best
 int  bsg_batch_set_tuning(bsg_batch *b, int items, int ctas_per_sm);
 int  bsg_batch_lanczos(bsg_batch *b, const bsg_lanczos_params *p, double *evals, double *const *evecs,
                        bsg_report *rep);
+/* adjoint gradients of every system of the batch in one launch over all
+ * (system, state, row tile) items (the per-system bsg_grad of each member,
+ * bitwise equal to it): evecs[s] host fp64 dim_s x nstates column-major;
+ * dpp[s], dnn[s], dpn[s] host fp64 [nstates x nmat*_s] (state-major), and
+ * dspe_p[s] / dspe_n[s] for members with SPE bundles (arrays may be NULL).
+ * kernel_ms (may be NULL): device time of the launch. */
+int  bsg_batch_grad(bsg_batch *b, const double *const *evecs, int nstates, double *const *dpp,
+                    double *const *dnn, double *const *dpn, double *const *dspe_p, double *const *dspe_n,
+                    double *kernel_ms);
+
+/* ---- on-device jump generation: the set-up stage that builds the jump
+ *      tables (weld / master1bodyjumps / master2bodyjumps,
+ *      src/bjumplib_weld.f90:296-809, src/bjumplib_master.f90:436-1196) and
+ *      sorts the PN bundles' ranges (sort1bjumps, src/bsortjumpslib.f90
+ *      :190-290), run as GPU kernels.  A species is described by its Slater
+ *      determinants; the generated arrays are the jumpNbody arrays of bsg.h
+ *      (p1b_*, n1b_*, p2b_*, n2b_*), in the host builder's order:
+ *        one-body, per sector jump (is -> fs): source SD ascending, then the
+ *          annihilated state k, then the created state i (a+_i a_k), the
+ *          jumps whose final SD lies in fs;
+ *        two-body, per sector: source SD, annihilated pair k<l, created pair
+ *          i<j of the same (M, parity) section, isd >= fsd kept;
+ *      isd/fsd hold pstart/nstart values, cop/dop the signed labels
+ *      (q < nl: -(q+1), else q-nl+1), op the hmatpp/hmatnn label. ---- */
+typedef struct bsg_species {
+    int32_t nsps;                 /* s.p. states (at most 22)                  */
+    int32_t nl;                   /* the first nl states have m < 0            */
+    const int32_t *m2, *par;      /* 2m and parity (+1/-1) per s.p. state      */
+    int64_t nsd;
+    const uint64_t *sd_bits;      /* occupation bitmask per SD (bit q: state q)*/
+    const int64_t *xstart;        /* pstart (protons) / nstart (neutrons) per SD */
+    int32_t nsectors;
+    const int64_t *sector_start, *sector_end;   /* 1-based SD range per sector */
+} bsg_species;
+typedef struct bsg_jumpgen bsg_jumpgen;
+int  bsg_jumpgen_create(int device, const bsg_species *sp, bsg_jumpgen **out);
+int  bsg_jumpgen_destroy(bsg_jumpgen *g);
+int  bsg_jumpgen_last_error(const bsg_jumpgen *g, char *buf, size_t len);
+/* one-body jumps of the sector jumps is[j] -> fs[j] (0-based sectors):
+ * starts[0..nsj] receives the first jump of each (starts[nsj] = total); the
+ * outputs (host arrays of starts[nsj] entries) may be NULL to count only */
+int  bsg_jumpgen_one(bsg_jumpgen *g, int nsj, const int32_t *is, const int32_t *fs, int64_t *starts,
+                     int64_t *isd, int64_t *fsd, int16_t *cop, int16_t *dop, int8_t *phase, double *kernel_ms);
+/* two-body jumps inside the sectors sec[j] */
+int  bsg_jumpgen_two(bsg_jumpgen *g, int nsec, const int32_t *sec, int64_t *starts,
+                     int64_t *isd, int64_t *fsd, int32_t *op, int8_t *phase, double *kernel_ms);
+/* sort1bjumps on the nr disjoint ranges [start, start+len) of host arrays of
+ * n jumps: key fsd (by_fsd = 1, the proton side of PN bundles) or isd */
+int  bsg_jumpgen_sort1(bsg_jumpgen *g, int nr, const int64_t *start, const int64_t *len, int by_fsd, int64_t n,
+                       int64_t *isd, int64_t *fsd, int16_t *cop, int16_t *dop, int8_t *phase, double *kernel_ms);
 
 /* ---- introspection used by tests and the benchmark ---- */
 typedef struct bsg_stats {
@@ -297,6 +356,7 @@ typedef struct bsg_stats {
     int32_t density_launches;
     int32_t reserved2;
     double  apply1b_ms;        /* last bsg_apply1b: device time of its kernels */
+    double  grad_ms;           /* last bsg_grad: device time of its kernels    */
 } bsg_stats;
 int  bsg_get_stats(const bsg_ctx *ctx, bsg_stats *st);
 

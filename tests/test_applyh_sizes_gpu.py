@@ -143,3 +143,19 @@ def test_sd6p6n_fp64_lanczos_matches_oracle(sd66):
     ref, _, _ = olz.lanczos(T, nkeep=10, niter=300, fixed_iter=True, pivot=piv, nthreads=NTHR)
     rel = np.abs(ev - ref) / np.abs(ref)
     assert rel.max() < 1e-10, rel
+
+
+def test_sd6p6n_mixed_fp32_history_against_fp64(sd66):
+    """sd 6p6n, 300 iterations: FP32 applyH with FP32-stored Lanczos vectors
+    (lanc_prec = 4) against the FP64 path from the same pivot: eigenvalues
+    within 1e-6 relative and eigenvector overlaps above 1 - 1e-6 for the
+    lowest 10 states."""
+    T, H = sd66
+    piv = np.random.default_rng(11).standard_normal(T.dim)
+    ev8, v8, _ = H.lanczos(nkeep=10, niter=300, matvec_prec=8, fixed_iter=True, pivot=piv, want_vectors=True)
+    ev4, v4, _ = H.lanczos(nkeep=10, niter=300, matvec_prec=4, lanc_prec=4, fixed_iter=True, pivot=piv,
+                           want_vectors=True)
+    rel = np.abs(ev4 - ev8) / np.abs(ev8)
+    assert rel.max() < 1e-6, rel
+    ov = np.abs(np.sum(v4 * v8, axis=0))
+    assert ov.min() > 1 - 1e-6, ov

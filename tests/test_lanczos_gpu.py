@@ -123,3 +123,74 @@ def test_block_thick_restart(sd22):
     assert rep["restarts"] >= 1
     rel = np.abs(ev - exact[:6]) / np.abs(exact[:6])
     assert rel.max() < 1e-6, (rel, rep)
+
+
+BLOCK_RUNS = {
+    # nb: (plain run, thick-restart run); stop steps verified stable for tol
+    # within +-2 % in the oracle, so round-off cannot move them
+    2: (dict(nkeep=6, niter=150), dict(nkeep=5, niter=20, nthick_add=7, max_restarts=40)),
+    4: (dict(nkeep=6, niter=80), dict(nkeep=5, niter=10, nthick_add=7, max_restarts=40)),
+    8: (dict(nkeep=6, niter=40), dict(nkeep=5, niter=8, nthick_add=11, max_restarts=40)),
+}
+
+
+@pytest.mark.parametrize("thick", [False, True])
+@pytest.mark.parametrize("nb", [2, 4, 8])
+def test_block_matches_oracle(sd22, nb, thick):
+    """Block Lanczos (and block thick restart) against the oracle's
+    lanczos_block restatement from the same pivot block: the same stop step
+    and restart count under the reference's convergence test (tol 1e-3), and
+    the same eigenvalues."""
+    T, H, exact = sd22
+    piv = generic_pivot(T.dim, nb)
+    kw = BLOCK_RUNS[nb][1 if thick else 0]
+    ev, _, rep = H.lanczos(nb=nb, matvec_prec=8, converge_tol=1e-3, pivot=piv, **kw)
+    ref, _, orep = olz.lanczos_block(T, nb, tol=1e-3, pivot=piv, **kw)
+    assert orep["converged"] == 1 and rep["converged"] == 1
+    assert rep["total_iterations"] == orep["total_iterations"], (rep, orep)
+    assert rep["restarts"] == orep["restarts"], (rep, orep)
+    if thick:
+        assert rep["restarts"] >= 1
+    assert np.abs(ev - ref).max() / np.abs(ref).max() < 1e-10, (ev, ref)
+
+
+@pytest.mark.parametrize("nb", [4, 8])
+def test_block_fixed_schedule_matches_oracle(sd22, nb):
+    """A fixed schedule with three block thick restarts: the eigenvalues after
+    the same steps agree with the oracle's to 1e-10."""
+    T, H, exact = sd22
+    piv = generic_pivot(T.dim, nb, seed=9)
+    kw = dict(nkeep=5, niter=6, nthick_add=11, max_restarts=3)
+    ev, _, rep = H.lanczos(nb=nb, matvec_prec=8, converge_tol=1e-30, pivot=piv, **kw)
+    ref, _, orep = olz.lanczos_block(T, nb, tol=1e-30, pivot=piv, **kw)
+    assert rep["restarts"] == orep["restarts"] == 3
+    assert rep["total_iterations"] == orep["total_iterations"]
+    assert np.abs(ev - ref).max() / np.abs(ref).max() < 1e-10, (ev, ref)
+
+
+@pytest.mark.parametrize("matvec_prec", [8, 4])
+def test_fp32_history_error_bound(sd22, matvec_prec):
+    """Lanczos vectors stored in FP32 (the reference's shipped lanc_prec = 4),
+    dots and updates accumulated in FP64: eigenvalues within 1e-6 relative of
+    exact diagonalization, with the FP64 or the FP32 applyH."""
+    T, H, exact = sd22
+    ev, vecs, rep = H.lanczos(nkeep=10, niter=300, matvec_prec=matvec_prec, lanc_prec=4, converge_tol=1e-10,
+                              pivot=generic_pivot(T.dim), want_vectors=True)
+    rel = np.abs(ev - exact[:10]) / np.abs(exact[:10])
+    assert rel.max() < 1e-6, rel
+    for k in range(3):
+        v = vecs[:, k]
+        assert abs(np.linalg.norm(v) - 1) < 1e-5
+        assert np.linalg.norm(oracle.applyh(T, v) - ev[k] * v) < 1e-4 * abs(ev[k])
+
+
+@pytest.mark.parametrize("nb", [1, 4])
+def test_fp32_history_thick_restart(sd22, nb):
+    """FP32 history through thick restarts (basis rotation stored in FP32)."""
+    T, H, exact = sd22
+    kw = dict(nkeep=5, niter=40 if nb == 1 else 10, nthick_add=7, max_restarts=60)
+    ev, _, rep = H.lanczos(nb=nb, matvec_prec=4, lanc_prec=4, converge_tol=1e-8, pivot=generic_pivot(T.dim, nb),
+                           **kw)
+    assert rep["restarts"] >= 1
+    rel = np.abs(ev - exact[:5]) / np.abs(exact[:5])
+    assert rel.max() < 1e-6, (rel, rep)
