@@ -354,6 +354,16 @@ struct bsg_batch {
 };
 
 namespace {
+// SplitMix64 finalizer (Steele, Lea and Flood 2014) for host-side seeded pivots
+inline uint64_t host_mix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+}  // namespace
+
+namespace {
 
 int berr(bsg_batch *b, int code, const std::string &m) {
     b->last_error = m;
@@ -517,6 +527,17 @@ int bsg_batch_destroy(bsg_batch *b) {
     return BSG_OK;
 }
 
+int bsg_batch_grad(bsg_batch *b, const double *const *evecs, int nstates, double *const *dpp, double *const *dnn,
+                   double *const *dpn, double *const *dspe_p, double *const *dspe_n, double *kernel_ms) {
+    if (!b) return BSG_ERR_ARG;
+    cudaSetDevice(b->device);
+    std::string err;
+    const int st = grad_many(b->ctx.data(), b->n, evecs, nstates, dpp, dnn, dpn, dspe_p, dspe_n, b->stream, err,
+                             kernel_ms);
+    if (st) return berr(b, st, "bsg_batch_grad: " + err);
+    return BSG_OK;
+}
+
 int bsg_batch_last_error(const bsg_batch *b, char *buf, size_t len) {
     if (!b || !buf || !len) return BSG_ERR_ARG;
     std::snprintf(buf, len, "%s", b->last_error.c_str());
@@ -612,7 +633,7 @@ int bsg_batch_set_tuning(bsg_batch *b, int items, int ctas_per_sm) {
 }
 
 // lock-step Lanczos over all systems: fixed p->niter iterations, uniform
-// pivot per system (or the given ones), lowest p->nkeep eigenvalues per
+// pivot per system (or seeded random ones, p->pivot == 1), lowest p->nkeep eigenvalues per
 // system into evals[s*nkeep + k]; evecs: NULL or n host pointers of
 // dim_s*nkeep doubles (column-major).
 int bsg_batch_lanczos(bsg_batch *b, const bsg_lanczos_params *p, double *evals, double *const *evecs,
@@ -676,9 +697,25 @@ int bsg_batch_lanczos(bsg_batch *b, const bsg_lanczos_params *p, double *evals, 
     }
     st = upload(c0, chd, chunks.data(), sizeof(BChunk) * chunks.size());
     if (!st) st = upload(c0, lzd, lz.data(), sizeof(BLz) * lz.size());
-    // pivots: uniform 1/sqrt(dim) per system (initialize_lanczos_vector option 0)
+    // pivots: uniform 1/sqrt(dim) per system (initialize_lanczos_vector
+    // option 0), or (p->pivot == 1) a seeded pseudo-random normalized vector
+    // per system: SplitMix64 of (seed, system, index) through Box-Muller, so
+    // that no symmetry of the uniform vector restricts the Krylov space
     for (int s = 0; s < n && !st; ++s) {
         std::vector<double> v(b->dims[s], 1.0 / std::sqrt((double)b->dims[s]));
+        if (p->pivot == 1) {
+            double nrm = 0.0;
+            for (int64_t i = 0; i < b->dims[s]; ++i) {
+                const uint64_t h = host_mix64(p->seed ^ host_mix64(((uint64_t)s << 40) ^ (uint64_t)i));
+                const uint64_t h2 = host_mix64(h);
+                const double u1 = ((double)(h >> 11) + 1.0) * (1.0 / 9007199254740992.0);
+                const double u2 = (double)(h2 >> 11) * (1.0 / 9007199254740992.0);
+                v[i] = std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+                nrm += v[i] * v[i];
+            }
+            const double inv = 1.0 / std::sqrt(nrm);
+            for (double &x : v) x *= inv;
+        }
         if (cudaMemcpyAsync(lz[s].hist, v.data(), 8 * v.size(), cudaMemcpyHostToDevice, s0) != cudaSuccess ||
             cudaStreamSynchronize(s0) != cudaSuccess)
             st = BSG_ERR_CUDA;

@@ -97,6 +97,11 @@ struct RowArgs {
     const PNRec *pnrec;
     const NNRec *nnrec;
     const int2 *sell;             // sliced PN / NN records (see NOp)
+    // the same sliced records packed into 32 bits (null when a position or a
+    // label does not fit): bits 0-15 input position, 16-30 the PN (b,d)
+    // index or the NN hmatnn label - 1, bit 31 the jump phase's sign
+    const uint32_t *sell32;
+    const float *hmatnn;          // hmatnn (1-based labels; the NN 32-bit records index it)
     const int32_t *slice_off;
     const BDPair *bd;
     const float *hmatpn;
@@ -141,6 +146,7 @@ struct bsg_ctx {
     std::vector<bsg::DevBuf> raw;
     // derived
     bsg::DevBuf row_off, pp_ptr, nn_ptr, pn_ptr, spe_ptr, pp, nn, pn, spe, nops, nptr, pnrec, nnrec, bd, sell, slice_off;
+    bsg::DevBuf sell32;
     bsg::DevBuf hmatpn, cpn, dpn, nspe, hmatpp_d, hmatnn_d;
     bsg::RowArgs args{};
     std::map<int, bsg::TileSet> tiles;   // tile size -> tiles
@@ -185,4 +191,10 @@ int launch_applyh(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec, i
 // H x for an interleaved input x (nb <= 16, dense and 16-byte aligned), the
 // result written as nb FP64 columns of length dim starting at cols
 int launch_applyh_cols(bsg_ctx *ctx, const void *vin, double *cols, int nb, int prec, cudaStream_t s);
+// adjoint gradients of nsys systems x nstates states in one launch
+// (grad.cu); evecs[s] host dim_s x nstates column-major; outputs host
+// [state][label] per system (dspe_* may be null); kernel_ms: device time
+int grad_many(bsg_ctx *const *ctxs, int nsys, const double *const *evecs, int nstates, double *const *dpp,
+              double *const *dnn, double *const *dpn, double *const *dspe_p, double *const *dspe_n, cudaStream_t s,
+              std::string &err, double *kernel_ms);
 }  // namespace bsg

@@ -1,130 +1,184 @@
 // bsg_grad: Hellmann-Feynman gradient of eigenvalues with respect to every
-// uncoupled matrix element, dE_k/dhmat(label) = sum over every appearance of
-// the label in H of phase * psi_k(out) * psi_k(in).
+// uncoupled matrix element (the transposed-jump contraction of the two-body
+// densities, src/bdenslib4.f90:129-729; the tile body is grad_tile.cuh).
 //
-// This is the traversal of the two-body densities applyh{PP,NN,PN}bundled_den
-// (src/bdenslib4.f90:129-729: dmat(op) += vout(f)*vin(i)*phase) with both
-// vectors equal to the eigenvector, run over the same row tiles and
-// (row, warp) slots as the matvec: PP contributions reduce a row-segment dot
-// product per jump; PN contributions accumulate per distinct (b,d) label pair
-// in shared memory and flush one atomic per pair and proton jump; NN records
-// and SPE terms go straight to their bins.  Every f and b appearance is
-// visited, so hermitian halves and the 1/2 on diagonal pair labels are
-// accounted for exactly as in the matvec.
+// One launch covers every (system, state, row tile) item: bsg_grad is the
+// one-system case of grad_many, bsg_batch_grad (batch.cu) the many-system
+// one.  Sums are 128-bit fixed point updated with integer atomics, so the
+// gradient is bitwise repeatable and does not depend on how the work is
+// split: a system's gradient is the same alone or inside a batch.
 
+#include <algorithm>
+#include <string>
 #include <vector>
 
-#include "bsg_internal.h"
+#include "grad_tile.cuh"
 
 namespace bsg {
 
-struct GradArgs {
-    const int32_t *pp_op;
-    const int8_t *pp_ph;
-    const int32_t *nnrec_op;
-    const int8_t *nnrec_ph;
-    double *dpp, *dnn, *dpn, *dspe_p, *dspe_n;
+struct GradDesc {
+    RowArgs a;
+    GradArgs g;
+    const double *psi;
+};
+struct GradItem {
+    int32_t desc;   // (system, state)
+    int32_t tile;
 };
 
-constexpr int kGradWarps = kRowWarps;
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
+__global__ void k_fix_to_double(const unsigned long long *__restrict__ acc, double *__restrict__ out, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = fix_value(acc + 2 * i);
 }
 
 template <int ITEMS>
-__global__ void __launch_bounds__(kGradWarps * 32) k_grad(const RowArgs a, const GradArgs g,
-                                                          const double *__restrict__ psi, const int mstride) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double *__restrict__ Aw = reinterpret_cast<double *>(smem) + (size_t)warp * mstride;
-    const Tile tile = a.tiles[blockIdx.x];
-    const int row = tile.row;
-    const int64_t roff = a.row_off[row];
-    const int slot = row * kGradWarps + warp;
-    int pos[ITEMS];
-    bool valid[ITEMS];
-    double pout[ITEMS];
-#pragma unroll
-    for (int i = 0; i < ITEMS; ++i) {
-        const int local = lane + 32 * i;
-        pos[i] = tile.pos0 + local;
-        valid[i] = local < tile.npos;
-        pout[i] = valid[i] ? psi[roff + pos[i]] : 0.0;
+__global__ void __launch_bounds__(kGradWarps * 32) k_grad_items(const GradDesc *__restrict__ desc,
+                                                                const GradItem *__restrict__ items, int mstride) {
+    double *Aw, *stage_v;
+    int *stage_k;
+    grad_smem(mstride, Aw, stage_k, stage_v);
+    const GradItem it = items[blockIdx.x];
+    const GradDesc *D = desc + it.desc;
+    grad_tile<ITEMS>(D->a, D->g, D->psi, D->a.tiles[it.tile], Aw, stage_k, stage_v);
+}
+
+namespace {
+constexpr int kGradItems = 4;  // 128-position tiles
+}
+
+int grad_many(bsg_ctx *const *ctxs, int nsys, const double *const *evecs, int nstates, double *const *dpp,
+              double *const *dnn, double *const *dpn, double *const *dspe_p, double *const *dspe_n, cudaStream_t s,
+              std::string &err, double *kernel_ms) {
+    auto fail = [&](int code, const std::string &m) {
+        err = m;
+        return code;
+    };
+    if (nsys < 1 || nstates < 1 || !evecs || !dpp || !dnn || !dpn) return fail(BSG_ERR_ARG, "null argument");
+    // per (system, state): psi offset, accumulator offsets; per system: sizes
+    std::vector<int64_t> psi_off(nsys), acc_off((size_t)nsys * nstates);
+    std::vector<int64_t> nlab(nsys);
+    int64_t npsi = 0, nacc = 0;
+    int32_t max_nbd = 0;
+    std::vector<const TileSet *> ts(nsys);
+    std::vector<GradItem> items;
+    for (int s2 = 0; s2 < nsys; ++s2) {
+        bsg_ctx *c = ctxs[s2];
+        if (!evecs[s2] || !dpp[s2] || !dnn[s2] || !dpn[s2]) return fail(BSG_ERR_ARG, "null output for a system");
+        const bool spe = c->t.call_spe && dspe_p && dspe_n && dspe_p[s2] && dspe_n[s2];
+        c->last_status = BSG_OK;
+        ts[s2] = get_tiles(c, 32 * kGradItems);
+        if (!ts[s2]) return fail(c->last_status ? c->last_status : BSG_ERR_NOMEM, "tiles: " + c->last_error);
+        max_nbd = std::max(max_nbd, c->args.max_nbd);
+        psi_off[s2] = npsi;
+        npsi += c->dim * nstates;
+        nlab[s2] = c->t.nmatpp + c->t.nmatnn + c->t.nmatpn + (spe ? c->t.nsd_p + c->t.nsd_n : 0);
+        for (int k = 0; k < nstates; ++k) {
+            acc_off[(size_t)s2 * nstates + k] = nacc;
+            nacc += nlab[s2];
+        }
     }
-    // ---- PP: dpp[op] += ph * sum_pos psi[row+pos] psi[q+pos]
-    for (int c = a.pp_ptr[slot]; c < a.pp_ptr[slot + 1]; ++c) {
-        const PPContrib pc = a.pp[c];
-        double s = 0.0;
-#pragma unroll
-        for (int i = 0; i < ITEMS; ++i)
-            if (valid[i] && pos[i] >= pc.lo && pos[i] <= pc.hi) s += pout[i] * psi[pc.q_off + pos[i]];
-        s = warp_sum(s);
-        if (lane == 0 && s != 0.0) atomicAdd(g.dpp + g.pp_op[c] - 1, (double)g.pp_ph[c] * s);
+    // 8 per-warp FP64 bin tables and staging within 227 KB of shared memory
+    if (max_nbd > 3392) return fail(BSG_ERR_UNSUPPORTED, "a neutron sector jump has more than 3392 distinct (b,d) pairs");
+    const int mstride = (max_nbd + 1) & ~1;
+    // items heaviest tiles first (the tile lists are already in that order
+    // per system); interleave states so that concurrent CTAs share records
+    for (int s2 = 0; s2 < nsys; ++s2)
+        for (int t = 0; t < ts[s2]->ntiles; ++t)
+            for (int k = 0; k < nstates; ++k) items.push_back(GradItem{s2 * nstates + k, t});
+    bsg_ctx *c0 = ctxs[0];
+    DevBuf psi, acc, out, descb, itemb;
+    auto cleanup = [&]() {
+        dev_free(psi); dev_free(acc); dev_free(out); dev_free(descb); dev_free(itemb);
+    };
+    int st;
+    if ((st = dev_alloc(c0, psi, sizeof(double) * (size_t)std::max<int64_t>(npsi, 1))) ||
+        (st = dev_alloc(c0, acc, 16 * (size_t)std::max<int64_t>(nacc, 1))) ||
+        (st = dev_alloc(c0, out, sizeof(double) * (size_t)std::max<int64_t>(nacc, 1)))) {
+        cleanup();
+        return fail(st, "device allocation: " + c0->last_error);
     }
-    // ---- NN: dnn[op_r] += ph_r * psi[row+pos] psi[row+in_r]
-    for (int c = a.nn_ptr[slot]; c < a.nn_ptr[slot + 1]; ++c) {
-        const NOp op = a.nops[a.nn[c].nop];
-        const int32_t *__restrict__ ptr = a.nptr + op.ptr_base;
-#pragma unroll
-        for (int i = 0; i < ITEMS; ++i) {
-            if (!valid[i] || pos[i] >= op.nout) continue;
-            const int k0 = ptr[pos[i]], k1 = ptr[pos[i] + 1];
-            for (int k = k0; k < k1; ++k) {
-                const int64_t r = op.rec_base + k;
-                const double v = pout[i] * psi[roff + a.nnrec[r].in];
-                atomicAdd(g.dnn + g.nnrec_op[r] - 1, (double)g.nnrec_ph[r] * v);
+    std::vector<GradDesc> desc((size_t)nsys * nstates);
+    for (int s2 = 0; s2 < nsys; ++s2) {
+        bsg_ctx *c = ctxs[s2];
+        const bool spe = c->t.call_spe && dspe_p && dspe_n && dspe_p[s2] && dspe_n[s2];
+        for (int k = 0; k < nstates; ++k) {
+            GradDesc &d = desc[(size_t)s2 * nstates + k];
+            d.a = c->args;
+            d.a.tiles = (const Tile *)ts[s2]->buf.p;
+            d.a.ntiles = ts[s2]->ntiles;
+            unsigned long long *base = (unsigned long long *)acc.p + 2 * acc_off[(size_t)s2 * nstates + k];
+            d.g.pp_op = (const int32_t *)c->pp_op.p;
+            d.g.pp_ph = (const int8_t *)c->pp_ph.p;
+            d.g.nnrec_op = (const int32_t *)c->nnrec_op.p;
+            d.g.nnrec_ph = (const int8_t *)c->nnrec_ph.p;
+            d.g.pp = base;
+            d.g.nn = d.g.pp + 2 * c->t.nmatpp;
+            d.g.pn = d.g.nn + 2 * c->t.nmatnn;
+            d.g.spe_p = spe ? d.g.pn + 2 * c->t.nmatpn : nullptr;
+            d.g.spe_n = spe ? d.g.spe_p + 2 * c->t.nsd_p : nullptr;
+            d.psi = (const double *)psi.p + psi_off[s2] + (int64_t)k * c->dim;
+        }
+    }
+    if ((st = upload(c0, descb, desc.data(), sizeof(GradDesc) * desc.size())) ||
+        (st = upload(c0, itemb, items.data(), sizeof(GradItem) * std::max<size_t>(items.size(), 1)))) {
+        cleanup();
+        return fail(st, "upload: " + c0->last_error);
+    }
+    cudaError_t e = cudaSuccess;
+    for (int s2 = 0; s2 < nsys && e == cudaSuccess; ++s2)
+        e = cudaMemcpyAsync((double *)psi.p + psi_off[s2], evecs[s2], sizeof(double) * ctxs[s2]->dim * nstates,
+                            cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(acc.p, 0, acc.bytes, s);
+    const size_t smem = grad_smem_bytes(mstride);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_grad_items<kGradItems>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s);
+    if (e == cudaSuccess && !items.empty()) {
+        k_grad_items<kGradItems><<<(unsigned)items.size(), kGradWarps * 32, smem, s>>>(
+            (const GradDesc *)descb.p, (const GradItem *)itemb.p, mstride);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && nacc > 0) {
+        k_fix_to_double<<<(unsigned)std::min<int64_t>((nacc + 255) / 256, 4096), 256, 0, s>>>(
+            (const unsigned long long *)acc.p, (double *)out.p, nacc);
+        e = cudaGetLastError();
+    }
+    cudaEventRecord(e1, s);
+    // outputs: per system, state-major blocks [state][label]
+    for (int s2 = 0; s2 < nsys && e == cudaSuccess; ++s2) {
+        bsg_ctx *c = ctxs[s2];
+        const bool spe = c->t.call_spe && dspe_p && dspe_n && dspe_p[s2] && dspe_n[s2];
+        for (int k = 0; k < nstates && e == cudaSuccess; ++k) {
+            const double *o = (const double *)out.p + acc_off[(size_t)s2 * nstates + k];
+            auto cp = [&](double *dst, const double *src, int64_t cnt) {
+                if (e == cudaSuccess && cnt > 0)
+                    e = cudaMemcpyAsync(dst, src, sizeof(double) * cnt, cudaMemcpyDeviceToHost, s);
+            };
+            cp(dpp[s2] + k * c->t.nmatpp, o, c->t.nmatpp);
+            cp(dnn[s2] + k * c->t.nmatnn, o + c->t.nmatpp, c->t.nmatnn);
+            cp(dpn[s2] + k * c->t.nmatpn, o + c->t.nmatpp + c->t.nmatnn, c->t.nmatpn);
+            if (spe) {
+                const int64_t b0 = c->t.nmatpp + c->t.nmatnn + c->t.nmatpn;
+                cp(dspe_p[s2] + k * c->t.nsd_p, o + b0, c->t.nsd_p);
+                cp(dspe_n[s2] + k * c->t.nsd_n, o + b0 + c->t.nsd_p, c->t.nsd_n);
             }
         }
     }
-    // ---- PN: dpn[cpn(b,a)+dpn(d,c)] += php * phn * psi[row+pos] psi[q+in]
-    for (int c = a.pn_ptr[slot]; c < a.pn_ptr[slot + 1]; ++c) {
-        const PNContrib pc = a.pn[c];
-        const NOp op = a.nops[pc.nop];
-        for (int k = lane; k < op.nbd; k += 32) Aw[k] = 0.0;
-        __syncwarp();
-        const int32_t *__restrict__ ptr = a.nptr + op.ptr_base;
-#pragma unroll
-        for (int i = 0; i < ITEMS; ++i) {
-            if (!valid[i] || pos[i] >= op.nout) continue;
-            const int k0 = ptr[pos[i]], k1 = ptr[pos[i] + 1];
-            for (int k = k0; k < k1; ++k) {
-                const PNRec r = a.pnrec[op.rec_base + k];
-                const double v = pout[i] * psi[pc.q_off + r.in] * (double)r.ph;
-                atomicAdd(Aw + r.k, v);
-            }
-        }
-        __syncwarp();
-        const int acol = pc.acol * a.ld_cpn, ccol = pc.ccol * a.ld_cpn;
-        for (int k = lane; k < op.nbd; k += 32) {
-            const double v = Aw[k];
-            if (v != 0.0) {
-                const BDPair bd = a.bd[op.bd_base + k];
-                const int idx = a.cpn[bd.b + acol] + a.dpn[bd.d + ccol];
-                atomicAdd(g.dpn + idx - 1, (double)pc.php * v);
-            }
-        }
-        __syncwarp();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (kernel_ms && e == cudaSuccess) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        *kernel_ms = ms;
     }
-    // ---- SPE: d/dpspe_h(ip) and d/dnspe_h(in) of sum psi^2 (pspe + nspe)
-    if (g.dspe_p) {
-        for (int c = a.spe_ptr[slot]; c < a.spe_ptr[slot + 1]; ++c) {
-            const SPEContrib sc = a.spe[c];
-            double s = 0.0;
-#pragma unroll
-            for (int i = 0; i < ITEMS; ++i) {
-                if (valid[i] && pos[i] >= sc.lo && pos[i] <= sc.hi) {
-                    const double p2 = pout[i] * pout[i];
-                    s += p2;
-                    atomicAdd(g.dspe_n + sc.n0 + (pos[i] - sc.lo), p2);
-                }
-            }
-            s = warp_sum(s);
-            if (lane == 0 && s != 0.0) atomicAdd(g.dspe_p + row, s);
-        }
-    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cleanup();
+    if (e != cudaSuccess) return fail(e == cudaErrorMemoryAllocation ? BSG_ERR_NOMEM : BSG_ERR_CUDA,
+                                      std::string("adjoint: ") + cudaGetErrorString(e));
+    return BSG_OK;
 }
 
 }  // namespace bsg
@@ -136,64 +190,15 @@ extern "C" int bsg_grad(bsg_ctx *ctx, const double *evecs, int nstates, double *
     if (!ctx) return BSG_ERR_ARG;
     if (!evecs || nstates < 1 || !dpp || !dnn || !dpn)
         return set_err(ctx, BSG_ERR_ARG, "bsg_grad: null argument or nstates < 1");
-    const bool spe = ctx->t.call_spe && dspe_p && dspe_n;
     int st = cuda_check(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
     if (st) return st;
-    const int64_t n = ctx->dim;
-    const size_t npp = (size_t)ctx->t.nmatpp, nnn = (size_t)ctx->t.nmatnn, npn = (size_t)ctx->t.nmatpn;
-    const size_t nsp = (size_t)ctx->t.nsd_p, nsn = (size_t)ctx->t.nsd_n;
-    DevBuf psi, gpp, gnn, gpn, gsp, gsn;
-    constexpr int ITEMS = 4;
-    ctx->last_status = BSG_OK;
-    const TileSet *ts = get_tiles(ctx, 32 * ITEMS);
-    if (!ts) return ctx->last_status ? ctx->last_status : BSG_ERR_NOMEM;
-    if ((st = dev_alloc(ctx, psi, sizeof(double) * n)) || (st = dev_alloc(ctx, gpp, sizeof(double) * npp)) ||
-        (st = dev_alloc(ctx, gnn, sizeof(double) * nnn)) || (st = dev_alloc(ctx, gpn, sizeof(double) * npn)) ||
-        (st = dev_alloc(ctx, gsp, sizeof(double) * nsp)) || (st = dev_alloc(ctx, gsn, sizeof(double) * nsn))) {
-        dev_free(psi); dev_free(gpp); dev_free(gnn); dev_free(gpn); dev_free(gsp); dev_free(gsn);
-        return st;
-    }
-    RowArgs a = ctx->args;
-    a.tiles = (const Tile *)ts->buf.p;
-    a.ntiles = ts->ntiles;
-    GradArgs g;
-    g.pp_op = (const int32_t *)ctx->pp_op.p;
-    g.pp_ph = (const int8_t *)ctx->pp_ph.p;
-    g.nnrec_op = (const int32_t *)ctx->nnrec_op.p;
-    g.nnrec_ph = (const int8_t *)ctx->nnrec_ph.p;
-    g.dpp = (double *)gpp.p;
-    g.dnn = (double *)gnn.p;
-    g.dpn = (double *)gpn.p;
-    g.dspe_p = spe ? (double *)gsp.p : nullptr;
-    g.dspe_n = spe ? (double *)gsn.p : nullptr;
-    const int mstride = (a.max_nbd + 1) & ~1;
-    // 8 per-warp FP64 tables within the 227 KB of shared memory per CTA
-    if (a.max_nbd > 3392) {
-        dev_free(psi); dev_free(gpp); dev_free(gnn); dev_free(gpn); dev_free(gsp); dev_free(gsn);
-        return set_err(ctx, BSG_ERR_UNSUPPORTED, "bsg_grad: a neutron sector jump has more than 3392 distinct (b,d) pairs");
-    }
-    const size_t smem = sizeof(double) * (size_t)kGradWarps * (mstride > 0 ? mstride : 2);
-    cudaStream_t s = ctx->stream;
-    cudaError_t e = cudaFuncSetAttribute(k_grad<ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    for (int k = 0; k < nstates && e == cudaSuccess; ++k) {
-        e = cudaMemcpyAsync(psi.p, evecs + (size_t)k * n, sizeof(double) * n, cudaMemcpyHostToDevice, s);
-        if (e == cudaSuccess) e = cudaMemsetAsync(gpp.p, 0, gpp.bytes, s);
-        if (e == cudaSuccess) e = cudaMemsetAsync(gnn.p, 0, gnn.bytes, s);
-        if (e == cudaSuccess) e = cudaMemsetAsync(gpn.p, 0, gpn.bytes, s);
-        if (e == cudaSuccess) e = cudaMemsetAsync(gsp.p, 0, gsp.bytes, s);
-        if (e == cudaSuccess) e = cudaMemsetAsync(gsn.p, 0, gsn.bytes, s);
-        if (e == cudaSuccess && ts->ntiles > 0) {
-            k_grad<ITEMS><<<ts->ntiles, kGradWarps * 32, smem, s>>>(a, g, (const double *)psi.p, mstride);
-            e = cudaGetLastError();
-        }
-        if (e == cudaSuccess && npp) e = cudaMemcpyAsync(dpp + k * npp, gpp.p, sizeof(double) * npp, cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess && nnn) e = cudaMemcpyAsync(dnn + k * nnn, gnn.p, sizeof(double) * nnn, cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess && npn) e = cudaMemcpyAsync(dpn + k * npn, gpn.p, sizeof(double) * npn, cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess && spe) e = cudaMemcpyAsync(dspe_p + k * nsp, gsp.p, sizeof(double) * nsp, cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess && spe) e = cudaMemcpyAsync(dspe_n + k * nsn, gsn.p, sizeof(double) * nsn, cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    }
-    st = cuda_check(ctx, e, "bsg_grad");
-    dev_free(psi); dev_free(gpp); dev_free(gnn); dev_free(gpn); dev_free(gsp); dev_free(gsn);
-    return st;
+    bsg_ctx *cs[1] = {ctx};
+    const double *ev[1] = {evecs};
+    double *p[1] = {dpp}, *nn[1] = {dnn}, *pn[1] = {dpn}, *sp[1] = {dspe_p}, *sn[1] = {dspe_n};
+    std::string err;
+    double ms = 0.0;
+    st = grad_many(cs, 1, ev, nstates, p, nn, pn, sp, sn, ctx->stream, err, &ms);
+    if (st) return set_err(ctx, st, "bsg_grad: " + err);
+    ctx->stats.grad_ms = ms;
+    return BSG_OK;
 }

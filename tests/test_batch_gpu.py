@@ -100,3 +100,21 @@ def test_batch_member_gradients_vs_fd():
                 em = np.linalg.eigvalsh(dense_h.dense_h(m.orbits, m.np_, m.nn, m.jz2, m.spe, [tuple(x) for x in tm])[0])[k]
                 assert abs((ep - em) / (2 * h) - gtb[i]) < 1e-5, (s, k, i)
     b.close()
+
+
+def test_batch_random_pivot_mixed_against_fp64(batch):
+    """From a seeded random pivot per system (no symmetry of the uniform
+    pivot restricting the Krylov space), the mixed batch (FP32 applyH) and
+    the FP64 batch give the same lowest 5 eigenvalues to 1e-6 relative and
+    eigenvector overlaps above 1 - 1e-5, system by system; the random pivot
+    is a pure function of (seed, system), so two runs are bitwise equal."""
+    tabs, b = batch
+    ev8, v8, _ = b.lanczos(nkeep=5, niter=150, matvec_prec=8, want_vectors=True, pivot="random", seed=77)
+    ev4, v4, _ = b.lanczos(nkeep=5, niter=150, matvec_prec=4, want_vectors=True, pivot="random", seed=77)
+    ev8b, _, _ = b.lanczos(nkeep=5, niter=150, matvec_prec=8, pivot="random", seed=77)
+    assert np.array_equal(ev8, ev8b)
+    for s in range(len(tabs)):
+        rel = np.abs(ev4[s] - ev8[s]) / np.abs(ev8[s])
+        assert rel.max() < 1e-6, (s, rel)
+        ov = np.abs(np.sum(v4[s] * v8[s], axis=0))
+        assert ov.min() > 1 - 1e-5, (s, ov)

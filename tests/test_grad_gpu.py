@@ -118,3 +118,44 @@ def test_euler_identity_sd6p6n():
     # float32 rounding of the uncoupled matrix elements bounds the agreement
     assert abs(e - ev[0]) < 1e-5 * abs(ev[0]), (e, ev[0])
     H.close()
+
+
+def test_grad_bitwise_repeatable():
+    """Every label's sum is exact 128-bit fixed point: two calls agree bit for
+    bit, and one state's gradient does not depend on the other states of the
+    call (the work split differs)."""
+    T = model.build_tables(model.sd_model(3, 3, seed=6))
+    rng = np.random.default_rng(1)
+    V = rng.standard_normal((T.dim, 3))
+    V /= np.linalg.norm(V, axis=0)
+    H = _H(T)
+    g1, g2 = H.grad(V), H.grad(V)
+    g0 = H.grad(V[:, :1])
+    H.close()
+    for key in ("pp", "nn", "pn"):
+        assert np.array_equal(g1[key], g2[key]), key
+        assert np.array_equal(g1[key][:1], g0[key]), key
+
+
+def test_batch_grad_one_launch_equals_per_system():
+    """bsg_batch_grad: all systems and states in one launch, bitwise equal to
+    each member's own bsg_grad, and equal to the oracle's density traversal."""
+    from bigstickpublick_b200.engine import Batch
+    tabs = [model.build_tables(model.batch_member(s)) for s in (1000, 1003, 1006)]
+    b = Batch(tabs)
+    rng = np.random.default_rng(2)
+    vecs = []
+    for t in tabs:
+        V = rng.standard_normal((t.dim, 2))
+        vecs.append(V / np.linalg.norm(V, axis=0))
+    gb = b.grad(vecs)
+    assert b.grad_ms > 0
+    for s, t in enumerate(tabs):
+        gs = b.system(s).grad(vecs[s])
+        for key in ("pp", "nn", "pn"):
+            assert np.array_equal(gb[s][key], gs[key]), (s, key)
+        ref = oracle.density(t, vecs[s][:, 1])
+        for key in ("pp", "nn", "pn"):
+            scale = max(1e-30, np.abs(ref[key]).max())
+            assert np.abs(gb[s][key][1] - ref[key]).max() / scale < 1e-10, (s, key)
+    b.close()
