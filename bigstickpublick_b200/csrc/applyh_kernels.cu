@@ -22,14 +22,14 @@
 
 namespace bsg {
 
-template <typename T, int NB, int ITEMS, bool FULL, int OUT>
+template <typename T, int NB, int ITEMS, bool FULL, int OUT, bool REC32 = false>
 __device__ __forceinline__ void rows_body(const RowArgs &a, const T *__restrict__ vin, T *__restrict__ vout,
                                           const int ld, const int v0, const int mstride) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int warp = threadIdx.x >> 5;
     float *__restrict__ Mw = reinterpret_cast<float *>(smem) + (size_t)warp * mstride;
     T *__restrict__ part = reinterpret_cast<T *>(smem + align16(sizeof(float) * (size_t)kWarps * mstride));
-    row_tile<T, NB, ITEMS, FULL, OUT>(a, a.tiles[blockIdx.x], vin, vout, ld, v0, Mw, part);
+    row_tile<T, NB, ITEMS, FULL, OUT, REC32>(a, a.tiles[blockIdx.x], vin, vout, ld, v0, Mw, part);
 }
 
 // OUT: store, accumulate, or FP64 columns (RowOut in applyh_tile.cuh)
@@ -44,26 +44,27 @@ __global__ void __launch_bounds__(kWarps * 32) k_rows(const RowArgs a, const T *
 // resident per SM to hide the gather latency (measured faster than the
 // compiler's own choice of 48 registers, the small spills included).  FP32
 // tiles of 256 positions (long rows) go further, to 32 registers and 8 CTAs:
-// pf 4p4n 1.80 -> 1.61 ms, while short rows lose more to the spills
-template <int ITEMS, bool FULL, int OUT>
+// pf 4p4n 1.80 -> 1.61 ms, while short rows lose more to the spills.
+// REC32: the 32-bit sliced records (half the record bytes of the L1 stream)
+template <int ITEMS, bool FULL, int OUT, bool REC32>
 __global__ void __launch_bounds__(kWarps * 32, ITEMS >= 8 ? 8 : 6) k_rows_f1(const RowArgs a, const float *__restrict__ vin,
                                                             float *__restrict__ vout, const int ld, const int v0,
                                                             const int mstride) {
-    rows_body<float, 1, ITEMS, FULL, OUT>(a, vin, vout, ld, v0, mstride);
+    rows_body<float, 1, ITEMS, FULL, OUT, REC32>(a, vin, vout, ld, v0, mstride);
 }
-template <int ITEMS, bool FULL, int OUT>
+template <int ITEMS, bool FULL, int OUT, bool REC32>
 __global__ void __launch_bounds__(kWarps * 32, 6) k_rows_d1(const RowArgs a, const double *__restrict__ vin,
                                                             double *__restrict__ vout, const int ld, const int v0,
                                                             const int mstride) {
-    rows_body<double, 1, ITEMS, FULL, OUT>(a, vin, vout, ld, v0, mstride);
+    rows_body<double, 1, ITEMS, FULL, OUT, REC32>(a, vin, vout, ld, v0, mstride);
 }
 
-template <typename T, int NB, int ITEMS, bool FULL, int OUT>
+template <typename T, int NB, int ITEMS, bool FULL, int OUT, bool REC32>
 constexpr auto rows_kernel() {
     if constexpr (std::is_same<T, float>::value && NB == 1)
-        return k_rows_f1<ITEMS, FULL, OUT>;
+        return k_rows_f1<ITEMS, FULL, OUT, REC32>;
     else if constexpr (std::is_same<T, double>::value && NB == 1)
-        return k_rows_d1<ITEMS, FULL, OUT>;
+        return k_rows_d1<ITEMS, FULL, OUT, REC32>;
     else
         return k_rows<T, NB, ITEMS, FULL, OUT>;
 }
@@ -101,13 +102,20 @@ static int launch_one(bsg_ctx *ctx, const T *vin, T *vout, int ld, int v0, int a
         if (r == cudaSuccess) k<<<ts->ntiles, kWarps * 32, smem, s>>>(a, vin, vout, ld, v0, mstride);
         return r;
     };
-    if (cols)
-        e = go(rows_kernel<T, NB, ITEMS, true, kColumns>());
-    else if (full)
-        e = accumulate ? go(rows_kernel<T, NB, ITEMS, true, kAccumulate>()) : go(rows_kernel<T, NB, ITEMS, true, kStore>());
+    // single vectors walk the 32-bit records when the context has them
+    auto pick = [&](auto rec32) -> cudaError_t {
+        constexpr bool R = decltype(rec32)::value && NB == 1;
+        if (cols) return go(rows_kernel<T, NB, ITEMS, true, kColumns, R>());
+        if (full)
+            return accumulate ? go(rows_kernel<T, NB, ITEMS, true, kAccumulate, R>())
+                              : go(rows_kernel<T, NB, ITEMS, true, kStore, R>());
+        return accumulate ? go(rows_kernel<T, NB, ITEMS, false, kAccumulate, R>())
+                          : go(rows_kernel<T, NB, ITEMS, false, kStore, R>());
+    };
+    if (NB == 1 && a.sell32)
+        e = pick(std::true_type{});
     else
-        e = accumulate ? go(rows_kernel<T, NB, ITEMS, false, kAccumulate>())
-                       : go(rows_kernel<T, NB, ITEMS, false, kStore>());
+        e = pick(std::false_type{});
     if (e != cudaSuccess) return cuda_check(ctx, e, "applyh smem attribute");
     return cuda_check(ctx, cudaGetLastError(), "applyh kernel launch");
 }

@@ -103,7 +103,9 @@ __host__ __device__ constexpr size_t align16(size_t x) { return (x + 15) & ~size
 // registers.
 enum RowOut { kStore = 0, kAccumulate = 1, kColumns = 2 };
 
-template <typename T, int NB, int ITEMS, bool FULL, int OUT = kStore>
+// REC32: walk the 32-bit sliced records (RowArgs::sell32) instead of the
+// 8-byte ones; the decoded values, and so the sums, are the same bit for bit.
+template <typename T, int NB, int ITEMS, bool FULL, int OUT = kStore, bool REC32 = false>
 __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, const T *__restrict__ vin,
                                          T *__restrict__ vout, const int ld_, const int v0_,
                                          float *__restrict__ Mw, T *__restrict__ part) {
@@ -158,6 +160,35 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
             for (int i = 0; i < ITEMS; ++i) {
                 if (!valid[i] || pos[i] >= op.nout) continue;
                 const int k0 = __ldg(ptr + pos[i]), k1 = __ldg(ptr + pos[i] + 1);
+                if constexpr (REC32) {
+                    // input position | hmatnn label - 1 | phase sign
+                    const uint32_t *c32 =
+                        a.sell32 + op.sell_base + __ldg(a.slice_off + op.slice_base + (pos[i] >> 5)) + lane;
+                    const int n = k1 - k0;
+                    int k = 0;
+                    for (; k + 1 < n; k += 2) {
+                        const uint32_t r0 = __ldg(c32 + 32 * k), r1 = __ldg(c32 + 32 * (k + 1));
+                        T x0[NB], x1[NB];
+                        Vec<T, NB, FULL>::load(src + (size_t)(r0 & 0xffffu) * ld, x0);
+                        Vec<T, NB, FULL>::load(src + (size_t)(r1 & 0xffffu) * ld, x1);
+                        const T m0 = (T)__int_as_float(__float_as_int(__ldg(a.hmatnn + ((r0 >> 16) & 0x7fffu))) ^
+                                                       (int)(r0 & 0x80000000u));
+                        const T m1 = (T)__int_as_float(__float_as_int(__ldg(a.hmatnn + ((r1 >> 16) & 0x7fffu))) ^
+                                                       (int)(r1 & 0x80000000u));
+#pragma unroll
+                        for (int v = 0; v < NB; ++v) { acc[i][v] += m0 * x0[v]; acc[i][v] += m1 * x1[v]; }
+                    }
+                    if (k < n) {
+                        const uint32_t r0 = __ldg(c32 + 32 * k);
+                        T x0[NB];
+                        Vec<T, NB, FULL>::load(src + (size_t)(r0 & 0xffffu) * ld, x0);
+                        const T m0 = (T)__int_as_float(__float_as_int(__ldg(a.hmatnn + ((r0 >> 16) & 0x7fffu))) ^
+                                                       (int)(r0 & 0x80000000u));
+#pragma unroll
+                        for (int v = 0; v < NB; ++v) acc[i][v] += m0 * x0[v];
+                    }
+                    continue;
+                }
                 const int2 *col;
                 int k, n;
                 record_column<T, NB>(a, op, rec, k0, k1, pos[i], lane, col, k, n);
@@ -206,6 +237,32 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
             for (int i = 0; i < ITEMS; ++i) {
                 if (!valid[i] || pos[i] >= op.nout) continue;
                 const int k0 = __ldg(ptr + pos[i]), k1 = __ldg(ptr + pos[i] + 1);
+                if constexpr (REC32) {
+                    // input position | (b,d) index | neutron phase sign
+                    const uint32_t *c32 =
+                        a.sell32 + op.sell_base + __ldg(a.slice_off + op.slice_base + (pos[i] >> 5)) + lane;
+                    const int n = k1 - k0;
+                    int k = 0;
+                    for (; k + 1 < n; k += 2) {
+                        const uint32_t r0 = __ldg(c32 + 32 * k), r1 = __ldg(c32 + 32 * (k + 1));
+                        T x0[NB], x1[NB];
+                        Vec<T, NB, FULL>::load(src + (size_t)(r0 & 0xffffu) * ld, x0);
+                        Vec<T, NB, FULL>::load(src + (size_t)(r1 & 0xffffu) * ld, x1);
+                        const T m0 = (T)__int_as_float(__float_as_int(Mw[(r0 >> 16) & 0x7fffu]) ^ (int)(r0 & 0x80000000u));
+                        const T m1 = (T)__int_as_float(__float_as_int(Mw[(r1 >> 16) & 0x7fffu]) ^ (int)(r1 & 0x80000000u));
+#pragma unroll
+                        for (int v = 0; v < NB; ++v) { acc[i][v] += m0 * x0[v]; acc[i][v] += m1 * x1[v]; }
+                    }
+                    if (k < n) {
+                        const uint32_t r0 = __ldg(c32 + 32 * k);
+                        T x0[NB];
+                        Vec<T, NB, FULL>::load(src + (size_t)(r0 & 0xffffu) * ld, x0);
+                        const T m0 = (T)__int_as_float(__float_as_int(Mw[(r0 >> 16) & 0x7fffu]) ^ (int)(r0 & 0x80000000u));
+#pragma unroll
+                        for (int v = 0; v < NB; ++v) acc[i][v] += m0 * x0[v];
+                    }
+                    continue;
+                }
                 const int2 *col;
                 int k, n;
                 record_column<T, NB>(a, op, rec, k0, k1, pos[i], lane, col, k, n);

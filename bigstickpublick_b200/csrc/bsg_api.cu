@@ -457,6 +457,11 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
     // of lane l at row k (padding rows hold {0, 0} and are never read)
     std::vector<int2> sell_all;
     std::vector<int32_t> slice_off_all;
+    // 32-bit copy when every input position, (b,d) index and hmatnn label fits
+    int32_t max_nbd_all = 0;
+    for (const NOp &op : nops) max_nbd_all = std::max(max_nbd_all, op.nbd);
+    const bool pack32 = ctx->max_rowlen <= 65536 && t->nmatnn <= 32768 && max_nbd_all <= 32768;
+    std::vector<uint32_t> sell32_all;
     for (NOp &op : nops) {
         op.sell_base = (int64_t)sell_all.size();
         op.slice_base = (int64_t)slice_off_all.size();
@@ -471,14 +476,24 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
             slice_off_all.push_back((int32_t)off);
             const size_t row0 = sell_all.size();
             sell_all.resize(row0 + (size_t)32 * width, make_int2(0, 0));
+            if (pack32) sell32_all.resize(row0 + (size_t)32 * width, 0u);
             for (int l = 0; l < 32 && 32 * sl + l < op.nout; ++l)
                 for (int32_t k = ptr[32 * sl + l]; k < ptr[32 * sl + l + 1]; ++k) {
                     int2 r;
-                    if (op.kind == 1)
-                        std::memcpy(&r, &pnrec_all[op.rec_base + k], sizeof(int2));
-                    else
+                    uint32_t r32;
+                    if (op.kind == 1) {
+                        const PNRec &pr = pnrec_all[op.rec_base + k];
+                        std::memcpy(&r, &pr, sizeof(int2));
+                        r32 = (uint32_t)pr.in | ((uint32_t)pr.k << 16) | (pr.ph < 0 ? 0x80000000u : 0u);
+                    } else {
                         std::memcpy(&r, &nnrec_all[op.rec_base + k], sizeof(int2));
-                    sell_all[row0 + (size_t)32 * (k - ptr[32 * sl + l]) + l] = r;
+                        r32 = (uint32_t)nnrec_all[op.rec_base + k].in |
+                              ((uint32_t)(nnrec_op_all[op.rec_base + k] - 1) << 16) |
+                              (nnrec_ph_all[op.rec_base + k] < 0 ? 0x80000000u : 0u);
+                    }
+                    const size_t at = row0 + (size_t)32 * (k - ptr[32 * sl + l]) + l;
+                    sell_all[at] = r;
+                    if (pack32) sell32_all[at] = r32;
                 }
             off += (int64_t)32 * width;
         }
@@ -621,6 +636,7 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
         (st = up(ctx->pnrec, pnrec_all.data(), sizeof(PNRec) * pnrec_all.size())) ||
         (st = up(ctx->nnrec, nnrec_all.data(), sizeof(NNRec) * nnrec_all.size())) ||
         (st = up(ctx->sell, sell_all.data(), sizeof(int2) * sell_all.size())) ||
+        (pack32 && (st = up(ctx->sell32, sell32_all.data(), 4 * sell32_all.size()))) ||
         (st = up(ctx->slice_off, slice_off_all.data(), 4 * slice_off_all.size())) ||
         (st = up(ctx->bd, bd_all.data(), sizeof(BDPair) * bd_all.size())) ||
         (st = up(ctx->cpn, cpn32.data(), 4 * cpn32.size())) || (st = up(ctx->dpn, dpn32.data(), 4 * dpn32.size())) ||
@@ -637,7 +653,8 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
                                          sizeof(PNContrib) * ctx->h_pn.size() + sizeof(SPEContrib) * h_spe.size() +
                                          sizeof(NOp) * nops.size() + 4 * nptr_all.size() +
                                          sizeof(PNRec) * pnrec_all.size() + sizeof(NNRec) * nnrec_all.size() +
-                                         sizeof(int2) * sell_all.size() + 4 * slice_off_all.size());
+                                         sizeof(int2) * sell_all.size() + 4 * sell32_all.size() +
+                                         4 * slice_off_all.size());
     ctx->stats.n_rows = nrows;
     ctx->stats.n_contrib = (int64_t)(ctx->h_pp.size() + ctx->h_nn.size() + ctx->h_pn.size() + h_spe.size());
 
@@ -656,6 +673,8 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
     a.pnrec = (const PNRec *)ctx->pnrec.p;
     a.nnrec = (const NNRec *)ctx->nnrec.p;
     a.sell = (const int2 *)ctx->sell.p;
+    a.sell32 = pack32 ? (const uint32_t *)ctx->sell32.p : nullptr;
+    a.hmatnn = (const float *)ctx->hmatnn_d.p;
     a.slice_off = (const int32_t *)ctx->slice_off.p;
     a.bd = (const BDPair *)ctx->bd.p;
     int32_t max_nbd = 0;
@@ -679,7 +698,7 @@ void free_ctx(bsg_ctx *ctx) {
     for (auto &b : ctx->raw) dev_free(b);
     DevBuf *bufs[] = {&ctx->row_off, &ctx->pp_ptr, &ctx->nn_ptr, &ctx->pn_ptr, &ctx->spe_ptr, &ctx->pp, &ctx->nn,
                       &ctx->pn, &ctx->spe, &ctx->nops, &ctx->nptr, &ctx->pnrec, &ctx->nnrec, &ctx->bd, &ctx->sell,
-                      &ctx->slice_off, &ctx->hmatpn,
+                      &ctx->sell32, &ctx->slice_off, &ctx->hmatpn,
                       &ctx->cpn, &ctx->dpn, &ctx->nspe, &ctx->pp_op, &ctx->nnrec_op, &ctx->nnrec_ph, &ctx->pp_ph,
                       &ctx->hmatpp_d,
                       &ctx->hmatnn_d, &ctx->scratch_in, &ctx->scratch_out};
