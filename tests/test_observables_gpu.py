@@ -67,3 +67,32 @@ def test_mg25_overlap_of_ref_ground_state_with_alt_states():
         tol = 1e-3 if g["n"] in (7, 8) else 5e-5
         assert abs(ov[f] ** 2 - g["overlap2"]) < tol, (g["n"], ov[f] ** 2, g["overlap2"])
         assert abs(abs(ov[f]) - abs(g["overlap"])) < max(tol, 5e-5)
+
+
+def test_mg25_states_written_to_wfn(tmp_path):
+    """lanczos_output's .wfn file for the mg25ref states: energies, J and
+    T(T+1) in each record, amplitudes in FP32 (the reference's lanc_prec);
+    the stored ground state gives back its energy through the engine's FP64
+    applyH to FP32-storage accuracy."""
+    from bigstickpublick_b200 import wfn
+    from bigstickpublick_b200.engine import Hamiltonian, angular_momentum_isospin
+    r = GOLD["runs"]["mg25ref"]
+    ss, ts = model.ModelSpec.scaling(*r["scaling"])
+    orbits = [tuple(o) for o in GOLD["orbits"]]
+    spec = model.ModelSpec(orbits, r["np"], r["nn"], r["jz2"], 1, GOLD["spe"], [tuple(t) for t in GOLD["tbme"]], ss, ts)
+    T = model.build_tables(spec)
+    H = Hamiltonian(T)
+    ev, vecs, rep = H.lanczos(nkeep=10, niter=400, matvec_prec=8, want_vectors=True, converge_tol=1e-12)
+    J, Tq = angular_momentum_isospin(spec, vecs)
+    p = tmp_path / "mg25ref.wfn"
+    wfn.write_wfn(p, spec, ev, vecs, J, Tq * (Tq + 1))
+    h, states = wfn.read_wfn(p)
+    assert h["dim"] == T.dim == 44133 and h["nkeep"] == 10 and (h["np"], h["nn"], h["jz2"]) == (4, 5, 1)
+    for s, g in zip(states, r["states"]):
+        assert abs(s["e"] - g["E"]) < 2e-5
+        assert abs(s["xj"] - g["J"]) < 1e-3
+        assert abs(s["xt2"] - g["T"] * (g["T"] + 1)) < 1e-2
+    v = states[0]["vec"].astype(np.float64)
+    e0 = float(v @ H.applyh(v)) / float(v @ v)
+    H.close()
+    assert abs(e0 - r["states"][0]["E"]) < 1e-4
