@@ -279,30 +279,37 @@ def _solve(H, **kw):
     return ev, vecs, info
 
 
+MIXED = dict(matvec_prec=4, lanc_prec=4)   # FP32 applyH, FP32-stored Lanczos vectors, FP64 sums
+FP64 = dict(matvec_prec=8, lanc_prec=8)
+
+
 def lanczos_sd6p6n_leg(args):
     """sd 6p6n, lowest 10 states, 300 iterations (fixed) from one seeded
-    pivot: FP64 applyH against mixed (FP32 applyH, FP64 Lanczos); the mixed
-    run's eigenvalue and wavefunction-overlap error against FP64, and the
-    iterations per second of each."""
+    pivot: the FP64 path against mixed precision (FP32 applyH, Lanczos
+    vectors stored in FP32 as the reference's lanc_prec = 4 stores them,
+    every dot product, alpha, beta and the projected eigenproblem in FP64);
+    the mixed run's eigenvalue and wavefunction-overlap error against FP64,
+    and the iterations per second of each."""
     from bigstickpublick_b200.engine import Hamiltonian
     T = make_tables("sd6p6n")
     H = Hamiltonian(T)
     try:
         piv = np.random.default_rng(11).standard_normal(T.dim)
-        for prec in (8, 4):  # untimed: the first use of a kernel loads its code
-            H.lanczos(nkeep=2, niter=6, matvec_prec=prec, fixed_iter=True, pivot=piv)
+        for prec in (FP64, MIXED):  # untimed: the first use of a kernel loads its code
+            H.lanczos(nkeep=2, niter=6, fixed_iter=True, pivot=piv, **prec)
         out = {}
         res = {}
-        for name, prec in (("fp64", 8), ("mixed", 4)):
-            ev, vecs, info = _solve(H, nkeep=10, niter=args.lanczos_iters, matvec_prec=prec, fixed_iter=True,
-                                    pivot=piv, want_vectors=True)
+        for name, prec in (("fp64", FP64), ("mixed", MIXED)):
+            ev, vecs, info = _solve(H, nkeep=10, niter=args.lanczos_iters, fixed_iter=True, pivot=piv,
+                                    want_vectors=True, **prec)
             res[name] = (ev, vecs)
             info["lowest"] = [float(x) for x in ev[:3]]
             out[name] = info
         out["mixed"].update(compare_states(*res["mixed"], *res["fp64"]))
         out["speedup_its_per_s"] = out["mixed"]["its_per_s"] / out["fp64"]["its_per_s"]
         out["config"] = (f"sd 6p6n, {args.lanczos_iters} iterations (fixed), lowest 10, seeded generic pivot; "
-                         "errors of mixed against FP64 from the same pivot")
+                         "mixed = FP32 applyH + FP32-stored Lanczos vectors with FP64 sums; errors of mixed "
+                         "against FP64 from the same pivot")
         return out
     finally:
         H.close()
@@ -324,16 +331,16 @@ def time_to_solution_leg(args):
         pivb = rng.standard_normal((T.dim, 8))
         pivb[:, 0] = piv
         pivb = pivb.reshape(-1)
-        for prec in (8, 4):
-            H.lanczos(nkeep=2, niter=6, matvec_prec=prec, fixed_iter=True, pivot=piv)
-        H.lanczos(nkeep=2, niter=3, nb=8, matvec_prec=4, fixed_iter=True, pivot=pivb)
+        for prec in (FP64, MIXED):
+            H.lanczos(nkeep=2, niter=6, fixed_iter=True, pivot=piv, **prec)
+        H.lanczos(nkeep=2, niter=3, nb=8, fixed_iter=True, pivot=pivb, **MIXED)
         scal = dict(nkeep=10, niter=args.tts_niter, nthick_add=10, max_restarts=200)
-        ev_ref, v_ref, info_ref = _solve(H, matvec_prec=8, converge_tol=1e-9, pivot=piv, want_vectors=True, **scal)
+        ev_ref, v_ref, info_ref = _solve(H, converge_tol=1e-9, pivot=piv, want_vectors=True, **FP64, **scal)
         out = {"reference": dict(info_ref, converge_tol=1e-9, lowest=[float(x) for x in ev_ref[:3]])}
-        runs = [("fp64", dict(matvec_prec=8, pivot=piv, **scal)),
-                ("mixed", dict(matvec_prec=4, pivot=piv, **scal)),
+        runs = [("fp64", dict(pivot=piv, **FP64, **scal)),
+                ("mixed", dict(pivot=piv, **MIXED, **scal)),
                 ("block8_mixed", dict(nkeep=10, niter=args.tts_block_niter, nb=8, nthick_add=10, max_restarts=200,
-                                      matvec_prec=4, pivot=pivb))]
+                                      pivot=pivb, **MIXED))]
         for name, kw in runs:
             ev, vecs, info = _solve(H, converge_tol=args.tts_tol, want_vectors=True, **kw)
             info.update(compare_states(ev, vecs, ev_ref, v_ref))
@@ -396,10 +403,11 @@ def density_leg(H, tables, k=10, reps=5):
 def batch_leg(args):
     """Config 4: 256 sd-shell Hamiltonians (seeds 1000..1255, valence Z and N
     uniform in 2..8), one persistent launch per batched matvec, lock-step
-    Lanczos with one captured graph per iteration (FP64 applyH, and mixed:
-    FP32 applyH, with its eigenvalue and overlap error against FP64 over all
-    systems), then the adjoint gradient of the lowest 5 eigenvalues of every
-    system with respect to its 63 TBMEs and 3 SPEs."""
+    Lanczos with one captured graph per iteration from a seeded random pivot
+    per system (FP64 applyH, and mixed: FP32 applyH, with its eigenvalue and
+    overlap error against FP64 over all systems), then the adjoint gradient
+    of the lowest 5 eigenvalues of every system with respect to its 63 TBMEs
+    and 3 SPEs."""
     import torch
     from bigstickpublick_b200 import model
     from bigstickpublick_b200.engine import Batch
@@ -427,15 +435,19 @@ def batch_leg(args):
         res = {}
         for name, prec in (("fp64", 8), ("mixed", 4)):
             t0 = time.perf_counter()
-            ev, vecs, rep = b.lanczos(nkeep=5, niter=args.batch_iters, matvec_prec=prec, want_vectors=True)
+            ev, vecs, rep = b.lanczos(nkeep=5, niter=args.batch_iters, matvec_prec=prec, want_vectors=True,
+                                      pivot="random", seed=77)
             res[name] = (ev, vecs, rep, time.perf_counter() - t0)
         ev64, v64 = res["fp64"][0], res["fp64"][1]
         evm, vm = res["mixed"][0], res["mixed"][1]
         rel = np.abs(evm - ev64) / np.abs(ev64)
         ovl = np.array([[abs(float(vm[s][:, j] @ v64[s][:, j])) for j in range(5)] for s in range(len(tabs))])
+        b.grad([v[:, :1] for v in v64[:2]] + [v[:, :1] for v in v64[2:]])  # untimed: loads the kernels
         t0 = time.perf_counter()
-        for s, t in enumerate(tabs):
-            g = b.system(s).grad(v64[s])
+        gb = b.grad(v64)  # all systems and states: one launch
+        t_grad_dev = time.perf_counter() - t0
+        grad_kernel_ms = b.grad_ms
+        for t, g in zip(tabs, gb):
             [model.chain_rule(t, {k: v[i] for k, v in g.items()}) for i in range(5)]
         t_grad = time.perf_counter() - t0
         return {"systems": len(tabs), "dims_min": min(dims), "dims_max": max(dims), "dims_sum": int(sum(dims)),
@@ -447,7 +459,8 @@ def batch_leg(args):
                 "mixed": {"graph_ms": res["mixed"][2]["t_matvec_ms"], "eig_ms": res["mixed"][2]["t_eig_ms"],
                           "wall_s": res["mixed"][3], "max_rel_eig_err": float(rel.max()),
                           "min_overlap": float(ovl.min())},
-                "grad_s_all_systems_5_states": t_grad,
+                "grad_s_all_systems_5_states": t_grad, "grad_call_s": t_grad_dev,
+                "grad_kernel_ms": grad_kernel_ms, "grad_launches": 2,
                 "ground_states_first4": [float(x) for x in ev64[:4, 0]]}
     finally:
         b.close()
@@ -455,8 +468,8 @@ def batch_leg(args):
 
 def large_leg(H, T, args):
     """Config 5 (the headline workload): thick-restart Lanczos for the lowest
-    5 states, keep 20, mixed (FP32 applyH, FP64 history and
-    reorthogonalization) and FP64 on the same fixed schedule from the same
+    5 states, keep 20, mixed (FP32 applyH, FP32-stored Lanczos vectors, FP64
+    sums) and FP64 on the same fixed schedule from the same
     seeded pivot, so that their difference is the precision alone; each
     state's FP64 residual |H psi - E psi| / |E|; the adjoint gradient of the
     ground state w.r.t. all 195 TBMEs and 4 SPEs with the Euler identity
@@ -467,8 +480,8 @@ def large_leg(H, T, args):
     kw = dict(nkeep=5, niter=args.large_iters, nthick_add=15, max_restarts=args.large_restarts, fixed_iter=True,
               pivot=piv, want_vectors=True)
     res, out = {}, {}
-    for name, prec in (("mixed", 4), ("fp64", 8)):
-        ev, vecs, info = _solve(H, matvec_prec=prec, **kw)
+    for name, prec in (("mixed", MIXED), ("fp64", FP64)):
+        ev, vecs, info = _solve(H, **prec, **kw)
         # FP64 residuals of the returned Ritz pairs
         r = []
         for j in range(len(ev)):
