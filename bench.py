@@ -315,43 +315,70 @@ def lanczos_sd6p6n_leg(args):
         H.close()
 
 
+TTS_TOLS = (1e-2, 3e-3, 1e-3, 3e-4, 1e-4, 1e-5)
+
+
 def time_to_solution_leg(args):
     """pf 4p4n, lowest 10 states to a relative eigenvalue error of 1e-6:
-    FP64 scalar Lanczos (the plain FP64 GPU path), mixed scalar and mixed
-    block (nb = 8), each with thick restart and the reference's convergence
-    test at the same tolerance, timed on the solver's device clock.  Errors
-    are against a tightly converged FP64 solve from the same pivot.  Also the
-    one-body density leg on the same Hamiltonian."""
+    the plain FP64 path (scalar Lanczos, FP64 applyH and vectors) against
+    mixed precision (FP32 applyH, FP32-stored vectors, FP64 sums), scalar
+    and block, each with thick restart (keep 20 or 30) and the reference's
+    convergence test.  For every method the convergence tolerance is swept
+    and the fastest run whose 10 eigenvalues all lie within 1e-6 of a
+    tightly converged FP64 solve (from the same pivot) is kept, so each
+    method is timed at its own best setting for the same accuracy.  Times
+    are the solver's device clock.  Also the one-body density leg on the same
+    Hamiltonian."""
     from bigstickpublick_b200.engine import Hamiltonian
     T = make_tables("pf4p4n")
     H = Hamiltonian(T)
     try:
         rng = np.random.default_rng(11)
         piv = rng.standard_normal(T.dim)
-        pivb = rng.standard_normal((T.dim, 8))
-        pivb[:, 0] = piv
-        pivb = pivb.reshape(-1)
+        pivs = {nb: np.concatenate([piv[:, None], rng.standard_normal((T.dim, nb - 1))], axis=1).reshape(-1)
+                for nb in (2, 4, 8)}
         for prec in (FP64, MIXED):
             H.lanczos(nkeep=2, niter=6, fixed_iter=True, pivot=piv, **prec)
-        H.lanczos(nkeep=2, niter=3, nb=8, fixed_iter=True, pivot=pivb, **MIXED)
-        scal = dict(nkeep=10, niter=args.tts_niter, nthick_add=10, max_restarts=200)
-        ev_ref, v_ref, info_ref = _solve(H, converge_tol=1e-9, pivot=piv, want_vectors=True, **FP64, **scal)
+        for nb in (2, 4, 8):
+            H.lanczos(nkeep=2, niter=3, nb=nb, fixed_iter=True, pivot=pivs[nb], **MIXED)
+        ev_ref, v_ref, info_ref = _solve(H, nkeep=10, niter=150, nthick_add=10, max_restarts=200, converge_tol=1e-9,
+                                         pivot=piv, want_vectors=True, **FP64)
         out = {"reference": dict(info_ref, converge_tol=1e-9, lowest=[float(x) for x in ev_ref[:3]])}
-        runs = [("fp64", dict(pivot=piv, **FP64, **scal)),
-                ("mixed", dict(pivot=piv, **MIXED, **scal)),
-                ("block8_mixed", dict(nkeep=10, niter=args.tts_block_niter, nb=8, nthick_add=10, max_restarts=200,
-                                      pivot=pivb, **MIXED))]
-        for name, kw in runs:
-            ev, vecs, info = _solve(H, converge_tol=args.tts_tol, want_vectors=True, **kw)
+        methods = [
+            ("fp64", [dict(nkeep=10, niter=n, nthick_add=10, max_restarts=200, pivot=piv, **FP64) for n in (100, 150)]),
+            ("mixed", [dict(nkeep=10, niter=n, nthick_add=10, max_restarts=200, pivot=piv, **MIXED) for n in (100, 150)]),
+            ("block2_mixed", [dict(nkeep=10, niter=80, nb=2, nthick_add=10, max_restarts=200, pivot=pivs[2], **MIXED)]),
+            ("block4_mixed", [dict(nkeep=10, niter=40, nb=4, nthick_add=a, max_restarts=200, pivot=pivs[4], **MIXED)
+                              for a in (10, 20)]),
+            ("block8_mixed", [dict(nkeep=10, niter=20, nb=8, nthick_add=20, max_restarts=200, pivot=pivs[8], **MIXED)]),
+        ]
+        for name, cfgs in methods:
+            best, tried = None, []
+            for kw in cfgs:
+                for tol in args.tts_tols:
+                    ev, _, info = _solve(H, converge_tol=tol, **kw)
+                    err = float(np.max(np.abs(ev - ev_ref) / np.abs(ev_ref)))
+                    desc = {"niter": kw["niter"], "nb": kw.get("nb", 1), "keep": kw["nkeep"] + kw["nthick_add"],
+                            "tol": tol, "solve_s": info["solve_s"], "max_rel_eig_err": err}
+                    tried.append(desc)
+                    if err <= 1e-6 and (best is None or info["solve_s"] < best[1]["solve_s"]):
+                        best = (kw, dict(info, **desc))
+            if best is None:
+                out[name] = {"meets_1e-6": False, "tried": tried}
+                continue
+            kw, info = best
+            # the chosen run again with its eigenvectors, for the overlap error
+            ev, vecs, _ = _solve(H, converge_tol=info["tol"], want_vectors=True, **kw)
             info.update(compare_states(ev, vecs, ev_ref, v_ref))
-            info["meets_1e-6"] = info["max_rel_eig_err"] <= 1e-6
+            info["meets_1e-6"] = True
+            info["tried"] = tried
             out[name] = info
-        for name in ("mixed", "block8_mixed"):
-            out[name]["speedup_time_to_solution_vs_fp64"] = out["fp64"]["solve_s"] / out[name]["solve_s"]
-            out[name]["its_per_s_vs_fp64"] = out[name]["its_per_s"] / out["fp64"]["its_per_s"]
-        out["config"] = (f"pf 4p4n, lowest 10, keep 20 on thick restart, convergence test option 0 at tol "
-                         f"{args.tts_tol} MeV; scalar {args.tts_niter} iterations per cycle, block nb=8 "
-                         f"{args.tts_block_niter} block iterations per cycle; errors against FP64 converged to 1e-9")
+        for name in ("mixed", "block2_mixed", "block4_mixed", "block8_mixed"):
+            if out.get(name, {}).get("meets_1e-6") and out["fp64"].get("meets_1e-6"):
+                out[name]["speedup_time_to_solution_vs_fp64"] = out["fp64"]["solve_s"] / out[name]["solve_s"]
+        out["config"] = ("pf 4p4n, lowest 10 within 1e-6 relative of an FP64 solve converged to 1e-9; per method "
+                         f"the fastest of convergence tolerances {list(args.tts_tols)} MeV and the listed bases; "
+                         "solver device clock")
         if not args.no_density:
             try:
                 out["density"] = density_leg(H, T)
@@ -579,9 +606,7 @@ def main():
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--no-tts", action="store_true")
     ap.add_argument("--lanczos-iters", type=int, default=300)
-    ap.add_argument("--tts-tol", type=float, default=1e-5)
-    ap.add_argument("--tts-niter", type=int, default=150)
-    ap.add_argument("--tts-block-niter", type=int, default=20)
+    ap.add_argument("--tts-tols", type=float, nargs="+", default=list(TTS_TOLS))
     ap.add_argument("--batch-n", type=int, default=256)
     ap.add_argument("--batch-iters", type=int, default=150)
     ap.add_argument("--tune-cache", action="store_true")

@@ -2,6 +2,8 @@
 // kernel (applyh_kernels.cu) and the persistent batched kernel (batch.cu).
 #pragma once
 
+#include <type_traits>
+
 #include "bsg_internal.h"
 
 namespace bsg {
@@ -160,7 +162,10 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
             for (int i = 0; i < ITEMS; ++i) {
                 if (!valid[i] || pos[i] >= op.nout) continue;
                 const int k0 = __ldg(ptr + pos[i]), k1 = __ldg(ptr + pos[i] + 1);
-                if constexpr (REC32) {
+                // NN takes the 32-bit records for FP64 vectors only: for FP32
+                // the extra hmatnn load per record cost more than the halved
+                // record bytes saved (pf 6p6n: 143.8 against 139.2 ms)
+                if constexpr (REC32 && std::is_same<T, double>::value) {
                     // input position | hmatnn label - 1 | phase sign
                     const uint32_t *c32 =
                         a.sell32 + op.sell_base + __ldg(a.slice_off + op.slice_base + (pos[i] >> 5)) + lane;
