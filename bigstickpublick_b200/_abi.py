@@ -93,7 +93,24 @@ class BsgStats(C.Structure):
         ("density_ms", C.c_double), ("density_rows", C.c_int64),
         ("density_launches", C.c_int32), ("reserved2", C.c_int32),
         ("apply1b_ms", C.c_double), ("grad_ms", C.c_double),
+        ("n_ops_ppp", C.c_int64), ("n_ops_nnn", C.c_int64), ("n_ops_ppn", C.c_int64), ("n_ops_pnn", C.c_int64),
     ]
+
+
+class BsgTables3(C.Structure):
+    _fields_ = [
+        ("p2b_cop", i32p), ("p2b_dop", i32p), ("n2b_cop", i32p), ("n2b_dop", i32p),
+        ("np3b", C.c_int64), ("p3b_isd", i64p), ("p3b_fsd", i64p), ("p3b_op", i32p), ("p3b_phase", i8p),
+        ("nn3b", C.c_int64), ("n3b_isd", i64p), ("n3b_fsd", i64p), ("n3b_op", i32p), ("n3b_phase", i8p),
+        ("nmatppp", C.c_int64), ("nmatnnn", C.c_int64), ("nmatppn", C.c_int64), ("nmatpnn", C.c_int64),
+        ("hmatppp", f32p), ("hmatnnn", f32p), ("hmatppn", f32p), ("hmatpnn", f32p),
+        ("npairs_p", C.c_int32), ("npairs_n", C.c_int32),
+        ("cppntriplet", i32p), ("dppntriplet", i32p), ("cpnntriplet", i32p), ("dpnntriplet", i32p),
+    ]
+
+
+class BsgModel3Spec(C.Structure):
+    _fields_ = [("w2", C.c_double), ("w3", C.c_double), ("seed", C.c_uint64)]
 
 
 class BsgOrbit(C.Structure):
@@ -140,6 +157,7 @@ class BsgHostTables(C.Structure):
         ("npairs_pp", C.c_int64), ("npairs_nn", C.c_int64), ("npairs_pn", C.c_int64),
         ("priv", C.c_void_p),
         ("dt", BsgDensityTables),
+        ("t3", C.POINTER(BsgTables3)),
     ]
 
 
@@ -161,6 +179,9 @@ def host_lib():
         lib = C.CDLL(path)
         lib.bsg_host_build.argtypes = [C.POINTER(BsgModelSpec), C.POINTER(C.POINTER(BsgHostTables))]
         lib.bsg_host_build.restype = C.c_int
+        lib.bsg_host_build3.argtypes = [C.POINTER(BsgModelSpec), C.POINTER(BsgModel3Spec),
+                                        C.POINTER(C.POINTER(BsgHostTables))]
+        lib.bsg_host_build3.restype = C.c_int
         lib.bsg_host_free.argtypes = [C.POINTER(BsgHostTables)]
         lib.bsg_host_free.restype = None
         lib.bsg_host_last_error.argtypes = []
@@ -184,6 +205,8 @@ def gpu_lib():
         vp = C.c_void_p
         lib.bsg_create.argtypes = [C.POINTER(BsgTables), C.POINTER(BsgConfig), C.POINTER(vp)]
         lib.bsg_create.restype = C.c_int
+        lib.bsg_create3.argtypes = [C.POINTER(BsgTables), C.POINTER(BsgTables3), C.POINTER(BsgConfig), C.POINTER(vp)]
+        lib.bsg_create3.restype = C.c_int
         lib.bsg_destroy.argtypes = [vp]
         lib.bsg_destroy.restype = C.c_int
         lib.bsg_strerror.argtypes = [C.c_int]
@@ -207,6 +230,8 @@ def gpu_lib():
         lib.bsg_get_stats.restype = C.c_int
         lib.bsg_validate_tables.argtypes = [C.POINTER(BsgTables), C.c_char_p, C.c_size_t]
         lib.bsg_validate_tables.restype = C.c_int
+        lib.bsg_validate_tables3.argtypes = [C.POINTER(BsgTables), C.POINTER(BsgTables3), C.c_char_p, C.c_size_t]
+        lib.bsg_validate_tables3.restype = C.c_int
         lib.bsg_applyh_noalloc.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_int]
         lib.bsg_applyh_noalloc.restype = C.c_int
         lib.bsg_batch_create.argtypes = [C.c_int, C.POINTER(C.POINTER(BsgTables)), C.POINTER(BsgConfig), C.POINTER(vp)]

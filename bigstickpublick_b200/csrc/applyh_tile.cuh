@@ -227,10 +227,9 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
         for (int c = a.pn_ptr[slot]; c < c1; ++c) {
             const PNContrib pc = a.pn[c];
             const NOp op = a.nops[pc.nop];
-            const int acol = pc.acol * a.ld_cpn, ccol = pc.ccol * a.ld_cpn;
             for (int k = lane; k < op.nbd; k += 32) {
                 const BDPair bd = a.bd[op.bd_base + k];
-                const int idx = __ldg(a.cpn + bd.b + acol) + __ldg(a.dpn + bd.d + ccol);
+                const int idx = __ldg(a.cpn + bd.b + pc.aoff) + __ldg(a.dpn + bd.d + pc.coff);
                 float xme = __ldg(a.hmatpn + idx - 1);
                 Mw[k] = xme * pc.php;
             }

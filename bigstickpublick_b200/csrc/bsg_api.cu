@@ -16,6 +16,7 @@
 #include <cstring>
 #include <new>
 #include <numeric>
+#include <set>
 #include <unordered_map>
 
 #include "bsg_internal.h"
@@ -124,20 +125,41 @@ void csr_by_out(const std::vector<int32_t> &out, const std::vector<Rec> &recs, i
     for (size_t k = 0; k < recs.size(); ++k) sorted[fill[out[k]]++] = recs[k];
 }
 
-int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
+// t3: the three-body arrays (bsg_create3), or null for a two-body context
+int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upload = true) {
     Validator V{ctx, ""};
+    const bool three = (t3 != nullptr);
+    ctx->threebody = three;
     // ---- basic presence and sizes
     if (t->dimbasis <= 0 || t->nsd_p <= 0 || t->nsd_n <= 0)
         return set_err(ctx, BSG_ERR_BAD_TABLE, "empty basis");
     if (!t->pstart || !t->nstart) return set_err(ctx, BSG_ERR_BAD_TABLE, "pstart/nstart missing");
+    // a three-body run labels its two-body jumps by pairs (t3 cop/dop), not by p2b_op/n2b_op
     if (!nonnull(t->p1b_isd, t->np1b) || !nonnull(t->p1b_fsd, t->np1b) || !nonnull(t->p1b_cop, t->np1b) ||
         !nonnull(t->p1b_dop, t->np1b) || !nonnull(t->p1b_phase, t->np1b) || !nonnull(t->n1b_isd, t->nn1b) ||
         !nonnull(t->n1b_fsd, t->nn1b) || !nonnull(t->n1b_cop, t->nn1b) || !nonnull(t->n1b_dop, t->nn1b) ||
         !nonnull(t->n1b_phase, t->nn1b) || !nonnull(t->p2b_isd, t->np2b) || !nonnull(t->p2b_fsd, t->np2b) ||
-        !nonnull(t->p2b_op, t->np2b) || !nonnull(t->p2b_phase, t->np2b) || !nonnull(t->n2b_isd, t->nn2b) ||
-        !nonnull(t->n2b_fsd, t->nn2b) || !nonnull(t->n2b_op, t->nn2b) || !nonnull(t->n2b_phase, t->nn2b) ||
-        !nonnull(t->hmatpp, t->nmatpp) || !nonnull(t->hmatnn, t->nmatnn) || !nonnull(t->hmatpn, t->nmatpn))
+        (!three && !nonnull(t->p2b_op, t->np2b)) || !nonnull(t->p2b_phase, t->np2b) ||
+        !nonnull(t->n2b_isd, t->nn2b) || !nonnull(t->n2b_fsd, t->nn2b) || (!three && !nonnull(t->n2b_op, t->nn2b)) ||
+        !nonnull(t->n2b_phase, t->nn2b) || !nonnull(t->hmatpp, t->nmatpp) || !nonnull(t->hmatnn, t->nmatnn) ||
+        !nonnull(t->hmatpn, t->nmatpn))
         return set_err(ctx, BSG_ERR_BAD_TABLE, "a table with nonzero length has a null pointer");
+    if (three) {
+        if (!nonnull(t3->p2b_cop, t->np2b) || !nonnull(t3->p2b_dop, t->np2b) || !nonnull(t3->n2b_cop, t->nn2b) ||
+            !nonnull(t3->n2b_dop, t->nn2b) || t3->np3b < 0 || t3->nn3b < 0 || !nonnull(t3->p3b_isd, t3->np3b) ||
+            !nonnull(t3->p3b_fsd, t3->np3b) || !nonnull(t3->p3b_op, t3->np3b) || !nonnull(t3->p3b_phase, t3->np3b) ||
+            !nonnull(t3->n3b_isd, t3->nn3b) || !nonnull(t3->n3b_fsd, t3->nn3b) || !nonnull(t3->n3b_op, t3->nn3b) ||
+            !nonnull(t3->n3b_phase, t3->nn3b) || t3->nmatppp < 0 || t3->nmatnnn < 0 || t3->nmatppn < 0 ||
+            t3->nmatpnn < 0 || !nonnull(t3->hmatppp, t3->nmatppp) || !nonnull(t3->hmatnnn, t3->nmatnnn) ||
+            !nonnull(t3->hmatppn, t3->nmatppn) || !nonnull(t3->hmatpnn, t3->nmatpnn) || t3->npairs_p < 0 ||
+            t3->npairs_n < 0 || t3->npairs_p > 65535 || t3->npairs_n > 65535)
+            return set_err(ctx, BSG_ERR_BAD_TABLE, "a three-body table with nonzero length has a null pointer, or a bad size");
+        if ((t3->nmatppn > 0 && (!t3->cppntriplet || !t3->dppntriplet)) ||
+            (t3->nmatpnn > 0 && (!t3->cpnntriplet || !t3->dpnntriplet)))
+            return set_err(ctx, BSG_ERR_BAD_TABLE, "cppntriplet/dppntriplet or cpnntriplet/dpnntriplet missing");
+        if (t->nmatpn + t3->nmatppn + t3->nmatpnn >= INT32_MAX || t->nmatnn + t3->nmatnnn >= INT32_MAX)
+            return set_err(ctx, BSG_ERR_UNSUPPORTED, "three-body tables beyond this build's index widths");
+    }
     if (t->nbundles < 0 || (t->nbundles > 0 && (!t->optype || !t->hchar || !t->pxstart || !t->pxend ||
                                                  !t->nxstart || !t->nxend || !t->cstride)))
         return set_err(ctx, BSG_ERR_BAD_TABLE, "opbundle arrays missing");
@@ -189,6 +211,45 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
             cpn32[i] = (int32_t)t->cpnpair[i];
             dpn32[i] = (int32_t)t->dpnpair[i];
         }
+    // three-body PPN / PNN tables appended to the PN ones, so that the PN
+    // machinery addresses all three: one table (cpn, dpn) and one matrix
+    // element array hmatpn | hmatppn | hmatpnn.  The c entries carry the
+    // matrix-element offset of their block; each combination is checked
+    // against its own block when a bundle uses it.
+    //   PPN block (base_ppn): (a + nhsps(-2)) + (bb - 1) * ld, a neutron s.p.
+    //     label, bb a proton pair -- one column per proton pair, the rows the
+    //     neutron labels the PN machinery tabulates;
+    //   PNN block (base_pnn): (bb - 1) + (a + nhsps(-1)) * npairs_n, as the
+    //     reference's cpnntriplet(bb, a).
+    const int64_t npp3 = three ? t3->npairs_p : 0, nnp3 = three ? t3->npairs_n : 0;
+    const int32_t ld_p = nl_p + nr_p + 1;
+    const int64_t base_ppn = ncpn, base_pnn = ncpn + (int64_t)ld * npp3;
+    const int64_t ncpn_all = base_pnn + nnp3 * ld_p;
+    const int64_t off_ppn = t->nmatpn, off_pnn = t->nmatpn + (three ? t3->nmatppn : 0);
+    if (ncpn_all >= INT32_MAX) return set_err(ctx, BSG_ERR_UNSUPPORTED, "triplet tables beyond this build's index widths");
+    // raw (reference-layout) PPN / PNN entries for the per-bundle checks
+    auto ppn_c = [&](int bb, int a) { return t3->cppntriplet[(int64_t)(bb - 1) + (int64_t)(a + nl_n) * npp3]; };
+    auto ppn_d = [&](int dd, int c) { return t3->dppntriplet[(int64_t)(dd - 1) + (int64_t)(c + nl_n) * npp3]; };
+    auto pnn_c = [&](int bb, int a) { return t3->cpnntriplet[(int64_t)(bb - 1) + (int64_t)(a + nl_p) * nnp3]; };
+    auto pnn_d = [&](int dd, int c) { return t3->dpnntriplet[(int64_t)(dd - 1) + (int64_t)(c + nl_p) * nnp3]; };
+    if (three) {
+        cpn32.resize(ncpn_all, 0);
+        dpn32.resize(ncpn_all, 0);
+        if (t3->nmatppn > 0)
+            for (int bb = 1; bb <= npp3; ++bb)
+                for (int a = -nl_n; a <= nr_n; ++a) {
+                    const int64_t at = base_ppn + (a + nl_n) + (int64_t)(bb - 1) * ld;
+                    cpn32[at] = ppn_c(bb, a) + (int32_t)off_ppn;
+                    dpn32[at] = ppn_d(bb, a);
+                }
+        if (t3->nmatpnn > 0)
+            for (int a = -nl_p; a <= nr_p; ++a)
+                for (int bb = 1; bb <= nnp3; ++bb) {
+                    const int64_t at = base_pnn + (bb - 1) + (int64_t)(a + nl_p) * nnp3;
+                    cpn32[at] = pnn_c(bb, a) + (int32_t)off_pnn;
+                    dpn32[at] = pnn_d(bb, a);
+                }
+    }
 
     // ---- neutron operators
     struct NKey {
@@ -207,6 +268,16 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
     std::vector<int32_t> nnrec_op_all;
     std::vector<int8_t> nnrec_ph_all;
     std::vector<BDPair> bd_all;
+    // neutron operators of a sector jump's jump range, by source:
+    //   0 NN  (n2b, hmatnn label records -> matrix-element records)
+    //   1 PN  (n1b, s.p. labels b, d -> label records)
+    //   2 PNN (n2b with pair labels bb, dd -> label records)
+    //   3 NNN (n3b, hmatnnn label records -> matrix-element records)
+    // Matrix-element records keep their label for the adjoint and for the
+    // 32-bit records; NNN labels are offset by nmatnn (one device array
+    // hmatnn | hmatnnn).
+    std::vector<int32_t> bdk_dense;        // (b,d) -> index in the op's list, reset after each op
+    std::vector<size_t> bdk_touched;
     auto get_nop = [&](int kind, int dir, int64_t x0, int64_t x1, int32_t &id) -> int {
         NKey k{kind, dir, x0, x1};
         auto it = nop_id.find(k);
@@ -215,24 +286,40 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
         std::vector<int32_t> out(n);
         int32_t maxin = -1, maxout = -1;
         NOp op{};
-        op.kind = kind;
-        if (kind == 1) {
+        op.kind = (kind == 1 || kind == 2) ? 1 : 0;
+        if (op.kind == 1) {
+            const bool pnn = (kind == 2);
+            const int64_t nkey = pnn ? nnp3 : ld;   // labels per side
+            if (bdk_dense.size() < (size_t)(nkey * nkey)) bdk_dense.assign((size_t)(nkey * nkey), -1);
             std::vector<PNRec> recs(n);
-            std::vector<int32_t> bdk((size_t)ld * ld, -1);
             std::vector<BDPair> bdl;
             for (int64_t x = x0; x <= x1; ++x) {
-                const int64_t isd = t->n1b_isd[x - 1], fsd = t->n1b_fsd[x - 1];
-                const int b = t->n1b_cop[x - 1], d = t->n1b_dop[x - 1];
+                const int64_t isd = pnn ? t->n2b_isd[x - 1] : t->n1b_isd[x - 1];
+                const int64_t fsd = pnn ? t->n2b_fsd[x - 1] : t->n1b_fsd[x - 1];
                 if (isd < 1 || fsd < 1 || isd > ctx->max_rowlen || fsd > ctx->max_rowlen)
-                    return V.fail("n1b isd/fsd out of range at jump " + std::to_string(x));
-                if (b < -nl_n || b > nr_n || d < -nl_n || d > nr_n || b == 0 || d == 0)
-                    return V.fail("n1b_cop/dop outside the neutron half spaces at jump " + std::to_string(x));
-                const int ph = t->n1b_phase[x - 1];
-                if (ph != 1 && ph != -1) return V.fail("n1b_phase not +-1");
-                int32_t &kk = bdk[(size_t)(b + nl_n) * ld + (d + nl_n)];
+                    return V.fail(std::string(pnn ? "n2b" : "n1b") + " isd/fsd out of range at jump " + std::to_string(x));
+                int kb, kd;   // row keys into the cpn / dpn tables
+                if (pnn) {
+                    const int bb = t3->n2b_cop[x - 1], dd = t3->n2b_dop[x - 1];
+                    if (bb < 1 || bb > nnp3 || dd < 1 || dd > nnp3)
+                        return V.fail("n2b_cop/dop outside the neutron pairs at jump " + std::to_string(x));
+                    kb = bb - 1;
+                    kd = dd - 1;
+                } else {
+                    const int b = t->n1b_cop[x - 1], d = t->n1b_dop[x - 1];
+                    if (b < -nl_n || b > nr_n || d < -nl_n || d > nr_n || b == 0 || d == 0)
+                        return V.fail("n1b_cop/dop outside the neutron half spaces at jump " + std::to_string(x));
+                    kb = b + nl_n;
+                    kd = d + nl_n;
+                }
+                const int ph = pnn ? t->n2b_phase[x - 1] : t->n1b_phase[x - 1];
+                if (ph != 1 && ph != -1) return V.fail(pnn ? "n2b_phase not +-1" : "n1b_phase not +-1");
+                const size_t key = (size_t)kb * nkey + kd;
+                int32_t &kk = bdk_dense[key];
                 if (kk < 0) {
                     kk = (int32_t)bdl.size();
-                    bdl.push_back(BDPair{(uint8_t)(b + nl_n), (uint8_t)(d + nl_n)});
+                    bdk_touched.push_back(key);
+                    bdl.push_back(BDPair{(uint16_t)kb, (uint16_t)kd});
                 }
                 PNRec r;
                 r.in = (int32_t)((dir == 0 ? isd : fsd) - 1);
@@ -243,8 +330,11 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
                 recs[x - x0] = r;
                 maxin = std::max(maxin, r.in);
                 maxout = std::max(maxout, out[x - x0]);
+                if (bdl.size() > 65535) break;
             }
-            if (bdl.size() > 65535) return V.fail("too many distinct (b,d) pairs in a neutron sector jump");
+            for (size_t key : bdk_touched) bdk_dense[key] = -1;
+            bdk_touched.clear();
+            if (bdl.size() > 65535) return V.fail("too many distinct (b,d) label pairs in a neutron sector jump");
             std::vector<int32_t> ptr;
             std::vector<PNRec> sorted;
             csr_by_out(out, recs, maxout + 1, ptr, sorted);
@@ -257,25 +347,35 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
             pnrec_all.insert(pnrec_all.end(), sorted.begin(), sorted.end());
             nptr_all.insert(nptr_all.end(), ptr.begin(), ptr.end());
         } else {
+            const bool nnn = (kind == 3);
+            const int64_t *xisd = nnn ? t3->n3b_isd : t->n2b_isd, *xfsd = nnn ? t3->n3b_fsd : t->n2b_fsd;
+            const int32_t *xop = nnn ? t3->n3b_op : t->n2b_op;
+            const int8_t *xph = nnn ? t3->n3b_phase : t->n2b_phase;
+            const float *hm = nnn ? t3->hmatnnn : t->hmatnn;
+            const int64_t nmat = nnn ? t3->nmatnnn : t->nmatnn;
+            const int32_t loff = nnn ? (int32_t)t->nmatnn : 0;
+            const char *nm = nnn ? "n3b" : "n2b";
             std::vector<NNRec> recs(n);
             std::vector<int32_t> ops(n);
             std::vector<int8_t> phs(n);
             for (int64_t x = x0; x <= x1; ++x) {
-                const int64_t isd = t->n2b_isd[x - 1], fsd = t->n2b_fsd[x - 1];
+                const int64_t isd = xisd[x - 1], fsd = xfsd[x - 1];
                 if (isd < 1 || fsd < 1 || isd > ctx->max_rowlen || fsd > ctx->max_rowlen)
-                    return V.fail("n2b isd/fsd out of range at jump " + std::to_string(x));
-                const int32_t opl = t->n2b_op[x - 1];
-                if (opl < 1 || opl > t->nmatnn) return V.fail("n2b_op outside hmatnn at jump " + std::to_string(x));
-                const int ph = t->n2b_phase[x - 1];
-                if (ph != 1 && ph != -1) return V.fail("n2b_phase not +-1");
+                    return V.fail(std::string(nm) + " isd/fsd out of range at jump " + std::to_string(x));
+                const int32_t opl = xop[x - 1];
+                if (opl < 1 || opl > nmat)
+                    return V.fail(std::string(nm) + (nnn ? "_op outside hmatnnn" : "_op outside hmatnn") + " at jump " +
+                                  std::to_string(x));
+                const int ph = xph[x - 1];
+                if (ph != 1 && ph != -1) return V.fail(std::string(nm) + "_phase not +-1");
                 NNRec r;
                 r.in = (int32_t)((dir == 0 ? isd : fsd) - 1);
                 out[x - x0] = (int32_t)((dir == 0 ? fsd : isd) - 1);
-                float xme = t->hmatnn[opl - 1];
+                float xme = hm[opl - 1];
                 xme = xme * (float)ph;
                 r.me = xme;
                 recs[x - x0] = r;
-                ops[x - x0] = opl;
+                ops[x - x0] = opl + loff;
                 phs[x - x0] = (int8_t)ph;
                 maxin = std::max(maxin, r.in);
                 maxout = std::max(maxout, out[x - x0]);
@@ -310,6 +410,25 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
     std::vector<std::pair<int32_t, PNContrib>> pn;
     std::vector<std::pair<int32_t, SPEContrib>> spe;
     int64_t ops[4] = {0, 0, 0, 0};
+    int64_t ops3[4] = {0, 0, 0, 0};   // PPP, NNN, PPN, PNN
+    // one proton-side PN-form contribution (PN, PPN, PNN) of the jump s1 -> s2
+    auto pn_contrib = [&](int64_t s1, int64_t s2, int32_t id, int32_t aoff, int32_t coff, int ph,
+                          const std::string &what) -> int {
+        int32_t ri, rf;
+        if (!rowof(s1, ri) || !rowof(s2, rf))
+            return set_err(ctx, BSG_ERR_OOB_INDEX, what + " isd/fsd is not a pstart value");
+        if (nops[id].nout > ctx->h_rowlen[rf] || nop_maxin[id] >= ctx->h_rowlen[ri])
+            return set_err(ctx, BSG_ERR_OOB_INDEX, what + ": neutron jump outside the row");
+        if (ph != 1 && ph != -1) return set_err(ctx, BSG_ERR_BAD_TABLE, what + " phase not +-1");
+        PNContrib c{};
+        c.q_off = s1;
+        c.nop = id;
+        c.aoff = aoff;
+        c.coff = coff;
+        c.php = (float)ph;
+        pn.push_back({rf, c});
+        return BSG_OK;
+    };
     for (int64_t ib = 0; ib < t->nbundles; ++ib) {
         const int op = t->optype[ib], hc = t->hchar[ib];
         const int64_t px0 = t->pxstart[ib], px1 = t->pxend[ib], nx0 = t->nxstart[ib], nx1 = t->nxend[ib];
@@ -319,6 +438,136 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
         if (cs < 1) return set_err(ctx, BSG_ERR_BAD_TABLE, "cstride < 1" + where);
         if (px1 < px0 || nx1 < nx0) continue;  // empty bundle: no work
         const bool bwd = (hc == 'b');
+        const bool is3 = (op == BSG_OP_PPP || op == BSG_OP_NNN || op == BSG_OP_PPN || op == BSG_OP_PNN);
+        if (is3 && !three) return set_err(ctx, BSG_ERR_BAD_TABLE, "three-body bundle in a two-body context" + where);
+        // applyHbundled_g with threebody set applies SPE and the three-body
+        // bundles only (src/bapplyhlib1.f90:107-235)
+        if (three && (op == BSG_OP_PP || op == BSG_OP_NN || op == BSG_OP_PN)) continue;
+        if (op == BSG_OP_PPP) {
+            // applyhPPPbundled_g (src/bapplyhlib1.f90:1390-1572): as PP
+            if (px0 < 1 || px1 > t3->np3b || nx0 < 1 || nx1 > t->nsd_n)
+                return set_err(ctx, BSG_ERR_OOB_INDEX, "PPP range" + where);
+            if (cs != 1) return set_err(ctx, BSG_ERR_UNSUPPORTED, "PPP cstride != 1" + where);
+            for (int64_t c = nx0 + 1; c <= nx1; ++c)
+                if (t->nstart[c - 1] != t->nstart[c - 2] + 1)
+                    return set_err(ctx, BSG_ERR_UNSUPPORTED, "PPP neutron run not contiguous" + where);
+            const int32_t lo = (int32_t)(t->nstart[nx0 - 1] - 1), hi = (int32_t)(t->nstart[nx1 - 1] - 1);
+            for (int64_t x = px0; x <= px1; ++x) {
+                int32_t ri, rf;
+                const int64_t s1 = bwd ? t3->p3b_fsd[x - 1] : t3->p3b_isd[x - 1];
+                const int64_t s2 = bwd ? t3->p3b_isd[x - 1] : t3->p3b_fsd[x - 1];
+                if (!rowof(s1, ri) || !rowof(s2, rf))
+                    return set_err(ctx, BSG_ERR_OOB_INDEX, "p3b isd/fsd is not a pstart value" + where);
+                if (hi >= ctx->h_rowlen[ri] || hi >= ctx->h_rowlen[rf])
+                    return set_err(ctx, BSG_ERR_OOB_INDEX, "PPP neutron run longer than the row" + where);
+                const int32_t opl = t3->p3b_op[x - 1];
+                if (opl < 1 || opl > t3->nmatppp) return set_err(ctx, BSG_ERR_OOB_INDEX, "p3b_op outside hmatppp" + where);
+                const int ph = t3->p3b_phase[x - 1];
+                if (ph != 1 && ph != -1) return set_err(ctx, BSG_ERR_BAD_TABLE, "p3b_phase not +-1" + where);
+                PPContrib c{};
+                c.q_off = s1;
+                float xme = t3->hmatppp[opl - 1];
+                xme = xme * (float)ph;
+                c.me = xme;
+                c.lo = lo;
+                c.hi = hi;
+                pp.push_back({rf, c});
+                pp_op_tmp.push_back(opl);
+                pp_ph_tmp.push_back((int8_t)ph);
+            }
+            ops3[0] += (px1 - px0 + 1) * (nx1 - nx0 + 1);
+            continue;
+        }
+        if (op == BSG_OP_NNN) {
+            // applyhNNNbundled_g (src/bapplyhlib1.f90:1579-1756): as NN
+            if (px0 < 1 || px1 > t->nsd_p || nx0 < 1 || nx1 > t3->nn3b)
+                return set_err(ctx, BSG_ERR_OOB_INDEX, "NNN range" + where);
+            int32_t id;
+            int st = get_nop(3, bwd ? 1 : 0, nx0, nx1, id);
+            if (st) return set_err(ctx, st, V.msg + where);
+            int64_t nrow_b = 0;
+            for (int64_t csd = px0; csd <= px1; csd += cs) {
+                const int32_t r = (int32_t)(csd - 1);
+                if (nops[id].nout > ctx->h_rowlen[r] || nop_maxin[id] >= ctx->h_rowlen[r])
+                    return set_err(ctx, BSG_ERR_OOB_INDEX, "NNN jump outside the row" + where);
+                nn.push_back({r, NNContrib{id}});
+                ++nrow_b;
+            }
+            ops3[1] += nrow_b * (nx1 - nx0 + 1);
+            continue;
+        }
+        if (op == BSG_OP_PPN || op == BSG_OP_PNN) {
+            // applyhPPNbundled_g / applyhPNNbundled_g (src/bapplyhlib1.f90:2295-2562,
+            // :2033-2285): PN-form contributions on the appended tables
+            const bool ppn = (op == BSG_OP_PPN);
+            const char *nm = ppn ? "PPN" : "PNN";
+            if (ppn ? (px0 < 1 || px1 > t->np2b || nx0 < 1 || nx1 > t->nn1b)
+                    : (px0 < 1 || px1 > t->np1b || nx0 < 1 || nx1 > t->nn2b))
+                return set_err(ctx, BSG_ERR_OOB_INDEX, std::string(nm) + " range" + where);
+            if ((ppn && t3->nmatppn == 0) || (!ppn && t3->nmatpnn == 0))
+                return set_err(ctx, BSG_ERR_BAD_TABLE, std::string(nm) + " bundle without matrix elements" + where);
+            int32_t id;
+            int st = get_nop(ppn ? 1 : 2, bwd ? 1 : 0, nx0, nx1, id);
+            if (st) return set_err(ctx, st, V.msg + where);
+            // every proton (created, destroyed) label pair x neutron (b,d) pair
+            // of the bundle must address its own matrix-element block
+            const NOp &no = nops[id];
+            std::vector<std::pair<int, int>> lab;
+            {
+                std::set<std::pair<int, int>> seen;
+                for (int64_t x = px0; x <= px1; ++x) {
+                    int cl, dl;
+                    if (ppn) {
+                        cl = t3->p2b_cop[x - 1];
+                        dl = t3->p2b_dop[x - 1];
+                        if (cl < 1 || cl > npp3 || dl < 1 || dl > npp3)
+                            return set_err(ctx, BSG_ERR_OOB_INDEX, "p2b_cop/dop outside the proton pairs" + where);
+                    } else {
+                        cl = t->p1b_cop[x - 1];
+                        dl = t->p1b_dop[x - 1];
+                        if (cl < -nl_p || cl > nr_p || dl < -nl_p || dl > nr_p || cl == 0 || dl == 0)
+                            return set_err(ctx, BSG_ERR_OOB_INDEX, "p1b_cop/dop outside the proton half spaces" + where);
+                    }
+                    if (seen.insert({cl, dl}).second) lab.push_back({cl, dl});
+                }
+            }
+            const int64_t nmat3 = ppn ? t3->nmatppn : t3->nmatpnn;
+            for (auto &pl : lab)
+                for (int32_t k = 0; k < no.nbd; ++k) {
+                    const BDPair bd = bd_all[no.bd_base + k];
+                    const int64_t idx = ppn ? (int64_t)ppn_c(pl.first, bd.b - nl_n) + ppn_d(pl.second, bd.d - nl_n)
+                                            : (int64_t)pnn_c(bd.b + 1, pl.first) + pnn_d(bd.d + 1, pl.second);
+                    if (idx < 1 || idx > nmat3)
+                        return set_err(ctx, BSG_ERR_OOB_INDEX,
+                                       std::string(ppn ? "cppntriplet+dppntriplet outside hmatppn" : "cpnntriplet+dpnntriplet outside hmatpnn") + where);
+                }
+            for (int64_t x = px0; x <= px1; ++x) {
+                int64_t isd, fsd;
+                int cl, dl, ph;
+                int32_t aoff, coff;
+                if (ppn) {
+                    isd = t->p2b_isd[x - 1];
+                    fsd = t->p2b_fsd[x - 1];
+                    cl = t3->p2b_cop[x - 1];
+                    dl = t3->p2b_dop[x - 1];
+                    ph = t->p2b_phase[x - 1];
+                    aoff = (int32_t)(base_ppn + (int64_t)(cl - 1) * ld);
+                    coff = (int32_t)(base_ppn + (int64_t)(dl - 1) * ld);
+                } else {
+                    isd = t->p1b_isd[x - 1];
+                    fsd = t->p1b_fsd[x - 1];
+                    cl = t->p1b_cop[x - 1];
+                    dl = t->p1b_dop[x - 1];
+                    ph = t->p1b_phase[x - 1];
+                    aoff = (int32_t)(base_pnn + (int64_t)(cl + nl_p) * nnp3);
+                    coff = (int32_t)(base_pnn + (int64_t)(dl + nl_p) * nnp3);
+                }
+                st = pn_contrib(bwd ? fsd : isd, bwd ? isd : fsd, id, aoff, coff, ph, std::string(nm) + where);
+                if (st) return st;
+            }
+            ops3[ppn ? 2 : 3] += (px1 - px0 + 1) * (nx1 - nx0 + 1);
+            continue;
+        }
         if (op == BSG_OP_PP) {
             if (px0 < 1 || px1 > t->np2b || nx0 < 1 || nx1 > t->nsd_n)
                 return set_err(ctx, BSG_ERR_OOB_INDEX, "PP range" + where);
@@ -412,8 +661,8 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
                 PNContrib c{};
                 c.q_off = s1;
                 c.nop = id;
-                c.acol = (int16_t)(t->p1b_cop[x - 1] + nl_p);
-                c.ccol = (int16_t)(t->p1b_dop[x - 1] + nl_p);
+                c.aoff = (int32_t)(t->p1b_cop[x - 1] + nl_p) * ld;
+                c.coff = (int32_t)(t->p1b_dop[x - 1] + nl_p) * ld;
                 c.php = (float)ph;
                 pn.push_back({rf, c});
             }
@@ -442,6 +691,10 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
     ctx->stats.n_ops_pp = ops[1];
     ctx->stats.n_ops_nn = ops[2];
     ctx->stats.n_ops_pn = ops[3];
+    ctx->stats.n_ops_ppp = ops3[0];
+    ctx->stats.n_ops_nnn = ops3[1];
+    ctx->stats.n_ops_ppn = ops3[2];
+    ctx->stats.n_ops_pnn = ops3[3];
 
     // ---- assign each row's contributions to the kWarps warps of its CTA by
     // longest-processing-time (heaviest first to the least loaded warp), then
@@ -460,7 +713,8 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
     // 32-bit copy when every input position, (b,d) index and hmatnn label fits
     int32_t max_nbd_all = 0;
     for (const NOp &op : nops) max_nbd_all = std::max(max_nbd_all, op.nbd);
-    const bool pack32 = ctx->max_rowlen <= 65536 && t->nmatnn <= 32768 && max_nbd_all <= 32768;
+    const int64_t nmatnn_all = t->nmatnn + (three ? t3->nmatnnn : 0);
+    const bool pack32 = ctx->max_rowlen <= 65536 && nmatnn_all <= 32768 && max_nbd_all <= 32768;
     std::vector<uint32_t> sell32_all;
     for (NOp &op : nops) {
         op.sell_base = (int64_t)sell_all.size();
@@ -608,18 +862,43 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
                                 8 * (size_t)t->nn2b, 8 * (size_t)t->nn2b, 4 * (size_t)t->nn2b, (size_t)t->nn2b,
                                 4 * (size_t)t->nmatpp, 4 * (size_t)t->nmatnn,
                                 t->cpnpair ? 8 * (size_t)ncpn : 0, t->dpnpair ? 8 * (size_t)ncpn : 0};
-    const int nraw = (int)(sizeof(raw_bytes) / sizeof(raw_bytes[0]));
+    std::vector<const void *> rp(raw_ptrs, raw_ptrs + sizeof(raw_ptrs) / sizeof(raw_ptrs[0]));
+    std::vector<size_t> rb(raw_bytes, raw_bytes + sizeof(raw_bytes) / sizeof(raw_bytes[0]));
+    if (three) {
+        const void *p3[] = {t3->p2b_cop, t3->p2b_dop, t3->n2b_cop, t3->n2b_dop, t3->p3b_isd, t3->p3b_fsd, t3->p3b_op,
+                            t3->p3b_phase, t3->n3b_isd, t3->n3b_fsd, t3->n3b_op, t3->n3b_phase, t3->hmatppp,
+                            t3->hmatnnn, t3->cppntriplet, t3->dppntriplet, t3->cpnntriplet, t3->dpnntriplet};
+        const size_t nt_p = (size_t)npp3 * ld, nt_n = (size_t)nnp3 * ld_p;
+        const size_t b3[] = {4 * (size_t)t->np2b, 4 * (size_t)t->np2b, 4 * (size_t)t->nn2b, 4 * (size_t)t->nn2b,
+                             8 * (size_t)t3->np3b, 8 * (size_t)t3->np3b, 4 * (size_t)t3->np3b, (size_t)t3->np3b,
+                             8 * (size_t)t3->nn3b, 8 * (size_t)t3->nn3b, 4 * (size_t)t3->nn3b, (size_t)t3->nn3b,
+                             4 * (size_t)t3->nmatppp, 4 * (size_t)t3->nmatnnn, 4 * nt_p, 4 * nt_p, 4 * nt_n, 4 * nt_n};
+        rp.insert(rp.end(), p3, p3 + sizeof(p3) / sizeof(p3[0]));
+        rb.insert(rb.end(), b3, b3 + sizeof(b3) / sizeof(b3[0]));
+    }
+    const int nraw = (int)rb.size();
     ctx->raw.resize(nraw);
     int64_t jb = 0;
     for (int i = 0; i < nraw && !st; ++i) {
-        st = up(ctx->raw[i], raw_ptrs[i], raw_bytes[i]);
-        jb += (int64_t)raw_bytes[i];
+        const size_t bytes = rp[i] ? rb[i] : 0;   // an unused table (e.g. p2b_op of a three-body run)
+        st = up(ctx->raw[i], rp[i], bytes);
+        jb += (int64_t)bytes;
     }
     if (st) return st;
     ctx->stats.jump_bytes = jb;
-    // hmatpn doubles as raw table and kernel operand
-    if ((st = up(ctx->hmatpn, t->hmatpn, 4 * (size_t)t->nmatpn))) return st;
-    ctx->stats.jump_bytes += 4 * t->nmatpn;
+    // hmatpn doubles as raw table and kernel operand; a three-body context
+    // appends hmatppn and hmatpnn (the PPN / PNN blocks of the cpn table)
+    {
+        std::vector<float> hpn(t->hmatpn ? t->hmatpn : nullptr, t->hmatpn ? t->hmatpn + t->nmatpn : nullptr);
+        if (three) {
+            if (t3->nmatppn) hpn.insert(hpn.end(), t3->hmatppn, t3->hmatppn + t3->nmatppn);
+            if (t3->nmatpnn) hpn.insert(hpn.end(), t3->hmatpnn, t3->hmatpnn + t3->nmatpnn);
+        }
+        if ((st = up(ctx->hmatpn, hpn.data(), 4 * hpn.size()))) return st;
+        ctx->stats.jump_bytes += 4 * (int64_t)hpn.size();
+    }
+    std::vector<float> hnn_all(t->hmatnn ? t->hmatnn : nullptr, t->hmatnn ? t->hmatnn + t->nmatnn : nullptr);
+    if (three && t3->nmatnnn) hnn_all.insert(hnn_all.end(), t3->hmatnnn, t3->hmatnnn + t3->nmatnnn);
     std::vector<float> nspe(t->nsd_n, 0.0f);
     if (t->call_spe && t->nspe_h) std::copy(t->nspe_h, t->nspe_h + t->nsd_n, nspe.begin());
     if ((st = up(ctx->row_off, row_off.data(), 8 * row_off.size())) ||
@@ -646,7 +925,7 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
         (st = up(ctx->nnrec_ph, nnrec_ph_all.data(), nnrec_ph_all.size())) ||
         (st = up(ctx->pp_ph, ctx->h_pp_ph.data(), ctx->h_pp_ph.size())) ||
         (st = up(ctx->hmatpp_d, t->hmatpp, 4 * (size_t)t->nmatpp)) ||
-        (st = up(ctx->hmatnn_d, t->hmatnn, 4 * (size_t)t->nmatnn)))
+        (st = up(ctx->hmatnn_d, hnn_all.data(), 4 * hnn_all.size())))
         return st;
     ctx->stats.derived_bytes = (int64_t)(8 * row_off.size() + 4 * (ctx->h_pp_ptr.size() * 3 + spe_ptr.size()) +
                                          sizeof(PPContrib) * ctx->h_pp.size() + sizeof(NNContrib) * ctx->h_nn.size() +
@@ -690,7 +969,7 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, bool do_upload = true) {
     a.dpn = (const int32_t *)ctx->dpn.p;
     a.nspe = (const float *)ctx->nspe.p;
     a.ld_cpn = ld;
-    a.ncpn = (int32_t)ncpn;
+    a.ncpn = (int32_t)cpn32.size();
     return BSG_OK;
 }
 
@@ -738,7 +1017,10 @@ int bsg_last_error(const bsg_ctx *ctx, char *buf, size_t len) {
     return BSG_OK;
 }
 
-int bsg_create(const bsg_tables *t, const bsg_config *cfg, bsg_ctx **out) {
+}  // extern "C"
+
+namespace {
+int create_ctx(const bsg_tables *t, const bsg_tables3 *t3, const bsg_config *cfg, bsg_ctx **out) {
     if (!out) return BSG_ERR_ARG;
     *out = nullptr;
     if (!t) return BSG_ERR_ARG;
@@ -754,7 +1036,7 @@ int bsg_create(const bsg_tables *t, const bsg_config *cfg, bsg_ctx **out) {
         ctx->t = *t;
         ctx->dim = t->dimbasis;
         try {
-            st = derive(ctx, t);
+            st = derive(ctx, t, t3);
         } catch (const std::bad_alloc &) {
             st = set_err(ctx, BSG_ERR_NOMEM, "host allocation failed while deriving row layouts");
         }
@@ -769,8 +1051,23 @@ int bsg_create(const bsg_tables *t, const bsg_config *cfg, bsg_ctx **out) {
     *out = ctx;
     return BSG_OK;
 }
+}  // namespace
 
-int bsg_validate_tables(const bsg_tables *t, char *msg, size_t len) {
+extern "C" {
+
+int bsg_create(const bsg_tables *t, const bsg_config *cfg, bsg_ctx **out) { return create_ctx(t, nullptr, cfg, out); }
+
+int bsg_create3(const bsg_tables *t, const bsg_tables3 *t3, const bsg_config *cfg, bsg_ctx **out) {
+    if (!t3) {
+        if (out) *out = nullptr;
+        return BSG_ERR_ARG;
+    }
+    return create_ctx(t, t3, cfg, out);
+}
+
+int bsg_validate_tables(const bsg_tables *t, char *msg, size_t len) { return bsg_validate_tables3(t, nullptr, msg, len); }
+
+int bsg_validate_tables3(const bsg_tables *t, const bsg_tables3 *t3, char *msg, size_t len) {
     if (msg && len) msg[0] = 0;
     if (!t) return BSG_ERR_ARG;
     bsg_ctx *ctx = new (std::nothrow) bsg_ctx();
@@ -779,7 +1076,7 @@ int bsg_validate_tables(const bsg_tables *t, char *msg, size_t len) {
     ctx->dim = t->dimbasis;
     int st;
     try {
-        st = derive(ctx, t, false);
+        st = derive(ctx, t, t3, false);
     } catch (const std::bad_alloc &) {
         st = set_err(ctx, BSG_ERR_NOMEM, "host allocation failed while validating");
     }

@@ -27,14 +27,18 @@ struct PPContrib {
     int32_t pad;
 };
 // PN row contribution: out[row][pos] += sum over neutron-op records r at pos of
-//   hmatpn(cpn(r.b,a)+dpn(r.d,c)) * php * r.ph * in[q_off + r.in]
+//   hmat(cpn[r.b + aoff] + dpn[r.d + coff]) * php * r.ph * in[q_off + r.in]
+// The same form carries the three-body PPN and PNN terms: cpn / dpn / hmat
+// on the device are the concatenation of the PN, PPN and PNN tables, and
+// aoff / coff select the column of the proton side's label in its table
+// (PN: proton s.p. a; PPN: proton pair bb; PNN: proton s.p. a with the
+// neutron pair as the row).
 struct PNContrib {
     int64_t q_off;
     int32_t nop;       // neutron operator id
-    int16_t acol;      // (a + nhsps(-1)) column of cpnpair
-    int16_t ccol;      // (c + nhsps(-1)) column of dpnpair
+    int32_t aoff;      // column offset of the created proton label in cpn
+    int32_t coff;      // column offset of the destroyed proton label in dpn
     float php;         // proton jump phase
-    int32_t pad;
 };
 // NN row contribution: out[row][pos] += sum over records r at pos of r.me * in[row + r.in]
 struct NNContrib {
@@ -69,9 +73,10 @@ struct PNRec {
     int8_t ph;
     int8_t pad;
 };
-// distinct (b,d) pair of a PN neutron operator: rows of cpnpair/dpnpair
+// distinct (b,d) label pair of a PN neutron operator: rows of the cpn/dpn
+// tables (a neutron s.p. label b + nhsps(-2), or for PNN a neutron pair - 1)
 struct BDPair {
-    uint8_t b, d;       // b + nhsps(-2), d + nhsps(-2)
+    uint16_t b, d;
 };
 // NN record: input position and hmatnn(op)*phase
 struct NNRec {
@@ -137,6 +142,7 @@ struct bsg_ctx {
     cudaStream_t stream = nullptr;
     std::string last_error;
     int last_status = 0;      // status of the last set_err
+    bool threebody = false;   // built by bsg_create3 (SPE + PPP/NNN/PPN/PNN)
     bsg_tables t{};           // sizes only (pointers are host-owned by caller)
     int64_t dim = 0, nrows = 0;
     int32_t max_rowlen = 0;

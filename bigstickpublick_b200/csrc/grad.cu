@@ -54,6 +54,9 @@ int grad_many(bsg_ctx *const *ctxs, int nsys, const double *const *evecs, int ns
         return code;
     };
     if (nsys < 1 || nstates < 1 || !evecs || !dpp || !dnn || !dpn) return fail(BSG_ERR_ARG, "null argument");
+    for (int i = 0; i < nsys; ++i)
+        if (ctxs[i]->threebody)
+            return fail(BSG_ERR_UNSUPPORTED, "the adjoint covers two-body contexts only (hmatpp, hmatnn, hmatpn)");
     // per (system, state): psi offset, accumulator offsets; per system: sizes
     std::vector<int64_t> psi_off(nsys), acc_off((size_t)nsys * nstates);
     std::vector<int64_t> nlab(nsys);

@@ -134,12 +134,11 @@ __device__ __forceinline__ void grad_tile(const RowArgs &a, const GradArgs &g, c
                 __syncwarp();
             }
         }
-        const int acol = pc.acol * a.ld_cpn, ccol = pc.ccol * a.ld_cpn;
         for (int k = lane; k < op.nbd; k += 32) {
             const double v = Aw[k];
             if (v != 0.0) {
                 const BDPair bd = a.bd[op.bd_base + k];
-                const int idx = a.cpn[bd.b + acol] + a.dpn[bd.d + ccol];
+                const int idx = a.cpn[bd.b + pc.aoff] + a.dpn[bd.d + pc.coff];
                 fix_add(g.pn + 2 * (size_t)(idx - 1), (double)pc.php * v);
             }
         }

@@ -40,7 +40,11 @@ def validate_tables(tables):
     lib = _abi.gpu_lib()
     t = tables.as_ctypes()
     buf = C.create_string_buffer(512)
-    st = lib.bsg_validate_tables(C.byref(t), buf, 512)
+    t3 = tables.as_ctypes3() if getattr(tables, "threebody", False) else None
+    if t3 is not None:
+        st = lib.bsg_validate_tables3(C.byref(t), C.byref(t3), buf, 512)
+    else:
+        st = lib.bsg_validate_tables(C.byref(t), buf, 512)
     return st, buf.value.decode()
 
 
@@ -51,7 +55,12 @@ class Hamiltonian:
         self._ct = tables.as_ctypes()
         cfg = _abi.BsgConfig(device, max_nb, 1 if validate else 0, 0)
         h = C.c_void_p()
-        st = self.lib.bsg_create(C.byref(self._ct), C.byref(cfg), C.byref(h))
+        # a three-body Hamiltonian (model.build_tables3) goes through bsg_create3
+        self._ct3 = tables.as_ctypes3() if getattr(tables, "threebody", False) else None
+        if self._ct3 is not None:
+            st = self.lib.bsg_create3(C.byref(self._ct), C.byref(self._ct3), C.byref(cfg), C.byref(h))
+        else:
+            st = self.lib.bsg_create(C.byref(self._ct), C.byref(cfg), C.byref(h))
         if st != 0:
             raise BsgError(st, "bsg_create failed (see stderr for the validator message)")
         self.h = h

@@ -34,6 +34,7 @@
 #include "bsg_host.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -304,6 +305,13 @@ struct Jumps2 {
     std::vector<int32_t> op;
     std::vector<int8_t> phase;
 };
+// two-body jumps of a three-body run: created / destroyed pair labels
+// (src/bjumplib_weld.f90:771-775)
+struct Jumps2P {
+    std::vector<int64_t> isd, fsd;
+    std::vector<int32_t> cop, dop;
+    std::vector<int8_t> phase;
+};
 
 inline int signed_label(const SpeciesBasis &sb, int q) { return q < sb.nl ? -(q + 1) : (q - sb.nl + 1); }
 
@@ -321,6 +329,22 @@ inline int phase2(uint64_t bits, int i, int j, int k, int l) {
     uint64_t b = bits & ~(1ull << k);
     p += nbelow(b, l);
     b &= ~(1ull << l);
+    p += nbelow(b, j);
+    b |= (1ull << j);
+    p += nbelow(b, i);
+    return (p & 1) ? -1 : 1;
+}
+
+// a^+_i a^+_j a^+_k a_n a_m a_l |s> with i<j<k, l<m<n
+inline int phase3(uint64_t bits, int i, int j, int k, int l, int m, int n) {
+    int p = nbelow(bits, l);
+    uint64_t b = bits & ~(1ull << l);
+    p += nbelow(b, m);
+    b &= ~(1ull << m);
+    p += nbelow(b, n);
+    b &= ~(1ull << n);
+    p += nbelow(b, k);
+    b |= (1ull << k);
     p += nbelow(b, j);
     b |= (1ull << j);
     p += nbelow(b, i);
@@ -460,6 +484,111 @@ void make_pn_pairs(const SpeciesBasis &pb, const SpeciesBasis &nb, Pairs &P) {
     P.make_dense(nsp, nsn);
 }
 
+// --------------------------------------------------------- triplets --------
+// Three-particle states of one kind in (M, parity) sections, as the
+// reference's XXX3 / XXY lists (src/b3bmelib2.f90:430-560):
+//  XXX: s.p. states q1<q2<q3 of one species, ordered by M, parity, then the
+//       colex index C(q3,3)+C(q2,2)+q1 -- the index weld3b forms before
+//       mapPPP / mapNNN (src/bjumplib_weld.f90:1108-1126); triangle-packed
+//       labels per section as the pairs (:1149-1155);
+//  XXY: a pair of species X (1-based pair label) and a s.p. state of
+//       species Y, ordered by M, parity, pair, s.p. state; square sections
+//       addressed by cXXYtriplet(pair, y) = start + (pos-1)*n and
+//       dXXYtriplet = pos (assign_XXY_maps, src/b3bmelib2.f90:500-545).
+struct Trips {
+    std::vector<std::array<int, 3>> list;   // XXX: q1, q2, q3 ; XXY: pair, qy, 0
+    std::vector<int> sec;                   // section of each sorted triplet
+    std::vector<int64_t> sec_first, sec_n, sec_mestart;  // first: 1-based
+    std::vector<int32_t> dense;             // XXX: colex -> 1-based sorted; XXY: (pair-1)*nsy + qy -> 1-based
+    std::vector<std::vector<int32_t>> by_sec;  // sorted indices (1-based) per section
+    int nsy = 0;
+    int64_t nmat = 0;
+};
+inline int64_t colex3(int a, int b, int c) {  // a < b < c, 0-based
+    return (int64_t)c * (c - 1) * (c - 2) / 6 + (int64_t)b * (b - 1) / 2 + a;
+}
+template <typename Tmp>
+void sections_of(std::vector<Tmp> &v, Trips &T, bool square) {
+    T.list.clear(); T.sec.clear(); T.sec_first.clear(); T.sec_n.clear(); T.sec_mestart.clear(); T.by_sec.clear();
+    int64_t nme = 0;
+    auto close = [&]() {
+        if (T.sec_n.empty()) return;
+        const int64_t n = T.sec_n.back();
+        nme += square ? n * n : n * (n + 1) / 2;
+    };
+    for (size_t i = 0; i < v.size(); ++i) {
+        if (i == 0 || v[i].m2 != v[i - 1].m2 || v[i].pidx != v[i - 1].pidx) {
+            close();
+            T.sec_first.push_back((int64_t)i + 1);
+            T.sec_n.push_back(0);
+            T.sec_mestart.push_back(nme);
+            T.by_sec.emplace_back();
+        }
+        T.sec_n.back() += 1;
+        T.list.push_back(v[i].key);
+        T.sec.push_back((int)T.sec_n.size() - 1);
+        T.by_sec.back().push_back((int32_t)i + 1);
+    }
+    close();
+    T.nmat = nme;
+}
+void make_xxx(const SpeciesBasis &sb, Trips &T) {
+    const int ns = sb.nl + sb.nr;
+    struct Tmp { std::array<int, 3> key; int m2, pidx; int64_t cx; };
+    std::vector<Tmp> v;
+    for (int c = 2; c < ns; ++c)
+        for (int b = 1; b < c; ++b)
+            for (int a = 0; a < b; ++a)
+                v.push_back({{a, b, c}, sb.q_m2[a] + sb.q_m2[b] + sb.q_m2[c],
+                             pidx_of(sb.q_par[a] * sb.q_par[b] * sb.q_par[c]), colex3(a, b, c)});
+    std::stable_sort(v.begin(), v.end(), [](const Tmp &x, const Tmp &y) {
+        if (x.m2 != y.m2) return x.m2 < y.m2;
+        if (x.pidx != y.pidx) return x.pidx < y.pidx;
+        return x.cx < y.cx;
+    });
+    sections_of(v, T, false);
+    T.dense.assign(ns >= 3 ? (size_t)colex3(ns - 3, ns - 2, ns - 1) + 1 : 0, 0);
+    for (size_t i = 0; i < v.size(); ++i) T.dense[v[i].cx] = (int32_t)i + 1;
+}
+void make_xxy(const Pairs &PX, const SpeciesBasis &sy, Trips &T) {
+    const int nsy = sy.nl + sy.nr;
+    struct Tmp { std::array<int, 3> key; int m2, pidx; };
+    std::vector<Tmp> v;
+    for (size_t bb = 1; bb <= PX.list.size(); ++bb)
+        for (int q = 0; q < nsy; ++q)
+            v.push_back({{(int)bb, q, 0}, 2 * PX.M[bb - 1] + sy.q_m2[q],
+                         pidx_of(par_of_idx(PX.pidx[bb - 1]) * sy.q_par[q])});
+    std::stable_sort(v.begin(), v.end(), [](const Tmp &x, const Tmp &y) {
+        if (x.m2 != y.m2) return x.m2 < y.m2;
+        return x.pidx < y.pidx;
+    });
+    sections_of(v, T, true);
+    T.nsy = nsy;
+    T.dense.assign(PX.list.size() * (size_t)nsy, 0);
+    for (size_t i = 0; i < v.size(); ++i) T.dense[(size_t)(v[i].key[0] - 1) * nsy + v[i].key[1]] = (int32_t)i + 1;
+}
+// label of sorted triplets c, d (1-based, same section) in a triangle section
+inline int64_t xxx_label(const Trips &T, int64_t c, int64_t d) {
+    const int s = T.sec[c - 1];
+    const int64_t iref = T.sec_first[s] - 1, istart = T.sec_mestart[s];
+    const int64_t hi = std::max(c, d), lo = std::min(c, d);
+    return istart + (hi - iref) * (hi - iref - 1) / 2 + lo - iref;
+}
+// the seeded three-body part R(T, T') (bsg_host.h)
+inline uint64_t mix64(uint64_t x) {
+    uint64_t z = x + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+double r3(uint64_t seed, int kind, std::array<int, 3> k1, std::array<int, 3> k2) {
+    if (k2 < k1) std::swap(k1, k2);
+    uint64_t x = mix64(seed ^ (uint64_t)kind);
+    for (int v : k1) x = mix64(x ^ (uint64_t)v);
+    for (int v : k2) x = mix64(x ^ (uint64_t)v);
+    return (double)(x >> 11) * 0x1.0p-52 - 1.0;
+}
+
 // ------------------------------------------------------------ sort ---------
 // sort1bjumps / sort1bjumps_ins (src/bsortjumpslib.f90:190-290): shell sort
 // with a fixed stride table, key = `key`, carried = the rest.
@@ -518,6 +647,17 @@ struct Built {
     std::vector<std::vector<std::pair<int, double>>> jac_pp, jac_nn, jac_pn;
     std::vector<std::vector<std::pair<int, double>>> jspe_pp, jspe_nn, jspe_pn;
     int ntbme = 0, norb = 0;
+    // uncoupled two-body interaction in double, without the folded s.p.
+    // energies and without the diagonal halving: vxx[0] pp, vxx[1] nn by
+    // triangle label, vpn by square label
+    std::vector<double> vxx[2], vpn;
+    // three-body run (bsg_host_build3)
+    bool three = false;
+    Jumps2P p2x, n2x;                 // two-body jumps with pair labels (PPN protons, PNN neutrons)
+    Jumps2 p3, n3;                    // three-body jumps inside a sector
+    std::vector<float> hmatppp, hmatnnn, hmatppn, hmatpnn;
+    std::vector<int32_t> cppn, dppn, cpnn, dpnn;
+    bsg_tables3 t3{};
 };
 
 // coupled matrix element table with per-line provenance for the jacobian
@@ -591,8 +731,10 @@ void compress(std::vector<std::pair<int, double>> &v) {
     v.resize(out);
 }
 
-int build(const bsg_model_spec *s, Built &B) {
+int build(const bsg_model_spec *s, const bsg_model3_spec *s3, Built &B) {
     init_lfact();
+    const bool three = (s3 != nullptr);
+    B.three = three;
     if (!s || s->norb <= 0 || !s->orbits) { g_err = "bad model spec"; return BSG_ERR_ARG; }
     if (s->np < 0 || s->nn < 0) { g_err = "negative particle number"; return BSG_ERR_ARG; }
     B.norb = s->norb;
@@ -712,7 +854,9 @@ int build(const bsg_model_spec *s, Built &B) {
     I.finalize();
     const double vscale = s->tbme_scale;
     const int A = s->np + s->nn;
-    const bool call_spe = (A <= 1);
+    // a three-body run keeps the s.p. energies as SPE bundles
+    const bool call_spe = (A <= 1) || three;
+    if (three && A < 3) { g_err = "a three-body run needs at least three valence particles"; return BSG_ERR_ARG; }
     const double afac = (A > 1) ? 1.0 / (double)(A - 1) : 0.0;
     std::vector<double> spe(s->norb, 0.0);
     for (int i = 0; i < s->norb; ++i) spe[i] = s->spe ? s->spe_scale * s->spe[i] : 0.0;
@@ -729,7 +873,8 @@ int build(const bsg_model_spec *s, Built &B) {
         H.assign(P.nmat, 0.0f);
         jac.assign(P.nmat, {});
         jspe.assign(P.nmat, {});
-        if (sb.N < 2) continue;
+        B.vxx[it].assign(P.nmat, 0.0);
+        if (sb.N < 2 && !three) continue;
         for (size_t s_ = 0; s_ < P.sec_n.size(); ++s_) {
             const int64_t first = P.sec_first[s_], n = P.sec_n[s_];
             for (int64_t c = first; c < first + n; ++c)
@@ -751,6 +896,7 @@ int build(const bsg_model_spec *s, Built &B) {
                         const double w = zab * zcd * cgab * cgcd * vscale;
                         v += w * coupled_with_prov(I, a, b, cc, dd, J, 1, w, &pv);
                     }
+                    B.vxx[it][lab - 1] = v;
                     std::vector<std::pair<int, double>> ps;
                     if (c == d) {  // SPE folded into the diagonal pair (bsppot.f90:83-106)
                         v += afac * (spe[a] + spe[b]);
@@ -779,7 +925,8 @@ int build(const bsg_model_spec *s, Built &B) {
         B.hmatpn.assign(P.nmat, 0.0f);
         B.jac_pn.assign(P.nmat, {});
         B.jspe_pn.assign(P.nmat, {});
-        const bool have_pn = (s->np >= 1 && s->nn >= 1);
+        B.vpn.assign(P.nmat, 0.0);
+        const bool have_pn = (s->np >= 1 && s->nn >= 1) || three;
         for (size_t s_ = 0; s_ < P.sec_n.size(); ++s_) {
             const int64_t first = P.sec_first[s_], n = P.sec_n[s_], nme = P.sec_mestart[s_];
             for (int64_t pos = 1; pos <= n; ++pos) {
@@ -818,6 +965,7 @@ int build(const bsg_model_spec *s, Built &B) {
                         const double w = 0.5 * zab * zcd * cgab * cgcd * vscale;
                         for (int T = 0; T <= 1; ++T) v += w * coupled_with_prov(I, a, b, c, d, J, T, w, &pv);
                     }
+                    B.vpn[lab - 1] = v;
                     std::vector<std::pair<int, double>> ps;
                     if (cpos == dpos) {  // SPE folded into pn (bsppot.f90:185-226)
                         v += afac * (spe[a] + spe[b]);
@@ -949,7 +1097,7 @@ int build(const bsg_model_spec *s, Built &B) {
             }
             B.p1sj.push_back(sj);
         }
-    if (s->np >= 2) {
+    if (s->np >= 2 && !three) {
         const auto by_sec = pairs_by_section(B.pb, B.ppairs);
         for (int is = 0; is < nps; ++is) {
             SectJump sj;
@@ -959,7 +1107,7 @@ int build(const bsg_model_spec *s, Built &B) {
             if (sj.njumps > 0) B.p2sj.push_back(sj);
         }
     }
-    if (s->nn >= 2) {
+    if (s->nn >= 2 && !three) {
         const auto by_sec = pairs_by_section(B.nb, B.npairs);
         for (int is = 0; is < nns; ++is) {
             SectJump sj;
@@ -968,6 +1116,265 @@ int build(const bsg_model_spec *s, Built &B) {
             sj.njumps = gen2(B.nb, B.nstart, B.npairs, by_sec, is, is, B.n2);
             if (sj.njumps > 0) B.n2sj.push_back(sj);
         }
+    }
+
+    // ---- three-body run: triplet tables, matrix elements and jumps
+    std::vector<SectJump> p3sj, n3sj, p2xsj, n2xsj;
+    std::vector<int> p2x_n1;      // neutron one-body sector jump of each PPN sector jump
+    std::vector<int> pnn_p1, pnn_n2x;  // PNN: proton one-body / neutron two-body sector jumps
+    if (three) {
+        Trips Tppp, Tnnn, Tppn, Tpnn;
+        make_xxx(B.pb, Tppp);
+        make_xxx(B.nb, Tnnn);
+        make_xxy(B.ppairs, B.nb, Tppn);
+        make_xxy(B.npairs, B.pb, Tpnn);
+        const double w2 = s3->w2 / (double)(A - 2), w3 = s3->w3;
+        const uint64_t seed = s3->seed;
+        // uncoupled two-body interaction between pair labels / pn labels
+        auto vxx = [&](int it, int64_t c, int64_t d) -> double {
+            const Pairs &P = it == 0 ? B.ppairs : B.npairs;
+            if (P.pair_sec[c - 1] != P.pair_sec[d - 1]) return 0.0;
+            return B.vxx[it][xx_label(P, c, d) - 1];
+        };
+        auto vpn = [&](int qp, int qn, int qpp, int qnn) -> double {
+            const Pairs &P = B.pnpairs;
+            const int64_t c = P.at(qp, qn), d = P.at(qpp, qnn);
+            const int sc = P.pair_sec[c - 1];
+            if (sc != P.pair_sec[d - 1]) return 0.0;
+            const int64_t first = P.sec_first[sc], n = P.sec_n[sc];
+            return B.vpn[P.sec_mestart[sc] + (c - first) * n + (d - first + 1) - 1];
+        };
+        auto bit = [](int q) { return 1ull << q; };
+        // <T| V_xx |T'> between three-particle states of one species
+        auto v3xxx = [&](int it, const std::array<int, 3> &T, const std::array<int, 3> &U) -> double {
+            const Pairs &P = it == 0 ? B.ppairs : B.npairs;
+            const uint64_t bu = bit(U[0]) | bit(U[1]) | bit(U[2]);
+            const uint64_t bt = bit(T[0]) | bit(T[1]) | bit(T[2]);
+            double v = 0.0;
+            for (int z : U) {
+                if (!(bt >> z & 1ull)) continue;     // spectator z in both
+                int x = -1, y = -1, i = -1, j = -1;
+                for (int q : U) if (q != z) { if (x < 0) x = q; else y = q; }
+                for (int q : T) if (q != z) { if (i < 0) i = q; else j = q; }
+                v += vxx(it, P.at(i, j), P.at(x, y)) * phase2(bu, i, j, x, y);
+            }
+            return v;
+        };
+        // <(XX pair bb, y a)| V |(XX pair dd, y c)>: V_xx on the pair with y a
+        // spectator, plus V_pn moving one X particle and the y particle
+        auto v3xxy = [&](int itx, int bb, int a, int dd, int c) -> double {
+            const Pairs &P = itx == 0 ? B.ppairs : B.npairs;
+            double v = (a == c) ? vxx(itx, bb, dd) : 0.0;
+            const int i = P.list[bb - 1].first, j = P.list[bb - 1].second;
+            const int l = P.list[dd - 1].first, m = P.list[dd - 1].second;
+            const uint64_t bd = bit(l) | bit(m), bc = bit(i) | bit(j);
+            for (int pd : {l, m}) {
+                const int z = (pd == l) ? m : l;     // X spectator
+                if (!(bc >> z & 1ull)) continue;
+                const int pc = (z == i) ? j : i;
+                const double x = itx == 0 ? vpn(pc, a, pd, c) : vpn(a, pc, c, pd);
+                if (x != 0.0) v += x * phase1(bd, pc, pd);
+            }
+            return v;
+        };
+        // ---- matrix elements: triangle sections (XXX), square sections (XXY)
+        auto fill_xxx = [&](int it, const Trips &T, std::vector<float> &H) {
+            H.assign(T.nmat, 0.0f);
+            const int kind = it == 0 ? 1 : 2;
+            for (size_t sc = 0; sc < T.sec_n.size(); ++sc) {
+                const int64_t first = T.sec_first[sc], n = T.sec_n[sc];
+                for (int64_t c = first; c < first + n; ++c)
+                    for (int64_t d = first; d <= c; ++d) {
+                        const auto &tc = T.list[c - 1], &td = T.list[d - 1];
+                        double w = w2 * v3xxx(it, tc, td) + w3 * r3(seed, kind, tc, td);
+                        if (c == d) w *= 0.5;    // applied by both 'f' and 'b'
+                        H[xxx_label(T, c, d) - 1] = (float)w;
+                    }
+            }
+        };
+        auto fill_xxy = [&](int itx, const Trips &T, std::vector<float> &H, std::vector<int32_t> &ct,
+                            std::vector<int32_t> &dt) {
+            const SpeciesBasis &sy = itx == 0 ? B.nb : B.pb;
+            const Pairs &P = itx == 0 ? B.ppairs : B.npairs;
+            const int64_t npr = (int64_t)P.list.size(), ldy = sy.nl + sy.nr + 1;
+            H.assign(T.nmat, 0.0f);
+            ct.assign((size_t)(npr * ldy), -1);
+            dt.assign((size_t)(npr * ldy), -1);
+            const int kind = itx == 0 ? 3 : 4;
+            auto key = [&](const std::array<int, 3> &t) -> std::array<int, 3> {
+                const auto &pr = P.list[t[0] - 1];
+                return itx == 0 ? std::array<int, 3>{pr.first, pr.second, t[1]}
+                                : std::array<int, 3>{t[1], pr.first, pr.second};
+            };
+            for (size_t sc = 0; sc < T.sec_n.size(); ++sc) {
+                const int64_t first = T.sec_first[sc], n = T.sec_n[sc], nme = T.sec_mestart[sc];
+                for (int64_t pos = 1; pos <= n; ++pos) {
+                    const auto &t = T.list[first + pos - 2];
+                    const int64_t at = (int64_t)(t[0] - 1) + (int64_t)(signed_label(sy, t[1]) + sy.nl) * npr;
+                    ct[at] = (int32_t)(nme + (pos - 1) * n);
+                    dt[at] = (int32_t)pos;
+                }
+                for (int64_t cp = 1; cp <= n; ++cp)
+                    for (int64_t dp = 1; dp <= n; ++dp) {
+                        const auto &tc = T.list[first + cp - 2], &td = T.list[first + dp - 2];
+                        double w = w2 * v3xxy(itx, tc[0], tc[1], td[0], td[1]) + w3 * r3(seed, kind, key(tc), key(td));
+                        if (tc[0] == td[0]) w *= 0.5;   // equal pairs: the X jump is diagonal
+                        H[nme + (cp - 1) * n + dp - 1] = (float)w;
+                    }
+            }
+        };
+        fill_xxx(0, Tppp, B.hmatppp);
+        fill_xxx(1, Tnnn, B.hmatnnn);
+        fill_xxy(0, Tppn, B.hmatppn, B.cppn, B.dppn);
+        fill_xxy(1, Tpnn, B.hmatpnn, B.cpnn, B.dpnn);
+
+        // ---- three-body jumps inside a sector (weld3b,
+        // src/bjumplib_weld.f90:819-1208): SD, destroyed triplet, created
+        // triplet of the same section; isd >= fsd
+        auto gen3 = [&](SpeciesBasis &sb, const std::vector<int64_t> &xstart, const Trips &T, int is, Jumps2 &J) {
+            int64_t cnt = 0;
+            const Sector &S = sb.sectors[is];
+            const int ns = sb.nl + sb.nr;
+            std::vector<int> occ;
+            for (int64_t sd = S.xsdstart - 1; sd < S.xsdend; ++sd) {
+                const uint64_t bits = sb.sd_bits[sd];
+                occ.clear();
+                for (int q = 0; q < ns; ++q)
+                    if (bits >> q & 1ull) occ.push_back(q);
+                for (size_t x = 0; x < occ.size(); ++x)
+                    for (size_t y = x + 1; y < occ.size(); ++y)
+                        for (size_t z = y + 1; z < occ.size(); ++z) {
+                            const int l = occ[x], m = occ[y], n = occ[z];
+                            const uint64_t rest = bits & ~(bit(l) | bit(m) | bit(n));
+                            const int64_t d = T.dense[colex3(l, m, n)];
+                            for (int32_t c : T.by_sec[T.sec[d - 1]]) {
+                                const auto &tc = T.list[c - 1];
+                                if ((rest >> tc[0] & 1ull) || (rest >> tc[1] & 1ull) || (rest >> tc[2] & 1ull)) continue;
+                                const int64_t f = sb.find_sd(rest | bit(tc[0]) | bit(tc[1]) | bit(tc[2]));
+                                if (f < 0 || sb.sd_sector[f] != is) continue;
+                                if (sd < f) continue;
+                                J.isd.push_back(xstart[sd]);
+                                J.fsd.push_back(xstart[f]);
+                                J.op.push_back((int32_t)xxx_label(T, c, d));
+                                J.phase.push_back((int8_t)phase3(bits, tc[0], tc[1], tc[2], l, m, n));
+                                ++cnt;
+                            }
+                        }
+            }
+            return cnt;
+        };
+        // ---- two-body jumps with pair labels out of one sector, bucketed by
+        // final sector (SD, destroyed pair, created pair); the diagonal bucket
+        // keeps isd >= fsd
+        std::map<std::pair<const SpeciesBasis *, int>, std::vector<Jumps2P>> jumps2_from;
+        auto gen2x = [&](SpeciesBasis &sb, const std::vector<int64_t> &xstart, const Pairs &P, int is, int fs,
+                         Jumps2P &J) -> int64_t {
+            auto k = std::make_pair((const SpeciesBasis *)&sb, is);
+            auto it = jumps2_from.find(k);
+            if (it == jumps2_from.end()) {
+                std::vector<Jumps2P> by(sb.sectors.size());
+                const Sector &S = sb.sectors[is];
+                const int ns = sb.nl + sb.nr;
+                std::vector<int> occ;
+                for (int64_t sd = S.xsdstart - 1; sd < S.xsdend; ++sd) {
+                    const uint64_t bits = sb.sd_bits[sd];
+                    occ.clear();
+                    for (int q = 0; q < ns; ++q)
+                        if (bits >> q & 1ull) occ.push_back(q);
+                    for (size_t x = 0; x < occ.size(); ++x)
+                        for (size_t y = x + 1; y < occ.size(); ++y) {
+                            const int kq = occ[x], lq = occ[y];
+                            const uint64_t rest = bits & ~(bit(kq) | bit(lq));
+                            const int64_t dpair = P.at(kq, lq);
+                            for (size_t c = 1; c <= P.list.size(); ++c) {
+                                const int i = P.list[c - 1].first, j = P.list[c - 1].second;
+                                if ((rest >> i & 1ull) || (rest >> j & 1ull)) continue;
+                                const int64_t f = sb.find_sd(rest | bit(i) | bit(j));
+                                if (f < 0) continue;
+                                const int fsec = sb.sd_sector[f];
+                                if (fsec == is && sd < f) continue;
+                                Jumps2P &Bk = by[fsec];
+                                Bk.isd.push_back(xstart[sd]);
+                                Bk.fsd.push_back(xstart[f]);
+                                Bk.cop.push_back((int32_t)c);
+                                Bk.dop.push_back((int32_t)dpair);
+                                Bk.phase.push_back((int8_t)phase2(bits, i, j, kq, lq));
+                            }
+                        }
+                }
+                it = jumps2_from.emplace(k, std::move(by)).first;
+            }
+            const Jumps2P &src = it->second[fs];
+            J.isd.insert(J.isd.end(), src.isd.begin(), src.isd.end());
+            J.fsd.insert(J.fsd.end(), src.fsd.begin(), src.fsd.end());
+            J.cop.insert(J.cop.end(), src.cop.begin(), src.cop.end());
+            J.dop.insert(J.dop.end(), src.dop.begin(), src.dop.end());
+            J.phase.insert(J.phase.end(), src.phase.begin(), src.phase.end());
+            return (int64_t)src.isd.size();
+        };
+        if (s->np >= 3)
+            for (int is = 0; is < nps; ++is) {
+                SectJump sj{is, is, (int64_t)B.p3.isd.size(), 0, true};
+                sj.njumps = gen3(B.pb, B.pstart, Tppp, is, B.p3);
+                if (sj.njumps > 0) p3sj.push_back(sj);
+            }
+        if (s->nn >= 3)
+            for (int in = 0; in < nns; ++in) {
+                SectJump sj{in, in, (int64_t)B.n3.isd.size(), 0, true};
+                sj.njumps = gen3(B.nb, B.nstart, Tnnn, in, B.n3);
+                if (sj.njumps > 0) n3sj.push_back(sj);
+            }
+        // PPN: proton two-body sector jumps is -> fs (is >= fs) with the
+        // conjugate neutron one-body sector jump
+        if (s->np >= 2 && s->nn >= 1)
+            for (int is = 0; is < nps; ++is)
+                for (int fs = 0; fs <= is; ++fs) {
+                    Jumps2P tmp;
+                    if (gen2x(B.pb, B.pstart, B.ppairs, is, fs, tmp) == 0) continue;
+                    const int in = pconj[is], fn = pconj[fs];
+                    int y;
+                    if (n1sj_of.count({in, fn})) {
+                        y = n1sj_of[{in, fn}];
+                    } else {
+                        SectJump nj{in, fn, (int64_t)B.n1.isd.size(), 0, in == fn};
+                        nj.njumps = gen1(B.nb, B.nstart, in, fn, B.n1);
+                        y = (int)B.n1sj.size();
+                        n1sj_of[{in, fn}] = y;
+                        B.n1sj.push_back(nj);
+                    }
+                    if (B.n1sj[y].njumps == 0) continue;
+                    SectJump sj{is, fs, (int64_t)B.p2x.isd.size(), (int64_t)tmp.isd.size(), is == fs};
+                    B.p2x.isd.insert(B.p2x.isd.end(), tmp.isd.begin(), tmp.isd.end());
+                    B.p2x.fsd.insert(B.p2x.fsd.end(), tmp.fsd.begin(), tmp.fsd.end());
+                    B.p2x.cop.insert(B.p2x.cop.end(), tmp.cop.begin(), tmp.cop.end());
+                    B.p2x.dop.insert(B.p2x.dop.end(), tmp.dop.begin(), tmp.dop.end());
+                    B.p2x.phase.insert(B.p2x.phase.end(), tmp.phase.begin(), tmp.phase.end());
+                    p2xsj.push_back(sj);
+                    p2x_n1.push_back(y);
+                }
+        // PNN: proton one-body sector jumps (those of the PN set-up) with the
+        // conjugate neutron two-body sector jump
+        if (s->np >= 1 && s->nn >= 2) {
+            std::map<std::pair<int, int>, int> n2x_of;
+            for (size_t x = 0; x < B.p1sj.size(); ++x) {
+                const int in = pconj[B.p1sj[x].is], fn = pconj[B.p1sj[x].fs];
+                int y;
+                if (n2x_of.count({in, fn})) {
+                    y = n2x_of[{in, fn}];
+                } else {
+                    SectJump nj{in, fn, (int64_t)B.n2x.isd.size(), 0, in == fn};
+                    nj.njumps = gen2x(B.nb, B.nstart, B.npairs, in, fn, B.n2x);
+                    y = (int)n2xsj.size();
+                    n2x_of[{in, fn}] = y;
+                    n2xsj.push_back(nj);
+                }
+                if (n2xsj[y].njumps == 0) continue;
+                pnn_p1.push_back((int)x);
+                pnn_n2x.push_back(y);
+            }
+        }
+        B.t3.npairs_p = (int32_t)B.ppairs.list.size();
+        B.t3.npairs_n = (int32_t)B.npairs.list.size();
     }
 
     // ---- one-body density jumps (set1bsectorjumps + master1bodyjumps for
@@ -1076,13 +1483,41 @@ int build(const bsg_model_spec *s, Built &B) {
             const Sector &ns = B.nb.sectors[pconj[is]];
             add(BSG_OP_SPE, BSG_H_HERM, ps.xsdstart, ps.xsdend, ns.xsdstart, ns.xsdend);
         }
-    emit("PP", BSG_H_FWD);
-    emit("NN", BSG_H_FWD);
-    emit("PN", BSG_H_FWD);
-    emit("PN", BSG_H_HERM);
-    emit("PP", BSG_H_BWD);
-    emit("NN", BSG_H_BWD);
-    emit("PN", BSG_H_BWD);
+    if (!three) {
+        emit("PP", BSG_H_FWD);
+        emit("NN", BSG_H_FWD);
+        emit("PN", BSG_H_FWD);
+        emit("PN", BSG_H_HERM);
+        emit("PP", BSG_H_BWD);
+        emit("NN", BSG_H_BWD);
+        emit("PN", BSG_H_BWD);
+    } else {
+        // applyHbundled_g's three-body order (src/bapplyhlib1.f90:160-235):
+        // PPP f/b, PPN f/b, PNN f/b, NNN f/b
+        for (int hc : {BSG_H_FWD, BSG_H_BWD})
+            for (const SectJump &sj : p3sj) {
+                const Sector &ns = B.nb.sectors[pconj[sj.is]];
+                add(BSG_OP_PPP, hc, sj.nstart + 1, sj.nstart + sj.njumps, ns.xsdstart, ns.xsdend);
+            }
+        for (int hc : {BSG_H_FWD, BSG_H_BWD})
+            for (size_t x = 0; x < p2xsj.size(); ++x) {
+                const SectJump &nj = B.n1sj[p2x_n1[x]];
+                add(BSG_OP_PPN, hc, p2xsj[x].nstart + 1, p2xsj[x].nstart + p2xsj[x].njumps, nj.nstart + 1,
+                    nj.nstart + nj.njumps);
+            }
+        for (int hc : {BSG_H_FWD, BSG_H_BWD})
+            for (size_t x = 0; x < pnn_p1.size(); ++x) {
+                const SectJump &pj = B.p1sj[pnn_p1[x]], &nj = n2xsj[pnn_n2x[x]];
+                add(BSG_OP_PNN, hc, pj.nstart + 1, pj.nstart + pj.njumps, nj.nstart + 1, nj.nstart + nj.njumps);
+            }
+        for (int hc : {BSG_H_FWD, BSG_H_BWD})
+            for (int is = 0; is < nps; ++is)
+                for (const SectJump &nj : n3sj) {
+                    if (nj.is != pconj[is]) continue;
+                    const Sector &ps = B.pb.sectors[is];
+                    add(BSG_OP_NNN, hc, ps.xsdstart, ps.xsdend, nj.nstart + 1, nj.nstart + nj.njumps);
+                }
+    }
 
     // ---- sort_bundled_jumps (src/bsortjumpslib.f90:21-175): per PN bundle,
     // protons on fsd, neutrons on isd
@@ -1121,14 +1556,16 @@ extern "C" {
 
 const char *bsg_host_last_error(void) { return g_err.c_str(); }
 
-int bsg_host_build(const bsg_model_spec *spec, bsg_host_tables **out) {
+int bsg_host_build(const bsg_model_spec *spec, bsg_host_tables **out) { return bsg_host_build3(spec, nullptr, out); }
+
+int bsg_host_build3(const bsg_model_spec *spec, const bsg_model3_spec *s3, bsg_host_tables **out) {
     if (!out) { g_err = "null output"; return BSG_ERR_ARG; }
     *out = nullptr;
     Built *B = new (std::nothrow) Built();
     if (!B) { g_err = "host allocation failed"; return BSG_ERR_NOMEM; }
     int st;
     try {
-        st = build(spec, *B);
+        st = build(spec, s3, *B);
     } catch (const std::bad_alloc &) {
         g_err = "host allocation failed";
         st = BSG_ERR_NOMEM;
@@ -1205,6 +1642,31 @@ int bsg_host_build(const bsg_model_spec *spec, bsg_host_tables **out) {
     d.pxstart = ptr_or_null(B->d_pxstart); d.pxend = ptr_or_null(B->d_pxend);
     d.nxstart = ptr_or_null(B->d_nxstart); d.nxend = ptr_or_null(B->d_nxend);
     d.cstride = ptr_or_null(B->d_cstride);
+    if (B->three) {
+        // two-body jumps carry pair labels (no p2b_op / n2b_op)
+        t.np2b = (int64_t)B->p2x.isd.size();
+        t.p2b_isd = ptr_or_null(B->p2x.isd); t.p2b_fsd = ptr_or_null(B->p2x.fsd);
+        t.p2b_op = nullptr; t.p2b_phase = ptr_or_null(B->p2x.phase);
+        t.nn2b = (int64_t)B->n2x.isd.size();
+        t.n2b_isd = ptr_or_null(B->n2x.isd); t.n2b_fsd = ptr_or_null(B->n2x.fsd);
+        t.n2b_op = nullptr; t.n2b_phase = ptr_or_null(B->n2x.phase);
+        bsg_tables3 &u = B->t3;
+        u.p2b_cop = ptr_or_null(B->p2x.cop); u.p2b_dop = ptr_or_null(B->p2x.dop);
+        u.n2b_cop = ptr_or_null(B->n2x.cop); u.n2b_dop = ptr_or_null(B->n2x.dop);
+        u.np3b = (int64_t)B->p3.isd.size();
+        u.p3b_isd = ptr_or_null(B->p3.isd); u.p3b_fsd = ptr_or_null(B->p3.fsd);
+        u.p3b_op = ptr_or_null(B->p3.op); u.p3b_phase = ptr_or_null(B->p3.phase);
+        u.nn3b = (int64_t)B->n3.isd.size();
+        u.n3b_isd = ptr_or_null(B->n3.isd); u.n3b_fsd = ptr_or_null(B->n3.fsd);
+        u.n3b_op = ptr_or_null(B->n3.op); u.n3b_phase = ptr_or_null(B->n3.phase);
+        u.nmatppp = (int64_t)B->hmatppp.size(); u.hmatppp = ptr_or_null(B->hmatppp);
+        u.nmatnnn = (int64_t)B->hmatnnn.size(); u.hmatnnn = ptr_or_null(B->hmatnnn);
+        u.nmatppn = (int64_t)B->hmatppn.size(); u.hmatppn = ptr_or_null(B->hmatppn);
+        u.nmatpnn = (int64_t)B->hmatpnn.size(); u.hmatpnn = ptr_or_null(B->hmatpnn);
+        u.cppntriplet = ptr_or_null(B->cppn); u.dppntriplet = ptr_or_null(B->dppn);
+        u.cpnntriplet = ptr_or_null(B->cpnn); u.dpnntriplet = ptr_or_null(B->dpnn);
+        h->t3 = &B->t3;
+    }
     h->priv = B;
     *out = h;
     return BSG_OK;

@@ -190,6 +190,16 @@ _DENSITY_FIELDS = [
     ("pxstart", "i8", "nbundles"), ("pxend", "i8", "nbundles"), ("nxstart", "i8", "nbundles"),
     ("nxend", "i8", "nbundles"), ("cstride", "i8", "nbundles"),
 ]
+# three-body arrays (bsg_tables3): name, dtype, length field (None: computed)
+_TABLE3_FIELDS = [
+    ("p2b_cop", "i4", "np2b"), ("p2b_dop", "i4", "np2b"), ("n2b_cop", "i4", "nn2b"), ("n2b_dop", "i4", "nn2b"),
+    ("p3b_isd", "i8", "np3b"), ("p3b_fsd", "i8", "np3b"), ("p3b_op", "i4", "np3b"), ("p3b_phase", "i1", "np3b"),
+    ("n3b_isd", "i8", "nn3b"), ("n3b_fsd", "i8", "nn3b"), ("n3b_op", "i4", "nn3b"), ("n3b_phase", "i1", "nn3b"),
+    ("hmatppp", "f4", "nmatppp"), ("hmatnnn", "f4", "nmatnnn"), ("hmatppn", "f4", "nmatppn"),
+    ("hmatpnn", "f4", "nmatpnn"),
+    ("cppntriplet", "i4", None), ("dppntriplet", "i4", None), ("cpnntriplet", "i4", None),
+    ("dpnntriplet", "i4", None),
+]
 _CTYPES = {"i1": C.c_int8, "i2": C.c_int16, "i4": C.c_int32, "i8": C.c_int64,
            "f4": C.c_float, "f8": C.c_double, "u8": C.c_uint64}
 
@@ -207,11 +217,33 @@ class Tables:
     ``as_ctypes()`` returns a ``bsg_tables`` view whose pointers reference
     these arrays (kept alive by this object)."""
 
-    def __init__(self, arrays, scalars, extra):
+    def __init__(self, arrays, scalars, extra, arrays3=None, scalars3=None):
         self.a = arrays
         self.s = scalars
         self.extra = extra
+        # three-body run (build_tables3): the bsg_tables3 arrays and sizes
+        self.a3 = arrays3
+        self.s3 = scalars3
         self._c = None
+        self._c3 = None
+
+    @property
+    def threebody(self):
+        return self.a3 is not None
+
+    def as_ctypes3(self):
+        """``bsg_tables3`` view of the three-body arrays (None for a
+        two-body Hamiltonian)."""
+        if self.a3 is None:
+            return None
+        t = _abi.BsgTables3()
+        for k, v in self.s3.items():
+            setattr(t, k, v)
+        for name, dt, _ in _TABLE3_FIELDS:
+            arr = self.a3.get(name)
+            setattr(t, name, None if arr is None or arr.size == 0 else arr.ctypes.data_as(C.POINTER(_CTYPES[dt])))
+        self._c3 = t
+        return t
 
     @property
     def dim(self):
@@ -245,8 +277,18 @@ class Tables:
         return t
 
 
-def build_tables(spec: ModelSpec) -> Tables:
-    """Run the host-side table builder (libbsghost.so) and copy its arrays."""
+def build_tables3(spec: ModelSpec, w2=1.0, w3=0.0, seed=0) -> Tables:
+    """Three-body tables (bsg_host_build3): SPE plus PPP / PPN / PNN / NNN
+    bundles with W = w2 * V2 / (A - 2) + w3 * R, V2 the two-body
+    interaction of `spec` between three-particle states and R the seeded
+    symmetric part of the builder (uniform in [-1, 1)).  With w3 = 0 the
+    Hamiltonian equals the two-body one of `spec`."""
+    return build_tables(spec, three=(w2, w3, seed))
+
+
+def build_tables(spec: ModelSpec, three=None) -> Tables:
+    """Run the host-side table builder (libbsghost.so) and copy its arrays.
+    three: (w2, w3, seed) for a three-body build (build_tables3)."""
     lib = _abi.host_lib()
     orbs = (_abi.BsgOrbit * len(spec.orbits))(*[_abi.BsgOrbit(*o) for o in spec.orbits])
     tb = (_abi.BsgTbme * max(1, len(spec.tbme)))()
@@ -256,7 +298,11 @@ def build_tables(spec: ModelSpec) -> Tables:
     ms = _abi.BsgModelSpec(len(spec.orbits), orbs, spec.np_, spec.nn, spec.jz2, spec.parity,
                            len(spec.tbme), tb, spe, spec.spe_scale, spec.tbme_scale)
     hp = C.POINTER(_abi.BsgHostTables)()
-    st = lib.bsg_host_build(C.byref(ms), C.byref(hp))
+    if three is None:
+        st = lib.bsg_host_build(C.byref(ms), C.byref(hp))
+    else:
+        s3 = _abi.BsgModel3Spec(float(three[0]), float(three[1]), int(three[2]) & ((1 << 64) - 1))
+        st = lib.bsg_host_build3(C.byref(ms), C.byref(s3), C.byref(hp))
     if st != 0:
         raise RuntimeError(f"bsg_host_build: {_abi.STATUS_NAMES.get(st, st)}: "
                            f"{lib.bsg_host_last_error().decode()}")
@@ -269,6 +315,18 @@ def build_tables(spec: ModelSpec) -> Tables:
         arrs = {}
         for name, dt, nfield in _TABLE_FIELDS:
             arrs[name] = _np_from(getattr(t, name), scal[nfield], dt)
+        arrs3 = scal3 = None
+        if three is not None:
+            u = h.t3.contents
+            scal3 = {k: getattr(u, k) for k in ("np3b", "nn3b", "nmatppp", "nmatnnn", "nmatppn", "nmatpnn",
+                                                "npairs_p", "npairs_n")}
+            lens = dict(scal3, np2b=t.np2b, nn2b=t.nn2b)
+            ntp = u.npairs_p * (t.nhsps_nl + t.nhsps_nr + 1)
+            ntn = u.npairs_n * (t.nhsps_pl + t.nhsps_pr + 1)
+            arrs3 = {}
+            for name, dt, nfield in _TABLE3_FIELDS:
+                n = lens[nfield] if nfield else (ntp if "ppn" in name else ntn)
+                arrs3[name] = _np_from(getattr(u, name), n, dt)
         ncp = (t.nhsps_nl + t.nhsps_nr + 1) * (t.nhsps_pl + t.nhsps_pr + 1)
         arrs["cpnpair"] = _np_from(t.cpnpair, ncp, "i8")
         arrs["dpnpair"] = _np_from(t.dpnpair, ncp, "i8")
@@ -311,7 +369,7 @@ def build_tables(spec: ModelSpec) -> Tables:
         extra["spec"] = spec
     finally:
         lib.bsg_host_free(hp)
-    return Tables(arrs, scal, extra)
+    return Tables(arrs, scal, extra, arrs3, scal3)
 
 
 def build_tables_many(specs, threads=None):

@@ -155,8 +155,58 @@ typedef struct bsg_report {
     double  t_total_ms;
 } bsg_report;
 
+/* ---- three-body opbundles (src/bapplyhlib1.f90:1390-2804) ---- */
+#define BSG_OP_PPP 7   /* p3b jumps px, conjugate neutron SDs nx (as PP)       */
+#define BSG_OP_NNN 8   /* proton SDs px (cstride), n3b jumps nx (as NN)        */
+#define BSG_OP_PPN 9   /* p2b jumps px (pair labels), n1b jumps nx             */
+#define BSG_OP_PNN 10  /* p1b jumps px, n2b jumps nx (pair labels)             */
+
+/*
+ * The arrays a three-body run adds (src/bmodules_3body.f90:26-103).  In such
+ * a run the two-body jumps carry the labels of their created (cop) and
+ * destroyed (dop) pair instead of a matrix-element label
+ * (src/bjumplib_weld.f90:771-775): bsg_tables' p2b_op / n2b_op are unused
+ * and the pair labels come from here.  Pair labels are 1-based indices of
+ * the species' pair list (XX2(it)%pair).
+ *   PPP: out(p3b_fsd + nstart(csd)) += hmatppp(p3b_op) * p3b_phase * in(p3b_isd + nstart(csd))
+ *   NNN: out(n3b_fsd + pstart(csd)) += hmatnnn(n3b_op) * n3b_phase * in(...)
+ *   PPN: xme = hmatppn(cppntriplet(bb,a) + dppntriplet(dd,c)) * phasep * phasen,
+ *        bb/dd = p2b cop/dop, a/c = n1b cop/dop (src/bapplyhlib1.f90:2295-2562)
+ *   PNN: xme = hmatpnn(cpnntriplet(bb,a) + dpnntriplet(dd,c)) * phasep * phasen,
+ *        a/c = p1b cop/dop, bb/dd = n2b cop/dop (src/bapplyhlib1.f90:2033-2285)
+ * 'f' bundles add out(statef) += xme*in(statei), 'b' bundles the transpose.
+ * cppntriplet / dppntriplet are column-major [npairs_p x (nhsps_nl+nhsps_nr+1)]
+ * as the reference's cppntriplet(npairs, -nhsps(-2):nhsps(2)): entry (bb, a)
+ * at (bb-1) + (a + nhsps_nl)*npairs_p.  cpnntriplet / dpnntriplet likewise
+ * [npairs_n x (nhsps_pl+nhsps_pr+1)], (bb, a) at (bb-1) + (a + nhsps_pl)*npairs_n.
+ */
+typedef struct bsg_tables3 {
+    const int32_t *p2b_cop, *p2b_dop;   /* [np2b] created / destroyed proton pair */
+    const int32_t *n2b_cop, *n2b_dop;   /* [nn2b]                                 */
+    int64_t np3b;
+    const int64_t *p3b_isd, *p3b_fsd;   /* pstart values                          */
+    const int32_t *p3b_op;              /* 1-based hmatppp label                  */
+    const int8_t  *p3b_phase;
+    int64_t nn3b;
+    const int64_t *n3b_isd, *n3b_fsd;   /* nstart values                          */
+    const int32_t *n3b_op;              /* 1-based hmatnnn label                  */
+    const int8_t  *n3b_phase;
+    int64_t nmatppp, nmatnnn, nmatppn, nmatpnn;
+    const float *hmatppp, *hmatnnn, *hmatppn, *hmatpnn;
+    int32_t npairs_p, npairs_n;
+    const int32_t *cppntriplet, *dppntriplet;
+    const int32_t *cpnntriplet, *dpnntriplet;
+} bsg_tables3;
+
 /* ---- lifecycle ---- */
 int  bsg_create(const bsg_tables *t, const bsg_config *cfg, bsg_ctx **out);
+/* a three-body Hamiltonian: the bundles of t are applied as
+ * applyHbundled_g does with threebody set (src/bapplyhlib1.f90:56-310): SPE,
+ * PPP, PPN, PNN and NNN; PP, NN and PN bundles are skipped.  bsg_grad is
+ * not available on such a context (BSG_ERR_UNSUPPORTED). */
+int  bsg_create3(const bsg_tables *t, const bsg_tables3 *t3, const bsg_config *cfg, bsg_ctx **out);
+/* bsg_validate_tables for a three-body run (t3 may be NULL: two-body) */
+int  bsg_validate_tables3(const bsg_tables *t, const bsg_tables3 *t3, char *msg, size_t len);
 int  bsg_destroy(bsg_ctx *ctx);
 /* the validator bsg_create runs, on the host only (no GPU needed): every
  * index of every table checked against its array (the reference's own checks
@@ -357,6 +407,8 @@ typedef struct bsg_stats {
     int32_t reserved2;
     double  apply1b_ms;        /* last bsg_apply1b: device time of its kernels */
     double  grad_ms;           /* last bsg_grad: device time of its kernels    */
+    /* three-body contexts: inner-loop updates per matvec of each kind */
+    int64_t n_ops_ppp, n_ops_nnn, n_ops_ppn, n_ops_pnn;
 } bsg_stats;
 int  bsg_get_stats(const bsg_ctx *ctx, bsg_stats *st);
 

@@ -79,9 +79,37 @@ typedef struct bsg_host_tables {
     /* one-body density jumps and P1B/N1B bundles for bsg_density1b
      * (master1bodyjumps for densities, src/bdenslib1.f90:190-213) */
     bsg_density_tables dt;
+    /* three-body arrays (bsg_host_build3), NULL for a two-body build */
+    const bsg_tables3 *t3;
 } bsg_host_tables;
 
 int  bsg_host_build(const bsg_model_spec *spec, bsg_host_tables **out);
+
+/* A three-body Hamiltonian for bsg_create3: SPE bundles (pspe_h / nspe_h)
+ * plus PPP, PPN, PNN and NNN bundles, no two-body bundles, as a BIGSTICK run
+ * with three-body forces is laid out (src/bapplyhlib1.f90:56-310).  The
+ * uncoupled three-body matrix elements are
+ *   W(T, T') = w2 * <T| V2 |T'> / (A - 2) + w3 * R(T, T'),
+ * where <T|V2|T'> is the two-body interaction of spec between three-particle
+ * states (the reference converts two-body into three-body matrix elements
+ * the same way, src/b3from2bme.f90; on A-particle states the w2 term alone is
+ * exactly V2), and R a seeded symmetric part, uniform in [-1, 1), that keeps
+ * M and parity: for the triplet keys kT, kT' (sorted combined s.p. labels q
+ * of the builder's order -- PPP (p,p,p) kind 1, NNN (n,n,n) kind 2, PPN
+ * (p,p,n) kind 3, PNN (p,n,n) kind 4) with lo <= hi in lexicographic order,
+ *   x = seed; for v in (kind, lo..., hi...): x = mix(x ^ v);
+ *   R = (x >> 11) * 2^-52 - 1,
+ * mix the SplitMix64 finalizer of (x + 0x9E3779B97F4A7C15).  Two-body jumps
+ * carry pair labels (t3->p2b_cop/dop), hmat of a diagonal label (T == T',
+ * or equal pairs bb == dd for PPN / PNN) is halved since 'f' and 'b'
+ * bundles both apply it, and three-body jumps inside a sector keep
+ * isd >= fsd (src/bjumplib_weld.f90:1072-1076).  Needs A >= 3. */
+typedef struct bsg_model3_spec {
+    double w2;
+    double w3;
+    uint64_t seed;
+} bsg_model3_spec;
+int  bsg_host_build3(const bsg_model_spec *spec, const bsg_model3_spec *s3, bsg_host_tables **out);
 void bsg_host_free(bsg_host_tables *h);
 const char *bsg_host_last_error(void);
 

@@ -5,7 +5,8 @@ this package, as the checker.  The product (bigstickpublick_b200) never
 imports, links or calls it.
 
 * liboracle.so (oracle_applyh.c): plain-C restatement of BIGSTICK's
-  applyHbundled_omp / applyHbundled_block_omp loops; its owner-computes
+  applyHbundled_omp / applyHbundled_block_omp loops, and of the three-body
+  bundle loops (applyhPPP/PPN/PNN/NNNbundled_g); its owner-computes
   OpenMP partition (each thread the output rows getLoadDist gives it), used
   as the timed CPU baseline and, restricted to a few rows, as the checker of
   large systems; and the serial-path split routines of applyHbundled_g.
@@ -53,6 +54,10 @@ def lib():
         L.oracle_applyh_owner.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
                                           C.c_void_p, C.c_int]
         L.oracle_applyh_owner.restype = C.c_int
+        L.oracle_applyh3.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]
+        L.oracle_applyh3.restype = C.c_int
+        L.oracle_count_ops3.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+        L.oracle_count_ops3.restype = None
         _LIB = L
     return _LIB
 
@@ -70,10 +75,22 @@ def applyh(tables, vin, nb=1, accumulate_into=None):
     prec = 4 if vin.dtype == np.float32 else 8
     out = np.zeros_like(vin) if accumulate_into is None else accumulate_into
     p, keep = _tp(tables)
-    st = lib().oracle_applyh(p, vin.ctypes.data, out.ctypes.data, nb, prec)
+    if getattr(tables, "threebody", False):
+        t3 = tables.as_ctypes3()
+        st = lib().oracle_applyh3(p, C.cast(C.pointer(t3), C.c_void_p), vin.ctypes.data, out.ctypes.data, nb, prec)
+    else:
+        st = lib().oracle_applyh(p, vin.ctypes.data, out.ctypes.data, nb, prec)
     if st != 0:
         raise RuntimeError(f"oracle_applyh status {st}")
     return out
+
+
+def count_ops3(tables):
+    """(ppp, nnn, ppn, pnn) inner-loop updates per matvec of a three-body run."""
+    ops = (C.c_int64 * 4)()
+    p, keep = _tp(tables)
+    lib().oracle_count_ops3(p, ops)
+    return tuple(int(x) for x in ops)
 
 
 def applyh_omp(tables, vin, nb=1, nthreads=None, out=None):

@@ -129,6 +129,126 @@ int oracle_applyh(const bsg_tables *t, const void *vin, void *vout, int nb, int 
     return BSG_OK;
 }
 
+/* ------------------------------------------------------ three-body ---- */
+/* The serial bundle loops of a three-body run (applyHbundled_g with
+ * threebody set, src/bapplyhlib1.f90:160-235; block forms
+ * src/bapplyhblocklib.f90:741-1541):
+ *   PPP  applyhPPPbundled_g   (src/bapplyhlib1.f90:1390-1572)
+ *   NNN  applyhNNNbundled_g   (:1579-1756)
+ *   PNN  applyhPNNbundled_g   (:2033-2285)
+ *   PPN  applyhPPNbundled_g   (:2295-2562)
+ * xme real(4) = hmat * phase(s), vout(statef) += xme * vin(statei) for 'f',
+ * the transpose for 'b'. */
+#define TRIP(tab, np_, lab, sp, nl) ((tab)[(int64_t)((lab) - 1) + (int64_t)((sp) + (nl)) * (int64_t)(np_)])
+#define DEFINE_BUNDLE3(T, NAME)                                                          \
+static void NAME(const bsg_tables *t, const bsg_tables3 *u, int64_t ib, const T *vin,      \
+                 T *vout, int nb) {                                                      \
+    const int op = t->optype[ib];                                                        \
+    const int hc = t->hchar[ib];                                                         \
+    const int64_t px0 = t->pxstart[ib], px1 = t->pxend[ib];                              \
+    const int64_t nx0 = t->nxstart[ib], nx1 = t->nxend[ib];                              \
+    const int64_t cs = t->cstride[ib] > 0 ? t->cstride[ib] : 1;                          \
+    if (op == BSG_OP_PPP) {                                                              \
+        const int64_t *s1 = hc == 'b' ? u->p3b_fsd : u->p3b_isd;                         \
+        const int64_t *s2 = hc == 'b' ? u->p3b_isd : u->p3b_fsd;                         \
+        for (int64_t csd = nx0; csd <= nx1; csd += cs) {                                 \
+            const int64_t nsd = t->nstart[csd - 1];                                      \
+            for (int64_t x = px0; x <= px1; ++x) {                                       \
+                float xme = u->hmatppp[u->p3b_op[x - 1] - 1];                            \
+                xme = xme * (float)u->p3b_phase[x - 1];                                  \
+                const int64_t si = s1[x - 1] + nsd, sf = s2[x - 1] + nsd;                \
+                for (int v = 0; v < nb; ++v)                                             \
+                    vout[(sf - 1) * nb + v] += (T)xme * vin[(si - 1) * nb + v];          \
+            }                                                                            \
+        }                                                                                \
+    } else if (op == BSG_OP_NNN) {                                                       \
+        const int64_t *s1 = hc == 'b' ? u->n3b_fsd : u->n3b_isd;                         \
+        const int64_t *s2 = hc == 'b' ? u->n3b_isd : u->n3b_fsd;                         \
+        for (int64_t csd = px0; csd <= px1; csd += cs) {                                 \
+            const int64_t psd = t->pstart[csd - 1];                                      \
+            for (int64_t x = nx0; x <= nx1; ++x) {                                       \
+                float xme = u->hmatnnn[u->n3b_op[x - 1] - 1];                            \
+                xme = xme * (float)u->n3b_phase[x - 1];                                  \
+                const int64_t si = s1[x - 1] + psd, sf = s2[x - 1] + psd;                \
+                for (int v = 0; v < nb; ++v)                                             \
+                    vout[(sf - 1) * nb + v] += (T)xme * vin[(si - 1) * nb + v];          \
+            }                                                                            \
+        }                                                                                \
+    } else if (op == BSG_OP_PPN || op == BSG_OP_PNN) {                                   \
+        const int ppn = (op == BSG_OP_PPN);                                              \
+        for (int64_t pj = px0; pj <= px1; ++pj) {                                        \
+            const int64_t psdi = ppn ? t->p2b_isd[pj - 1] : t->p1b_isd[pj - 1];          \
+            const int64_t psdf = ppn ? t->p2b_fsd[pj - 1] : t->p1b_fsd[pj - 1];          \
+            const int phasep = ppn ? t->p2b_phase[pj - 1] : t->p1b_phase[pj - 1];        \
+            const int pc = ppn ? u->p2b_cop[pj - 1] : t->p1b_cop[pj - 1];                \
+            const int pd = ppn ? u->p2b_dop[pj - 1] : t->p1b_dop[pj - 1];                \
+            for (int64_t nj = nx0; nj <= nx1; ++nj) {                                    \
+                const int phasen = ppn ? t->n1b_phase[nj - 1] : t->n2b_phase[nj - 1];    \
+                const int nc = ppn ? t->n1b_cop[nj - 1] : u->n2b_cop[nj - 1];            \
+                const int nd = ppn ? t->n1b_dop[nj - 1] : u->n2b_dop[nj - 1];            \
+                int64_t lab;                                                             \
+                if (ppn)                                                                 \
+                    lab = (int64_t)TRIP(u->cppntriplet, u->npairs_p, pc, nc, t->nhsps_nl) + \
+                          TRIP(u->dppntriplet, u->npairs_p, pd, nd, t->nhsps_nl);        \
+                else                                                                     \
+                    lab = (int64_t)TRIP(u->cpnntriplet, u->npairs_n, nc, pc, t->nhsps_pl) + \
+                          TRIP(u->dpnntriplet, u->npairs_n, nd, pd, t->nhsps_pl);        \
+                float xme = ppn ? u->hmatppn[lab - 1] : u->hmatpnn[lab - 1];             \
+                xme = xme * (float)phasep * (float)phasen;                               \
+                const int64_t nsdi = ppn ? t->n1b_isd[nj - 1] : t->n2b_isd[nj - 1];      \
+                const int64_t nsdf = ppn ? t->n1b_fsd[nj - 1] : t->n2b_fsd[nj - 1];      \
+                const int64_t si = nsdi + psdi, sf = nsdf + psdf;                        \
+                if (hc != 'b') {                                                         \
+                    for (int v = 0; v < nb; ++v)                                         \
+                        vout[(sf - 1) * nb + v] += (T)xme * vin[(si - 1) * nb + v];      \
+                } else {                                                                 \
+                    for (int v = 0; v < nb; ++v)                                         \
+                        vout[(si - 1) * nb + v] += (T)xme * vin[(sf - 1) * nb + v];      \
+                }                                                                        \
+            }                                                                            \
+        }                                                                                \
+    }                                                                                    \
+}
+
+DEFINE_BUNDLE3(float, bundle3_f32)
+DEFINE_BUNDLE3(double, bundle3_f64)
+
+/* vout += H vin for a three-body run: SPE and the three-body bundles, PP /
+ * NN / PN bundles skipped (src/bapplyhlib1.f90:107-235) */
+int oracle_applyh3(const bsg_tables *t, const bsg_tables3 *u, const void *vin, void *vout, int nb, int prec) {
+    if (!t || !u || !vin || !vout || nb < 1) return BSG_ERR_ARG;
+    for (int64_t ib = 0; ib < t->nbundles; ++ib) {
+        const int op = t->optype[ib];
+        if (op == BSG_OP_PP || op == BSG_OP_NN || op == BSG_OP_PN) continue;
+        if (op == BSG_OP_SPE) {
+            if (prec == BSG_PREC_FP32)
+                bundle_f32(t, ib, (const float *)vin, (float *)vout, nb);
+            else
+                bundle_f64(t, ib, (const double *)vin, (double *)vout, nb);
+        } else if (prec == BSG_PREC_FP32) {
+            bundle3_f32(t, u, ib, (const float *)vin, (float *)vout, nb);
+        } else {
+            bundle3_f64(t, u, ib, (const double *)vin, (double *)vout, nb);
+        }
+    }
+    return BSG_OK;
+}
+
+/* inner-loop updates of each three-body kind: ops[0..3] = PPP, NNN, PPN, PNN */
+void oracle_count_ops3(const bsg_tables *t, int64_t *ops) {
+    for (int k = 0; k < 4; ++k) ops[k] = 0;
+    for (int64_t ib = 0; ib < t->nbundles; ++ib) {
+        const int op = t->optype[ib];
+        const int64_t np_ = t->pxend[ib] - t->pxstart[ib] + 1, nn_ = t->nxend[ib] - t->nxstart[ib] + 1;
+        const int64_t cs = t->cstride[ib] > 0 ? t->cstride[ib] : 1;
+        if (np_ <= 0 || nn_ <= 0) continue;
+        if (op == BSG_OP_PPP) ops[0] += np_ * ((nn_ + cs - 1) / cs);
+        else if (op == BSG_OP_NNN) ops[1] += ((np_ + cs - 1) / cs) * nn_;
+        else if (op == BSG_OP_PPN) ops[2] += np_ * nn_;
+        else if (op == BSG_OP_PNN) ops[3] += np_ * nn_;
+    }
+}
+
 /* ----------------------------------------------------------- OpenMP ---- */
 /* chunk boundaries of [lo, hi] (1-based, inclusive) into at most nthr pieces,
  * each cut moved forward until key[] changes (src/bsortjumpslib.f90:491-713

@@ -41,14 +41,16 @@ def test_host_builder_exports_every_declared_symbol():
 
 def test_struct_sizes_match_c(tmp_path):
     src = tmp_path / "sz.c"
-    src.write_text('#include "bsg_host.h"\n#include <stdio.h>\nint main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu\\n",'
+    src.write_text('#include "bsg_host.h"\n#include <stdio.h>\nint main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n",'
                    'sizeof(bsg_tables),sizeof(bsg_config),sizeof(bsg_lanczos_params),sizeof(bsg_report),'
-                   'sizeof(bsg_stats),sizeof(bsg_model_spec),sizeof(bsg_host_tables),sizeof(bsg_tbme));}\n')
+                   'sizeof(bsg_stats),sizeof(bsg_model_spec),sizeof(bsg_host_tables),sizeof(bsg_tbme),'
+                   'sizeof(bsg_tables3),sizeof(bsg_model3_spec));}\n')
     exe = tmp_path / "sz"
     subprocess.check_call(["gcc", "-I" + os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
     c_sizes = [int(x) for x in subprocess.check_output([str(exe)]).split()]
     py = [C.sizeof(s) for s in (_abi.BsgTables, _abi.BsgConfig, _abi.BsgLanczosParams, _abi.BsgReport,
-                               _abi.BsgStats, _abi.BsgModelSpec, _abi.BsgHostTables, _abi.BsgTbme)]
+                               _abi.BsgStats, _abi.BsgModelSpec, _abi.BsgHostTables, _abi.BsgTbme,
+                               _abi.BsgTables3, _abi.BsgModel3Spec)]
     assert c_sizes == py
 
 
@@ -68,7 +70,7 @@ def test_validator_accepts_builder_tables(tables):
     ("n2b_isd", 0, 10 ** 6, 1, "n2b isd/fsd"),
     ("pstart", 1, 0, 1, "pstart"),
     ("hchar", 0, ord("x"), 1, "hchar"),
-    ("optype", 0, 9, 1, "optype"),
+    ("optype", 0, 99, 1, "optype"),
 ])
 def test_validator_rejects_corrupted_tables(tables, field, index, value, status, needle):
     tables.a[field] = tables.a[field].copy()
