@@ -19,8 +19,9 @@ Legs beside the headline (rank 0): Lanczos on sd 6p6n (FP64 against mixed),
 time to a 1e-6 solution on pf 4p4n (FP64 scalar against mixed scalar and
 mixed block nb = 8), the 256-system batch with its gradients, the pf 6p6n
 thick-restart solve (mixed against FP64 on the same schedule) with the
-ground-state gradient, one-body densities; each reports its eigenvalue and
-wavefunction-overlap error against FP64.
+ground-state gradient, one-body densities, and a three-body Hamiltonian
+(pf 4p4n, PPP/PPN/PNN/NNN bundles); each reports its eigenvalue and
+wavefunction-overlap error against FP64 where it solves.
 
 `--impl reference` times the reference's CPU algorithm for this path on the
 host cores: the reference is Fortran and no Fortran compiler exists in this
@@ -493,6 +494,93 @@ def batch_leg(args):
         b.close()
 
 
+def threebody_leg(args):
+    """Three-body Hamiltonian (PPP / PPN / PNN / NNN bundles,
+    src/bapplyhlib1.f90:1390-2804): pf 4p4n, 2Jz = 0 (dim 1,963,461), the
+    seeded pf interaction (seed 5) in three-body form, W = V2/(A-2), plus a
+    seeded three-body part 0.1 MeV * R.  FP32 and FP64 applyH timed alone
+    (256 MiB written before each launch); hermiticity <u|Hv> = <v|Hu> in
+    FP64; the same interaction with R = 0 against the two-body engine on the
+    same basis (equal up to the float rounding of the matrix elements); the
+    oracle's restated bundle loops on one thread over a seeded sample of
+    bundles as the CPU figure."""
+    import torch
+    import oracle
+    from bigstickpublick_b200 import model
+    from bigstickpublick_b200.engine import Hamiltonian
+    spec = model.pf_model(4, 4, seed=5, jz2=0)
+    t0 = time.perf_counter()
+    T = model.build_tables3(spec, w2=1.0, w3=0.1, seed=5)
+    t_build = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    H = Hamiltonian(T)
+    t_create = time.perf_counter() - t0
+    st = H.stats()
+    ops = {k: int(st["n_ops_" + k]) for k in ("spe", "ppp", "nnn", "ppn", "pnn")}
+    nops = sum(ops.values())
+    peaks, peak_kind = load_peaks()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    out = {"config": "pf 4p4n 2Jz=0, W = V2/(A-2) + 0.1 MeV R (seeded), nb = 1", "dim": T.dim,
+           "ops_per_matvec": ops, "build_s": t_build, "create_s": t_create, "launches_per_matvec": 1}
+    g = torch.Generator(device="cuda").manual_seed(4321)
+    x64 = torch.randn(T.dim, dtype=torch.float64, device="cuda", generator=g)
+    S, S3 = T.s, T.s3
+    jumps = S["np1b"] + S["nn1b"] + S["np2b"] + S["nn2b"] + S3["np3b"] + S3["nn3b"]
+    jb = 21 * jumps + 8 * (S["nsd_p"] + S["nsd_n"]) + 4 * (S3["nmatppp"] + S3["nmatnnn"] + S3["nmatppn"] +
+                                                           S3["nmatpnn"])
+    for name, dt, sb in (("fp32", torch.float32, 4), ("fp64", torch.float64, 8)):
+        x = x64.to(dt)
+        y = torch.empty_like(x)
+        for _ in range(3):
+            H.applyh(x, y)
+        reps = 10
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+        for k in range(reps):
+            flush.fill_(float(k))
+            evs[k][0].record()
+            H.applyh(x, y)
+            evs[k][1].record()
+        torch.cuda.synchronize()
+        ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+        balg = nops * 3 * sb + jb + T.dim * 2 * sb
+        out[name] = {"matvec_ms": ms, "matvec_per_s": 1e3 / ms, "gupdates_per_s": nops / ms / 1e6,
+                     "alg_GBps": balg / ms / 1e6, "alg_frac_of_hbm": balg / ms / 1e6 / peaks["hbm_gbs"],
+                     "peak_kind": peak_kind}
+    u64 = torch.randn(T.dim, dtype=torch.float64, device="cuda", generator=g)
+    hv, hu = H.applyh(x64), H.applyh(u64)
+    a, b = float(torch.dot(u64, hv)), float(torch.dot(x64, hu))
+    out["hermiticity_rel"] = abs(a - b) / abs(a)
+    H.close()
+    del H, hv, hu, flush
+    # the two-body interaction in three-body form against the two-body engine
+    H0 = Hamiltonian(model.build_tables3(spec, w2=1.0, w3=0.0, seed=5))
+    H2 = Hamiltonian(model.build_tables(spec))
+    y0, y2 = H0.applyh(x64), H2.applyh(x64)
+    out["three_vs_two_body_rel"] = float(torch.linalg.vector_norm(y0 - y2) / torch.linalg.vector_norm(y2))
+    H0.close()
+    H2.close()
+    # CPU: the oracle's bundle loops, one thread, a seeded sample of bundles
+    a_ = T.a
+    size = (a_["pxend"] - a_["pxstart"] + 1) * (a_["nxend"] - a_["nxstart"] + 1)
+    order = np.random.default_rng(5).permutation(len(size))
+    pick, acc = [], 0
+    for ib in order:
+        if a_["optype"][ib] == 1:
+            continue
+        pick.append(int(ib))
+        acc += int(size[ib])
+        if acc >= 4e8:
+            break
+    xin = x64.cpu().numpy().astype(np.float32)
+    t0 = time.perf_counter()
+    oracle.applyh3_bundles(T, xin, pick)
+    secs = time.perf_counter() - t0
+    out["cpu_oracle_1thread"] = {"matvec_per_s": acc / secs / nops, "sample_updates": acc,
+                                 "sample_share": acc / nops, "seconds": secs}
+    out["speedup_fp32_vs_cpu_1thread"] = out["fp32"]["matvec_per_s"] / out["cpu_oracle_1thread"]["matvec_per_s"]
+    return out
+
+
 def large_leg(H, T, args):
     """Config 5 (the headline workload): thick-restart Lanczos for the lowest
     5 states, keep 20, mixed (FP32 applyH, FP32-stored Lanczos vectors, FP64
@@ -605,6 +693,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--no-tts", action="store_true")
+    ap.add_argument("--no-three", action="store_true")
     ap.add_argument("--lanczos-iters", type=int, default=300)
     ap.add_argument("--tts-tols", type=float, nargs="+", default=list(TTS_TOLS))
     ap.add_argument("--batch-n", type=int, default=256)
@@ -616,6 +705,7 @@ def main():
     args.warmup = max(args.warmup, 3)
     if args.quick:
         args.no_cpu = args.no_lanczos = args.no_density = args.no_batch = args.no_large = args.no_tts = True
+        args.no_three = True
 
     if args.impl == "reference":
         return run_reference(args)
@@ -723,6 +813,8 @@ def main():
         _leg(line, "time_to_solution", time_to_solution_leg, args)
     if rank == 0 and not args.no_batch:
         _leg(line, "batch", batch_leg, args)
+    if rank == 0 and not args.no_three:
+        _leg(line, "threebody", threebody_leg, args)
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, cores, shares, secs = cpu_baseline(tables, nb, prec, budget_s=args.cpu_budget)
         line["cpu_baseline"] = {"value": rate, "unit": "matvec/s", "cores": cores, "kind": "port",

@@ -56,6 +56,9 @@ def lib():
         L.oracle_applyh_owner.restype = C.c_int
         L.oracle_applyh3.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]
         L.oracle_applyh3.restype = C.c_int
+        L.oracle_applyh3_bundles.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                             C.c_void_p, C.c_int64]
+        L.oracle_applyh3_bundles.restype = C.c_int
         L.oracle_count_ops3.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
         L.oracle_count_ops3.restype = None
         _LIB = L
@@ -82,6 +85,22 @@ def applyh(tables, vin, nb=1, accumulate_into=None):
         st = lib().oracle_applyh(p, vin.ctypes.data, out.ctypes.data, nb, prec)
     if st != 0:
         raise RuntimeError(f"oracle_applyh status {st}")
+    return out
+
+
+def applyh3_bundles(tables, vin, bundles, nb=1, out=None):
+    """vout += H vin over the listed bundles (0-based) of a three-body run."""
+    vin = np.ascontiguousarray(vin)
+    prec = 4 if vin.dtype == np.float32 else 8
+    if out is None:
+        out = np.zeros_like(vin)
+    lst = np.ascontiguousarray(bundles, dtype=np.int64)
+    p, keep = _tp(tables)
+    t3 = tables.as_ctypes3()
+    st = lib().oracle_applyh3_bundles(p, C.cast(C.pointer(t3), C.c_void_p), vin.ctypes.data, out.ctypes.data, nb,
+                                      prec, lst.ctypes.data, len(lst))
+    if st != 0:
+        raise RuntimeError(f"oracle_applyh3_bundles status {st}")
     return out
 
 

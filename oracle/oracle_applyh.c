@@ -234,6 +234,30 @@ int oracle_applyh3(const bsg_tables *t, const bsg_tables3 *u, const void *vin, v
     return BSG_OK;
 }
 
+/* the same for the listed bundles only (0-based indices): a bounded sample
+ * of one matvec for the timed CPU baseline */
+int oracle_applyh3_bundles(const bsg_tables *t, const bsg_tables3 *u, const void *vin, void *vout, int nb, int prec,
+                           const int64_t *list, int64_t nlist) {
+    if (!t || !u || !vin || !vout || nb < 1 || (nlist > 0 && !list)) return BSG_ERR_ARG;
+    for (int64_t k = 0; k < nlist; ++k) {
+        const int64_t ib = list[k];
+        if (ib < 0 || ib >= t->nbundles) return BSG_ERR_ARG;
+        const int op = t->optype[ib];
+        if (op == BSG_OP_PP || op == BSG_OP_NN || op == BSG_OP_PN) continue;
+        if (op == BSG_OP_SPE) {
+            if (prec == BSG_PREC_FP32)
+                bundle_f32(t, ib, (const float *)vin, (float *)vout, nb);
+            else
+                bundle_f64(t, ib, (const double *)vin, (double *)vout, nb);
+        } else if (prec == BSG_PREC_FP32) {
+            bundle3_f32(t, u, ib, (const float *)vin, (float *)vout, nb);
+        } else {
+            bundle3_f64(t, u, ib, (const double *)vin, (double *)vout, nb);
+        }
+    }
+    return BSG_OK;
+}
+
 /* inner-loop updates of each three-body kind: ops[0..3] = PPP, NNN, PPN, PNN */
 void oracle_count_ops3(const bsg_tables *t, int64_t *ops) {
     for (int k = 0; k < 4; ++k) ops[k] = 0;
