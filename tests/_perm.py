@@ -21,7 +21,9 @@ from bigstickpublick_b200 import model
 
 
 def _clone(T):
-    return model.Tables({k: v.copy() for k, v in T.a.items()}, dict(T.s), copy.copy(T.extra))
+    a3 = {k: v.copy() for k, v in T.a3.items()} if T.a3 is not None else None
+    return model.Tables({k: v.copy() for k, v in T.a.items()}, dict(T.s), copy.copy(T.extra), a3,
+                        dict(T.s3) if T.s3 is not None else None)
 
 
 def permute_jumps(T, rng):
@@ -100,4 +102,33 @@ def permute_labels(T, rng):
                 for d in range(n):
                     newh[nme + sig[c] * n + sig[d]] = h[nme + c * n + d]
         a["cpnpair"], a["dpnpair"], a["hmatpn"] = cpn, dpn, newh
+    return T2
+
+
+def permute_jumps3(T, rng):
+    """A random order inside every jump range of a three-body run's bundles:
+    p3b (PPP), n3b (NNN), the pair-labelled p2b (PPN) and n2b (PNN), and the
+    one-body jumps they pair with (n1b of PPN, p1b of PNN)."""
+    T2 = _clone(T)
+    a, a3 = T2.a, T2.a3
+    fam = {  # jump family -> (arrays in a, arrays in a3), optype, side of the bundle range
+        "p3b": ([], ["p3b_isd", "p3b_fsd", "p3b_op", "p3b_phase"], 7, "px"),
+        "n3b": ([], ["n3b_isd", "n3b_fsd", "n3b_op", "n3b_phase"], 8, "nx"),
+        "p2b": (["p2b_isd", "p2b_fsd", "p2b_phase"], ["p2b_cop", "p2b_dop"], 9, "px"),
+        "n1b": (["n1b_isd", "n1b_fsd", "n1b_cop", "n1b_dop", "n1b_phase"], [], 9, "nx"),
+        "p1b": (["p1b_isd", "p1b_fsd", "p1b_cop", "p1b_dop", "p1b_phase"], [], 10, "px"),
+        "n2b": (["n2b_isd", "n2b_fsd", "n2b_phase"], ["n2b_cop", "n2b_dop"], 10, "nx"),
+    }
+    for name, (ka, k3, optype, side) in fam.items():
+        sel = a["optype"] == optype
+        ranges = sorted({(int(s), int(e)) for s, e in zip(a[side + "start"][sel], a[side + "end"][sel])})
+        for (s0, e0), (s1, e1) in zip(ranges, ranges[1:]):
+            assert s1 > e0, f"{name}: overlapping jump ranges"
+        keys = [(a, k) for k in ka] + [(a3, k) for k in k3]
+        n = len(keys[0][0][keys[0][1]])
+        perm = np.arange(n)
+        for s, e in ranges:
+            perm[s - 1:e] = s - 1 + rng.permutation(e - s + 1)
+        for d, k in keys:
+            d[k] = d[k][perm].copy()
     return T2

@@ -196,3 +196,15 @@ def test_three_body_bundle_in_a_two_body_context_is_rejected():
 def test_three_body_needs_three_particles():
     with pytest.raises(RuntimeError, match="three valence particles"):
         model.build_tables3(_spec("sd", 1, 1, 0), w2=1.0)
+
+
+@pytest.mark.parametrize("orb,z,n,jz2", [("sd", 3, 2, 1), ("sd", 2, 3, 1), ("pf", 3, 1, 2)])
+def test_three_body_jump_order_invariance(orb, z, n, jz2):
+    from _perm import permute_jumps3
+    T = model.build_tables3(_spec(orb, z, n, jz2), w2=1.0, w3=0.3, seed=4)
+    T2 = permute_jumps3(T, np.random.default_rng(1))
+    assert not np.array_equal(T.a3["p2b_cop"], T2.a3["p2b_cop"]) or not np.array_equal(T.a["p1b_isd"], T2.a["p1b_isd"])
+    assert engine.validate_tables(T2) == (0, "")
+    v = np.random.default_rng(2).standard_normal(T.dim)
+    y, y2 = oracle.applyh(T, v), oracle.applyh(T2, v)
+    assert np.abs(y - y2).max() < 1e-12 * np.abs(y).max()

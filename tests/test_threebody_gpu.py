@@ -100,3 +100,35 @@ def test_threebody_grad_is_refused(built):
     with pytest.raises(BsgError) as e:
         H.grad(v)
     assert e.value.status == 8
+
+
+@pytest.mark.parametrize("tmax", [32, 100])
+def test_split_neutron_operators_match_oracle(tmax):
+    # neutron operators with more (b,d) pairs than pn_table_max are split into
+    # sub-operators; two-body PN and three-body PPN / PNN both
+    from bigstickpublick_b200.engine import Hamiltonian
+    rng = np.random.default_rng(tmax)
+    for T in (model.build_tables(model.pf_model(3, 3, seed=5)),
+              model.build_tables3(model.sd_model(3, 3, seed=3), w2=1.0, w3=0.4, seed=8)):
+        H = Hamiltonian(T, pn_table_max=tmax)
+        for prec, tol in ((8, 1e-12), (4, 2e-5)):
+            v = rng.standard_normal(T.dim).astype(np.float64 if prec == 8 else np.float32)
+            ref = oracle.applyh(T, v)
+            got = H.applyh(v)
+            assert np.abs(got - ref).max() / np.abs(ref).max() < tol
+        H.close()
+
+
+def test_threebody_engine_on_reordered_jumps():
+    # the engine consumes any jump order inside a sector jump: the same
+    # matvec (to summation order) on the three-body tables with every jump
+    # range of every bundle permuted
+    from _perm import permute_jumps3
+    from bigstickpublick_b200.engine import Hamiltonian
+    T = model.build_tables3(model.sd_model(4, 3, seed=3, jz2=1), w2=1.0, w3=0.3, seed=4)
+    T2 = permute_jumps3(T, np.random.default_rng(5))
+    H2 = Hamiltonian(T2)
+    v = np.random.default_rng(6).standard_normal(T.dim)
+    ref = oracle.applyh(T, v)
+    assert np.abs(H2.applyh(v) - ref).max() < 1e-12 * np.abs(ref).max()
+    H2.close()
