@@ -53,7 +53,7 @@ class BsgTables(C.Structure):
 
 class BsgConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("max_nb", C.c_int32),
-                ("validate", C.c_int32), ("reserved", C.c_int32)]
+                ("validate", C.c_int32), ("pn_table_max", C.c_int32)]
 
 
 class BsgLanczosParams(C.Structure):

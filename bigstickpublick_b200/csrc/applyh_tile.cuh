@@ -119,14 +119,15 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
     const int row = tile.row;
     const int64_t roff = a.row_off[row];
 
+    // position of item i: p0 + 32 i, in the tile while 32 i < lim (derived
+    // from two registers instead of held per item: the 32-register kernels
+    // spill less)
     T acc[ITEMS][NB];
-    int pos[ITEMS];
-    bool valid[ITEMS];
+    const int p0 = tile.pos0 + lane, lim = tile.npos - lane;
+#define BSG_POS(i) (p0 + 32 * (i))
+#define BSG_VALID(i) (32 * (i) < lim)
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) {
-        const int local = lane + 32 * i;
-        pos[i] = tile.pos0 + local;
-        valid[i] = local < tile.npos;
 #pragma unroll
         for (int v = 0; v < NB; ++v) acc[i][v] = T(0);
     }
@@ -140,9 +141,9 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
             const T me = (T)pc.me;
 #pragma unroll
             for (int i = 0; i < ITEMS; ++i) {
-                if (valid[i] && pos[i] >= pc.lo && pos[i] <= pc.hi) {
+                if (BSG_VALID(i) && BSG_POS(i) >= pc.lo && BSG_POS(i) <= pc.hi) {
                     T x[NB];
-                    Vec<T, NB, FULL>::load(vin + (size_t)(pc.q_off + pos[i]) * ld + v0, x);
+                    Vec<T, NB, FULL>::load(vin + (size_t)(pc.q_off + BSG_POS(i)) * ld + v0, x);
 #pragma unroll
                     for (int v = 0; v < NB; ++v) acc[i][v] += me * x[v];
                 }
@@ -160,15 +161,15 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
             const int2 *__restrict__ rec = reinterpret_cast<const int2 *>(a.nnrec + op.rec_base);
 #pragma unroll
             for (int i = 0; i < ITEMS; ++i) {
-                if (!valid[i] || pos[i] >= op.nout) continue;
-                const int k0 = __ldg(ptr + pos[i]), k1 = __ldg(ptr + pos[i] + 1);
+                if (!BSG_VALID(i) || BSG_POS(i) >= op.nout) continue;
+                const int k0 = __ldg(ptr + BSG_POS(i)), k1 = __ldg(ptr + BSG_POS(i) + 1);
                 // NN takes the 32-bit records for FP64 vectors only: for FP32
                 // the extra hmatnn load per record cost more than the halved
                 // record bytes saved (pf 6p6n: 143.8 against 139.2 ms)
                 if constexpr (REC32 && std::is_same<T, double>::value) {
                     // input position | hmatnn label - 1 | phase sign
                     const uint32_t *c32 =
-                        a.sell32 + op.sell_base + __ldg(a.slice_off + op.slice_base + (pos[i] >> 5)) + lane;
+                        a.sell32 + op.sell_base + __ldg(a.slice_off + op.slice_base + (BSG_POS(i) >> 5)) + lane;
                     const int n = k1 - k0;
                     int k = 0;
                     for (; k + 1 < n; k += 2) {
@@ -196,7 +197,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
                 }
                 const int2 *col;
                 int k, n;
-                record_column<T, NB>(a, op, rec, k0, k1, pos[i], lane, col, k, n);
+                record_column<T, NB>(a, op, rec, k0, k1, BSG_POS(i), lane, col, k, n);
                 for (; k + 1 < n; k += 2) {
                     const int2 r0 = __ldg(col + kRecStride<T, NB> * k), r1 = __ldg(col + kRecStride<T, NB> * (k + 1));
                     T x0[NB], x1[NB];
@@ -239,12 +240,12 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
             const T *__restrict__ src = vin + (size_t)pc.q_off * ld + v0;
 #pragma unroll
             for (int i = 0; i < ITEMS; ++i) {
-                if (!valid[i] || pos[i] >= op.nout) continue;
-                const int k0 = __ldg(ptr + pos[i]), k1 = __ldg(ptr + pos[i] + 1);
+                if (!BSG_VALID(i) || BSG_POS(i) >= op.nout) continue;
+                const int k0 = __ldg(ptr + BSG_POS(i)), k1 = __ldg(ptr + BSG_POS(i) + 1);
                 if constexpr (REC32) {
                     // input position | (b,d) index | neutron phase sign
                     const uint32_t *c32 =
-                        a.sell32 + op.sell_base + __ldg(a.slice_off + op.slice_base + (pos[i] >> 5)) + lane;
+                        a.sell32 + op.sell_base + __ldg(a.slice_off + op.slice_base + (BSG_POS(i) >> 5)) + lane;
                     const int n = k1 - k0;
                     int k = 0;
                     for (; k + 1 < n; k += 2) {
@@ -269,7 +270,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
                 }
                 const int2 *col;
                 int k, n;
-                record_column<T, NB>(a, op, rec, k0, k1, pos[i], lane, col, k, n);
+                record_column<T, NB>(a, op, rec, k0, k1, BSG_POS(i), lane, col, k, n);
                 for (; k + 1 < n; k += 2) {
                     const int2 r0 = __ldg(col + kRecStride<T, NB> * k), r1 = __ldg(col + kRecStride<T, NB> * (k + 1));
                     T x0[NB], x1[NB];
@@ -303,10 +304,10 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
             const SPEContrib sc = a.spe[c];
 #pragma unroll
             for (int i = 0; i < ITEMS; ++i) {
-                if (valid[i] && pos[i] >= sc.lo && pos[i] <= sc.hi) {
-                    const float e = sc.pspe + __ldg(a.nspe + sc.n0 + (pos[i] - sc.lo));
+                if (BSG_VALID(i) && BSG_POS(i) >= sc.lo && BSG_POS(i) <= sc.hi) {
+                    const float e = sc.pspe + __ldg(a.nspe + sc.n0 + (BSG_POS(i) - sc.lo));
                     T x[NB];
-                    Vec<T, NB, FULL>::load(vin + (size_t)(roff + pos[i]) * ld + v0, x);
+                    Vec<T, NB, FULL>::load(vin + (size_t)(roff + BSG_POS(i)) * ld + v0, x);
 #pragma unroll
                     for (int v = 0; v < NB; ++v) acc[i][v] += x[v] * (T)e;
                 }
@@ -347,5 +348,8 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
     }
 }
 
+
+#undef BSG_POS
+#undef BSG_VALID
 
 }  // namespace bsg

@@ -276,6 +276,8 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
     // Matrix-element records keep their label for the adjoint and for the
     // 32-bit records; NNN labels are offset by nmatnn (one device array
     // hmatnn | hmatnnn).
+    std::vector<int32_t> nop_nsub;         // label operators: sub-operators from this id on (0: a later one)
+    std::vector<int32_t> nop_nbd;          // label operators: pairs over all sub-operators
     std::vector<int32_t> bdk_dense;        // (b,d) -> index in the op's list, reset after each op
     std::vector<size_t> bdk_touched;
     auto get_nop = [&](int kind, int dir, int64_t x0, int64_t x1, int32_t &id) -> int {
@@ -335,17 +337,51 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
             for (size_t key : bdk_touched) bdk_dense[key] = -1;
             bdk_touched.clear();
             if (bdl.size() > 65535) return V.fail("too many distinct (b,d) label pairs in a neutron sector jump");
-            std::vector<int32_t> ptr;
-            std::vector<PNRec> sorted;
-            csr_by_out(out, recs, maxout + 1, ptr, sorted);
-            op.rec_base = (int64_t)pnrec_all.size();
-            op.ptr_base = (int64_t)nptr_all.size();
-            op.nout = maxout + 1;
-            op.bd_base = (int32_t)bd_all.size();
-            op.nbd = (int32_t)bdl.size();
+            // more label pairs than one shared table holds: consecutive
+            // sub-operators over slices of the pair list, each with the
+            // records whose pair falls in its slice (same output positions,
+            // record order kept); a contribution on the operator becomes one
+            // contribution per sub-operator
+            const int32_t tmax = std::max<int32_t>(32, ctx->pn_table_max);
+            const int32_t nbd_all = (int32_t)bdl.size();
+            const int32_t nsub = std::max<int32_t>(1, (nbd_all + tmax - 1) / tmax);
+            const int32_t bd0 = (int32_t)bd_all.size();
             bd_all.insert(bd_all.end(), bdl.begin(), bdl.end());
-            pnrec_all.insert(pnrec_all.end(), sorted.begin(), sorted.end());
-            nptr_all.insert(nptr_all.end(), ptr.begin(), ptr.end());
+            id = (int32_t)nops.size();
+            for (int32_t sb = 0; sb < nsub; ++sb) {
+                const int32_t k0 = sb * tmax, k1 = std::min(nbd_all, k0 + tmax);
+                std::vector<int32_t> sout;
+                std::vector<PNRec> srec;
+                if (nsub == 1) {
+                    sout.swap(out);
+                    srec.swap(recs);
+                } else {
+                    for (int64_t x = 0; x < n; ++x)
+                        if (recs[x].k >= k0 && recs[x].k < k1) {
+                            PNRec r = recs[x];
+                            r.k = (uint16_t)(r.k - k0);
+                            srec.push_back(r);
+                            sout.push_back(out[x]);
+                        }
+                }
+                std::vector<int32_t> ptr;
+                std::vector<PNRec> sorted;
+                csr_by_out(sout, srec, maxout + 1, ptr, sorted);
+                NOp so = op;
+                so.rec_base = (int64_t)pnrec_all.size();
+                so.ptr_base = (int64_t)nptr_all.size();
+                so.nout = maxout + 1;
+                so.bd_base = bd0 + k0;
+                so.nbd = k1 - k0;
+                pnrec_all.insert(pnrec_all.end(), sorted.begin(), sorted.end());
+                nptr_all.insert(nptr_all.end(), ptr.begin(), ptr.end());
+                nops.push_back(so);
+                nop_maxin.push_back(maxin);
+                nop_nsub.push_back(sb == 0 ? nsub : 0);
+                nop_nbd.push_back(sb == 0 ? nbd_all : 0);
+            }
+            nop_id[k] = id;
+            return BSG_OK;
         } else {
             const bool nnn = (kind == 3);
             const int64_t *xisd = nnn ? t3->n3b_isd : t->n2b_isd, *xfsd = nnn ? t3->n3b_fsd : t->n2b_fsd;
@@ -398,6 +434,8 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
         id = (int32_t)nops.size();
         nops.push_back(op);
         nop_maxin.push_back(maxin);
+        nop_nsub.push_back(1);
+        nop_nbd.push_back(0);
         nop_id[k] = id;
         return BSG_OK;
     };
@@ -420,13 +458,15 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
         if (nops[id].nout > ctx->h_rowlen[rf] || nop_maxin[id] >= ctx->h_rowlen[ri])
             return set_err(ctx, BSG_ERR_OOB_INDEX, what + ": neutron jump outside the row");
         if (ph != 1 && ph != -1) return set_err(ctx, BSG_ERR_BAD_TABLE, what + " phase not +-1");
-        PNContrib c{};
-        c.q_off = s1;
-        c.nop = id;
-        c.aoff = aoff;
-        c.coff = coff;
-        c.php = (float)ph;
-        pn.push_back({rf, c});
+        for (int32_t sb = 0; sb < nop_nsub[id]; ++sb) {
+            PNContrib c{};
+            c.q_off = s1;
+            c.nop = id + sb;
+            c.aoff = aoff;
+            c.coff = coff;
+            c.php = (float)ph;
+            pn.push_back({rf, c});
+        }
         return BSG_OK;
     };
     for (int64_t ib = 0; ib < t->nbundles; ++ib) {
@@ -533,7 +573,7 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
             }
             const int64_t nmat3 = ppn ? t3->nmatppn : t3->nmatpnn;
             for (auto &pl : lab)
-                for (int32_t k = 0; k < no.nbd; ++k) {
+                for (int32_t k = 0; k < nop_nbd[id]; ++k) {
                     const BDPair bd = bd_all[no.bd_base + k];
                     const int64_t idx = ppn ? (int64_t)ppn_c(pl.first, bd.b - nl_n) + ppn_d(pl.second, bd.d - nl_n)
                                             : (int64_t)pnn_c(bd.b + 1, pl.first) + pnn_d(bd.d + 1, pl.second);
@@ -658,13 +698,15 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
                     return set_err(ctx, BSG_ERR_OOB_INDEX, "PN neutron jump outside the row" + where);
                 const int ph = t->p1b_phase[x - 1];
                 if (ph != 1 && ph != -1) return set_err(ctx, BSG_ERR_BAD_TABLE, "p1b_phase not +-1" + where);
-                PNContrib c{};
-                c.q_off = s1;
-                c.nop = id;
-                c.aoff = (int32_t)(t->p1b_cop[x - 1] + nl_p) * ld;
-                c.coff = (int32_t)(t->p1b_dop[x - 1] + nl_p) * ld;
-                c.php = (float)ph;
-                pn.push_back({rf, c});
+                for (int32_t sb = 0; sb < nop_nsub[id]; ++sb) {
+                    PNContrib c{};
+                    c.q_off = s1;
+                    c.nop = id + sb;
+                    c.aoff = (int32_t)(t->p1b_cop[x - 1] + nl_p) * ld;
+                    c.coff = (int32_t)(t->p1b_dop[x - 1] + nl_p) * ld;
+                    c.php = (float)ph;
+                    pn.push_back({rf, c});
+                }
             }
             ops[3] += (px1 - px0 + 1) * (nx1 - nx0 + 1);
         } else if (op == BSG_OP_SPE) {
@@ -1028,6 +1070,7 @@ int create_ctx(const bsg_tables *t, const bsg_tables3 *t3, const bsg_config *cfg
     if (!ctx) return BSG_ERR_NOMEM;
     ctx->device = cfg ? cfg->device : 0;
     ctx->max_nb = (cfg && cfg->max_nb > 0) ? cfg->max_nb : 16;
+    ctx->pn_table_max = (cfg && cfg->pn_table_max > 0) ? cfg->pn_table_max : 512;
     int st = cuda_check(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
     if (!st) st = cuda_check(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "stream");
     if (!st) st = cuda_check(ctx, cudaEventCreate(&ctx->ev0), "event");

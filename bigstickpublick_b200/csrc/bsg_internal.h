@@ -148,6 +148,7 @@ struct bsg_ctx {
     int32_t max_rowlen = 0;
     int32_t median_rowlen = 0;
     int32_t max_nb = 16;
+    int32_t pn_table_max = 512;   // bsg_config.pn_table_max
     // raw tables on the device (byte-identical copies)
     std::vector<bsg::DevBuf> raw;
     // derived

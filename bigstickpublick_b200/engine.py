@@ -49,11 +49,13 @@ def validate_tables(tables):
 
 
 class Hamiltonian:
-    def __init__(self, tables, device=0, max_nb=16, validate=True):
+    def __init__(self, tables, device=0, max_nb=16, validate=True, pn_table_max=0):
+        """pn_table_max: largest (b,d) table of one neutron operator before
+        it is split into sub-operators (bsg_config.pn_table_max; 0 = 512)."""
         self.lib = _abi.gpu_lib()
         self.tables = tables
         self._ct = tables.as_ctypes()
-        cfg = _abi.BsgConfig(device, max_nb, 1 if validate else 0, 0)
+        cfg = _abi.BsgConfig(device, max_nb, 1 if validate else 0, int(pn_table_max))
         h = C.c_void_p()
         # a three-body Hamiltonian (model.build_tables3) goes through bsg_create3
         self._ct3 = tables.as_ctypes3() if getattr(tables, "threebody", False) else None

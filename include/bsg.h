@@ -115,7 +115,10 @@ typedef struct bsg_config {
     int32_t device;        /* CUDA device ordinal                              */
     int32_t max_nb;        /* largest block size bsg_applyh will be given      */
     int32_t validate;      /* 1: run the host-side table validator at create   */
-    int32_t reserved;
+    int32_t pn_table_max;  /* largest (b,d) label-pair table of one neutron
+                              operator (the PN-form shared-memory table); a
+                              larger operator is split into sub-operators of
+                              at most this many pairs.  0: 512 */
 } bsg_config;
 
 typedef struct bsg_ctx bsg_ctx;
