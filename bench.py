@@ -297,12 +297,16 @@ def lanczos_sd6p6n_leg(args):
     try:
         piv = np.random.default_rng(11).standard_normal(T.dim)
         for prec in (FP64, MIXED):  # untimed: the first use of a kernel loads its code
-            H.lanczos(nkeep=2, niter=6, fixed_iter=True, pivot=piv, **prec)
+            H.lanczos(nkeep=10, niter=20, fixed_iter=True, pivot=piv, **prec)
         out = {}
         res = {}
         for name, prec in (("fp64", FP64), ("mixed", MIXED)):
-            ev, vecs, info = _solve(H, nkeep=10, niter=args.lanczos_iters, fixed_iter=True, pivot=piv,
-                                    want_vectors=True, **prec)
+            # the faster of two identical runs (a run is 60-70 ms, so one
+            # stall of the host or the box would decide a single sample)
+            runs = [_solve(H, nkeep=10, niter=args.lanczos_iters, fixed_iter=True, pivot=piv, want_vectors=True,
+                           **prec) for _ in range(2)]
+            ev, vecs, info = min(runs, key=lambda r: r[2]["solve_s"])
+            info["solve_s_runs"] = [r[2]["solve_s"] for r in runs]
             res[name] = (ev, vecs)
             info["lowest"] = [float(x) for x in ev[:3]]
             out[name] = info
@@ -310,7 +314,7 @@ def lanczos_sd6p6n_leg(args):
         out["speedup_its_per_s"] = out["mixed"]["its_per_s"] / out["fp64"]["its_per_s"]
         out["config"] = (f"sd 6p6n, {args.lanczos_iters} iterations (fixed), lowest 10, seeded generic pivot; "
                          "mixed = FP32 applyH + FP32-stored Lanczos vectors with FP64 sums; errors of mixed "
-                         "against FP64 from the same pivot")
+                         "against FP64 from the same pivot; each the faster of two identical runs")
         return out
     finally:
         H.close()

@@ -126,8 +126,10 @@ template <typename T, int NB>
 static int launch_nb(bsg_ctx *ctx, const T *vin, T *vout, int ld, int v0, int accumulate, cudaStream_t s,
                      TileLookup lk, double *cols = nullptr) {
     // nb = 8 measured fastest at two positions per lane (pf 4p4n: 5.10 ms at
-    // one, 4.86 at two, 5.08 at four)
-    constexpr int cap = NB >= 16 ? 1 : (NB >= 4 ? 2 : (NB == 2 ? 4 : 8));
+    // one, 4.86 at two, 5.08 at four); single FP64 vectors at four (pf 6p6n:
+    // 194.4 ms against 219.5 at eight, pf 4p4n 2.11 against 2.30 ms), single
+    // FP32 vectors at eight (pf 6p6n 138.9 against 159.0 ms at four)
+    constexpr int cap = NB >= 16 ? 1 : (NB >= 4 ? 2 : (NB == 2 ? 4 : (std::is_same<T, double>::value ? 4 : 8)));
     int items = 1;
     while (items < cap && 32 * items < ctx->median_rowlen) items *= 2;
     if (items >= 8 && cap >= 8) return launch_one<T, NB, (cap >= 8 ? 8 : 1)>(ctx, vin, vout, ld, v0, accumulate, s, lk, cols);

@@ -48,99 +48,140 @@ struct DChunk {
     int32_t label;          // output label (species-combined)
 };
 
-// [dim x ns] column-major -> [dim x ns] interleaved (row of all states contiguous)
-__global__ void k_interleave(const double *__restrict__ cols, double *__restrict__ x, int64_t dim, int ns) {
-    const int64_t n = dim * ns;
+// [dim x ns] column-major -> [dim x nsp] interleaved (row of all states
+// contiguous, nsp = ns rounded up to even, the padding state zero): every row
+// starts on a 16-byte boundary
+__global__ void k_interleave(const double *__restrict__ cols, double *__restrict__ x, int64_t dim, int ns, int nsp) {
+    const int64_t n = dim * nsp;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t row = e / ns;
-        const int k = (int)(e - row * ns);
-        x[e] = cols[(int64_t)k * dim + row];
+        const int64_t row = e / nsp;
+        const int k = (int)(e - row * nsp);
+        x[e] = k < ns ? cols[(int64_t)k * dim + row] : 0.0;
     }
 }
 
-// rows of all states staged per pass: tile * ns doubles per side
+__host__ __device__ inline int den_nsp(int ns) { return (ns + 1) & ~1; }
+// rows staged per pass: tile * nsp <= 1024 doubles per side and buffer, so
+// that 32 KB of shared memory per CTA leaves room for 6 CTAs per SM
 __host__ __device__ inline int den_tile(int ns) {
-    int t = (2048 / ns) / 32 * 32;
+    int t = (1024 / den_nsp(ns)) / 32 * 32;
     return t < 32 ? 32 : (t > kDenThreads ? kDenThreads : t);
 }
-// shared layout: s_f, s_i [ns rounded up to even][tile + 1] (odd stride: the
-// rows of different states fall in different banks), signs, row indices,
-// and the per-thread partial sums
+// shared layout: two buffers of (final rows, initial rows) [tile][nsp] and
+// their row signs; the per-thread partial sums reuse the buffers at the end
 inline size_t den_smem(int ns) {
-    const int tile = den_tile(ns), nsp = (ns + 1) & ~1;
-    return sizeof(double) * (size_t)(2 * nsp * (tile + 1) + tile) + 2 * sizeof(int64_t) * tile +
-           sizeof(double) * 4 * kDenThreads;
+    const int tile = den_tile(ns), nsp = den_nsp(ns);
+    return sizeof(double) * (size_t)(4 * tile * nsp + 2 * tile);
 }
 
-// One CTA per chunk.  Per pass: the first `tile` threads map the next rows
-// of the chunk to (final row, initial row, sign), walking forward from the
-// segment the previous pass ended in; all threads stage those rows of every
-// state in shared memory; then each thread accumulates a 2 x 2 block of
-// (final, initial) pairs over its share of the rows: the h*h blocks
-// (h = ceil(ns/2)) take G = 256 / (h*h) row groups, summed in group order
-// at the end.
-__global__ void __launch_bounds__(kDenThreads) k_density_chunks(const DSeg *__restrict__ segs,
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// One CTA per chunk, passes of `tile` rows, double-buffered: while the
+// threads multiply pass p out of one buffer, the copies of pass p+1 are in
+// flight into the other (cp.async, 16 bytes each, no registers held).  In
+// each pass thread t maps row t of the pass to (final row, initial row,
+// sign), walking forward from the segment the previous pass ended in, and
+// copies both rows of all states.  Each thread then accumulates a 2 x 2 block
+// of (final, initial) pairs over its share of the rows: the h*h blocks
+// (h = nsp/2) take G = 256 / (h*h) row groups, summed in group order at the
+// end.
+__global__ void __launch_bounds__(kDenThreads, 6) k_density_chunks(const DSeg *__restrict__ segs,
                                                               const DChunk *__restrict__ chunks,
                                                               const double *__restrict__ x, int ns,
                                                               double *__restrict__ partial) {
     extern __shared__ __align__(16) unsigned char smem[];
-    const int tile = den_tile(ns), ld = tile + 1;
-    const int h = (ns + 1) >> 1, nsp = 2 * h;
-    double *s_f = reinterpret_cast<double *>(smem);
-    double *s_i = s_f + nsp * ld;
-    double *s_sg = s_i + nsp * ld;
-    int64_t *s_rf = reinterpret_cast<int64_t *>(s_sg + tile);
-    int64_t *s_ri = s_rf + tile;
-    double *s_red = reinterpret_cast<double *>(s_ri + tile);
-    __shared__ int s_next;
+    const int nsp = den_nsp(ns), tile = den_tile(ns);
+    double *buf = reinterpret_cast<double *>(smem);     // [2 buffers][2 sides][tile][nsp]
+    double *s_sg = buf + (size_t)4 * tile * nsp;        // [2 buffers][tile]
+    __shared__ int s_next[2];
     const DChunk ch = chunks[blockIdx.x];
     const int t = threadIdx.x;
-    const int nbk = h * h, groups = kDenThreads / nbk;
+    const int h = nsp >> 1, nbk = h * h, groups = kDenThreads / nbk;
     const int g = t / nbk, bk = t - g * nbk;
     const int f0 = 2 * (bk / h), i0 = 2 * (bk % h);
-    // the padding state (ns odd) stays zero
-    if (nsp != ns)
-        for (int r = t; r < ld; r += kDenThreads) { s_f[ns * ld + r] = 0.0; s_i[ns * ld + r] = 0.0; }
-    double a00 = 0.0, a01 = 0.0, a10 = 0.0, a11 = 0.0;
-    int seg = ch.seg0;
-    for (int base = 0; base < ch.nitems; base += tile) {
-        const int nrow = min(tile, ch.nitems - base);
+    const int npass = (ch.nitems + tile - 1) / tile;
+    auto issue = [&](int p, int seg) {
+        const int base = p * tile, nrow = min(tile, ch.nitems - base), b = p & 1;
         if (t < nrow) {
             const int item = base + t;
             int s = seg;
             while (s + 1 < ch.seg1 && segs[s + 1].item0 <= item) ++s;
             const DSeg sgm = segs[s];
             const int64_t c = item - sgm.item0;
-            s_rf[t] = sgm.row_f + c * sgm.step;
-            s_ri[t] = sgm.row_i + c * sgm.step;
-            s_sg[t] = (double)sgm.sign;
-            if (t == nrow - 1) s_next = s;
+            const double *rf = x + (sgm.row_f + c * sgm.step) * nsp;
+            const double *ri = x + (sgm.row_i + c * sgm.step) * nsp;
+            double *df = buf + ((size_t)(2 * b) * tile + t) * nsp;
+            double *di = buf + ((size_t)(2 * b + 1) * tile + t) * nsp;
+            for (int k = 0; k < nsp; k += 2) {
+                cp_async16(df + k, rf + k);
+                cp_async16(di + k, ri + k);
+            }
+            s_sg[b * tile + t] = (double)sgm.sign;
+            if (t == nrow - 1) s_next[b] = s;
         }
-        __syncthreads();
-        seg = s_next;
-        for (int e = t; e < nrow * ns; e += kDenThreads) {
-            const int r = e / ns, k = e - r * ns;
-            s_f[k * ld + r] = x[s_rf[r] * ns + k];
-            s_i[k * ld + r] = s_sg[r] * x[s_ri[r] * ns + k];
+        cp_async_commit();
+    };
+    // two accumulator sets (alternate rows of a thread), summed at the end:
+    // independent FMA chains
+    double a00 = 0.0, a01 = 0.0, a10 = 0.0, a11 = 0.0;
+    double b00 = 0.0, b01 = 0.0, b10 = 0.0, b11 = 0.0;
+    if (npass > 0) issue(0, ch.seg0);
+    __syncthreads();
+    for (int p = 0; p < npass; ++p) {
+        if (p + 1 < npass) {
+            issue(p + 1, s_next[p & 1]);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
-        __syncthreads();
+        __syncthreads();   // pass p's rows and signs are in shared memory
+        const int nrow = min(tile, ch.nitems - p * tile), b = p & 1;
+        const double *__restrict__ F = buf + (size_t)(2 * b) * tile * nsp;
+        const double *__restrict__ I = F + (size_t)tile * nsp;
+        const double *__restrict__ S = s_sg + b * tile;
         if (g < groups) {
-            const double *__restrict__ fa = s_f + f0 * ld, *__restrict__ fb = fa + ld;
-            const double *__restrict__ ia = s_i + i0 * ld, *__restrict__ ib = ia + ld;
-            for (int r = g; r < nrow; r += groups) {
-                const double x0 = fa[r], x1 = fb[r], y0 = ia[r], y1 = ib[r];
-                a00 = fma(x0, y0, a00);
-                a01 = fma(x0, y1, a01);
-                a10 = fma(x1, y0, a10);
-                a11 = fma(x1, y1, a11);
+            int r = g;
+            for (; r + groups < nrow; r += 2 * groups) {
+                const int q = r + groups;
+                const double2 xf = *reinterpret_cast<const double2 *>(F + r * nsp + f0);
+                const double2 yi = *reinterpret_cast<const double2 *>(I + r * nsp + i0);
+                const double2 xg = *reinterpret_cast<const double2 *>(F + q * nsp + f0);
+                const double2 yj = *reinterpret_cast<const double2 *>(I + q * nsp + i0);
+                const double sg = S[r], sh = S[q];
+                const double y0 = sg * yi.x, y1 = sg * yi.y, z0 = sh * yj.x, z1 = sh * yj.y;
+                a00 = fma(xf.x, y0, a00);
+                a01 = fma(xf.x, y1, a01);
+                a10 = fma(xf.y, y0, a10);
+                a11 = fma(xf.y, y1, a11);
+                b00 = fma(xg.x, z0, b00);
+                b01 = fma(xg.x, z1, b01);
+                b10 = fma(xg.y, z0, b10);
+                b11 = fma(xg.y, z1, b11);
+            }
+            if (r < nrow) {
+                const double2 xf = *reinterpret_cast<const double2 *>(F + r * nsp + f0);
+                const double2 yi = *reinterpret_cast<const double2 *>(I + r * nsp + i0);
+                const double sg = S[r];
+                const double y0 = sg * yi.x, y1 = sg * yi.y;
+                a00 = fma(xf.x, y0, a00);
+                a01 = fma(xf.x, y1, a01);
+                a10 = fma(xf.y, y0, a10);
+                a11 = fma(xf.y, y1, a11);
             }
         }
-        __syncthreads();
+        __syncthreads();   // buffer b is free for pass p+2
     }
-    s_red[4 * t + 0] = a00;
-    s_red[4 * t + 1] = a01;
-    s_red[4 * t + 2] = a10;
-    s_red[4 * t + 3] = a11;
+    double *s_red = buf;   // all copies have landed: the buffers are free
+    s_red[4 * t + 0] = a00 + b00;
+    s_red[4 * t + 1] = a01 + b01;
+    s_red[4 * t + 2] = a10 + b10;
+    s_red[4 * t + 3] = a11 + b11;
     __syncthreads();
     const int np = ns * ns;
     for (int p = t; p < np; p += kDenThreads) {
@@ -420,7 +461,7 @@ extern "C" int bsg_density1b(bsg_ctx *ctx, const bsg_density_tables *dt, const d
         dev_free(d_l0); dev_free(d_lid); dev_free(d_outp); dev_free(d_outn);
     };
     const size_t vbytes = sizeof(double) * (size_t)dim * ns;
-    if ((st = dev_alloc(ctx, d_cols, vbytes)) || (st = dev_alloc(ctx, d_x, vbytes)) ||
+    if ((st = dev_alloc(ctx, d_cols, vbytes)) || (st = dev_alloc(ctx, d_x, sizeof(double) * (size_t)dim * den_nsp(ns))) ||
         (st = upload(ctx, d_segs, segs.data(), sizeof(DSeg) * segs.size())) ||
         (st = upload(ctx, d_chunks, chunks.data(), sizeof(DChunk) * chunks.size())) ||
         (st = dev_alloc(ctx, d_part, sizeof(double) * (size_t)np * chunks.size())) ||
@@ -437,7 +478,7 @@ extern "C" int bsg_density1b(bsg_ctx *ctx, const bsg_density_tables *dt, const d
     if (e == cudaSuccess) e = cudaMemsetAsync(d_outn.p, 0, d_outn.bytes, s);
     if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, s);
     if (e == cudaSuccess) {
-        k_interleave<<<148 * 8, 256, 0, s>>>((const double *)d_cols.p, (double *)d_x.p, dim, ns);
+        k_interleave<<<148 * 8, 256, 0, s>>>((const double *)d_cols.p, (double *)d_x.p, dim, ns, den_nsp(ns));
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) {

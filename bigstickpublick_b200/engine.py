@@ -51,7 +51,8 @@ def validate_tables(tables):
 class Hamiltonian:
     def __init__(self, tables, device=0, max_nb=16, validate=True, pn_table_max=0):
         """pn_table_max: largest (b,d) table of one neutron operator before
-        it is split into sub-operators (bsg_config.pn_table_max; 0 = 512)."""
+        it is split into sub-operators (bsg_config.pn_table_max; 0 = 512, or
+        384 for a three-body Hamiltonian)."""
         self.lib = _abi.gpu_lib()
         self.tables = tables
         self._ct = tables.as_ctypes()

@@ -118,7 +118,8 @@ typedef struct bsg_config {
     int32_t pn_table_max;  /* largest (b,d) label-pair table of one neutron
                               operator (the PN-form shared-memory table); a
                               larger operator is split into sub-operators of
-                              at most this many pairs.  0: 512 */
+                              at most this many pairs.  0: 512 (384 for
+                              bsg_create3) */
 } bsg_config;
 
 typedef struct bsg_ctx bsg_ctx;

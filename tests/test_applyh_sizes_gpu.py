@@ -4,15 +4,16 @@ kernels run.
 The small systems of test_applyh_gpu.py all have median rows of at most 32
 positions, so they only reach the one-position-per-lane tiles.  These cases
 reach the tiles that the benchmark workloads use (tile width = the smallest
-power of two times 32 covering the median row, capped by register room):
+power of two times 32 covering the median row, capped at 256 positions for
+FP32 and 128 for FP64 single vectors):
 
 * sd 6p6n (dim 93,710, median row 109): single vectors in 128-position tiles
   (k_rows_f1<4,...> / k_rows_d1<4,...>), nb = 8 in 64-position tiles
   (k_rows<float|double, 8, 2, ...>);
 * pf 4p4n (dim 1,963,461, median row 483): single FP32 vectors in
   256-position tiles at 32 registers (k_rows_f1<8,...>), FP64 in
-  k_rows_d1<8,...>, nb = 8 in k_rows<float, 8, 2, ...>;
-* pf 6p6n (dim 109,954,620): k_rows_f1<8,...> / k_rows_d1<8,...> on the full
+  128-position tiles (k_rows_d1<4,...>), nb = 8 in k_rows<float, 8, 2, ...>;
+* pf 6p6n (dim 109,954,620): k_rows_f1<8,...> / k_rows_d1<4,...> on the full
   vector, compared row by row with the oracle restricted to a few output rows
   (the owner-computes share of applyHbundled_omp, src/bapplyhlibOMP.f90
   :954-1442: one thread's rows, every jump whose output lands there).
