@@ -57,6 +57,13 @@ WORKLOADS = {
     "pf6p5n": ("pf", 6, 5, 1, 5),
     "pf6p6n": ("pf", 6, 6, 0, 5),
 }
+# three-body Hamiltonians (PPP / PPN / PNN / NNN bundles): the seeded pf
+# interaction in three-body form plus a seeded three-body part of 0.1 MeV
+# (model.build_tables3(w2=1, w3=0.1, seed=5)); headline path only (--quick)
+WORKLOADS3 = {
+    "pf4p3n3b": ("pf", 4, 3, 1, 5),
+    "pf4p4n3b": ("pf", 4, 4, 0, 5),
+}
 DEFAULT_WORKLOAD = "pf6p6n"
 
 
@@ -71,8 +78,10 @@ def load_peaks():
 
 def make_tables(name):
     from bigstickpublick_b200 import model
-    shell, np_, nn, jz2, seed = WORKLOADS[name]
+    shell, np_, nn, jz2, seed = WORKLOADS[name] if name in WORKLOADS else WORKLOADS3[name]
     m = model.sd_model(np_, nn, seed=seed, jz2=jz2) if shell == "sd" else model.pf_model(np_, nn, seed=seed, jz2=jz2)
+    if name in WORKLOADS3:
+        return model.build_tables3(m, w2=1.0, w3=0.1, seed=seed)
     return model.build_tables(m)
 
 
@@ -131,10 +140,13 @@ class ClockSampler:
 def alg_bytes(stats, tables, nb, s):
     """B_alg = N_ops*nb*(s_in + 2 s_out) + J_bytes + dim*nb*(s_in + s_out).
     J_bytes = 21 B per stored jump + pstart/nstart (8 B each) + hmat (4 B each)."""
-    nops = stats["n_ops_pp"] + stats["n_ops_nn"] + stats["n_ops_pn"] + stats["n_ops_spe"]
+    nops = sum(stats["n_ops_" + k] for k in ("pp", "nn", "pn", "spe", "ppp", "nnn", "ppn", "pnn"))
     S = tables.s
     jumps = S["np1b"] + S["nn1b"] + S["np2b"] + S["nn2b"]
     jb = 21 * jumps + 8 * (S["nsd_p"] + S["nsd_n"]) + 4 * (S["nmatpp"] + S["nmatnn"] + S["nmatpn"])
+    if getattr(tables, "threebody", False):
+        S3 = tables.s3
+        jb += 21 * (S3["np3b"] + S3["nn3b"]) + 4 * (S3["nmatppp"] + S3["nmatnnn"] + S3["nmatppn"] + S3["nmatpnn"])
     return nops * nb * 3 * s + jb + tables.dim * nb * 2 * s, nops
 
 
@@ -632,7 +644,8 @@ def large_leg(H, T, args):
 def workload_config(args, tables, world):
     """The `config` object of both arms' JSON lines."""
     return {"workload": args.workload, "dim": tables.dim, "nb": args.nb,
-            "interaction": "seeded synthetic isospin TBMEs N(0,1) MeV",
+            "interaction": "seeded synthetic isospin TBMEs N(0,1) MeV" + (
+                ", in three-body form W = V2/(A-2) + 0.1 MeV R (seeded)" if args.workload in WORKLOADS3 else ""),
             "l2": "vectors larger than L2, and a 256 MiB write before every timed matvec; kernel timed alone",
             "parallelism": f"replicas x{world}"}
 
@@ -685,7 +698,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS) + sorted(WORKLOADS3))
     ap.add_argument("--nb", type=int, default=1)
     ap.add_argument("--prec", type=int, default=4, choices=[4, 8])
     ap.add_argument("--ref-budget", type=float, default=4.0, help="seconds of CPU work per reference step")
@@ -711,6 +724,13 @@ def main():
         args.no_cpu = args.no_lanczos = args.no_density = args.no_batch = args.no_large = args.no_tts = True
         args.no_three = True
 
+    if args.workload in WORKLOADS3:
+        # the CPU restatements time the two-body bundles only
+        args.no_cpu = True
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "three-body workloads have no OpenMP CPU port; "
+                              "the threebody leg times the oracle's three-body loops on one thread"}))
+            return 0
     if args.impl == "reference":
         return run_reference(args)
 
