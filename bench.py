@@ -436,7 +436,7 @@ def density_leg(H, tables, k=10, reps=5):
     for _ in range(reps):
         H.apply1b(P, N, X)
         ams.append(H.stats()["apply1b_ms"])
-    return {"workload": "pf4p4n", "states": k, "pairs": k * k, "rows": rows, "kernel_ms": kms,
+    return {"states": k, "pairs": k * k, "rows": rows, "kernel_ms": kms,
             "e2e_ms": float(np.median(wall)) * 1e3, "launches": st["density_launches"],
             "fp64_gflop_per_s": 2.0 * rows * k * k / (kms * 1e-3) / 1e9,
             "gathered_gb_per_s": rows * 2 * k * 8 / (kms * 1e-3) / 1e9,
@@ -711,6 +711,8 @@ def main():
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--no-tts", action="store_true")
     ap.add_argument("--no-three", action="store_true")
+    ap.add_argument("--density", action="store_true",
+                    help="also run the one-body density leg on the headline workload (with --quick)")
     ap.add_argument("--lanczos-iters", type=int, default=300)
     ap.add_argument("--tts-tols", type=float, nargs="+", default=list(TTS_TOLS))
     ap.add_argument("--batch-n", type=int, default=256)
@@ -829,6 +831,8 @@ def main():
     }
     if rank == 0 and not args.no_large and args.workload == "pf6p6n":
         _leg(line, "large", large_leg, H, tables, args)
+    if rank == 0 and args.density:
+        _leg(line, "density", density_leg, H, tables)
     H.close()
     del H
     if rank == 0 and not args.no_lanczos:
