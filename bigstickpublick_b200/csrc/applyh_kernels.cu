@@ -112,7 +112,8 @@ static int launch_one(bsg_ctx *ctx, const T *vin, T *vout, int ld, int v0, int a
         return accumulate ? go(rows_kernel<T, NB, ITEMS, false, kAccumulate, R>())
                           : go(rows_kernel<T, NB, ITEMS, false, kStore, R>());
     };
-    if (NB == 1 && a.sell32)
+    // FP32 reads only the PN part of the 32-bit records; FP64 also their NN labels
+    if (NB == 1 && a.sell32 && (std::is_same<T, float>::value || ctx->rec32_nn))
         e = pick(std::true_type{});
     else
         e = pick(std::false_type{});

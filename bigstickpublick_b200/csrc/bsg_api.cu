@@ -12,11 +12,13 @@
 // that land in it.
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <new>
 #include <numeric>
 #include <set>
+#include <thread>
 #include <unordered_map>
 
 #include "bsg_internal.h"
@@ -100,6 +102,56 @@ const TileSet *get_tiles(bsg_ctx *ctx, int tp) {
 using namespace bsg;
 
 namespace {
+
+// fn(i) for every i in [0, n), on up to 32 host threads taking chunks of
+// `chunk` indices from a shared counter.  Callers write only to locations
+// that index i owns, so the result does not depend on the schedule.
+template <typename F>
+void parallel_for(int64_t n, int64_t chunk, F fn) {
+    const int64_t nchunks = (n + chunk - 1) / chunk;
+    const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    const int nt = (int)std::min<int64_t>((int64_t)hw, nchunks);
+    if (nt <= 1) {
+        for (int64_t i = 0; i < n; ++i) fn(i);
+        return;
+    }
+    std::atomic<int64_t> next{0};
+    std::atomic<bool> oom{false};
+    auto work = [&]() {
+        try {
+            for (;;) {
+                const int64_t c = next.fetch_add(1);
+                if (c >= nchunks || oom) return;
+                const int64_t i1 = std::min(n, (c + 1) * chunk);
+                for (int64_t i = c * chunk; i < i1; ++i) fn(i);
+            }
+        } catch (const std::bad_alloc &) {
+            oom = true;   // reported to the caller below as an allocation failure
+        }
+    };
+    std::vector<std::thread> th;
+    for (int k = 1; k < nt; ++k) th.emplace_back(work);
+    work();
+    for (auto &x : th) x.join();
+    if (oom) throw std::bad_alloc();
+}
+// f() on its own host thread; join() waits and reports an allocation failure
+struct Task {
+    std::thread th;
+    bool oom = false;
+    template <typename F>
+    explicit Task(F f) : th([this, f]() {
+        try {
+            f();
+        } catch (const std::bad_alloc &) {
+            oom = true;
+        }
+    }) {}
+    bool join() {
+        th.join();
+        return !oom;
+    }
+};
 
 struct Validator {
     bsg_ctx *ctx;
@@ -449,6 +501,8 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
     std::vector<std::pair<int32_t, SPEContrib>> spe;
     int64_t ops[4] = {0, 0, 0, 0};
     int64_t ops3[4] = {0, 0, 0, 0};   // PPP, NNN, PPN, PNN
+    struct PPBundle { int64_t ib, px0, px1, nx0, nx1; bool bwd; };
+    std::vector<PPBundle> pp_bundles;
     // one proton-side PN-form contribution (PN, PPN, PNN) of the jump s1 -> s2
     auto pn_contrib = [&](int64_t s1, int64_t s2, int32_t id, int32_t aoff, int32_t coff, int ph,
                           const std::string &what) -> int {
@@ -615,30 +669,10 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
             for (int64_t c = nx0 + 1; c <= nx1; ++c)
                 if (t->nstart[c - 1] != t->nstart[c - 2] + 1)
                     return set_err(ctx, BSG_ERR_UNSUPPORTED, "PP neutron run not contiguous" + where);
-            const int32_t lo = (int32_t)(t->nstart[nx0 - 1] - 1), hi = (int32_t)(t->nstart[nx1 - 1] - 1);
-            for (int64_t x = px0; x <= px1; ++x) {
-                int32_t ri, rf;
-                const int64_t s1 = bwd ? t->p2b_fsd[x - 1] : t->p2b_isd[x - 1];
-                const int64_t s2 = bwd ? t->p2b_isd[x - 1] : t->p2b_fsd[x - 1];
-                if (!rowof(s1, ri) || !rowof(s2, rf))
-                    return set_err(ctx, BSG_ERR_OOB_INDEX, "p2b isd/fsd is not a pstart value" + where);
-                if (hi >= ctx->h_rowlen[ri] || hi >= ctx->h_rowlen[rf])
-                    return set_err(ctx, BSG_ERR_OOB_INDEX, "PP neutron run longer than the row" + where);
-                const int32_t opl = t->p2b_op[x - 1];
-                if (opl < 1 || opl > t->nmatpp) return set_err(ctx, BSG_ERR_OOB_INDEX, "p2b_op outside hmatpp" + where);
-                const int ph = t->p2b_phase[x - 1];
-                if (ph != 1 && ph != -1) return set_err(ctx, BSG_ERR_BAD_TABLE, "p2b_phase not +-1" + where);
-                PPContrib c{};
-                c.q_off = s1;
-                float xme = t->hmatpp[opl - 1];
-                xme = xme * (float)ph;
-                c.me = xme;
-                c.lo = lo;
-                c.hi = hi;
-                pp.push_back({rf, c});
-                pp_op_tmp.push_back(opl);
-                pp_ph_tmp.push_back((int8_t)ph);
-            }
+            // the jumps are checked and turned into contributions after the
+            // loop, all PP bundles at once on host threads (PP contributions
+            // only go to `pp`, which keeps the bundle order)
+            pp_bundles.push_back({ib, px0, px1, nx0, nx1, bwd});
             ops[1] += (px1 - px0 + 1) * (nx1 - nx0 + 1);
         } else if (op == BSG_OP_NN) {
             if (px0 < 1 || px1 > t->nsd_p || nx0 < 1 || nx1 > t->nn2b)
@@ -729,6 +763,52 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
             return set_err(ctx, BSG_ERR_BAD_TABLE, "unknown optype" + where);
         }
     }
+    if (!pp_bundles.empty()) {
+        // PP bundles (src/bapplyhlibOMP.f90:1068-1241), one per task; the
+        // first failing bundle in table order reports
+        // one contribution per jump: every bundle writes its own slice
+        const size_t nb_pp = pp_bundles.size();
+        std::vector<size_t> at0(nb_pp + 1, pp.size());
+        for (size_t j = 0; j < nb_pp; ++j) at0[j + 1] = at0[j] + (size_t)(pp_bundles[j].px1 - pp_bundles[j].px0 + 1);
+        pp.resize(at0[nb_pp]);
+        pp_op_tmp.resize(at0[nb_pp]);
+        pp_ph_tmp.resize(at0[nb_pp]);
+        std::vector<int> bst(nb_pp, BSG_OK);
+        std::vector<std::string> bmsg(nb_pp);
+        parallel_for((int64_t)nb_pp, 1, [&](int64_t j) {
+            const PPBundle &B = pp_bundles[j];
+            const int32_t lo = (int32_t)(t->nstart[B.nx0 - 1] - 1), hi = (int32_t)(t->nstart[B.nx1 - 1] - 1);
+            auto fail = [&](int code, const char *m) {
+                bst[j] = code;
+                bmsg[j] = std::string(m) + " (opbundle " + std::to_string(B.ib + 1) + ")";
+            };
+            size_t at = at0[j];
+            for (int64_t x = B.px0; x <= B.px1; ++x, ++at) {
+                int32_t ri, rf;
+                const int64_t s1 = B.bwd ? t->p2b_fsd[x - 1] : t->p2b_isd[x - 1];
+                const int64_t s2 = B.bwd ? t->p2b_isd[x - 1] : t->p2b_fsd[x - 1];
+                if (!rowof(s1, ri) || !rowof(s2, rf)) return fail(BSG_ERR_OOB_INDEX, "p2b isd/fsd is not a pstart value");
+                if (hi >= ctx->h_rowlen[ri] || hi >= ctx->h_rowlen[rf])
+                    return fail(BSG_ERR_OOB_INDEX, "PP neutron run longer than the row");
+                const int32_t opl = t->p2b_op[x - 1];
+                if (opl < 1 || opl > t->nmatpp) return fail(BSG_ERR_OOB_INDEX, "p2b_op outside hmatpp");
+                const int ph = t->p2b_phase[x - 1];
+                if (ph != 1 && ph != -1) return fail(BSG_ERR_BAD_TABLE, "p2b_phase not +-1");
+                PPContrib c{};
+                c.q_off = s1;
+                float xme = t->hmatpp[opl - 1];
+                xme = xme * (float)ph;
+                c.me = xme;
+                c.lo = lo;
+                c.hi = hi;
+                pp[at] = {rf, c};
+                pp_op_tmp[at] = opl;
+                pp_ph_tmp[at] = (int8_t)ph;
+            }
+        });
+        for (size_t j = 0; j < nb_pp; ++j)
+            if (bst[j]) return set_err(ctx, bst[j], bmsg[j]);
+    }
     ctx->stats.n_ops_spe = ops[0];
     ctx->stats.n_ops_pp = ops[1];
     ctx->stats.n_ops_nn = ops[2];
@@ -742,10 +822,25 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
     // longest-processing-time (heaviest first to the least loaded warp), then
     // flatten into CSR over (row, warp) slots.  Inside a slot the bundle order
     // is kept (PN grouped by neutron operator for cache reuse).
-    std::stable_sort(pn.begin(), pn.end(), [](const std::pair<int32_t, PNContrib> &x, const std::pair<int32_t, PNContrib> &y) {
-        if (x.first != y.first) return x.first < y.first;
-        return x.second.nop < y.second.nop;
-    });
+    {
+        // stable sort by (row, operator): a counting sort by row, then each
+        // row's run stably by operator (rows in parallel)
+        std::vector<int64_t> rs(nrows + 1, 0);
+        for (auto &e : pn) rs[e.first + 1]++;
+        for (int64_t r = 0; r < nrows; ++r) rs[r + 1] += rs[r];
+        std::vector<std::pair<int32_t, PNContrib>> sorted(pn.size());
+        {
+            std::vector<int64_t> fill(rs.begin(), rs.end() - 1);
+            for (auto &e : pn) sorted[fill[e.first]++] = e;
+        }
+        parallel_for(nrows, 256, [&](int64_t r) {
+            std::stable_sort(sorted.begin() + rs[r], sorted.begin() + rs[r + 1],
+                             [](const std::pair<int32_t, PNContrib> &x, const std::pair<int32_t, PNContrib> &y) {
+                                 return x.second.nop < y.second.nop;
+                             });
+        });
+        pn.swap(sorted);
+    }
     auto nrec_of = [&](int32_t id) -> int64_t { return nptr_all[nops[id].ptr_base + nops[id].nout]; };
     // ---- sliced records: per operator, output positions in slices of 32;
     // a slice holds its longest position's count of 32-record rows, record k
@@ -755,44 +850,76 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
     // 32-bit copy when every input position, (b,d) index and hmatnn label fits
     int32_t max_nbd_all = 0;
     for (const NOp &op : nops) max_nbd_all = std::max(max_nbd_all, op.nbd);
+    // PN records need the position and the (b,d) index to fit; NN records
+    // carry the hmatnn label, which only the FP64 kernels read: when the
+    // labels do not fit, the NN entries stay zero and FP64 keeps the 8-byte
+    // records (ctx->rec32_nn)
     const int64_t nmatnn_all = t->nmatnn + (three ? t3->nmatnnn : 0);
-    const bool pack32 = ctx->max_rowlen <= 65536 && nmatnn_all <= 32768 && max_nbd_all <= 32768;
+    const bool pack32 = ctx->max_rowlen <= 65536 && max_nbd_all <= 32768;
+    const bool nn32 = pack32 && nmatnn_all <= 32768;
+    ctx->rec32_nn = nn32;
     std::vector<uint32_t> sell32_all;
-    for (NOp &op : nops) {
-        op.sell_base = (int64_t)sell_all.size();
-        op.slice_base = (int64_t)slice_off_all.size();
-        const int32_t *ptr = nptr_all.data() + op.ptr_base;
-        const int nslice = (op.nout + 31) / 32;
-        int64_t off = 0;
-        for (int sl = 0; sl < nslice; ++sl) {
-            int32_t width = 0;
-            for (int l = 0; l < 32 && 32 * sl + l < op.nout; ++l)
-                width = std::max(width, ptr[32 * sl + l + 1] - ptr[32 * sl + l]);
-            if (off > INT32_MAX) return V.fail("a neutron operator has more than 2^31 sliced records");
-            slice_off_all.push_back((int32_t)off);
-            const size_t row0 = sell_all.size();
-            sell_all.resize(row0 + (size_t)32 * width, make_int2(0, 0));
-            if (pack32) sell32_all.resize(row0 + (size_t)32 * width, 0u);
-            for (int l = 0; l < 32 && 32 * sl + l < op.nout; ++l)
-                for (int32_t k = ptr[32 * sl + l]; k < ptr[32 * sl + l + 1]; ++k) {
-                    int2 r;
-                    uint32_t r32;
-                    if (op.kind == 1) {
-                        const PNRec &pr = pnrec_all[op.rec_base + k];
-                        std::memcpy(&r, &pr, sizeof(int2));
-                        r32 = (uint32_t)pr.in | ((uint32_t)pr.k << 16) | (pr.ph < 0 ? 0x80000000u : 0u);
-                    } else {
-                        std::memcpy(&r, &nnrec_all[op.rec_base + k], sizeof(int2));
-                        r32 = (uint32_t)nnrec_all[op.rec_base + k].in |
-                              ((uint32_t)(nnrec_op_all[op.rec_base + k] - 1) << 16) |
-                              (nnrec_ph_all[op.rec_base + k] < 0 ? 0x80000000u : 0u);
-                    }
-                    const size_t at = row0 + (size_t)32 * (k - ptr[32 * sl + l]) + l;
-                    sell_all[at] = r;
-                    if (pack32) sell32_all[at] = r32;
-                }
-            off += (int64_t)32 * width;
+    {
+        // sizes per operator (parallel), offsets (in operator order), fill (parallel)
+        const int64_t nop_all = (int64_t)nops.size();
+        std::vector<int64_t> op_recs(nop_all, 0);
+        std::atomic<bool> too_big{false};
+        parallel_for(nop_all, 16, [&](int64_t o) {
+            const NOp &op = nops[o];
+            const int32_t *ptr = nptr_all.data() + op.ptr_base;
+            int64_t off = 0;
+            for (int sl = 0; sl < (op.nout + 31) / 32; ++sl) {
+                int32_t width = 0;
+                for (int l = 0; l < 32 && 32 * sl + l < op.nout; ++l)
+                    width = std::max(width, ptr[32 * sl + l + 1] - ptr[32 * sl + l]);
+                if (off > INT32_MAX) too_big = true;
+                off += (int64_t)32 * width;
+            }
+            op_recs[o] = off;
+        });
+        if (too_big) return V.fail("a neutron operator has more than 2^31 sliced records");
+        int64_t nrec_tot = 0, nslice_tot = 0;
+        for (int64_t o = 0; o < nop_all; ++o) {
+            nops[o].sell_base = nrec_tot;
+            nops[o].slice_base = nslice_tot;
+            nrec_tot += op_recs[o];
+            nslice_tot += (nops[o].nout + 31) / 32;
         }
+        sell_all.assign((size_t)nrec_tot, make_int2(0, 0));   // padding rows hold {0, 0}
+        if (pack32) sell32_all.assign((size_t)nrec_tot, 0u);
+        slice_off_all.assign((size_t)nslice_tot, 0);
+        parallel_for(nop_all, 16, [&](int64_t o) {
+            const NOp &op = nops[o];
+            const int32_t *ptr = nptr_all.data() + op.ptr_base;
+            int64_t off = 0;
+            for (int sl = 0; sl < (op.nout + 31) / 32; ++sl) {
+                int32_t width = 0;
+                for (int l = 0; l < 32 && 32 * sl + l < op.nout; ++l)
+                    width = std::max(width, ptr[32 * sl + l + 1] - ptr[32 * sl + l]);
+                slice_off_all[op.slice_base + sl] = (int32_t)off;
+                const size_t row0 = (size_t)(op.sell_base + off);
+                for (int l = 0; l < 32 && 32 * sl + l < op.nout; ++l)
+                    for (int32_t k = ptr[32 * sl + l]; k < ptr[32 * sl + l + 1]; ++k) {
+                        int2 r;
+                        uint32_t r32;
+                        if (op.kind == 1) {
+                            const PNRec &pr = pnrec_all[op.rec_base + k];
+                            std::memcpy(&r, &pr, sizeof(int2));
+                            r32 = (uint32_t)pr.in | ((uint32_t)pr.k << 16) | (pr.ph < 0 ? 0x80000000u : 0u);
+                        } else {
+                            std::memcpy(&r, &nnrec_all[op.rec_base + k], sizeof(int2));
+                            r32 = nn32 ? (uint32_t)nnrec_all[op.rec_base + k].in |
+                                             ((uint32_t)(nnrec_op_all[op.rec_base + k] - 1) << 16) |
+                                             (nnrec_ph_all[op.rec_base + k] < 0 ? 0x80000000u : 0u)
+                                       : 0u;
+                        }
+                        const size_t at = row0 + (size_t)32 * (k - ptr[32 * sl + l]) + l;
+                        sell_all[at] = r;
+                        if (pack32) sell32_all[at] = r32;
+                    }
+                off += (int64_t)32 * width;
+            }
+        });
     }
     const int W = kRowWarps;
     std::vector<uint8_t> w_pp(pp.size()), w_nn(nn.size()), w_pn(pn.size()), w_spe(spe.size());
@@ -810,8 +937,9 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
             for (size_t i = 0; i < v.size(); ++i) start[k][fill[v[i].first]++] = (int32_t)i;
         };
         bucket(pp, 0); bucket(nn, 1); bucket(pn, 2); bucket(spe, 3);
-        std::vector<Ref> refs;
-        for (int64_t r = 0; r < nrows; ++r) {
+        // rows are independent: each writes only its own contributions' warps
+        parallel_for(nrows, 256, [&](int64_t r) {
+            thread_local std::vector<Ref> refs;
             refs.clear();
             for (int32_t q = cnt[0][r]; q < cnt[0][r + 1]; ++q) {
                 const auto &c = pp[start[0][q]].second;
@@ -836,7 +964,7 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
                 load[best] += f.wgt;
                 (f.type == 0 ? w_pp : f.type == 1 ? w_nn : f.type == 2 ? w_pn : w_spe)[f.idx] = (uint8_t)best;
             }
-        }
+        });
     }
     // CSR over (row, warp) slots; inside a slot the contributions keep their
     // order (a counting sort by slot, stable in the input order)
@@ -844,7 +972,7 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
                        std::vector<int32_t> *perm) {
         const int64_t nslot = nrows * W;
         std::vector<int64_t> key(v.size());
-        for (size_t i = 0; i < v.size(); ++i) key[i] = (int64_t)v[i].first * W + wv[i];
+        parallel_for((int64_t)v.size(), 1 << 16, [&](int64_t i) { key[i] = (int64_t)v[i].first * W + wv[i]; });
         ptr.assign(nslot + 1, 0);
         for (int64_t k : key) ptr[k + 1]++;
         for (int64_t r = 0; r < nslot; ++r) ptr[r + 1] += ptr[r];
@@ -855,25 +983,37 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
         }
         flat.resize(v.size());
         if (perm) perm->resize(v.size());
-        for (size_t k = 0; k < idx.size(); ++k) {
+        parallel_for((int64_t)idx.size(), 1 << 16, [&](int64_t k) {
             flat[k] = v[idx[k]].second;
             if (perm) (*perm)[k] = (int32_t)idx[k];
-        }
+        });
     };
     if (pp.size() > (size_t)INT32_MAX || pn.size() > (size_t)INT32_MAX)
         return set_err(ctx, BSG_ERR_UNSUPPORTED, "more than 2^31 row contributions");
     std::vector<int32_t> spe_ptr, pp_perm;
     std::vector<SPEContrib> h_spe;
-    by_slot(pp, w_pp, ctx->h_pp_ptr, ctx->h_pp, &pp_perm);
+    {
+        // the four slot layouts are independent
+        Task tnn([&]() { by_slot(nn, w_nn, ctx->h_nn_ptr, ctx->h_nn, nullptr); });
+        Task tpn([&]() { by_slot(pn, w_pn, ctx->h_pn_ptr, ctx->h_pn, nullptr); });
+        Task tspe([&]() { by_slot(spe, w_spe, spe_ptr, h_spe, nullptr); });
+        bool ok = true;
+        try {
+            by_slot(pp, w_pp, ctx->h_pp_ptr, ctx->h_pp, &pp_perm);
+        } catch (const std::bad_alloc &) {
+            ok = false;
+        }
+        ok = tnn.join() && ok;
+        ok = tpn.join() && ok;
+        ok = tspe.join() && ok;
+        if (!ok) throw std::bad_alloc();
+    }
     ctx->h_pp_op.resize(pp_perm.size());
     ctx->h_pp_ph.resize(pp_perm.size());
     for (size_t k = 0; k < pp_perm.size(); ++k) {
         ctx->h_pp_op[k] = pp_op_tmp[pp_perm[k]];
         ctx->h_pp_ph[k] = pp_ph_tmp[pp_perm[k]];
     }
-    by_slot(nn, w_nn, ctx->h_nn_ptr, ctx->h_nn, nullptr);
-    by_slot(pn, w_pn, ctx->h_pn_ptr, ctx->h_pn, nullptr);
-    by_slot(spe, w_spe, spe_ptr, h_spe, nullptr);
     ctx->h_nops = nops;
     ctx->h_nnrec_op = nnrec_op_all;
 

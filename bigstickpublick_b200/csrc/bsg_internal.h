@@ -143,6 +143,7 @@ struct bsg_ctx {
     std::string last_error;
     int last_status = 0;      // status of the last set_err
     bool threebody = false;   // built by bsg_create3 (SPE + PPP/NNN/PPN/PNN)
+    bool rec32_nn = false;    // the 32-bit records hold NN labels too (FP64 reads them)
     bsg_tables t{};           // sizes only (pointers are host-owned by caller)
     int64_t dim = 0, nrows = 0;
     int32_t max_rowlen = 0;
