@@ -35,6 +35,8 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
+#include <thread>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -47,6 +49,33 @@
 namespace {
 
 thread_local std::string g_err;
+
+// fn(i) for every i in [0, n) on up to 32 host threads, indices taken from a
+// shared counter; each index writes only what it owns, so the tables do not
+// depend on the schedule
+template <typename F>
+void parallel_for(int64_t n, F fn) {
+    const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    const int nt = (int)std::min<int64_t>((int64_t)hw, n);
+    if (nt <= 1) {
+        for (int64_t i = 0; i < n; ++i) fn(i);
+        return;
+    }
+    std::atomic<int64_t> next{0};
+    std::atomic<bool> oom{false};
+    auto work = [&]() {
+        try {
+            for (int64_t i; (i = next.fetch_add(1)) < n && !oom;) fn(i);
+        } catch (const std::bad_alloc &) {
+            oom = true;
+        }
+    };
+    std::vector<std::thread> th;
+    for (int k = 1; k < nt; ++k) th.emplace_back(work);
+    work();
+    for (auto &x : th) x.join();
+    if (oom) throw std::bad_alloc();
+}
 
 struct SPS {
     int nr, l, j2, m2, w, par, orb;
@@ -998,33 +1027,49 @@ int build(const bsg_model_spec *s, const bsg_model3_spec *s3, Built &B) {
     // (SD, then annihilated k, then created i) and bucketed by the final
     // sector; gen1 appends one bucket, so each (is, fs) keeps that order
     std::map<std::pair<const SpeciesBasis *, int>, std::vector<Jumps1>> jumps1_from;
+    // every one-body jump out of sector `is`, bucketed by final sector
+    auto jumps1_out = [&](const SpeciesBasis &sb, const std::vector<int64_t> &xstart, int is) {
+        std::vector<Jumps1> by(sb.sectors.size());
+        const Sector &S = sb.sectors[is];
+        const int ns = sb.nl + sb.nr;
+        for (int64_t sd = S.xsdstart - 1; sd < S.xsdend; ++sd) {
+            const uint64_t bits = sb.sd_bits[sd];
+            for (int k = 0; k < ns; ++k) {
+                if (!(bits >> k & 1ull)) continue;
+                for (int i = 0; i < ns; ++i) {
+                    if (i != k && (bits >> i & 1ull)) continue;
+                    const uint64_t nb2 = (bits & ~(1ull << k)) | (1ull << i);
+                    const int64_t f = sb.find_sd(nb2);
+                    if (f < 0) continue;
+                    Jumps1 &B1 = by[sb.sd_sector[f]];
+                    B1.isd.push_back(xstart[sd]);
+                    B1.fsd.push_back(xstart[f]);
+                    B1.cop.push_back((int16_t)signed_label(sb, i));
+                    B1.dop.push_back((int16_t)signed_label(sb, k));
+                    B1.phase.push_back((int8_t)phase1(bits, i, k));
+                }
+            }
+        }
+        return by;
+    };
+    // fill the cache for every source sector of both species on host threads
+    // (the generators below then only copy buckets)
+    if (s->np >= 1 || s->nn >= 1) {
+        std::vector<std::pair<SpeciesBasis *, int>> srcs;
+        for (int is = 0; is < nps; ++is) srcs.push_back({&B.pb, is});
+        for (int is = 0; is < nns; ++is) srcs.push_back({&B.nb, is});
+        std::vector<std::vector<Jumps1>> made(srcs.size());
+        parallel_for((int64_t)srcs.size(), [&](int64_t j) {
+            const SpeciesBasis &sb = *srcs[j].first;
+            made[j] = jumps1_out(sb, &sb == &B.pb ? B.pstart : B.nstart, srcs[j].second);
+        });
+        for (size_t j = 0; j < srcs.size(); ++j)
+            jumps1_from.emplace(std::make_pair((const SpeciesBasis *)srcs[j].first, srcs[j].second), std::move(made[j]));
+    }
     auto gen1 = [&](SpeciesBasis &sb, const std::vector<int64_t> &xstart, int is, int fs, Jumps1 &J) {
         auto key = std::make_pair((const SpeciesBasis *)&sb, is);
         auto it = jumps1_from.find(key);
-        if (it == jumps1_from.end()) {
-            std::vector<Jumps1> by(sb.sectors.size());
-            const Sector &S = sb.sectors[is];
-            const int ns = sb.nl + sb.nr;
-            for (int64_t sd = S.xsdstart - 1; sd < S.xsdend; ++sd) {
-                const uint64_t bits = sb.sd_bits[sd];
-                for (int k = 0; k < ns; ++k) {
-                    if (!(bits >> k & 1ull)) continue;
-                    for (int i = 0; i < ns; ++i) {
-                        if (i != k && (bits >> i & 1ull)) continue;
-                        const uint64_t nb2 = (bits & ~(1ull << k)) | (1ull << i);
-                        const int64_t f = sb.find_sd(nb2);
-                        if (f < 0) continue;
-                        Jumps1 &B1 = by[sb.sd_sector[f]];
-                        B1.isd.push_back(xstart[sd]);
-                        B1.fsd.push_back(xstart[f]);
-                        B1.cop.push_back((int16_t)signed_label(sb, i));
-                        B1.dop.push_back((int16_t)signed_label(sb, k));
-                        B1.phase.push_back((int8_t)phase1(bits, i, k));
-                    }
-                }
-            }
-            it = jumps1_from.emplace(key, std::move(by)).first;
-        }
+        if (it == jumps1_from.end()) it = jumps1_from.emplace(key, jumps1_out(sb, xstart, is)).first;
         const Jumps1 &src = it->second[fs];
         J.isd.insert(J.isd.end(), src.isd.begin(), src.isd.end());
         J.fsd.insert(J.fsd.end(), src.fsd.begin(), src.fsd.end());
@@ -1097,26 +1142,28 @@ int build(const bsg_model_spec *s, const bsg_model3_spec *s3, Built &B) {
             }
             B.p1sj.push_back(sj);
         }
-    if (s->np >= 2 && !three) {
-        const auto by_sec = pairs_by_section(B.pb, B.ppairs);
-        for (int is = 0; is < nps; ++is) {
+    // two-body jumps inside each sector: sectors on host threads, appended in
+    // sector order
+    auto two_body = [&](SpeciesBasis &sb, const std::vector<int64_t> &xstart, const Pairs &P, int nsec, Jumps2 &out,
+                        std::vector<SectJump> &sjs) {
+        const auto by_sec = pairs_by_section(sb, P);
+        std::vector<Jumps2> per(nsec);
+        parallel_for(nsec, [&](int64_t is) { gen2(sb, xstart, P, by_sec, (int)is, (int)is, per[is]); });
+        for (int is = 0; is < nsec; ++is) {
             SectJump sj;
             sj.is = is; sj.fs = is; sj.diag = true;
-            sj.nstart = (int64_t)B.p2.isd.size();
-            sj.njumps = gen2(B.pb, B.pstart, B.ppairs, by_sec, is, is, B.p2);
-            if (sj.njumps > 0) B.p2sj.push_back(sj);
+            sj.nstart = (int64_t)out.isd.size();
+            sj.njumps = (int64_t)per[is].isd.size();
+            if (sj.njumps == 0) continue;
+            out.isd.insert(out.isd.end(), per[is].isd.begin(), per[is].isd.end());
+            out.fsd.insert(out.fsd.end(), per[is].fsd.begin(), per[is].fsd.end());
+            out.op.insert(out.op.end(), per[is].op.begin(), per[is].op.end());
+            out.phase.insert(out.phase.end(), per[is].phase.begin(), per[is].phase.end());
+            sjs.push_back(sj);
         }
-    }
-    if (s->nn >= 2 && !three) {
-        const auto by_sec = pairs_by_section(B.nb, B.npairs);
-        for (int is = 0; is < nns; ++is) {
-            SectJump sj;
-            sj.is = is; sj.fs = is; sj.diag = true;
-            sj.nstart = (int64_t)B.n2.isd.size();
-            sj.njumps = gen2(B.nb, B.nstart, B.npairs, by_sec, is, is, B.n2);
-            if (sj.njumps > 0) B.n2sj.push_back(sj);
-        }
-    }
+    };
+    if (s->np >= 2 && !three) two_body(B.pb, B.pstart, B.ppairs, nps, B.p2, B.p2sj);
+    if (s->nn >= 2 && !three) two_body(B.nb, B.nstart, B.npairs, nns, B.n2, B.n2sj);
 
     // ---- three-body run: triplet tables, matrix elements and jumps
     std::vector<SectJump> p3sj, n3sj, p2xsj, n2xsj;
@@ -1521,14 +1568,32 @@ int build(const bsg_model_spec *s, const bsg_model3_spec *s3, Built &B) {
 
     // ---- sort_bundled_jumps (src/bsortjumpslib.f90:21-175): per PN bundle,
     // protons on fsd, neutrons on isd
-    for (size_t ib = 0; ib < B.optype.size(); ++ib) {
-        if (B.optype[ib] != BSG_OP_PN) continue;
-        const int64_t sp0 = B.pxstart[ib] - 1, np_ = B.pxend[ib] - sp0;
-        const int64_t sn0 = B.nxstart[ib] - 1, nn_ = B.nxend[ib] - sn0;
-        shell_sort_1b(np_, B.p1.isd.data() + sp0, B.p1.fsd.data() + sp0, B.p1.cop.data() + sp0,
-                      B.p1.dop.data() + sp0, B.p1.phase.data() + sp0);
-        shell_sort_1b(nn_, B.n1.fsd.data() + sn0, B.n1.isd.data() + sn0, B.n1.cop.data() + sn0,
-                      B.n1.dop.data() + sn0, B.n1.phase.data() + sn0);
+    // The 'f', 'h' and 'b' bundles of a sector jump share its ranges, and the
+    // sort leaves a sorted range as it is, so each distinct range is sorted
+    // once; the ranges of different sector jumps are disjoint, so they are
+    // sorted on host threads.
+    {
+        std::vector<std::pair<int64_t, int64_t>> pr, nr;   // (0-based start, length)
+        for (size_t ib = 0; ib < B.optype.size(); ++ib) {
+            if (B.optype[ib] != BSG_OP_PN) continue;
+            pr.push_back({B.pxstart[ib] - 1, B.pxend[ib] - B.pxstart[ib] + 1});
+            nr.push_back({B.nxstart[ib] - 1, B.nxend[ib] - B.nxstart[ib] + 1});
+        }
+        for (auto *v : {&pr, &nr}) {
+            std::sort(v->begin(), v->end());
+            v->erase(std::unique(v->begin(), v->end()), v->end());
+        }
+        parallel_for((int64_t)(pr.size() + nr.size()), [&](int64_t j) {
+            if (j < (int64_t)pr.size()) {
+                const int64_t sp0 = pr[j].first, np_ = pr[j].second;
+                shell_sort_1b(np_, B.p1.isd.data() + sp0, B.p1.fsd.data() + sp0, B.p1.cop.data() + sp0,
+                              B.p1.dop.data() + sp0, B.p1.phase.data() + sp0);
+            } else {
+                const int64_t sn0 = nr[j - pr.size()].first, nn_ = nr[j - pr.size()].second;
+                shell_sort_1b(nn_, B.n1.fsd.data() + sn0, B.n1.isd.data() + sn0, B.n1.cop.data() + sn0,
+                              B.n1.dop.data() + sn0, B.n1.phase.data() + sn0);
+            }
+        });
     }
 
     // ---- sector / s.p. bookkeeping for the caller
