@@ -106,10 +106,12 @@ namespace {
 // fn(i) for every i in [0, n), on up to 32 host threads taking chunks of
 // `chunk` indices from a shared counter.  Callers write only to locations
 // that index i owns, so the result does not depend on the schedule.
+// max_threads 1 runs inline: small systems (and the many systems of a batch,
+// which are already set up on parallel host threads) skip the thread start-up.
 template <typename F>
-void parallel_for(int64_t n, int64_t chunk, F fn) {
+void parallel_for(int64_t n, int64_t chunk, F fn, int max_threads = 32) {
     const int64_t nchunks = (n + chunk - 1) / chunk;
-    const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    const unsigned hw = std::max(1u, std::min((unsigned)std::max(1, max_threads), std::thread::hardware_concurrency()));
     const int nt = (int)std::min<int64_t>((int64_t)hw, nchunks);
     if (nt <= 1) {
         for (int64_t i = 0; i < n; ++i) fn(i);
@@ -182,6 +184,8 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
     Validator V{ctx, ""};
     const bool three = (t3 != nullptr);
     ctx->threebody = three;
+    // host threads for the derivation only where it is worth their start-up
+    const int nthr = t->dimbasis >= (int64_t)1 << 20 ? 32 : 1;
     // ---- basic presence and sizes
     if (t->dimbasis <= 0 || t->nsd_p <= 0 || t->nsd_n <= 0)
         return set_err(ctx, BSG_ERR_BAD_TABLE, "empty basis");
@@ -805,7 +809,7 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
                 pp_op_tmp[at] = opl;
                 pp_ph_tmp[at] = (int8_t)ph;
             }
-        });
+        }, nthr);
         for (size_t j = 0; j < nb_pp; ++j)
             if (bst[j]) return set_err(ctx, bst[j], bmsg[j]);
     }
@@ -838,7 +842,7 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
                              [](const std::pair<int32_t, PNContrib> &x, const std::pair<int32_t, PNContrib> &y) {
                                  return x.second.nop < y.second.nop;
                              });
-        });
+        }, nthr);
         pn.swap(sorted);
     }
     auto nrec_of = [&](int32_t id) -> int64_t { return nptr_all[nops[id].ptr_base + nops[id].nout]; };
@@ -876,7 +880,7 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
                 off += (int64_t)32 * width;
             }
             op_recs[o] = off;
-        });
+        }, nthr);
         if (too_big) return V.fail("a neutron operator has more than 2^31 sliced records");
         int64_t nrec_tot = 0, nslice_tot = 0;
         for (int64_t o = 0; o < nop_all; ++o) {
@@ -919,7 +923,7 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
                     }
                 off += (int64_t)32 * width;
             }
-        });
+        }, nthr);
     }
     const int W = kRowWarps;
     std::vector<uint8_t> w_pp(pp.size()), w_nn(nn.size()), w_pn(pn.size()), w_spe(spe.size());
@@ -964,7 +968,7 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
                 load[best] += f.wgt;
                 (f.type == 0 ? w_pp : f.type == 1 ? w_nn : f.type == 2 ? w_pn : w_spe)[f.idx] = (uint8_t)best;
             }
-        });
+        }, nthr);
     }
     // CSR over (row, warp) slots; inside a slot the contributions keep their
     // order (a counting sort by slot, stable in the input order)
@@ -972,7 +976,7 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
                        std::vector<int32_t> *perm) {
         const int64_t nslot = nrows * W;
         std::vector<int64_t> key(v.size());
-        parallel_for((int64_t)v.size(), 1 << 16, [&](int64_t i) { key[i] = (int64_t)v[i].first * W + wv[i]; });
+        parallel_for((int64_t)v.size(), 1 << 16, [&](int64_t i) { key[i] = (int64_t)v[i].first * W + wv[i]; }, nthr);
         ptr.assign(nslot + 1, 0);
         for (int64_t k : key) ptr[k + 1]++;
         for (int64_t r = 0; r < nslot; ++r) ptr[r + 1] += ptr[r];
@@ -986,13 +990,18 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
         parallel_for((int64_t)idx.size(), 1 << 16, [&](int64_t k) {
             flat[k] = v[idx[k]].second;
             if (perm) (*perm)[k] = (int32_t)idx[k];
-        });
+        }, nthr);
     };
     if (pp.size() > (size_t)INT32_MAX || pn.size() > (size_t)INT32_MAX)
         return set_err(ctx, BSG_ERR_UNSUPPORTED, "more than 2^31 row contributions");
     std::vector<int32_t> spe_ptr, pp_perm;
     std::vector<SPEContrib> h_spe;
-    {
+    if (nthr == 1) {
+        by_slot(pp, w_pp, ctx->h_pp_ptr, ctx->h_pp, &pp_perm);
+        by_slot(nn, w_nn, ctx->h_nn_ptr, ctx->h_nn, nullptr);
+        by_slot(pn, w_pn, ctx->h_pn_ptr, ctx->h_pn, nullptr);
+        by_slot(spe, w_spe, spe_ptr, h_spe, nullptr);
+    } else {
         // the four slot layouts are independent
         Task tnn([&]() { by_slot(nn, w_nn, ctx->h_nn_ptr, ctx->h_nn, nullptr); });
         Task tpn([&]() { by_slot(pn, w_pn, ctx->h_pn_ptr, ctx->h_pn, nullptr); });
