@@ -49,13 +49,17 @@
 namespace {
 
 thread_local std::string g_err;
+// host threads one build may use: set from the basis size once it is known
+// (small systems build in one thread, so many builds can run side by side
+// without oversubscribing the cores)
+thread_local unsigned g_max_threads = 1;
 
-// fn(i) for every i in [0, n) on up to 32 host threads, indices taken from a
-// shared counter; each index writes only what it owns, so the tables do not
-// depend on the schedule
+// fn(i) for every i in [0, n) on up to g_max_threads host threads, indices
+// taken from a shared counter; each index writes only what it owns, so the
+// tables do not depend on the schedule
 template <typename F>
 void parallel_for(int64_t n, F fn) {
-    const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    const unsigned hw = std::max(1u, std::min(g_max_threads, std::thread::hardware_concurrency()));
     const int nt = (int)std::min<int64_t>((int64_t)hw, n);
     if (nt <= 1) {
         for (int64_t i = 0; i < n; ++i) fn(i);
@@ -762,6 +766,7 @@ void compress(std::vector<std::pair<int, double>> &v) {
 
 int build(const bsg_model_spec *s, const bsg_model3_spec *s3, Built &B) {
     init_lfact();
+    g_max_threads = 1;
     const bool three = (s3 != nullptr);
     B.three = three;
     if (!s || s->norb <= 0 || !s->orbits) { g_err = "bad model spec"; return BSG_ERR_ARG; }
@@ -862,6 +867,7 @@ int build(const bsg_model_spec *s, const bsg_model3_spec *s3, Built &B) {
     }
     dimbasis -= 1;
     if (pcount != nsdp || ncount != nsdn) { g_err = "combinebasis count mismatch"; return BSG_ERR_BAD_TABLE; }
+    g_max_threads = dimbasis >= ((int64_t)1 << 18) ? 32u : 1u;
 
     // ---- interaction: coupled V_JT canonicalized with provenance
     Interaction I;
