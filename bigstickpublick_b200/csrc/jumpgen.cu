@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "bsg_internal.h"
+#include "ref_order.h"
 
 struct bsg_jumpgen {
     int device = 0;
@@ -382,22 +383,18 @@ int bsg_jumpgen_create(int device, const bsg_species *sp, bsg_jumpgen **out) {
         }
         dense[b] = (int32_t)k;
     }
-    // pairs q1 < q2 in the reference's order (src/bjumplib_weld.f90:635-642):
-    // sections of equal M = (m1+m2)/2 and parity, M ascending, parity 1 then
-    // 2, within a section the triangle index q1 + (q2-1)(q2-2)/2 (1-based)
-    struct P { int q1, q2, M, pidx; int64_t tri; };
+    // pairs q1 < q2 in the reference's order: generated with the higher state
+    // outer (count_create_pairs, src/btbme.f90:208-308), then sortpair
+    // (:548-703) into sections of equal M = (m1+m2)/2 and parity, M
+    // descending, parity 1 then 2
+    struct P { int q1, q2, M, pidx; };
     std::vector<P> v;
-    for (int q2 = 0; q2 < ns; ++q2)
+    for (int q2 = 1; q2 < ns; ++q2)
         for (int q1 = 0; q1 < q2; ++q1) {
             const int pp = sp->par[q1] * sp->par[q2];
-            v.push_back(P{q1, q2, (sp->m2[q1] + sp->m2[q2]) / 2, pp > 0 ? 1 : 2,
-                          (int64_t)(q1 + 1) + (int64_t)q2 * (q2 - 1) / 2});
+            v.push_back(P{q1, q2, (sp->m2[q1] + sp->m2[q2]) / 2, pp > 0 ? 1 : 2});
         }
-    std::stable_sort(v.begin(), v.end(), [](const P &x, const P &y) {
-        if (x.M != y.M) return x.M < y.M;
-        if (x.pidx != y.pidx) return x.pidx < y.pidx;
-        return x.tri < y.tri;
-    });
+    bsg_order::sortpair(v);
     std::vector<int32_t> pair_at((size_t)ns * ns, 0), pair_sec(v.size());
     std::vector<int64_t> sec_first, sec_me;
     int64_t nme = 0, secn = 0;

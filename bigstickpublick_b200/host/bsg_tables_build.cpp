@@ -12,12 +12,17 @@
 //    then jz (ascending for protons, descending for neutrons,
 //    src/bbasislib.f90:227-324); inside a sector SDs come in (right block,
 //    left block) pairs with the left haiku as the slow index
-//    (src/bjumplib_weld.f90:377-382);
+//    (src/bjumplib_weld.f90:377-382); inside a block the haikus are in
+//    count_create_haikus order (src/bbasis_haikus.f90:327-411, one W
+//    section);
 //  * basis index = pstart(ip) + nstart(in) (combinebasis,
 //    src/bbasislib.f90:540-677);
 //  * jump isd/fsd hold pstart/nstart values (bjumplib_weld.f90:791-792);
 //    two-body jumps inside one sector keep only isd >= fsd (:414-420) and the
 //    diagonal pair matrix element carries a factor 1/2 (btbme.f90:1402-1407);
+//  * pairs are generated as count_create_pairs / count_create_pnpairs make
+//    them and put in (M,par) sections, M descending, by sortpair's heap sorts
+//    (src/btbme.f90:208-423, :548-703);
 //  * uncoupled pp/nn matrix elements are packed lower triangles per (M,par)
 //    section of pairs (bjumplib_weld.f90:635-642); pn ones are full squares
 //    per (M,par) section, addressed by cpnpair(b,a)+dpnpair(d,c)
@@ -26,12 +31,13 @@
 //    energies are folded into the two-body part with the factor 1/(A-1)
 //    (src/bsppot.f90:20-238).
 //
-// Where the reference's internal orderings could not be reproduced without
-// running it (haiku order inside a block, jump order inside a sector jump,
-// pair order inside an (M,par) section) a fixed deterministic order is used;
-// the GPU path never depends on those orders.
+// The order of the jumps inside one sector jump is the builder's own (initial
+// SDs in basis order); the reference's comes from its hop and chain lists
+// (src/bjumplib_chains.f90, src/bhopslib.f90).  The GPU path never depends on
+// that order.
 
 #include "bsg_host.h"
+#include "../csrc/ref_order.h"
 
 #include <algorithm>
 #include <array>
@@ -239,7 +245,8 @@ void make_sps(const bsg_model_spec *s, bool allsamepar, bool allsameW, SpeciesBa
     }
 }
 
-// all haikus of size k over `states`, grouped into blocks keyed (k, pidx, jz2)
+// all haikus of size k over `states`, grouped into blocks keyed (k, pidx, jz2),
+// each block in the order count_create_haikus makes them
 void make_blocks(const std::vector<SPS> &states, int kmin, int kmax, std::vector<HBlock> &blocks) {
     const int ns = (int)states.size();
     std::map<std::tuple<int, int, int>, std::vector<uint64_t>> groups;
@@ -269,6 +276,10 @@ void make_blocks(const std::vector<SPS> &states, int kmin, int kmax, std::vector
         b.pidx = std::get<1>(g.first);
         b.jz2 = std::get<2>(g.first);
         b.haikus = std::move(g.second);
+        // the reference's creation order inside the block
+        std::sort(b.haikus.begin(), b.haikus.end(), [ns](uint64_t x, uint64_t y) {
+            return bsg_order::haiku_rank(x, ns) < bsg_order::haiku_rank(y, ns);
+        });
         blocks.push_back(std::move(b));
     }
 }
@@ -430,25 +441,23 @@ struct Pairs {
     int64_t at(int q1, int q2) const { return dense[(size_t)q1 * ns2 + q2]; }
 };
 
+// pairs q1 < q2 of one species in count_create_pairs order (the higher
+// state outer, src/btbme.f90:208-308), then sortpair: sections of (M, parity)
+// with M descending, in the order find_pair_start lays out the matrix
+// elements (:726-785)
 void make_xx_pairs(const SpeciesBasis &sb, Pairs &P) {
     const int ns = sb.nl + sb.nr;
-    struct Tmp { int q1, q2, M, pidx; int64_t tri; };
+    struct Tmp { int q1, q2, M, pidx; };
     std::vector<Tmp> v;
-    for (int q2 = 0; q2 < ns; ++q2)
+    for (int q2 = 1; q2 < ns; ++q2)
         for (int q1 = 0; q1 < q2; ++q1) {
             Tmp t;
             t.q1 = q1; t.q2 = q2;
             t.M = (sb.q_m2[q1] + sb.q_m2[q2]) / 2;
             t.pidx = pidx_of(sb.q_par[q1] * sb.q_par[q2]);
-            const int64_t a = q1 + 1, b = q2 + 1;  // pair = isps + (jsps-1)(jsps-2)/2
-            t.tri = a + (b - 1) * (b - 2) / 2;
             v.push_back(t);
         }
-    std::stable_sort(v.begin(), v.end(), [](const Tmp &x, const Tmp &y) {
-        if (x.M != y.M) return x.M < y.M;
-        if (x.pidx != y.pidx) return x.pidx < y.pidx;
-        return x.tri < y.tri;
-    });
+    bsg_order::sortpair(v);
     P.list.clear(); P.M.clear(); P.pidx.clear(); P.pair_sec.clear();
     P.sec_first.clear(); P.sec_n.clear(); P.sec_mestart.clear(); P.index.clear();
     int64_t nme = 0;
@@ -479,6 +488,9 @@ inline int64_t xx_label(const Pairs &P, int64_t c, int64_t d) {
     return istart + (hi - iref) * (hi - iref - 1) / 2 + lo - iref;
 }
 
+// (proton state, neutron state) pairs in count_create_pnpairs order (proton
+// outer, src/btbme.f90:324-423), then sortpair as for like-particle pairs
+// (src/btbmepn.f90:86); count_uncouplepn lays the squares out in that order
 void make_pn_pairs(const SpeciesBasis &pb, const SpeciesBasis &nb, Pairs &P) {
     struct Tmp { int qp, qn, M, pidx; };
     std::vector<Tmp> v;
@@ -491,10 +503,7 @@ void make_pn_pairs(const SpeciesBasis &pb, const SpeciesBasis &nb, Pairs &P) {
             t.pidx = pidx_of(pb.q_par[qp] * nb.q_par[qn]);
             v.push_back(t);
         }
-    std::stable_sort(v.begin(), v.end(), [](const Tmp &x, const Tmp &y) {
-        if (x.M != y.M) return x.M < y.M;
-        return x.pidx < y.pidx;
-    });
+    bsg_order::sortpair(v);
     P.list.clear(); P.M.clear(); P.pidx.clear(); P.pair_sec.clear();
     P.sec_first.clear(); P.sec_n.clear(); P.sec_mestart.clear(); P.index.clear();
     int64_t nme = 0;

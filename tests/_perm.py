@@ -1,9 +1,9 @@
 """Reorderings of built tables that leave the Hamiltonian unchanged up to a
 basis permutation, for the order-invariance tests.
 
-The table builder fixes three orders that the reference produces with code
-this image cannot run (haiku order inside a block, jump order inside a sector
-jump, pair order inside an (M, parity) section).  The engine consumes any
+A Fortran host hands over tables in its own orders: the jumps inside a
+sector jump (the builder's order there is its own), the hmatpp / hmatnn
+labels and the pairs inside an (M, parity) section.  The engine consumes any
 valid table, so each of these orders may be changed freely:
 
 * jumps: every sector jump's jump range (the ranges the opbundles point at)

@@ -1,5 +1,5 @@
-"""The engine's answer does not depend on the table orders the builder picks
-where the reference's could not be run here (jump order inside a sector jump,
+"""The engine's answer does not depend on the table orders (jump order inside
+a sector jump, where the builder's order is its own; matrix-element labels and
 pair order inside an (M, parity) section): permuted tables give the same
 matvec to summation order and the same spectrum (oracle on the CPU; the GPU
 engine in test_order_invariance_gpu.py)."""
