@@ -62,6 +62,8 @@ struct Lz {
     int hprec = 8;   // history storage: 8 FP64, 4 FP32 (lanc_prec)
     int maxcol;      // history columns
     DevBuf hist, W, X, tmp, partial, coef, sqp, sq, Adev, Vtmp, Zdev, wdev, al, bt, ev, M, tau, ework;
+    DevBuf ticket;   // zeroed counter of the dot / update passes (their last CTA reduces)
+    unsigned *tk() { return (unsigned *)ticket.p; }
     DevBuf Ydev;     // Ritz coefficients of a thick restart (maxcol x 128)
     std::vector<double> T;  // host projected matrix (maxcol x maxcol), row-major
     float t_mv = 0, t_ort = 0, t_eig = 0;
@@ -217,9 +219,10 @@ int cgs(Lz &L, int k, std::vector<double> *sq, bool sq_on_device = false) {
     double *C = (double *)L.coef.p;
     const bool want_sq = sq || sq_on_device;
     if (k > 0)
-        CK(multidot(L.col(0), L.hprec, k, (const double *)L.W.p, L.nb, L.n, L.n, (double *)L.partial.p, C, L.s));
+        CK(multidot(L.col(0), L.hprec, k, (const double *)L.W.p, L.nb, L.n, L.n, (double *)L.partial.p, C, L.s,
+                    L.tk()));
     CK(sub_gemv(L.col(0), L.hprec, k, C, (double *)L.W.p, L.nb, L.n, L.n, want_sq ? (double *)L.sqp.p : nullptr,
-                want_sq ? (double *)L.sq.p : nullptr, L.s));
+                want_sq ? (double *)L.sq.p : nullptr, L.s, L.tk()));
     if (sq) {
         sq->resize(L.nb);
         CK(cudaMemcpyAsync(sq->data(), L.sq.p, sizeof(double) * L.nb, cudaMemcpyDeviceToHost, L.s));
@@ -326,7 +329,7 @@ int next_block(Lz &L, int dst, const std::vector<double> &sq, std::vector<double
     }
     // S = W^T W, then the decomposition on the host
     CK(multidot((const double *)L.W.p, nb, (const double *)L.W.p, nb, L.n, L.n, (double *)L.partial.p,
-                (double *)L.coef.p, L.s));
+                (double *)L.coef.p, L.s, L.tk()));
     CK(cudaMemcpyAsync(L.hpin + Lz::kPinS, L.coef.p, sizeof(double) * nb * nb, cudaMemcpyDeviceToHost, L.s));
     CK(cudaStreamSynchronize(L.s));
     return block_finish(L, dst, L.hpin + Lz::kPinS, beta, lmin, lmax);
@@ -388,12 +391,16 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
         // ---- alpha = V^T W ; W -= V alpha ; CGS against [0, cur), all queued
         // without a host round trip; the scalar recursion also normalizes
         // the residual on the device (V_{i+1} = W / |W|), which the
-        // safeguards below redo in the rare steps where they trigger
+        // safeguards below redo in the rare steps where they trigger.
+        // alpha is removed first, as br_remove_prev_overlap does: one pass
+        // against [0, cur + nb) that takes alpha with the rest loses
+        // orthogonality (measured: spurious Ritz values below the spectrum
+        // after 40-150 steps)
         CK(multidot(L.col(cur), L.hprec, nb, (const double *)L.W.p, nb, n, n, (double *)L.partial.p,
-                    (double *)L.coef.p, L.s));
+                    (double *)L.coef.p, L.s, L.tk()));
         CK(cudaMemcpyAsync(L.hpin + Lz::kPinAlpha, L.coef.p, sizeof(double) * nb * nb, cudaMemcpyDeviceToHost, L.s));
         CK(sub_gemv(L.col(cur), L.hprec, nb, (const double *)L.coef.p, (double *)L.W.p, nb, n, n, nullptr, nullptr,
-                    L.s));
+                    L.s, L.tk()));
         ST(cgs(L, cur, nullptr, true));
         CK(cudaMemcpyAsync(L.hpin + Lz::kPinSq, L.sq.p, sizeof(double) * nb, cudaMemcpyDeviceToHost, L.s));
         if (nb == 1) {
@@ -402,7 +409,7 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
         } else {
             // W^T W for the block step, read back with alpha and the norms
             CK(multidot((const double *)L.W.p, nb, (const double *)L.W.p, nb, n, n, (double *)L.partial.p,
-                        (double *)L.coef.p, L.s));
+                        (double *)L.coef.p, L.s, L.tk()));
             CK(cudaMemcpyAsync(L.hpin + Lz::kPinS, L.coef.p, sizeof(double) * nb * nb, cudaMemcpyDeviceToHost, L.s));
         }
         CK(cudaEventRecord(L.e2, L.s));
@@ -672,7 +679,9 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
         (st = dev_alloc(ctx, L.al, sizeof(double) * N)) ||
         (st = dev_alloc(ctx, L.bt, sizeof(double) * N)) || (st = dev_alloc(ctx, L.ev, sizeof(double) * N)) ||
         (st = dev_alloc(ctx, L.M, sizeof(double) * 16 * 16)) || (st = dev_alloc(ctx, L.tau, sizeof(double) * N)) ||
-        (st = dev_alloc(ctx, L.ework, sizeof(double) * ((size_t)2 * N + (size_t)6 * N * std::min(N, 128))))) {
+        (st = dev_alloc(ctx, L.ework, sizeof(double) * ((size_t)2 * N + (size_t)6 * N * std::min(N, 128)))) ||
+        (st = dev_alloc(ctx, L.ticket, 16)) ||
+        (st = cuda_check(ctx, cudaMemsetAsync(L.ticket.p, 0, 16, L.s), "cudaMemsetAsync (pass ticket)"))) {
         // fall through to cleanup
     }
     L.maxcol = maxcol;
@@ -733,7 +742,7 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
     if (L.econv) cudaEventDestroy(L.econv);
     DevBuf *bufs[] = {&L.hist, &L.W, &L.X, &L.tmp, &L.partial, &L.coef, &L.sqp, &L.sq, &L.Adev,
                       &L.Vtmp, &L.Zdev, &L.wdev, &L.al, &L.bt, &L.ev, &L.M, &L.tau, &L.ework,
-                      &L.al2, &L.bt2, &L.w2, &L.Adev2, &L.Vtmp2, &L.tau2, &L.ework2, &L.Ydev};
+                      &L.al2, &L.bt2, &L.w2, &L.Adev2, &L.Vtmp2, &L.tau2, &L.ework2, &L.Ydev, &L.ticket};
     cudaStreamSynchronize(L.s);
     for (DevBuf *b : bufs) dev_free(*b);
     if (L.hpin) cudaFreeHost(L.hpin);

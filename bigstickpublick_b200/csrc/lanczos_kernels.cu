@@ -30,6 +30,44 @@ namespace bsg {
 
 constexpr int kDotThreads = 256;
 constexpr int kDotTile = 512;      // rows per tile
+// partial sums that the last CTA of a pass adds up itself; above this the
+// separate k_reduce_partials grid is faster than one CTA
+constexpr int64_t kFusedPartials = 32768;
+
+// The CTA that finishes a pass last adds the partials up: out[p] = sum over g
+// of partial[p*G + g], p < np, in k_reduce_partials' order (lanes take g =
+// lane, lane + 32, ..., then the same shuffle tree), so the fused and the
+// separate reduction give the same bits.  Every CTA calls it after writing
+// its partials; the ticket counts the CTAs done and is left at zero for the
+// next pass on the stream.  No CTA waits on another.
+__device__ __forceinline__ void finish_partials(const double *partial, int np, int G, double *out, unsigned *ticket,
+                                                unsigned nblocks) {
+    __shared__ unsigned s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = (atomicAdd(ticket, 1u) == nblocks - 1u) ? 1u : 0u;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int p = warp; p < np; p += nw) {
+        const double *row = partial + (int64_t)p * G;
+        double v = 0.0;
+        // four loads in flight ahead of the additions, which stay in g order
+        for (int g0 = lane; g0 < G; g0 += 128) {
+            double x[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) x[u] = (g0 + 32 * u < G) ? __ldcg(row + g0 + 32 * u) : 0.0;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (g0 + 32 * u < G) v += x[u];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) out[p] = v;
+    }
+    if (threadIdx.x == 0) atomicExch(ticket, 0u);
+}
 
 // C[p] partials: pairs p = a*nB + b, a < nA, b < nB; A, B column-major with
 // leading dimension ld (vector j at base + j*ld).  CTA (x, y) walks the row
@@ -37,14 +75,17 @@ constexpr int kDotTile = 512;      // rows per tile
 // spread the A vectors over gridDim.y CTAs).  The chunk of B is staged in
 // shared memory, column-major so that lanes read consecutive rows; warp w
 // takes its vectors (two at a time for NB >= 4, halving the shared loads per
-// multiply-add) and reads them coalesced, lanes keep NB partial sums per
+// multiply-add, and for FP32 columns with NB <= 2, doubling the loads in
+// flight) and reads them coalesced, lanes keep NB partial sums per
 // vector, and a warp reduction adds them into the CTA's shared accumulator
 // (each (a,b) owned by one warp, added in chunk order).  The CTA writes
-// partial[p * gridDim.x + x] for its vectors.
+// partial[p * gridDim.x + x] for its vectors; with a ticket, the last CTA
+// also writes out[p] (finish_partials).
 template <typename TA, int NB, int PAIR>
 __global__ void __launch_bounds__(kDotThreads) k_multidot(const TA *__restrict__ A, int nA,
                                                          const double *__restrict__ B, int64_t n, int64_t ld,
-                                                         double *__restrict__ partial) {
+                                                         double *__restrict__ partial, double *__restrict__ out,
+                                                         unsigned *__restrict__ ticket) {
     extern __shared__ double sm[];
     double *sB = sm;                       // [NB][kDotTile]
     double *sAcc = sm + kDotTile * NB;     // [nA][NB]
@@ -67,17 +108,21 @@ __global__ void __launch_bounds__(kDotThreads) k_multidot(const TA *__restrict__
             double acc0[NB], acc1[NB];
 #pragma unroll
             for (int b = 0; b < NB; ++b) acc0[b] = acc1[b] = 0.0;
-            // four rows per lane and step, loads first (the sum stays in row order)
+            // U rows per lane and step, loads first (the sum stays in row
+            // order): eight for one or two FP32 vectors, whose passes are
+            // bound by the loads in flight (measured; FP64 history columns
+            // ran slower with eight)
+            constexpr int U = (NB <= 2 && sizeof(TA) == 4) ? 8 : 4;
             int r = lane;
-            for (; r + 96 < rows; r += 128) {
-                double x0[4], x1[4];
+            for (; r + 32 * (U - 1) < rows; r += 32 * U) {
+                double x0[U], x1[U];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
+                for (int u = 0; u < U; ++u) {
                     x0[u] = (double)__ldg(col0 + r + 32 * u);
                     x1[u] = PAIR == 2 ? (double)__ldg(col1 + r + 32 * u) : 0.0;
                 }
 #pragma unroll
-                for (int u = 0; u < 4; ++u)
+                for (int u = 0; u < U; ++u)
 #pragma unroll
                     for (int b = 0; b < NB; ++b) {
                         const double y = sB[b * kDotTile + r + 32 * u];
@@ -113,6 +158,7 @@ __global__ void __launch_bounds__(kDotThreads) k_multidot(const TA *__restrict__
     __syncthreads();
     for (int e = a_lo * NB + threadIdx.x; e < a_hi * NB; e += kDotThreads)
         partial[(int64_t)e * gridDim.x + blockIdx.x] = sAcc[e];
+    if (ticket) finish_partials(partial, nA * NB, gridDim.x, out, ticket, gridDim.x * gridDim.y);
 }
 
 // out[p] = sum over g of partial[p*G + g]: one warp per p, lanes take g = lane,
@@ -129,11 +175,13 @@ __global__ void k_reduce_partials(const double *__restrict__ partial, int npairs
 }
 
 // W[b] -= sum_j H[j] * C[j*nB + b]   (j < k), fused sum of squares of the
-// result per column when sq != nullptr (partials per block, NB entries)
+// result per column when sq != nullptr (partials per block, NB entries; with
+// a ticket the last block adds them into sq_out)
 template <typename TH, int NB>
 __global__ void __launch_bounds__(256) k_sub_gemv(const TH *__restrict__ H, int k, const double *__restrict__ C,
                                                   double *__restrict__ W, int64_t n, int64_t ld,
-                                                  double *__restrict__ sq) {
+                                                  double *__restrict__ sq, double *__restrict__ sq_out,
+                                                  unsigned *__restrict__ ticket) {
     extern __shared__ double sC[];  // [k*NB] then [8][NB] warp sums
     for (int e = threadIdx.x; e < k * NB; e += blockDim.x) sC[e] = C[e];
     __syncthreads();
@@ -145,15 +193,38 @@ __global__ void __launch_bounds__(256) k_sub_gemv(const TH *__restrict__ H, int 
 #pragma unroll
         for (int b = 0; b < NB; ++b) acc[b] = 0.0;
         int j = 0;
-        for (; j + 1 < k; j += 2) {
-            const double h0 = (double)__ldg(H + (int64_t)j * ld + i), h1 = (double)__ldg(H + (int64_t)(j + 1) * ld + i);
+        if constexpr (NB <= 2 && sizeof(TH) == 4) {
+            // eight FP32 history rows loaded ahead of their multiply-adds,
+            // which stay in j order: the pass of one or two vectors is bound
+            // by the loads in flight (measured faster)
+            for (; j + 8 <= k; j += 8) {
+                double h[8];
 #pragma unroll
-            for (int b = 0; b < NB; ++b) acc[b] = fma(h1, sC[(j + 1) * NB + b], fma(h0, sC[j * NB + b], acc[b]));
-        }
-        if (j < k) {
-            const double h0 = (double)__ldg(H + (int64_t)j * ld + i);
+                for (int u = 0; u < 8; ++u) h[u] = (double)__ldg(H + (int64_t)(j + u) * ld + i);
 #pragma unroll
-            for (int b = 0; b < NB; ++b) acc[b] = fma(h0, sC[j * NB + b], acc[b]);
+                for (int u = 0; u < 8; ++u)
+#pragma unroll
+                    for (int b = 0; b < NB; ++b) acc[b] = fma(h[u], sC[(j + u) * NB + b], acc[b]);
+            }
+            for (; j < k; ++j) {
+                const double h0 = (double)__ldg(H + (int64_t)j * ld + i);
+#pragma unroll
+                for (int b = 0; b < NB; ++b) acc[b] = fma(h0, sC[j * NB + b], acc[b]);
+            }
+        } else {
+            // two rows per step (more raised the registers of FP64 passes
+            // above the 6 CTAs per SM that stream_grid assumes)
+            for (; j + 1 < k; j += 2) {
+                const double h0 = (double)__ldg(H + (int64_t)j * ld + i),
+                             h1 = (double)__ldg(H + (int64_t)(j + 1) * ld + i);
+#pragma unroll
+                for (int b = 0; b < NB; ++b) acc[b] = fma(h1, sC[(j + 1) * NB + b], fma(h0, sC[j * NB + b], acc[b]));
+            }
+            if (j < k) {
+                const double h0 = (double)__ldg(H + (int64_t)j * ld + i);
+#pragma unroll
+                for (int b = 0; b < NB; ++b) acc[b] = fma(h0, sC[j * NB + b], acc[b]);
+            }
         }
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
@@ -178,6 +249,7 @@ __global__ void __launch_bounds__(256) k_sub_gemv(const TH *__restrict__ H, int 
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[w * NB + threadIdx.x];
         sq[(int64_t)threadIdx.x * gridDim.x + blockIdx.x] = v;
     }
+    if (ticket) finish_partials(sq, NB, gridDim.x, sq_out, ticket, gridDim.x);
 }
 
 // out[l] = sum_j V[j] * Y[j*ldy + l], l < K (K <= 16 per launch)
@@ -621,7 +693,7 @@ static int stream_grid(int64_t n) {
 
 template <typename TA, int NB>
 static cudaError_t multidot_nb(const TA *A, int nA, const double *B, int64_t n, int64_t ld, double *partial,
-                               double *out, cudaStream_t s) {
+                               double *out, cudaStream_t s, unsigned *ticket) {
     const int64_t tiles = (n + kDotTile - 1) / kDotTile;
     const int G = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, stream_grid<NB>(n)));
     const int maxa = 4096 / NB;  // shared accumulator of at most 4096 doubles
@@ -631,16 +703,22 @@ static cudaError_t multidot_nb(const TA *A, int nA, const double *B, int64_t n, 
         // vectors over more CTAs, at least 8 vectors each
         const int gy = std::max(1, std::min((592 + G - 1) / G, na / 8));
         const size_t smem = sizeof(double) * ((size_t)kDotTile * NB + (size_t)na * NB);
+        // few partials: the last CTA reduces them, no second launch
+        unsigned *tk = (ticket && (int64_t)na * NB * G <= kFusedPartials) ? ticket : nullptr;
+        double *o = out + (int64_t)a0 * NB;
         // two A vectors per warp pass halve the shared loads per multiply-add
-        // for NB >= 4, once there are enough vectors to keep all 8 warps busy
-        if (NB >= 4 && na >= 16) {
+        // for NB >= 4 and double the loads in flight for NB <= 2, once there
+        // are enough vectors to keep all 8 warps of each CTA busy
+        if ((NB >= 4 && na >= 16) || (NB <= 2 && sizeof(TA) == 4 && na >= 16 * gy)) {
             cudaFuncSetAttribute(k_multidot<TA, NB, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            k_multidot<TA, NB, 2><<<dim3(G, gy), kDotThreads, smem, s>>>(A + (int64_t)a0 * ld, na, B, n, ld, partial);
+            k_multidot<TA, NB, 2><<<dim3(G, gy), kDotThreads, smem, s>>>(A + (int64_t)a0 * ld, na, B, n, ld, partial,
+                                                                         o, tk);
         } else {
             cudaFuncSetAttribute(k_multidot<TA, NB, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            k_multidot<TA, NB, 1><<<dim3(G, gy), kDotThreads, smem, s>>>(A + (int64_t)a0 * ld, na, B, n, ld, partial);
+            k_multidot<TA, NB, 1><<<dim3(G, gy), kDotThreads, smem, s>>>(A + (int64_t)a0 * ld, na, B, n, ld, partial,
+                                                                         o, tk);
         }
-        k_reduce_partials<<<(na * NB * 32 + 255) / 256, 256, 0, s>>>(partial, na * NB, G, out + (int64_t)a0 * NB);
+        if (!tk) k_reduce_partials<<<(na * NB * 32 + 255) / 256, 256, 0, s>>>(partial, na * NB, G, o);
         a0 += na;
     }
     return cudaGetLastError();
@@ -648,34 +726,37 @@ static cudaError_t multidot_nb(const TA *A, int nA, const double *B, int64_t n, 
 
 template <typename TA>
 static cudaError_t multidot_t(const TA *A, int nA, const double *B, int nB, int64_t n, int64_t ld, double *partial,
-                              double *out, cudaStream_t s) {
+                              double *out, cudaStream_t s, unsigned *ticket) {
     if (nA <= 0 || nB <= 0) return cudaSuccess;
     switch (nB) {
-    case 1: return multidot_nb<TA, 1>(A, nA, B, n, ld, partial, out, s);
-    case 2: return multidot_nb<TA, 2>(A, nA, B, n, ld, partial, out, s);
-    case 4: return multidot_nb<TA, 4>(A, nA, B, n, ld, partial, out, s);
-    case 8: return multidot_nb<TA, 8>(A, nA, B, n, ld, partial, out, s);
-    case 16: return multidot_nb<TA, 16>(A, nA, B, n, ld, partial, out, s);
+    case 1: return multidot_nb<TA, 1>(A, nA, B, n, ld, partial, out, s, ticket);
+    case 2: return multidot_nb<TA, 2>(A, nA, B, n, ld, partial, out, s, ticket);
+    case 4: return multidot_nb<TA, 4>(A, nA, B, n, ld, partial, out, s, ticket);
+    case 8: return multidot_nb<TA, 8>(A, nA, B, n, ld, partial, out, s, ticket);
+    case 16: return multidot_nb<TA, 16>(A, nA, B, n, ld, partial, out, s, ticket);
     default:
         return cudaErrorInvalidValue;
     }
 }
 
 cudaError_t multidot(const void *A, int aprec, int nA, const double *B, int nB, int64_t n, int64_t ld,
-                     double *partial, double *out, cudaStream_t s) {
-    if (aprec == 4) return multidot_t<float>((const float *)A, nA, B, nB, n, ld, partial, out, s);
-    return multidot_t<double>((const double *)A, nA, B, nB, n, ld, partial, out, s);
+                     double *partial, double *out, cudaStream_t s, unsigned *ticket) {
+    if (aprec == 4) return multidot_t<float>((const float *)A, nA, B, nB, n, ld, partial, out, s, ticket);
+    return multidot_t<double>((const double *)A, nA, B, nB, n, ld, partial, out, s, ticket);
 }
 
 cudaError_t multidot(const double *A, int nA, const double *B, int nB, int64_t n, int64_t ld, double *partial,
-                     double *out, cudaStream_t s) {
-    return multidot_t<double>(A, nA, B, nB, n, ld, partial, out, s);
+                     double *out, cudaStream_t s, unsigned *ticket) {
+    return multidot_t<double>(A, nA, B, nB, n, ld, partial, out, s, ticket);
 }
 
 template <typename TH, int NB>
 static cudaError_t sub_gemv_nb(const TH *H, int k, const double *C, double *W, int64_t n, int64_t ld,
-                               double *sq_partial, double *sq_out, cudaStream_t s) {
+                               double *sq_partial, double *sq_out, cudaStream_t s, unsigned *ticket) {
     const int G = stream_grid<NB>(n);
+    // the sums of squares: the last block of the last pass adds them up when
+    // there is a ticket, else a separate reduction
+    unsigned *tk = (sq_partial && sq_out) ? ticket : nullptr;
     int j0 = 0;
     do {
         const int kk = (k - j0) < 512 ? (k - j0) : 512;
@@ -683,35 +764,36 @@ static cudaError_t sub_gemv_nb(const TH *H, int k, const double *C, double *W, i
         const size_t smem = sizeof(double) * ((size_t)kk * NB + 8 * NB);
         cudaFuncSetAttribute(k_sub_gemv<TH, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(smem + 256));
         k_sub_gemv<TH, NB><<<G, 256, smem, s>>>(H + (int64_t)j0 * ld, kk, C + (int64_t)j0 * NB, W, n, ld,
-                                                 last ? sq_partial : nullptr);
+                                                 last ? sq_partial : nullptr, sq_out, last ? tk : nullptr);
         j0 += kk;
     } while (j0 < k);
-    if (sq_partial && sq_out) k_reduce_partials<<<(NB * 32 + 255) / 256, 256, 0, s>>>(sq_partial, NB, G, sq_out);
+    if (sq_partial && sq_out && !tk)
+        k_reduce_partials<<<(NB * 32 + 255) / 256, 256, 0, s>>>(sq_partial, NB, G, sq_out);
     return cudaGetLastError();
 }
 
 template <typename TH>
 static cudaError_t sub_gemv_t(const TH *H, int k, const double *C, double *W, int nB, int64_t n, int64_t ld,
-                              double *sq_partial, double *sq_out, cudaStream_t s) {
+                              double *sq_partial, double *sq_out, cudaStream_t s, unsigned *ticket) {
     switch (nB) {
-    case 1: return sub_gemv_nb<TH, 1>(H, k, C, W, n, ld, sq_partial, sq_out, s);
-    case 2: return sub_gemv_nb<TH, 2>(H, k, C, W, n, ld, sq_partial, sq_out, s);
-    case 4: return sub_gemv_nb<TH, 4>(H, k, C, W, n, ld, sq_partial, sq_out, s);
-    case 8: return sub_gemv_nb<TH, 8>(H, k, C, W, n, ld, sq_partial, sq_out, s);
-    case 16: return sub_gemv_nb<TH, 16>(H, k, C, W, n, ld, sq_partial, sq_out, s);
+    case 1: return sub_gemv_nb<TH, 1>(H, k, C, W, n, ld, sq_partial, sq_out, s, ticket);
+    case 2: return sub_gemv_nb<TH, 2>(H, k, C, W, n, ld, sq_partial, sq_out, s, ticket);
+    case 4: return sub_gemv_nb<TH, 4>(H, k, C, W, n, ld, sq_partial, sq_out, s, ticket);
+    case 8: return sub_gemv_nb<TH, 8>(H, k, C, W, n, ld, sq_partial, sq_out, s, ticket);
+    case 16: return sub_gemv_nb<TH, 16>(H, k, C, W, n, ld, sq_partial, sq_out, s, ticket);
     default: return cudaErrorInvalidValue;
     }
 }
 
 cudaError_t sub_gemv(const void *H, int hprec, int k, const double *C, double *W, int nB, int64_t n, int64_t ld,
-                     double *sq_partial, double *sq_out, cudaStream_t s) {
-    if (hprec == 4) return sub_gemv_t<float>((const float *)H, k, C, W, nB, n, ld, sq_partial, sq_out, s);
-    return sub_gemv_t<double>((const double *)H, k, C, W, nB, n, ld, sq_partial, sq_out, s);
+                     double *sq_partial, double *sq_out, cudaStream_t s, unsigned *ticket) {
+    if (hprec == 4) return sub_gemv_t<float>((const float *)H, k, C, W, nB, n, ld, sq_partial, sq_out, s, ticket);
+    return sub_gemv_t<double>((const double *)H, k, C, W, nB, n, ld, sq_partial, sq_out, s, ticket);
 }
 
 cudaError_t sub_gemv(const double *H, int k, const double *C, double *W, int nB, int64_t n, int64_t ld,
-                     double *sq_partial, double *sq_out, cudaStream_t s) {
-    return sub_gemv_t<double>(H, k, C, W, nB, n, ld, sq_partial, sq_out, s);
+                     double *sq_partial, double *sq_out, cudaStream_t s, unsigned *ticket) {
+    return sub_gemv_t<double>(H, k, C, W, nB, n, ld, sq_partial, sq_out, s, ticket);
 }
 
 template <typename TV, typename TO>

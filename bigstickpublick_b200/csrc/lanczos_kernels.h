@@ -10,16 +10,19 @@ int dot_grid(int64_t n);
 // Operands marked "prec" are history columns stored in FP32 (4) or FP64
 // (8); every sum accumulates in FP64.
 // out[a*nB + b] = A_a . B_b   (partial: scratch of nA*nB*dot_grid(n) doubles)
+// ticket (optional): a device counter at zero, used by one pass at a time on
+// the stream; with it the last CTA of a pass with few partials adds them up
+// itself instead of a second launch, with the same summation order
 cudaError_t multidot(const void *A, int aprec, int nA, const double *B, int nB, int64_t n, int64_t ld,
-                     double *partial, double *out, cudaStream_t s);
+                     double *partial, double *out, cudaStream_t s, unsigned *ticket = nullptr);
 cudaError_t multidot(const double *A, int nA, const double *B, int nB, int64_t n, int64_t ld, double *partial,
-                     double *out, cudaStream_t s);
+                     double *out, cudaStream_t s, unsigned *ticket = nullptr);
 // W_b -= sum_j H_j C[j*nB+b]; optional column sums of squares of the result
-// (sq_partial: nB*888 doubles, sq_out: nB doubles)
+// (sq_partial: nB*888 doubles, sq_out: nB doubles; ticket as for multidot)
 cudaError_t sub_gemv(const void *H, int hprec, int k, const double *C, double *W, int nB, int64_t n, int64_t ld,
-                     double *sq_partial, double *sq_out, cudaStream_t s);
+                     double *sq_partial, double *sq_out, cudaStream_t s, unsigned *ticket = nullptr);
 cudaError_t sub_gemv(const double *H, int k, const double *C, double *W, int nB, int64_t n, int64_t ld,
-                     double *sq_partial, double *sq_out, cudaStream_t s);
+                     double *sq_partial, double *sq_out, cudaStream_t s, unsigned *ticket = nullptr);
 // out_l = sum_j V_j Y[j*ldy + l], l < K
 // xpack (optional, K <= 16): the result also as the interleaved applyH input
 // (FP32 for xprec 4, FP64 for 8), as pack() would make it
