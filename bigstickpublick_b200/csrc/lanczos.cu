@@ -63,6 +63,10 @@ struct Lz {
     int maxcol;      // history columns
     DevBuf hist, W, X, tmp, partial, coef, sqp, sq, Adev, Vtmp, Zdev, wdev, al, bt, ev, M, tau, ework;
     DevBuf ticket;   // zeroed counter of the dot / update passes (their last CTA reduces)
+    // scalar recursion: the next step's applyH is queued before the host has
+    // read this step's alpha and beta, into W2; W and W2 swap when it is used
+    DevBuf W2;
+    cudaEvent_t es0[2] = {nullptr, nullptr}, es1[2] = {nullptr, nullptr}, eb = nullptr;
     unsigned *tk() { return (unsigned *)ticket.p; }
     DevBuf Ydev;     // Ritz coefficients of a thick restart (maxcol x 128)
     std::vector<double> T;  // host projected matrix (maxcol x maxcol), row-major
@@ -373,6 +377,8 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
     bool finished = false, converged = false;
     std::vector<double> eold, e;
     bool post_pending = false;  // e3 -> e4 of the last step not yet accounted
+    bool spec_ready = false;    // W2 holds H col(cur), queued during the previous step
+    int spair = 0;              // event pair of the next speculative applyH
     int iter = 0;         // block iterations in this cycle (the reference's iter)
     struct {
         bool active = false;
@@ -382,12 +388,22 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
         ++iter;
         ++total;
         // ---- W = H V
-        if (!L.x_ready) CK(pack(L.col(cur), L.hprec, nb, n, n, L.X.p, L.prec, L.s));
+        cudaEvent_t m0 = L.e0, m1 = L.e1;   // its start and end
+        if (spec_ready) {
+            // queued by the previous step, whose next vector stood
+            std::swap(L.W, L.W2);
+            m0 = L.es0[spair ^ 1];
+            m1 = L.es1[spair ^ 1];
+        } else {
+            if (!L.x_ready) CK(pack(L.col(cur), L.hprec, nb, n, n, L.X.p, L.prec, L.s));
+            CK(cudaEventRecord(L.e0, L.s));
+            ST(launch_applyh_cols(ctx, L.X.p, (double *)L.W.p, nb, L.prec, L.s));  // W columns directly
+            CK(cudaEventRecord(L.e1, L.s));
+        }
+        spec_ready = false;
         L.x_ready = false;
-        CK(cudaEventRecord(L.e0, L.s));
-        ST(launch_applyh_cols(ctx, L.X.p, (double *)L.W.p, nb, L.prec, L.s));  // W columns directly
-        CK(cudaEventRecord(L.e1, L.s));
         ++matvecs;
+        CK(cudaEventRecord(L.eb, L.s));
         // ---- alpha = V^T W ; W -= V alpha ; CGS against [0, cur), all queued
         // without a host round trip; the scalar recursion also normalizes
         // the residual on the device (V_{i+1} = W / |W|), which the
@@ -413,12 +429,24 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
             CK(cudaMemcpyAsync(L.hpin + Lz::kPinS, L.coef.p, sizeof(double) * nb * nb, cudaMemcpyDeviceToHost, L.s));
         }
         CK(cudaEventRecord(L.e2, L.s));
+        // ---- the next step's applyH, queued before the host reads this
+        // step's alpha and beta (scalar recursion): the normalization above
+        // just wrote its packed input.  It is kept when the next vector
+        // stands, i.e. unless a safeguard below rewrites it, the run stops,
+        // or a restart comes first (each of these clears x_ready)
+        const bool spec = nb == 1 && cur + nb < niter * nb && !(thick && cur + 2 * nb > (niter - 1) * nb) &&
+                          (int64_t)(cur + nb) < n;
+        if (spec) {
+            CK(cudaEventRecord(L.es0[spair], L.s));
+            ST(launch_applyh_cols(ctx, L.X.p, (double *)L.W2.p, nb, L.prec, L.s));
+            CK(cudaEventRecord(L.es1[spair], L.s));
+        }
         CK(cudaEventSynchronize(L.e2));
         {
             float ms = 0.f;
-            cudaEventElapsedTime(&ms, L.e0, L.e1);
+            cudaEventElapsedTime(&ms, m0, m1);
             L.t_mv += ms;
-            cudaEventElapsedTime(&ms, L.e1, L.e2);
+            cudaEventElapsedTime(&ms, L.eb, L.e2);
             L.t_ort += ms;
             if (post_pending) {  // the previous step's work after its synchronization
                 cudaEventElapsedTime(&ms, L.e3, L.e4);
@@ -534,6 +562,12 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
         }
         if (mT >= (int64_t)n) { finished = true; converged = true; }  // Krylov space exhausted
         if (p->fixed_iter && finished) converged = true;
+        if (spec && L.x_ready && !finished) {
+            // the queued applyH stands unless the restart below moves the
+            // continuation vector (it clears x_ready, checked again there)
+            spec_ready = true;
+            spair ^= 1;
+        }
         // ---- thick restart
         if (thick && !finished && cur + nb > (niter - 1) * nb) {
             if (restarts >= p->max_restarts) {
@@ -583,6 +617,7 @@ int run(Lz &L, const bsg_lanczos_params *p, const double *pivot, double *evals, 
             // be packed again; block: the continuation is the block whose
             // packed input the last spectral step already wrote
             if (nb == 1) L.x_ready = false;
+            spec_ready = false;
             iter = k / nb;
             beta_prev = -1.0;
         }
@@ -680,7 +715,7 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
         (st = dev_alloc(ctx, L.bt, sizeof(double) * N)) || (st = dev_alloc(ctx, L.ev, sizeof(double) * N)) ||
         (st = dev_alloc(ctx, L.M, sizeof(double) * 16 * 16)) || (st = dev_alloc(ctx, L.tau, sizeof(double) * N)) ||
         (st = dev_alloc(ctx, L.ework, sizeof(double) * ((size_t)2 * N + (size_t)6 * N * std::min(N, 128)))) ||
-        (st = dev_alloc(ctx, L.ticket, 16)) ||
+        (st = dev_alloc(ctx, L.ticket, 16)) || (L.nb == 1 && (st = dev_alloc(ctx, L.W2, vb))) ||
         (st = cuda_check(ctx, cudaMemsetAsync(L.ticket.p, 0, 16, L.s), "cudaMemsetAsync (pass ticket)"))) {
         // fall through to cleanup
     }
@@ -716,6 +751,11 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
         cudaEventCreate(&L.e2);
         cudaEventCreate(&L.e3);
         cudaEventCreate(&L.e4);
+        cudaEventCreate(&L.eb);
+        for (int i = 0; i < 2; ++i) {
+            cudaEventCreate(&L.es0[i]);
+            cudaEventCreate(&L.es1[i]);
+        }
         cudaEventCreateWithFlags(&L.econv, cudaEventDisableTiming);
         cudaEvent_t t0, t1;
         cudaEventCreate(&t0);
@@ -734,6 +774,11 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
         cudaEventDestroy(L.e2);
         cudaEventDestroy(L.e3);
         cudaEventDestroy(L.e4);
+        cudaEventDestroy(L.eb);
+        for (int i = 0; i < 2; ++i) {
+            cudaEventDestroy(L.es0[i]);
+            cudaEventDestroy(L.es1[i]);
+        }
     }
     if (L.s2) {
         cudaStreamSynchronize(L.s2);
@@ -742,7 +787,8 @@ extern "C" int bsg_lanczos(bsg_ctx *ctx, const bsg_lanczos_params *p, const doub
     if (L.econv) cudaEventDestroy(L.econv);
     DevBuf *bufs[] = {&L.hist, &L.W, &L.X, &L.tmp, &L.partial, &L.coef, &L.sqp, &L.sq, &L.Adev,
                       &L.Vtmp, &L.Zdev, &L.wdev, &L.al, &L.bt, &L.ev, &L.M, &L.tau, &L.ework,
-                      &L.al2, &L.bt2, &L.w2, &L.Adev2, &L.Vtmp2, &L.tau2, &L.ework2, &L.Ydev, &L.ticket};
+                      &L.al2, &L.bt2, &L.w2, &L.Adev2, &L.Vtmp2, &L.tau2, &L.ework2, &L.Ydev, &L.ticket,
+                      &L.W2};
     cudaStreamSynchronize(L.s);
     for (DevBuf *b : bufs) dev_free(*b);
     if (L.hpin) cudaFreeHost(L.hpin);
