@@ -1175,6 +1175,12 @@ void free_ctx(bsg_ctx *ctx) {
     for (DevBuf *b : bufs) dev_free(*b);
     for (auto &kv : ctx->tiles) dev_free(kv.second.buf);
     ctx->tiles.clear();
+    for (auto &kv : ctx->chunk_tiles) dev_free(kv.second.buf);
+    ctx->chunk_tiles.clear();
+    for (cudaEvent_t e : ctx->chunk_ev) cudaEventDestroy(e);
+    ctx->chunk_ev.clear();
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+    ctx->copy_stream = nullptr;
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1290,6 +1296,77 @@ int bsg_destroy(bsg_ctx *ctx) {
 }
 
 namespace {
+
+// host-pointer applyH in kChunks row-range chunks when the output is at least
+// kChunkBytes: each chunk's states are final when its launch ends, so their
+// copy back overlaps the launches after it
+constexpr int kChunks = 4;
+constexpr size_t kChunkBytes = (size_t)32 << 20;
+
+// the chunked tiles of width tp: rows cut into kChunks contiguous ranges of
+// about equal estimated work, each range's tiles heaviest row first
+const ChunkTiles *get_chunk_tiles(bsg_ctx *ctx, int tp) {
+    auto it = ctx->chunk_tiles.find(tp);
+    if (it != ctx->chunk_tiles.end()) return &it->second;
+    ChunkTiles ct;
+    int64_t total = 0;
+    for (int32_t r = 0; r < ctx->nrows; ++r) total += ctx->h_work[r];
+    std::vector<int32_t> rcut(1, 0);
+    int64_t acc = 0;
+    for (int32_t r = 0; r < ctx->nrows && (int)rcut.size() < kChunks; ++r) {
+        acc += ctx->h_work[r];
+        if (acc * kChunks >= total * (int64_t)rcut.size()) rcut.push_back(r + 1);
+    }
+    while ((int)rcut.size() <= kChunks) rcut.push_back(ctx->nrows);
+    rcut.back() = ctx->nrows;
+    std::vector<Tile> tiles;
+    int64_t state = 0;
+    for (int c = 0; c < kChunks; ++c) {
+        std::vector<int32_t> order;
+        for (int32_t r = rcut[c]; r < rcut[c + 1]; ++r) order.push_back(r);
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int32_t x, int32_t y) { return ctx->h_work[x] > ctx->h_work[y]; });
+        ct.start.push_back((int32_t)tiles.size());
+        ct.s0.push_back(state);
+        for (int32_t r : order)
+            for (int32_t p0 = 0; p0 < ctx->h_rowlen[r]; p0 += tp) {
+                Tile t;
+                t.row = r;
+                t.pos0 = p0;
+                t.npos = std::min(tp, ctx->h_rowlen[r] - p0);
+                t.pad = 0;
+                tiles.push_back(t);
+            }
+        for (int32_t r = rcut[c]; r < rcut[c + 1]; ++r) state += ctx->h_rowlen[r];
+    }
+    ct.start.push_back((int32_t)tiles.size());
+    ct.s0.push_back(state);
+    if (upload(ctx, ct.buf, tiles.data(), tiles.size() * sizeof(Tile))) return nullptr;
+    for (int c = 0; c < kChunks; ++c) {
+        TileSet v;
+        v.buf.p = (char *)ct.buf.p + (size_t)ct.start[c] * sizeof(Tile);
+        v.buf.bytes = (size_t)(ct.start[c + 1] - ct.start[c]) * sizeof(Tile);
+        v.ntiles = ct.start[c + 1] - ct.start[c];
+        ct.view.push_back(v);
+    }
+    auto res = ctx->chunk_tiles.emplace(tp, std::move(ct));
+    return &res.first->second;
+}
+
+// the chunk the next launch covers (the lookup has no other argument)
+thread_local int t_chunk = 0;
+const TileSet *chunk_lookup(bsg_ctx *ctx, int tp) {
+    const ChunkTiles *ct = get_chunk_tiles(ctx, tp);
+    return ct ? &ct->view[t_chunk] : nullptr;
+}
+
+// states of chunk c for the launch's tile width: every tile width cuts the
+// rows the same way (the cut depends on the rows only), so any cached entry
+// gives the ranges
+const ChunkTiles *any_chunk_tiles(bsg_ctx *ctx) {
+    return ctx->chunk_tiles.empty() ? nullptr : &ctx->chunk_tiles.begin()->second;
+}
+
 int applyh_on(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec, int flags, cudaStream_t s) {
     if (!vin || !vout || nb < 1 || nb > 64 || (prec != BSG_PREC_FP32 && prec != BSG_PREC_FP64))
         return set_err(ctx, BSG_ERR_ARG, "bsg_applyh: bad arguments");
@@ -1305,9 +1382,44 @@ int applyh_on(bsg_ctx *ctx, const void *vin, void *vout, int nb, int prec, int f
     }
     st = cuda_check(ctx, cudaMemcpyAsync(ctx->scratch_in.p, vin, bytes, cudaMemcpyHostToDevice, s), "H2D vin");
     if (!st && acc) st = cuda_check(ctx, cudaMemcpyAsync(ctx->scratch_out.p, vout, bytes, cudaMemcpyHostToDevice, s), "H2D vout");
-    if (!st) st = launch_applyh(ctx, ctx->scratch_in.p, ctx->scratch_out.p, nb, prec, acc, s);
-    if (!st) st = cuda_check(ctx, cudaMemcpyAsync(vout, ctx->scratch_out.p, bytes, cudaMemcpyDeviceToHost, s), "D2H vout");
-    if (!st) st = cuda_check(ctx, cudaStreamSynchronize(s), "applyh sync");
+    if (st) return st;
+    if (bytes < kChunkBytes || ctx->nrows < kChunks) {
+        st = launch_applyh(ctx, ctx->scratch_in.p, ctx->scratch_out.p, nb, prec, acc, s);
+        if (!st) st = cuda_check(ctx, cudaMemcpyAsync(vout, ctx->scratch_out.p, bytes, cudaMemcpyDeviceToHost, s), "D2H vout");
+        if (!st) st = cuda_check(ctx, cudaStreamSynchronize(s), "applyh sync");
+        return st;
+    }
+    // chunked: all launches queued first (each followed by its event), then
+    // each chunk's copy on the copy stream after its event, so the copies
+    // overlap the later launches whether vout is pinned or not
+    if (!ctx->copy_stream &&
+        (st = cuda_check(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "copy stream")))
+        return st;
+    while ((int)ctx->chunk_ev.size() < kChunks) {
+        cudaEvent_t e = nullptr;
+        if ((st = cuda_check(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "chunk event"))) return st;
+        ctx->chunk_ev.push_back(e);
+    }
+    for (int c = 0; c < kChunks && !st; ++c) {
+        t_chunk = c;
+        st = launch_applyh(ctx, ctx->scratch_in.p, ctx->scratch_out.p, nb, prec, acc, s, chunk_lookup);
+        if (!st) st = cuda_check(ctx, cudaEventRecord(ctx->chunk_ev[c], s), "chunk event record");
+    }
+    t_chunk = 0;
+    const ChunkTiles *ct = any_chunk_tiles(ctx);
+    if (!st && !ct) st = set_err(ctx, BSG_ERR_NOMEM, "bsg_applyh: chunked row tiles");
+    const size_t esz = (size_t)nb * (prec == BSG_PREC_FP32 ? 4 : 8);
+    for (int c = 0; c < kChunks && !st; ++c) {
+        const size_t off = (size_t)ct->s0[c] * esz, len = (size_t)(ct->s0[c + 1] - ct->s0[c]) * esz;
+        st = cuda_check(ctx, cudaStreamWaitEvent(ctx->copy_stream, ctx->chunk_ev[c], 0), "chunk wait");
+        if (!st && len)
+            st = cuda_check(ctx, cudaMemcpyAsync((char *)vout + off, (const char *)ctx->scratch_out.p + off, len,
+                                                 cudaMemcpyDeviceToHost, ctx->copy_stream),
+                            "D2H vout chunk");
+    }
+    // both streams drained before returning, also after an error
+    const cudaError_t e1 = cudaStreamSynchronize(ctx->copy_stream), e2 = cudaStreamSynchronize(s);
+    if (!st) st = cuda_check(ctx, e1 != cudaSuccess ? e1 : e2, "applyh sync");
     return st;
 }
 

@@ -135,6 +135,17 @@ struct TileSet {
     int32_t ntiles = 0;
 };
 
+// row tiles cut into row-range chunks (host-pointer applyH copies each
+// chunk's output out while the next chunks run): one owned buffer, chunk c's
+// tiles at [start[c], start[c+1]) in longest-processing-time order, its
+// states [s0[c], s0[c+1]); view[c] points into the buffer (not owned)
+struct ChunkTiles {
+    DevBuf buf;
+    std::vector<int32_t> start;
+    std::vector<int64_t> s0;
+    std::vector<TileSet> view;
+};
+
 }  // namespace bsg
 
 struct bsg_ctx {
@@ -179,6 +190,11 @@ struct bsg_ctx {
     bsg_stats stats{};
     // scratch vectors for host-pointer applyh
     bsg::DevBuf scratch_in, scratch_out;
+    // chunked host-pointer applyh: tiles per tile size, the copy stream and
+    // one event per chunk
+    std::map<int, bsg::ChunkTiles> chunk_tiles;
+    cudaStream_t copy_stream = nullptr;
+    std::vector<cudaEvent_t> chunk_ev;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
