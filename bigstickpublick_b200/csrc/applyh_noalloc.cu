@@ -15,10 +15,8 @@
 //    BSG_NOALLOC_MAX_VECTOR_BYTES; larger calls are rejected with
 //    BSG_ERR_ARG before anything is copied;
 //  * the call is synchronous: it copies vin in, runs the matvec and copies
-//    vout back on the context's stream, then waits for that stream.  It must
-//    not be made while that stream is being captured into a CUDA graph (a
-//    synchronizing call would invalidate the capture); it checks, and returns
-//    BSG_ERR_ARG instead;
+//    vout back on the context's stream, then waits for that stream (a stream
+//    that cannot be waited on gets BSG_ERR_ARG before anything is queued);
 //  * the first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (once per device, with that device current);
 //  * the row tiles of the context are used when an earlier bsg_applyh or

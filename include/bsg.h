@@ -239,9 +239,9 @@ int  bsg_applyh_stream(bsg_ctx *ctx, const void *vin, void *vout, int nb, int pr
  *      footprint after set-up.  vin/vout are staged through one static
  *      __device__ array instead of buffers allocated on first use.  Each
  *      vector (dim*nb*element size) must fit in BSG_NOALLOC_MAX_VECTOR_BYTES,
- *      else BSG_ERR_ARG.  The call is synchronous on the context's stream and
- *      returns BSG_ERR_ARG if that stream is being captured.  The first call
- *      on a device looks up the array's address.  Row tiles: the context's
+ *      else BSG_ERR_ARG.  The call is synchronous: it waits for the
+ *      context's stream before it returns.  The first call on a device looks
+ *      up the array's address.  Row tiles: the context's
  *      own when an earlier applyH built them, else at most 65536 tiles in the
  *      static array (more: BSG_ERR_ARG).  All calls in the process share the
  *      array: calls that overlap on the GPU race.  Same semantics as
