@@ -252,6 +252,23 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
         r = it->second;
         return true;
     };
+    // the rows of every proton jump's isd and fsd, looked up once (bundles
+    // share the jumps; -1: not a pstart value, reported where it is used)
+    auto jump_rows = [&](const int64_t *isd, const int64_t *fsd, int64_t n, std::vector<int32_t> &ri,
+                         std::vector<int32_t> &rf) {
+        ri.assign((size_t)std::max<int64_t>(n, 0), -1);
+        rf.assign((size_t)std::max<int64_t>(n, 0), -1);
+        if (n <= 0 || !isd || !fsd) return;
+        parallel_for(n, 1 << 14, [&](int64_t x) {
+            int32_t r;
+            if (rowof(isd[x], r)) ri[x] = r;
+            if (rowof(fsd[x], r)) rf[x] = r;
+        }, nthr);
+    };
+    std::vector<int32_t> p1b_ri, p1b_rf, p2b_ri, p2b_rf, p3b_ri, p3b_rf;
+    jump_rows(t->p1b_isd, t->p1b_fsd, t->np1b, p1b_ri, p1b_rf);
+    jump_rows(t->p2b_isd, t->p2b_fsd, t->np2b, p2b_ri, p2b_rf);
+    if (t3) jump_rows(t3->p3b_isd, t3->p3b_fsd, t3->np3b, p3b_ri, p3b_rf);
 
     const int nl_n = t->nhsps_nl, nr_n = t->nhsps_nr, nl_p = t->nhsps_pl, nr_p = t->nhsps_pr;
     if (nl_n < 0 || nr_n < 0 || nl_p < 0 || nr_p < 0 || nl_n + nr_n > 250)
@@ -508,11 +525,9 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
     struct PPBundle { int64_t ib, px0, px1, nx0, nx1; bool bwd; };
     std::vector<PPBundle> pp_bundles;
     // one proton-side PN-form contribution (PN, PPN, PNN) of the jump s1 -> s2
-    auto pn_contrib = [&](int64_t s1, int64_t s2, int32_t id, int32_t aoff, int32_t coff, int ph,
+    auto pn_contrib = [&](int64_t s1, int32_t ri, int32_t rf, int32_t id, int32_t aoff, int32_t coff, int ph,
                           const std::string &what) -> int {
-        int32_t ri, rf;
-        if (!rowof(s1, ri) || !rowof(s2, rf))
-            return set_err(ctx, BSG_ERR_OOB_INDEX, what + " isd/fsd is not a pstart value");
+        if (ri < 0 || rf < 0) return set_err(ctx, BSG_ERR_OOB_INDEX, what + " isd/fsd is not a pstart value");
         if (nops[id].nout > ctx->h_rowlen[rf] || nop_maxin[id] >= ctx->h_rowlen[ri])
             return set_err(ctx, BSG_ERR_OOB_INDEX, what + ": neutron jump outside the row");
         if (ph != 1 && ph != -1) return set_err(ctx, BSG_ERR_BAD_TABLE, what + " phase not +-1");
@@ -527,6 +542,22 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
         }
         return BSG_OK;
     };
+    {
+        // one PN-form contribution per proton jump and neutron sub-operator:
+        // room for one per jump up front (most operators have one part), so
+        // the vector is not copied over and over while it grows
+        int64_t npn = 0, nnn = 0, nspe = 0;
+        for (int64_t ib = 0; ib < t->nbundles; ++ib) {
+            const int op = t->optype[ib];
+            const int64_t n = std::max<int64_t>(0, t->pxend[ib] - t->pxstart[ib] + 1);
+            if (op == BSG_OP_PN || op == BSG_OP_PPN || op == BSG_OP_PNN) npn += n;
+            else if (op == BSG_OP_NN || op == BSG_OP_NNN) nnn += n;
+            else if (op == BSG_OP_SPE) nspe += n;
+        }
+        pn.reserve((size_t)npn);
+        nn.reserve((size_t)nnn);
+        spe.reserve((size_t)nspe);
+    }
     for (int64_t ib = 0; ib < t->nbundles; ++ib) {
         const int op = t->optype[ib], hc = t->hchar[ib];
         const int64_t px0 = t->pxstart[ib], px1 = t->pxend[ib], nx0 = t->nxstart[ib], nx1 = t->nxend[ib];
@@ -551,10 +582,9 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
                     return set_err(ctx, BSG_ERR_UNSUPPORTED, "PPP neutron run not contiguous" + where);
             const int32_t lo = (int32_t)(t->nstart[nx0 - 1] - 1), hi = (int32_t)(t->nstart[nx1 - 1] - 1);
             for (int64_t x = px0; x <= px1; ++x) {
-                int32_t ri, rf;
                 const int64_t s1 = bwd ? t3->p3b_fsd[x - 1] : t3->p3b_isd[x - 1];
-                const int64_t s2 = bwd ? t3->p3b_isd[x - 1] : t3->p3b_fsd[x - 1];
-                if (!rowof(s1, ri) || !rowof(s2, rf))
+                const int32_t ri = bwd ? p3b_rf[x - 1] : p3b_ri[x - 1], rf = bwd ? p3b_ri[x - 1] : p3b_rf[x - 1];
+                if (ri < 0 || rf < 0)
                     return set_err(ctx, BSG_ERR_OOB_INDEX, "p3b isd/fsd is not a pstart value" + where);
                 if (hi >= ctx->h_rowlen[ri] || hi >= ctx->h_rowlen[rf])
                     return set_err(ctx, BSG_ERR_OOB_INDEX, "PPP neutron run longer than the row" + where);
@@ -641,11 +671,14 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
                 }
             for (int64_t x = px0; x <= px1; ++x) {
                 int64_t isd, fsd;
+                int32_t risd, rfsd;
                 int cl, dl, ph;
                 int32_t aoff, coff;
                 if (ppn) {
                     isd = t->p2b_isd[x - 1];
                     fsd = t->p2b_fsd[x - 1];
+                    risd = p2b_ri[x - 1];
+                    rfsd = p2b_rf[x - 1];
                     cl = t3->p2b_cop[x - 1];
                     dl = t3->p2b_dop[x - 1];
                     ph = t->p2b_phase[x - 1];
@@ -654,13 +687,16 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
                 } else {
                     isd = t->p1b_isd[x - 1];
                     fsd = t->p1b_fsd[x - 1];
+                    risd = p1b_ri[x - 1];
+                    rfsd = p1b_rf[x - 1];
                     cl = t->p1b_cop[x - 1];
                     dl = t->p1b_dop[x - 1];
                     ph = t->p1b_phase[x - 1];
                     aoff = (int32_t)(base_pnn + (int64_t)(cl + nl_p) * nnp3);
                     coff = (int32_t)(base_pnn + (int64_t)(dl + nl_p) * nnp3);
                 }
-                st = pn_contrib(bwd ? fsd : isd, bwd ? isd : fsd, id, aoff, coff, ph, std::string(nm) + where);
+                st = pn_contrib(bwd ? fsd : isd, bwd ? rfsd : risd, bwd ? risd : rfsd, id, aoff, coff, ph,
+                                std::string(nm) + where);
                 if (st) return st;
             }
             ops3[ppn ? 2 : 3] += (px1 - px0 + 1) * (nx1 - nx0 + 1);
@@ -727,10 +763,9 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
                     }
             }
             for (int64_t x = px0; x <= px1; ++x) {
-                int32_t ri, rf;
                 const int64_t s1 = bwd ? t->p1b_fsd[x - 1] : t->p1b_isd[x - 1];
-                const int64_t s2 = bwd ? t->p1b_isd[x - 1] : t->p1b_fsd[x - 1];
-                if (!rowof(s1, ri) || !rowof(s2, rf))
+                const int32_t ri = bwd ? p1b_rf[x - 1] : p1b_ri[x - 1], rf = bwd ? p1b_ri[x - 1] : p1b_rf[x - 1];
+                if (ri < 0 || rf < 0)
                     return set_err(ctx, BSG_ERR_OOB_INDEX, "p1b isd/fsd is not a pstart value" + where);
                 if (nops[id].nout > ctx->h_rowlen[rf] || nop_maxin[id] >= ctx->h_rowlen[ri])
                     return set_err(ctx, BSG_ERR_OOB_INDEX, "PN neutron jump outside the row" + where);
@@ -788,10 +823,9 @@ int derive(bsg_ctx *ctx, const bsg_tables *t, const bsg_tables3 *t3, bool do_upl
             };
             size_t at = at0[j];
             for (int64_t x = B.px0; x <= B.px1; ++x, ++at) {
-                int32_t ri, rf;
                 const int64_t s1 = B.bwd ? t->p2b_fsd[x - 1] : t->p2b_isd[x - 1];
-                const int64_t s2 = B.bwd ? t->p2b_isd[x - 1] : t->p2b_fsd[x - 1];
-                if (!rowof(s1, ri) || !rowof(s2, rf)) return fail(BSG_ERR_OOB_INDEX, "p2b isd/fsd is not a pstart value");
+                const int32_t ri = B.bwd ? p2b_rf[x - 1] : p2b_ri[x - 1], rf = B.bwd ? p2b_ri[x - 1] : p2b_rf[x - 1];
+                if (ri < 0 || rf < 0) return fail(BSG_ERR_OOB_INDEX, "p2b isd/fsd is not a pstart value");
                 if (hi >= ctx->h_rowlen[ri] || hi >= ctx->h_rowlen[rf])
                     return fail(BSG_ERR_OOB_INDEX, "PP neutron run longer than the row");
                 const int32_t opl = t->p2b_op[x - 1];
