@@ -589,22 +589,24 @@ int bsg_batch_autotune(bsg_batch *b, int *items_out, int *ctas_out, double *best
     cudaEventCreate(&e1);
     double best = 1e300;
     int bi = 4, bc = 4;
+    // 2 CTAs per SM never won on the measured batches; one warm-up and three
+    // timed launches per candidate
     const int cand_items[] = {1, 2, 4, 8};
-    const int cand_ctas[] = {2, 4, 8};
+    const int cand_ctas[] = {4, 8};
     for (int it : cand_items) {
         if ((st = build_items(b, it))) break;
         if ((st = set_vectors(b, vi.data(), vo.data()))) break;
         for (int cps : cand_ctas) {
             b->ctas_per_sm = cps;
-            for (int w = 0; w < 2; ++w) launch_batch(b, BSG_PREC_FP32, b->stream);
+            launch_batch(b, BSG_PREC_FP32, b->stream);
             cudaEventRecord(e0, b->stream);
-            for (int r = 0; r < 5; ++r) launch_batch(b, BSG_PREC_FP32, b->stream);
+            for (int r = 0; r < 3; ++r) launch_batch(b, BSG_PREC_FP32, b->stream);
             cudaEventRecord(e1, b->stream);
             cudaEventSynchronize(e1);
             float ms = 0;
             cudaEventElapsedTime(&ms, e0, e1);
-            if (ms / 5 < best) {
-                best = ms / 5;
+            if (ms / 3 < best) {
+                best = ms / 3;
                 bi = it;
                 bc = cps;
             }
