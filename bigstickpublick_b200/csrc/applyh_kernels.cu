@@ -22,14 +22,14 @@
 
 namespace bsg {
 
-template <typename T, int NB, int ITEMS, bool FULL, int OUT, bool REC32 = false>
+template <typename T, int NB, int ITEMS, bool FULL, int OUT, bool REC32 = false, bool SACC = false>
 __device__ __forceinline__ void rows_body(const RowArgs &a, const T *__restrict__ vin, T *__restrict__ vout,
                                           const int ld, const int v0, const int mstride) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int warp = threadIdx.x >> 5;
     float *__restrict__ Mw = reinterpret_cast<float *>(smem) + (size_t)warp * mstride;
     T *__restrict__ part = reinterpret_cast<T *>(smem + align16(sizeof(float) * (size_t)kWarps * mstride));
-    row_tile<T, NB, ITEMS, FULL, OUT, REC32>(a, a.tiles[blockIdx.x], vin, vout, ld, v0, Mw, part);
+    row_tile<T, NB, ITEMS, FULL, OUT, REC32, SACC>(a, a.tiles[blockIdx.x], vin, vout, ld, v0, Mw, part);
 }
 
 // OUT: store, accumulate, or FP64 columns (RowOut in applyh_tile.cuh)
@@ -45,12 +45,17 @@ __global__ void __launch_bounds__(kWarps * 32) k_rows(const RowArgs a, const T *
 // compiler's own choice of 48 registers, the small spills included).  FP32
 // tiles of 256 positions (long rows) go further, to 32 registers and 8 CTAs:
 // pf 4p4n 1.80 -> 1.61 ms, while short rows lose more to the spills.
-// REC32: the 32-bit sliced records (half the record bytes of the L1 stream)
+// REC32: the 32-bit sliced records (half the record bytes of the L1 stream).
+// With 4 or more items per lane the running sums stay in shared memory during
+// the NN and PN record walks (row_tile's SACC): spill loads of the 8-item
+// kernel 372 -> 64 bytes, and pf 6p6n 141.1 -> 133.1 ms, bitwise the same
+// output.  FP64 keeps its sums in registers: there the extra shared traffic
+// cost more than the spills (sd 6p6n 81.1 -> 87.2 us).
 template <int ITEMS, bool FULL, int OUT, bool REC32>
 __global__ void __launch_bounds__(kWarps * 32, ITEMS >= 8 ? 8 : 6) k_rows_f1(const RowArgs a, const float *__restrict__ vin,
                                                             float *__restrict__ vout, const int ld, const int v0,
                                                             const int mstride) {
-    rows_body<float, 1, ITEMS, FULL, OUT, REC32>(a, vin, vout, ld, v0, mstride);
+    rows_body<float, 1, ITEMS, FULL, OUT, REC32, (ITEMS >= 4)>(a, vin, vout, ld, v0, mstride);
 }
 template <int ITEMS, bool FULL, int OUT, bool REC32>
 __global__ void __launch_bounds__(kWarps * 32, 6) k_rows_d1(const RowArgs a, const double *__restrict__ vin,

@@ -93,7 +93,8 @@ __host__ __device__ constexpr size_t align16(size_t x) { return (x + 15) & ~size
 
 // One CTA = one tile of one output row: positions pos0 + lane + 32*i.  Warp w
 // handles the contributions assigned to slot (row, w) at setup (balanced by
-// estimated work) and accumulates in registers; the eight partial sums are
+// estimated work) and accumulates in registers (SACC below: in its own shared
+// entries between record walks); the eight partial sums are
 // added in fixed warp order at the end, so the result does not depend on
 // scheduling.
 // ld: elements between consecutive states (the block size nb); v0: first
@@ -107,7 +108,12 @@ enum RowOut { kStore = 0, kAccumulate = 1, kColumns = 2 };
 
 // REC32: walk the 32-bit sliced records (RowArgs::sell32) instead of the
 // 8-byte ones; the decoded values, and so the sums, are the same bit for bit.
-template <typename T, int NB, int ITEMS, bool FULL, int OUT = kStore, bool REC32 = false>
+// SACC: between the PP and SPE passes the running sums live in this thread's
+// entries of `part` instead of registers; each NN / PN record walk loads its
+// item's sum, accumulates in registers and stores it back.  The operations
+// and their order are unchanged (bitwise the same sums); what changes is that
+// the ITEMS sums are not live across the walks.
+template <typename T, int NB, int ITEMS, bool FULL, int OUT = kStore, bool REC32 = false, bool SACC = false>
 __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, const T *__restrict__ vin,
                                          T *__restrict__ vout, const int ld_, const int v0_,
                                          float *__restrict__ Mw, T *__restrict__ part) {
@@ -150,6 +156,15 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
             }
         }
     }
+    // item i's sums: mine[32 * i * NB + v], this thread's entries of part
+    constexpr int TP = 32 * ITEMS;
+    T *__restrict__ mine = part + ((size_t)warp * TP + lane) * NB;
+    if constexpr (SACC) {
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i)
+#pragma unroll
+            for (int v = 0; v < NB; ++v) mine[32 * i * NB + v] = acc[i][v];
+    }
     // ---- NN: out[pos] += sum r.me * in[row + r.in]   (:1012-1066)
     {
         const int slot = row * kWarps + warp;
@@ -163,6 +178,18 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
             for (int i = 0; i < ITEMS; ++i) {
                 if (!BSG_VALID(i) || BSG_POS(i) >= op.nout) continue;
                 const int k0 = __ldg(ptr + BSG_POS(i)), k1 = __ldg(ptr + BSG_POS(i) + 1);
+                T sv[NB];
+                if constexpr (SACC) {
+#pragma unroll
+                    for (int v = 0; v < NB; ++v) sv[v] = mine[32 * i * NB + v];
+                }
+                T (&A)[NB] = SACC ? sv : acc[i];
+                auto put = [&]() {
+                    if constexpr (SACC) {
+#pragma unroll
+                        for (int v = 0; v < NB; ++v) mine[32 * i * NB + v] = sv[v];
+                    }
+                };
                 // NN takes the 32-bit records for FP64 vectors only: for FP32
                 // the extra hmatnn load per record cost more than the halved
                 // record bytes saved (pf 6p6n: 143.8 against 139.2 ms)
@@ -182,7 +209,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
                         const T m1 = (T)__int_as_float(__float_as_int(__ldg(a.hmatnn + ((r1 >> 16) & 0x7fffu))) ^
                                                        (int)(r1 & 0x80000000u));
 #pragma unroll
-                        for (int v = 0; v < NB; ++v) { acc[i][v] += m0 * x0[v]; acc[i][v] += m1 * x1[v]; }
+                        for (int v = 0; v < NB; ++v) { A[v] += m0 * x0[v]; A[v] += m1 * x1[v]; }
                     }
                     if (k < n) {
                         const uint32_t r0 = __ldg(c32 + 32 * k);
@@ -191,8 +218,9 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
                         const T m0 = (T)__int_as_float(__float_as_int(__ldg(a.hmatnn + ((r0 >> 16) & 0x7fffu))) ^
                                                        (int)(r0 & 0x80000000u));
 #pragma unroll
-                        for (int v = 0; v < NB; ++v) acc[i][v] += m0 * x0[v];
+                        for (int v = 0; v < NB; ++v) A[v] += m0 * x0[v];
                     }
+                    put();
                     continue;
                 }
                 const int2 *col;
@@ -205,7 +233,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
                     Vec<T, NB, FULL>::load(src + (size_t)r1.x * ld, x1);
                     const T m0 = (T)__int_as_float(r0.y), m1 = (T)__int_as_float(r1.y);
 #pragma unroll
-                    for (int v = 0; v < NB; ++v) { acc[i][v] += m0 * x0[v]; acc[i][v] += m1 * x1[v]; }
+                    for (int v = 0; v < NB; ++v) { A[v] += m0 * x0[v]; A[v] += m1 * x1[v]; }
                 }
                 if (k < n) {
                     const int2 r0 = __ldg(col + kRecStride<T, NB> * k);
@@ -213,8 +241,9 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
                     Vec<T, NB, FULL>::load(src + (size_t)r0.x * ld, x0);
                     const T m0 = (T)__int_as_float(r0.y);
 #pragma unroll
-                    for (int v = 0; v < NB; ++v) acc[i][v] += m0 * x0[v];
+                    for (int v = 0; v < NB; ++v) A[v] += m0 * x0[v];
                 }
+                put();
             }
         }
     }
@@ -242,6 +271,18 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
             for (int i = 0; i < ITEMS; ++i) {
                 if (!BSG_VALID(i) || BSG_POS(i) >= op.nout) continue;
                 const int k0 = __ldg(ptr + BSG_POS(i)), k1 = __ldg(ptr + BSG_POS(i) + 1);
+                T sv[NB];
+                if constexpr (SACC) {
+#pragma unroll
+                    for (int v = 0; v < NB; ++v) sv[v] = mine[32 * i * NB + v];
+                }
+                T (&A)[NB] = SACC ? sv : acc[i];
+                auto put = [&]() {
+                    if constexpr (SACC) {
+#pragma unroll
+                        for (int v = 0; v < NB; ++v) mine[32 * i * NB + v] = sv[v];
+                    }
+                };
                 if constexpr (REC32) {
                     // input position | (b,d) index | neutron phase sign
                     const uint32_t *c32 =
@@ -256,7 +297,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
                         const T m0 = (T)__int_as_float(__float_as_int(Mw[(r0 >> 16) & 0x7fffu]) ^ (int)(r0 & 0x80000000u));
                         const T m1 = (T)__int_as_float(__float_as_int(Mw[(r1 >> 16) & 0x7fffu]) ^ (int)(r1 & 0x80000000u));
 #pragma unroll
-                        for (int v = 0; v < NB; ++v) { acc[i][v] += m0 * x0[v]; acc[i][v] += m1 * x1[v]; }
+                        for (int v = 0; v < NB; ++v) { A[v] += m0 * x0[v]; A[v] += m1 * x1[v]; }
                     }
                     if (k < n) {
                         const uint32_t r0 = __ldg(c32 + 32 * k);
@@ -264,8 +305,9 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
                         Vec<T, NB, FULL>::load(src + (size_t)(r0 & 0xffffu) * ld, x0);
                         const T m0 = (T)__int_as_float(__float_as_int(Mw[(r0 >> 16) & 0x7fffu]) ^ (int)(r0 & 0x80000000u));
 #pragma unroll
-                        for (int v = 0; v < NB; ++v) acc[i][v] += m0 * x0[v];
+                        for (int v = 0; v < NB; ++v) A[v] += m0 * x0[v];
                     }
+                    put();
                     continue;
                 }
                 const int2 *col;
@@ -281,7 +323,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
                     const float f1 = __int_as_float(__float_as_int(Mw[r1.y & 0xffff]) ^ ((r1.y << 8) & 0x80000000));
                     const T m0 = (T)f0, m1 = (T)f1;
 #pragma unroll
-                    for (int v = 0; v < NB; ++v) { acc[i][v] += m0 * x0[v]; acc[i][v] += m1 * x1[v]; }
+                    for (int v = 0; v < NB; ++v) { A[v] += m0 * x0[v]; A[v] += m1 * x1[v]; }
                 }
                 if (k < n) {
                     const int2 r0 = __ldg(col + kRecStride<T, NB> * k);
@@ -290,13 +332,20 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
                     const float f0 = __int_as_float(__float_as_int(Mw[r0.y & 0xffff]) ^ ((r0.y << 8) & 0x80000000));
                     const T m0 = (T)f0;
 #pragma unroll
-                    for (int v = 0; v < NB; ++v) acc[i][v] += m0 * x0[v];
+                    for (int v = 0; v < NB; ++v) A[v] += m0 * x0[v];
                 }
+                put();
             }
             __syncwarp();
         }
     }
     // ---- SPE: out[pos] += (pspe + nspe) * in[pos]   (:988-1011)
+    if constexpr (SACC) {
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i)
+#pragma unroll
+            for (int v = 0; v < NB; ++v) acc[i][v] = mine[32 * i * NB + v];
+    }
     {
         const int slot = row * kWarps + warp;
         const int c1 = a.spe_ptr[slot + 1];
@@ -315,7 +364,6 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, const Tile tile, cons
         }
     }
     // ---- fixed-order reduction over the warps, single write per element
-    constexpr int TP = 32 * ITEMS;
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i)
 #pragma unroll
