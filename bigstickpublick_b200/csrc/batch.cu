@@ -66,7 +66,7 @@ struct BChunk {
 
 constexpr int kChunk = 2048;
 
-template <typename T, int ITEMS>
+template <typename T, int ITEMS, bool SACC = false>
 __device__ __forceinline__ void rows_batch_body(const BatchSys *__restrict__ sys, const BatchItem *__restrict__ items,
                                                 int nitems, int *__restrict__ counter, int mstride) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -82,7 +82,7 @@ __device__ __forceinline__ void rows_batch_body(const BatchSys *__restrict__ sys
         if (it >= nitems) return;
         const BatchItem w = items[it];
         const BatchSys *S = sys + w.sys;
-        row_tile<T, 1, ITEMS, false>(S->a, S->a.tiles[w.tile], (const T *)S->vin, (T *)S->vout, 1, 0, Mw, part);
+        row_tile<T, 1, ITEMS, false, kStore, false, SACC>(S->a, S->a.tiles[w.tile], (const T *)S->vin, (T *)S->vout, 1, 0, Mw, part);
         __syncthreads();
     }
 }
@@ -97,12 +97,14 @@ __global__ void __launch_bounds__(kWarps * 32) k_rows_batch(const BatchSys *__re
 // FP32: capped at 40 registers so that 6 CTAs of 256 threads stay resident
 // per SM; the system descriptors come from global memory, and the compiler's
 // own choice (64 registers, 4 CTAs) was measured slower than the spills the
-// cap costs
+// cap costs.  From 2 items per lane up the running sums stay in shared memory
+// during the record walks (row_tile's SACC): spill loads of the 4-item kernel
+// 180 -> 112 bytes, the 256-system matvec 5.98 -> 5.79 ms, bitwise the same.
 template <int ITEMS>
 __global__ void __launch_bounds__(kWarps * 32, 6) k_rows_batch_f32(const BatchSys *__restrict__ sys,
                                                                    const BatchItem *__restrict__ items, int nitems,
                                                                    int *__restrict__ counter, int mstride) {
-    rows_batch_body<float, ITEMS>(sys, items, nitems, counter, mstride);
+    rows_batch_body<float, ITEMS, (ITEMS >= 2)>(sys, items, nitems, counter, mstride);
 }
 
 template <typename T, int ITEMS>
