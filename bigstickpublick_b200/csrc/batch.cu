@@ -100,8 +100,12 @@ __global__ void __launch_bounds__(kWarps * 32) k_rows_batch(const BatchSys *__re
 // cap costs.  From 2 items per lane up the running sums stay in shared memory
 // during the record walks (row_tile's SACC): spill loads of the 4-item kernel
 // 180 -> 112 bytes, the 256-system matvec 5.98 -> 5.79 ms, bitwise the same.
+// With 4 or 8 items the cap is 32 registers (8 CTAs per SM), as for the
+// single-system kernel: more spills, but at the autotuned 4 items x 8 CTAs
+// 5.75 -> 5.63 ms (the 4-CTA grid settings got slower; the autotuner does not
+// pick them).
 template <int ITEMS>
-__global__ void __launch_bounds__(kWarps * 32, 6) k_rows_batch_f32(const BatchSys *__restrict__ sys,
+__global__ void __launch_bounds__(kWarps * 32, ITEMS >= 4 ? 8 : 6) k_rows_batch_f32(const BatchSys *__restrict__ sys,
                                                                    const BatchItem *__restrict__ items, int nitems,
                                                                    int *__restrict__ counter, int mstride) {
     rows_batch_body<float, ITEMS, (ITEMS >= 2)>(sys, items, nitems, counter, mstride);
