@@ -40,6 +40,25 @@ def _write_spec(path, spec):
     path.write_text("\n".join(lines) + "\n")
 
 
+def _parse(stdout):
+    """dim and the eigenvalues (by index) from the program's "dim D" and
+    "eval K E" lines."""
+    dim, evals = None, {}
+    for ln in stdout.splitlines():
+        f = ln.split()
+        if f and f[0] == "dim":
+            dim = int(f[1])
+        elif f and f[0] == "eval":
+            evals[int(f[1])] = float(f[2])
+    return dim, np.array([evals[k] for k in range(len(evals))])
+
+
+def test_output_parser():
+    out = "dim 640\neval 0 -23.153591760000001\neval 1 -22.7033493\niterations 40 converged 1\n"
+    dim, ev = _parse(out)
+    assert dim == 640 and ev.tolist() == [-23.153591760000001, -22.7033493]
+
+
 def test_c_caller_builds_against_the_headers(tmp_path):
     exe = _compile(tmp_path)
     r = subprocess.run([exe], capture_output=True, text=True)
@@ -74,10 +93,8 @@ def test_c_caller_matches_python_and_oracle(tmp_path, name, spec):
     out = tmp_path / "vout.bin"
     r = subprocess.run([exe, str(p), str(out)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
-    lines = dict((ln.split(" ", 1)[0] + ("" if not ln.startswith("eval") else ln.split()[1]),
-                  ln.split()[-1]) for ln in r.stdout.splitlines())
-    dim = int(lines["dim"])
-    evals_c = np.array([float(lines[f"eval{k}"]) for k in range(5)])
+    dim, evals_c = _parse(r.stdout)
+    assert evals_c.size == 5
     vout_c = np.fromfile(out, dtype=np.float64)
     assert vout_c.size == dim
 
