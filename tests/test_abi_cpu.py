@@ -1,6 +1,7 @@
 """The C ABI without a GPU: the libraries load, export every function the
-headers declare, the ctypes mirror has the C struct sizes, and the host-side
-table validator rejects corrupted tables with the right status."""
+headers declare, the ctypes mirror has the C struct sizes, the headers build
+under -pedantic -Werror as C99/C11/C++11/C++17 and link from C and C++, and the
+host-side table validator rejects corrupted tables with the right status."""
 import ctypes as C
 import os
 import re
@@ -86,3 +87,39 @@ def test_validator_rejects_range_past_array(tables):
     tables.a["pxend"][ib] = tables.s["np1b"] + 5
     st, msg = engine.validate_tables(tables)
     assert st == 2 and "PN range" in msg
+
+
+_HOST_PROGRAM = r'''
+#include "bsg_host.h"
+#include <stdio.h>
+#include <string.h>
+int main(void) {
+    bsg_tables t;
+    char msg[256];
+    int st;
+    memset(&t, 0, sizeof t);
+    st = bsg_validate_tables(&t, msg, sizeof msg);
+    printf("%d|%s|%s|%d\n", st, msg, bsg_strerror(BSG_ERR_BAD_TABLE), bsg_host_build(NULL, NULL));
+    return 0;
+}
+'''
+
+
+@pytest.mark.parametrize("lang,std", [("c", "c99"), ("c", "c11"), ("c++", "c++11"), ("c++", "c++17")])
+def test_headers_build_strictly_and_link_from_c_and_cpp(tmp_path, lang, std):
+    # a C or C++ host includes both headers under -pedantic -Werror and calls
+    # host-only entry points through the extern "C" declarations (no GPU call)
+    src = tmp_path / ("prog.c" if lang == "c" else "prog.cpp")
+    src.write_text(_HOST_PROGRAM)
+    exe = tmp_path / "prog"
+    pkg = os.path.join(ROOT, "bigstickpublick_b200")
+    cc = "gcc" if lang == "c" else "g++"
+    r = subprocess.run([cc, "-std=" + std, "-Wall", "-Wextra", "-pedantic", "-Werror",
+                        "-I" + os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                        "-L" + pkg, "-lbsgpu", "-lbsghost", "-Wl,-rpath," + pkg],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    st, msg, name, host_st = subprocess.check_output([str(exe)], text=True).strip().split("|")
+    assert _abi.STATUS_NAMES[int(st)] == "BSG_ERR_BAD_TABLE" and "empty basis" in msg
+    assert name == "table failed validation"
+    assert _abi.STATUS_NAMES[int(host_st)] == "BSG_ERR_ARG"   # null output pointer
